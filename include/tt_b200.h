@@ -1,0 +1,188 @@
+/*
+ * tt_b200.h -- C ABI of the B200 two-site DMRG inner loop.
+ *
+ * This is the boundary between the C++ host classes that mirror
+ * tensor-tools' qtensor / big_qtensor / svd_bond / Davidson / dmrg interface
+ * and the sm_100a kernels.  Every entry point is extern "C", takes plain
+ * pointers and sizes, returns an int status (TT_OK == 0) and never throws;
+ * the message of the last failure on the calling thread is returned by
+ * tt_get_last_error().
+ *
+ * Reference interfaces replaced (paths relative to the tensor-tools tree):
+ *   tt_contract_plan/exec    qtensor<T>::operator*      qtensor/qtensor.cpp:523-734
+ *                            dtensor<T>::operator*      dtensor/dtensor.cpp:300-368
+ *   tt_vec_*                 qtensor<T>::inner_product / add / contract / norm /
+ *                            normalize / operator*=     qtensor/qtensor.cpp:1031-1179,1606-1647
+ *                            dtensor<T>::add / inner_product / norm
+ *                                                       dtensor/dtensor.cpp:792-849
+ *   tt_vec_fill_random       qtensor<T>::setRandom      qtensor/qtensor.cpp:381-388
+ *   tt_vec_precondition      elemWiseDivide             linalg/tensor_davidson.cpp:25-36
+ *   tt_sym_eig_batched       CTF Matrix::svd per QN sector (ScaLAPACK pdgesvd)
+ *                                                       qtensor/qtensor_op.cpp:1269,
+ *                                                       dtensor/dtensor_op.cpp:175
+ *                            DIAG (dsyev)               linalg/lapack_wrapper.cpp:40-54
+ *   tt_copy2d_batched        CTF slice of sector matrices into U/V blocks
+ *                                                       qtensor/qtensor_op.cpp:1229-1246,1389-1436
+ *   tt_strided_copy          dtensor<T>::diagonal / qtensor permute
+ *                                                       dtensor/dtensor.cpp:511-571
+ *
+ * The object-level API that big_qtensor / dmrg callers bind (qtensor
+ * handles, svd_bond, the DMRG drivers) is declared in tt_dmrg.h.
+ */
+#ifndef TT_B200_H
+#define TT_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define TT_OK              0
+#define TT_ERR_INVALID     1  /* bad argument, plan or descriptor            */
+#define TT_ERR_OOM         2  /* device or host allocation failed            */
+#define TT_ERR_CUDA        3  /* CUDA runtime or launch error                */
+#define TT_ERR_TIMEOUT     4  /* a bounded device wait gave up               */
+#define TT_ERR_NOCONV      5  /* an iterative kernel did not converge        */
+#define TT_ERR_NO_DEVICE   6  /* no usable sm_100 device                     */
+
+/* ---- precision of the block contractions -------------------------------- */
+#define TT_PREC_FP64       0  /* DMMA f64 tensor-core tiles                  */
+
+#define TT_MAX_MODES       6  /* tensor modes per GEMM dimension of a pair   */
+
+typedef struct tt_ctx tt_ctx;
+typedef struct tt_plan tt_plan;
+
+/* ---- context, memory ---------------------------------------------------- */
+/* One context per device and host thread: a CUDA stream, a stream-ordered
+ * memory pool and the plan cache.  A context is not thread-safe. */
+int tt_ctx_create(int device, tt_ctx** out);
+int tt_ctx_destroy(tt_ctx* ctx);
+int tt_ctx_synchronize(tt_ctx* ctx);
+/* cudaStream_t of the context, as an opaque pointer (for event timing). */
+int tt_ctx_stream(tt_ctx* ctx, void** stream);
+const char* tt_get_last_error(void);
+
+int tt_device_alloc(tt_ctx* ctx, size_t bytes, void** dptr);
+int tt_device_free(tt_ctx* ctx, void* dptr);
+int tt_memcpy_h2d(tt_ctx* ctx, void* dst, const void* src, size_t bytes);
+int tt_memcpy_d2h(tt_ctx* ctx, void* dst, const void* src, size_t bytes);
+int tt_memcpy_d2d(tt_ctx* ctx, void* dst, const void* src, size_t bytes);
+int tt_memset_zero(tt_ctx* ctx, void* dst, size_t bytes);
+/* Counts kernel launches issued through this context (all tt_* kernels). */
+int tt_ctx_launch_count(tt_ctx* ctx, int64_t* count);
+/* CUDA events on the context's stream, for device-side timing. */
+int tt_event_create(tt_ctx* ctx, void** ev);
+int tt_event_record(tt_ctx* ctx, void* ev);
+int tt_event_elapsed_ms(void* ev_start, void* ev_stop, float* ms);  /* waits for ev_stop */
+int tt_event_destroy(void* ev);
+
+/* ---- grouped block contraction ------------------------------------------
+ * One launch computes, for every output block o,
+ *     C_o = alpha * sum_{pairs p of o} A_p (M x K) * B_p (K x N)
+ * where C_o is stored column-major at C + c_off with leading dimension ldc,
+ * and the GEMM views of A_p and B_p are arbitrary strided tensor blocks:
+ *     A_p(m,k) = A[a_off + sum_i m_i*a_m_stride[i] + sum_j k_j*a_k_stride[j]]
+ *     B_p(k,n) = B[b_off + sum_j k_j*b_k_stride[j] + sum_i n_i*b_n_stride[i]]
+ * with m, k, n decomposed mixed-radix over m_dims, k_dims, n_dims (first mode
+ * fastest).  Output blocks without pairs are written with zeros.  This is
+ * qtensor::operator*'s inner loop "C[indC] += A_L*B_R" over all block pairs
+ * of one contraction (qtensor/qtensor.cpp:652-726), flattened into one launch.
+ */
+typedef struct {
+  int64_t c_off;
+  int32_t m, n;
+  int32_t ldc;
+} tt_out_block;
+
+typedef struct {
+  int32_t out_block;             /* index into the tt_out_block list        */
+  int32_t n_m, n_k, n_n;         /* number of modes in each GEMM dimension   */
+  int64_t a_off, b_off;
+  int32_t m_dims[TT_MAX_MODES];
+  int32_t k_dims[TT_MAX_MODES];
+  int32_t n_dims[TT_MAX_MODES];
+  int64_t a_m_stride[TT_MAX_MODES];
+  int64_t a_k_stride[TT_MAX_MODES];
+  int64_t b_k_stride[TT_MAX_MODES];
+  int64_t b_n_stride[TT_MAX_MODES];
+} tt_block_pair;
+
+int tt_contract_plan(tt_ctx* ctx, const tt_out_block* outs, int n_out,
+                     const tt_block_pair* pairs, int n_pairs, int precision,
+                     tt_plan** plan);
+int tt_contract_exec(tt_ctx* ctx, const tt_plan* plan, const double* A,
+                     const double* B, double* C, double alpha);
+int tt_plan_destroy(tt_ctx* ctx, tt_plan* plan);
+/* Algorithmic work of one exec: sum over pairs of 2*m*n*k. */
+int tt_plan_flops(const tt_plan* plan, double* flops);
+
+/* ---- Davidson vector kernels (flat, deterministic reductions) -----------
+ * Vectors are contiguous FP64 arrays of n elements (all blocks of a
+ * block-sparse tensor laid out back to back).  Scalars that feed the host
+ * (dots, norms) are written to device memory; read them with
+ * tt_memcpy_d2h.  Coefficient arrays may live on the device so that no host
+ * round trip is needed between dependent kernels. */
+int tt_vec_dot(tt_ctx* ctx, int64_t n, const double* x, const double* y, double* d_out);
+/* d_out[j] = <xs[j], y> for j < nvec (1..16), reading y once.  xs is a
+ * HOST array of nvec device pointers. */
+int tt_vec_multidot(tt_ctx* ctx, int64_t n, int nvec, const double* const* xs,
+                    const double* y, double* d_out);
+int tt_vec_nrm2(tt_ctx* ctx, int64_t n, const double* x, double* d_out);
+int tt_vec_axpy(tt_ctx* ctx, int64_t n, double a, const double* x, double* y);
+int tt_vec_scal(tt_ctx* ctx, int64_t n, double a, double* x);
+/* x *= 1/ *d_nrm, with the norm read on the device. */
+int tt_vec_scal_inv_dev(tt_ctx* ctx, int64_t n, const double* d_nrm, double* x);
+/* y = sum_j sign * coef[j] * xs[j] (+ y if accumulate), coefficients on the
+ * device: the Gram-Schmidt projection and Ritz-vector build in one pass.
+ * xs is a HOST array of nvec (0..16) device pointers. */
+int tt_vec_lincomb_dev(tt_ctx* ctx, int64_t n, int nvec, const double* const* xs,
+                       const double* d_coef, double sign, int accumulate, double* y);
+/* x[r] = uniform(0,1) for every element inside the given [begin,end) element
+ * ranges (blocks present in the tensor), 0 elsewhere; counter-based RNG. */
+int tt_vec_fill_random(tt_ctx* ctx, int64_t n, double* x, int nranges,
+                       const int64_t* d_ranges, uint64_t seed);
+/* x[i] = x[i] / (D[i] - theta) where D[i] != theta. */
+int tt_vec_precondition(tt_ctx* ctx, int64_t n, double* x, const double* D, double theta);
+
+/* ---- strided copies ------------------------------------------------------
+ * dst[dst_off + sum_i j_i*dst_stride[i]] = src[src_off + sum_i j_i*src_stride[i]]
+ * over all j in dims (up to TT_MAX_MODES modes). */
+typedef struct {
+  int32_t n_modes;
+  int32_t dims[TT_MAX_MODES];
+  int64_t src_off, dst_off;
+  int64_t src_stride[TT_MAX_MODES];
+  int64_t dst_stride[TT_MAX_MODES];
+} tt_copy_desc;
+int tt_strided_copy_batched(tt_ctx* ctx, const tt_copy_desc* descs, int n,
+                            const double* src, double* dst);
+
+/* ---- symmetric eigensolver (density matrices of the block SVD) ----------
+ * For each problem p: G_p is n x n symmetric, column-major with leading
+ * dimension n, at G + g_off[p].  On return the eigenvalues are in
+ * w[w_off[p] ...] in DESCENDING order and the matching orthonormal
+ * eigenvectors are the columns of Z_p at Z + g_off[p] (same layout).  G is
+ * destroyed.  Cyclic Jacobi with a bounded sweep count; status
+ * TT_ERR_NOCONV if a problem did not reach the off-diagonal tolerance. */
+#define TT_EIG_ROW_1X2  1  /* problem is the 2x2 Gram of a 1x2 sector matrix */
+typedef struct {
+  int64_t g_off;
+  int64_t w_off;
+  int64_t a_off;        /* TT_EIG_ROW_1X2: the 1x2 matrix (a, b) at A + a_off */
+  int32_t n;
+  int32_t flags;
+} tt_eig_problem;
+/* TT_EIG_ROW_1X2 reproduces the reference's 1x2 workaround for ScaLAPACK
+ * (qtensor/qtensor_op.cpp:1247-1267): the leading eigenvector is (a,b)/d,
+ * d = |(a,b)|, or (1,1)/sqrt(2) when d == 0; eigenvalues d*d and 0. */
+int tt_sym_eig_batched(tt_ctx* ctx, const tt_eig_problem* probs, int n_probs,
+                       double* G, double* Z, double* w, const double* A);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* TT_B200_H */

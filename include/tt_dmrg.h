@@ -1,0 +1,158 @@
+/*
+ * tt_dmrg.h -- object-level C ABI of the B200 two-site DMRG inner loop.
+ *
+ * Handles wrap the C++ host classes that mirror tensor-tools' interface; a
+ * foreign-language binding of that interface (ctypes, cgo, JNI ...) binds
+ * these.  Every call returns TT_OK (0) or a TT_ERR_* code from tt_b200.h;
+ * tt_get_last_error() explains the last failure of the calling thread.
+ * Objects are bound to the context passed to tt_dmrg_bind on this thread.
+ *
+ * Reference interfaces replaced (paths relative to the tensor-tools tree):
+ *   tt_qtensor_*             qtensor<T> and qtensor_index    qtensor/qtensor.h:47-164,
+ *                                                            qtensor/qtensor_index.h:35-118
+ *   tt_qtensor_init_blocks   qtensor<T>::initBlock           qtensor/qtensor.cpp:301-345
+ *   tt_qtensor_contract      qtensor<T>::operator*           qtensor/qtensor.cpp:523-734
+ *   tt_qtensor_norm/scale/add/inner_product
+ *                            norm / operator*= / add / inner_product
+ *                                                            qtensor/qtensor.cpp:1031-1179,1606-1647
+ *   tt_qtensor_svd           svd(A,left,right,U,V,S,dir,cutoff,K)
+ *                                                            qtensor/qtensor_op.cpp:1097-1453
+ *   tt_qtensor_svd_bond      svd_bond(combined,...)          qtensor/qtensor_op.cpp:1506-1544
+ *   tt_bigq_*                big_qtensor<T> setLeft/addMid/setRight/product/size
+ *                                                            qtensor/big_qtensor.{h,cpp}
+ *   tt_bigq_davidson         tensor_davidsonIT               linalg/tensor_davidson.cpp:193-347
+ *   tt_qmps_product_spinhalf qMPS(sites, product string)     mps/qtt.cpp:58-80,205-311
+ *   tt_qmpo_heisenberg       Heisenberg<T>::buildHam(qMPO&)  models/hams/Heisenberg.cpp:333-402
+ *   tt_qmps_position         qTensorTrain::position          mps/qtt.cpp:932-994
+ *   tt_qdmrg_*               buildEnv / updateSite / updateEnv / dmrg (schedule overload)
+ *                                                            algos/dmrg/dmrg.cpp:56-85,300-372,
+ *                                                            491-509,702-755
+ *   tt_ddmrg_*               the dense dtensor / big_dtensor path and its dmrg
+ *                                                            dtensor/dtensor.cpp, dtensor/big_dtensor.cpp,
+ *                                                            dtensor/dtensor_op.cpp,
+ *                                                            algos/dmrg/dmrg.cpp:24-51,228-295,
+ *                                                            466-486,591-646
+ */
+#ifndef TT_DMRG_H
+#define TT_DMRG_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#include "tt_b200.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct tt_qtensor tt_qtensor;
+typedef struct tt_bigq tt_bigq;
+typedef struct tt_qmps tt_qmps;
+typedef struct tt_qmpo tt_qmpo;
+typedef struct tt_qdmrg tt_qdmrg;
+
+/* arrow: 0 Inward, 1 Outward; type: 0 Link, 1 Site; qn: 2 ints per sector */
+typedef struct {
+  int32_t arrow;
+  int32_t type;
+  int32_t level;
+  int32_t n_sectors;
+  const char* name;
+  const int32_t* qn;
+  const int32_t* qdim;
+} tt_index_desc;
+
+int tt_dmrg_bind(tt_ctx* ctx);
+int tt_dmrg_unbind(void);
+
+/* ---- qtensor ------------------------------------------------------------- */
+int tt_qtensor_create(int rank, const tt_index_desc* idx, tt_qtensor** out);
+int tt_qtensor_init_blocks(tt_qtensor* t);
+/* explicit block list: qi holds n_blocks*rank sector positions; blocks are
+ * zero-filled, laid out in the given order (blocks created by the
+ * reference's contraction or SVD need not be all legal combinations) */
+int tt_qtensor_set_blocks(tt_qtensor* t, int n_blocks, const int32_t* qi);
+int tt_qtensor_destroy(tt_qtensor* t);
+int tt_qtensor_copy(const tt_qtensor* t, tt_qtensor** out);
+int tt_qtensor_rank(const tt_qtensor* t, int* rank);
+/* name copied into name_buf (NUL-terminated); qn/qdim need 2*cap / cap ints */
+int tt_qtensor_index(const tt_qtensor* t, int i, int32_t* arrow, int32_t* type, int32_t* level,
+                     int32_t* n_sectors, char* name_buf, int name_cap, int32_t* qn, int32_t* qdim, int cap);
+int tt_qtensor_num_blocks(const tt_qtensor* t, int* n);
+int tt_qtensor_block_info(const tt_qtensor* t, int b, int32_t* qn, int32_t* qi, int32_t* qd, int64_t* size);
+/* b = -1 when no block has these QNs (2*rank ints, in the tensor's index order) */
+int tt_qtensor_find_block(const tt_qtensor* t, const int32_t* qn, int* b);
+int tt_qtensor_get_block(const tt_qtensor* t, int b, double* host);
+int tt_qtensor_set_block(tt_qtensor* t, int b, const double* host);
+int tt_qtensor_prime(tt_qtensor* t, int inc);
+int tt_qtensor_dag(tt_qtensor* t);
+int tt_qtensor_contract(const tt_qtensor* A, const tt_qtensor* B, tt_qtensor** C);
+int tt_qtensor_norm(const tt_qtensor* t, double* out);
+int tt_qtensor_scale(tt_qtensor* t, double c);
+int tt_qtensor_add(tt_qtensor* y, const tt_qtensor* x, double c);
+int tt_qtensor_inner_product(const tt_qtensor* a, const tt_qtensor* b, double* out);
+/* left_axes: the nleft axes of A forming the row index (in order); the rest
+ * (in A's order) form the column index.  Outputs are new handles. */
+int tt_qtensor_svd(const tt_qtensor* A, int nleft, const int* left_axes, int direction, double cutoff,
+                   unsigned K, tt_qtensor** U, tt_qtensor** V, tt_qtensor** S, double* trunc_err,
+                   unsigned* kept);
+/* svd_bond(combined, A_left, A_right, mid = A_left's axis mid_axis, ...): replaces A_left, A_right */
+int tt_qtensor_svd_bond(const tt_qtensor* combined, tt_qtensor* A_left, tt_qtensor* A_right, int mid_axis,
+                        int direction, double cutoff, unsigned long K, tt_qtensor** S, double* trunc_err,
+                        unsigned* kept);
+
+/* ---- big_qtensor and Davidson --------------------------------------------- */
+/* W2 may be NULL (one-site operator).  L, W1, W2, R are copied. */
+int tt_bigq_create(const tt_qtensor* L, const tt_qtensor* W1, const tt_qtensor* W2, const tt_qtensor* R,
+                   tt_bigq** out);
+int tt_bigq_product(tt_bigq* op, const tt_qtensor* v, tt_qtensor** out);
+int tt_bigq_size(tt_bigq* op, uint64_t* size);
+/* tensor_davidsonIT(op, x, 3, max_restart, tol, 'S'); x is updated in place */
+int tt_bigq_davidson(tt_bigq* op, tt_qtensor* x, int max_restart, double tol, double* eval, int* matvecs);
+int tt_bigq_destroy(tt_bigq* op);
+
+/* ---- U(1) MPS / MPO / DMRG --------------------------------------------------- */
+/* spin-1/2 sites: state[i] = 0 (Dn) or 1 (Up) */
+int tt_qmps_product_spinhalf(int L, const int* state, unsigned id, tt_qmps** out);
+int tt_qmps_destroy(tt_qmps* psi);
+int tt_qmps_length(const tt_qmps* psi, int* L);
+int tt_qmps_bond_dims(const tt_qmps* psi, int* out);       /* L+1 entries */
+int tt_qmps_center(const tt_qmps* psi, int* center);
+int tt_qmps_position(tt_qmps* psi, int site);
+/* copy of site tensor i as a new handle */
+int tt_qmps_tensor(const tt_qmps* psi, int i, tt_qtensor** out);
+/* block data of all site tensors, site by site and block by block (the
+ * block structure stays on the host): size in doubles, device -> host and
+ * host -> device (host buffers should be pinned for full bandwidth) */
+int tt_qmps_data_size(const tt_qmps* psi, int64_t* n);
+int tt_qmps_get_data(const tt_qmps* psi, double* host);
+int tt_qmps_set_data(tt_qmps* psi, const double* host);
+/* dh: L site fields (may be NULL), tE: energy shift */
+int tt_qmpo_heisenberg(int L, const double* dh, double tE, unsigned id, tt_qmpo** out);
+int tt_qmpo_destroy(tt_qmpo* H);
+int tt_qmpo_tensor(const tt_qmpo* H, int i, tt_qtensor** out);
+
+/* Step-wise driver: create = position(0), normalize, buildEnv, initial energy. */
+int tt_qdmrg_create(tt_qmps* psi, tt_qmpo* H, tt_qdmrg** out);
+/* one full sweep (L->R, R->L, normalize) with this sweep's schedule entries */
+int tt_qdmrg_sweep(tt_qdmrg* run, int max_bd, double cutoff, int max_restart, double* energy);
+int tt_qdmrg_finish(tt_qdmrg* run);                          /* psi.position(0) */
+int tt_qdmrg_destroy(tt_qdmrg* run);
+/* whole schedule overload dmrg(psi, H, nsweeps, maxm[], cutoff[], max_restart[]);
+ * log_out (may be NULL) receives the run record (destroy with tt_qdmrg_destroy) */
+int tt_qdmrg_run(tt_qmps* psi, tt_qmpo* H, int nsweeps, const int* maxm, int n_maxm, const double* cutoff,
+                 int n_cutoff, const int* max_restart, int n_mr, double* energy, tt_qdmrg** log_out);
+int tt_qdmrg_num_steps(const tt_qdmrg* run, int* n);
+int tt_qdmrg_step(const tt_qdmrg* run, int i, int* site, int* direction, double* energy, double* trunc_err,
+                  unsigned* kept, int* matvecs, double* heff_flops);
+int tt_qdmrg_step_sectors(const tt_qdmrg* run, int i, int* n, int32_t* qn, uint32_t* kept, int cap);
+int tt_qdmrg_stats(const tt_qdmrg* run, double* heff_flops, double* heff_seconds, double* initial_energy);
+/* copy of the left (which = 0, TL[i]) or right (which = 1, TR[i]) environment */
+int tt_qdmrg_env(const tt_qdmrg* run, int which, int i, tt_qtensor** out);
+int tt_qdmrg_num_sweeps(const tt_qdmrg* run, int* n);
+int tt_qdmrg_sweep_info(const tt_qdmrg* run, int i, double* energy, double* seconds);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* TT_DMRG_H */

@@ -1,0 +1,171 @@
+// Context, stream-ordered device memory and error reporting of the C ABI.
+#include <cstring>
+#include <string>
+
+#include "tt_internal.h"
+
+namespace tt {
+
+static thread_local std::string g_last_error;
+
+void set_error(const std::string& msg) { g_last_error = msg; }
+
+int fail(int code, const std::string& msg) {
+  g_last_error = msg;
+  return code;
+}
+
+int cuda_fail(cudaError_t e, const char* what, const char* file, int line) {
+  char buf[512];
+  snprintf(buf, sizeof(buf), "%s failed: %s (%s:%d)", what, cudaGetErrorString(e), file, line);
+  g_last_error = buf;
+  return e == cudaErrorMemoryAllocation ? TT_ERR_OOM : TT_ERR_CUDA;
+}
+
+double* partials(tt_ctx* ctx, int n) {
+  if (n > ctx->partials_cap) {
+    if (ctx->d_partials) cudaFree(ctx->d_partials);
+    ctx->d_partials = nullptr;
+    int cap = n < 4096 ? 4096 : n;
+    if (cudaMalloc(&ctx->d_partials, sizeof(double) * cap) != cudaSuccess) {
+      ctx->partials_cap = 0;
+      return nullptr;
+    }
+    ctx->partials_cap = cap;
+  }
+  return ctx->d_partials;
+}
+
+}  // namespace tt
+
+extern "C" {
+
+const char* tt_get_last_error(void) { return tt::g_last_error.c_str(); }
+
+int tt_ctx_create(int device, tt_ctx** out) {
+  TT_REQUIRE(out != nullptr, "tt_ctx_create: null output");
+  *out = nullptr;
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0)
+    return tt::fail(TT_ERR_NO_DEVICE, "tt_ctx_create: no CUDA device");
+  TT_REQUIRE(device >= 0 && device < n, "tt_ctx_create: device ordinal out of range");
+  TT_CUDA(cudaSetDevice(device));
+  cudaDeviceProp prop;
+  TT_CUDA(cudaGetDeviceProperties(&prop, device));
+  if (prop.major < 10)
+    return tt::fail(TT_ERR_NO_DEVICE, "tt_ctx_create: kernels are built for sm_100a only");
+  tt_ctx* ctx = new tt_ctx();
+  ctx->device = device;
+  ctx->num_sms = prop.multiProcessorCount;
+  TT_CUDA(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+  TT_CUDA(cudaDeviceGetDefaultMemPool(&ctx->pool, device));
+  uint64_t thresh = UINT64_MAX;  // keep freed blocks cached in the pool
+  TT_CUDA(cudaMemPoolSetAttribute(ctx->pool, cudaMemPoolAttrReleaseThreshold, &thresh));
+  TT_CUDA(cudaMallocHost(&ctx->h_scalars, 4096 * sizeof(double)));
+  if (!tt::partials(ctx, 16 * 4 * ctx->num_sms + 64)) {
+    delete ctx;
+    return tt::fail(TT_ERR_OOM, "tt_ctx_create: scratch allocation failed");
+  }
+  *out = ctx;
+  return TT_OK;
+}
+
+int tt_ctx_destroy(tt_ctx* ctx) {
+  if (!ctx) return TT_OK;
+  cudaSetDevice(ctx->device);
+  cudaStreamSynchronize(ctx->stream);
+  if (ctx->d_partials) cudaFree(ctx->d_partials);
+  if (ctx->h_scalars) cudaFreeHost(ctx->h_scalars);
+  cudaStreamDestroy(ctx->stream);
+  delete ctx;
+  return TT_OK;
+}
+
+int tt_ctx_synchronize(tt_ctx* ctx) {
+  TT_REQUIRE(ctx, "null context");
+  TT_CUDA(cudaStreamSynchronize(ctx->stream));
+  return TT_OK;
+}
+
+int tt_ctx_stream(tt_ctx* ctx, void** stream) {
+  TT_REQUIRE(ctx && stream, "null argument");
+  *stream = (void*)ctx->stream;
+  return TT_OK;
+}
+
+int tt_ctx_launch_count(tt_ctx* ctx, int64_t* count) {
+  TT_REQUIRE(ctx && count, "null argument");
+  *count = ctx->launches;
+  return TT_OK;
+}
+
+int tt_event_create(tt_ctx* ctx, void** ev) {
+  TT_REQUIRE(ctx && ev, "null argument");
+  cudaEvent_t e;
+  TT_CUDA(cudaEventCreate(&e));
+  *ev = (void*)e;
+  return TT_OK;
+}
+
+int tt_event_record(tt_ctx* ctx, void* ev) {
+  TT_REQUIRE(ctx && ev, "null argument");
+  TT_CUDA(cudaEventRecord((cudaEvent_t)ev, ctx->stream));
+  return TT_OK;
+}
+
+int tt_event_elapsed_ms(void* a, void* b, float* ms) {
+  TT_REQUIRE(a && b && ms, "null argument");
+  TT_CUDA(cudaEventSynchronize((cudaEvent_t)b));
+  TT_CUDA(cudaEventElapsedTime(ms, (cudaEvent_t)a, (cudaEvent_t)b));
+  return TT_OK;
+}
+
+int tt_event_destroy(void* ev) {
+  if (ev) cudaEventDestroy((cudaEvent_t)ev);
+  return TT_OK;
+}
+
+int tt_device_alloc(tt_ctx* ctx, size_t bytes, void** dptr) {
+  TT_REQUIRE(ctx && dptr, "null argument");
+  *dptr = nullptr;
+  if (bytes == 0) bytes = 16;
+  TT_CUDA(cudaMallocAsync(dptr, bytes, ctx->stream));
+  return TT_OK;
+}
+
+int tt_device_free(tt_ctx* ctx, void* dptr) {
+  TT_REQUIRE(ctx, "null context");
+  if (dptr) TT_CUDA(cudaFreeAsync(dptr, ctx->stream));
+  return TT_OK;
+}
+
+int tt_memcpy_h2d(tt_ctx* ctx, void* dst, const void* src, size_t bytes) {
+  TT_REQUIRE(ctx, "null context");
+  if (bytes == 0) return TT_OK;
+  TT_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, ctx->stream));
+  return TT_OK;
+}
+
+int tt_memcpy_d2h(tt_ctx* ctx, void* dst, const void* src, size_t bytes) {
+  TT_REQUIRE(ctx, "null context");
+  if (bytes == 0) return TT_OK;
+  TT_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+  TT_CUDA(cudaStreamSynchronize(ctx->stream));
+  return TT_OK;
+}
+
+int tt_memcpy_d2d(tt_ctx* ctx, void* dst, const void* src, size_t bytes) {
+  TT_REQUIRE(ctx, "null context");
+  if (bytes == 0) return TT_OK;
+  TT_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, ctx->stream));
+  return TT_OK;
+}
+
+int tt_memset_zero(tt_ctx* ctx, void* dst, size_t bytes) {
+  TT_REQUIRE(ctx, "null context");
+  if (bytes == 0) return TT_OK;
+  TT_CUDA(cudaMemsetAsync(dst, 0, bytes, ctx->stream));
+  return TT_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,808 @@
+// big_qtensor, device-resident tensor_davidsonIT, qMPS/qMPO and the U(1)
+// two-site DMRG driver (see dmrg_q.h for the reference lines followed).
+#include "dmrg_q.h"
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+
+namespace ttb {
+
+namespace {
+
+tt_ctx* ctx() {
+  if (!rt().ctx) throw std::runtime_error("ttb: no device context bound");
+  return rt().ctx;
+}
+
+// Tensor sharing another tensor's device data (indices may then be primed or
+// dagged without copying the blocks).
+qtensor shallow(const qtensor& T) {
+  qtensor r;
+  r.idx_set = T.idx_set;
+  r.rank = T.rank;
+  r.blocks = T.blocks;
+  r.block_id = T.block_id;
+  r.data = T.data;
+  r.arena = T.arena;
+  r._initted = T._initted;
+  return r;
+}
+
+}  // namespace
+
+// ---- DIAG -------------------------------------------------------------------
+void DIAG(int n, double* M, double* evals) {
+  // cyclic Jacobi on a copy; eigenvectors accumulated in V (column-major)
+  std::vector<double> A(M, M + (size_t)n * n), V((size_t)n * n, 0.0);
+  for (int i = 0; i < n; ++i) V[i + (size_t)n * i] = 1.0;
+  auto a = [&](int i, int j) -> double& { return A[i + (size_t)n * j]; };
+  for (int sweep = 0; sweep < 100; ++sweep) {
+    double off = 0.0, fro = 0.0;
+    for (int j = 0; j < n; ++j)
+      for (int i = 0; i < n; ++i) {
+        fro += a(i, j) * a(i, j);
+        if (i != j) off += a(i, j) * a(i, j);
+      }
+    if (off <= 1e-32 * fro || off == 0.0) break;
+    for (int p = 0; p < n - 1; ++p)
+      for (int q = p + 1; q < n; ++q) {
+        double apq = a(p, q);
+        if (apq == 0.0) continue;
+        double tau = (a(q, q) - a(p, p)) / (2.0 * apq);
+        double t = (tau >= 0.0 ? 1.0 : -1.0) / (std::fabs(tau) + std::sqrt(1.0 + tau * tau));
+        double c = 1.0 / std::sqrt(1.0 + t * t), s = t * c;
+        for (int k = 0; k < n; ++k) {  // A <- A J
+          double akp = a(k, p), akq = a(k, q);
+          a(k, p) = c * akp - s * akq;
+          a(k, q) = s * akp + c * akq;
+        }
+        for (int k = 0; k < n; ++k) {  // A <- J^T A
+          double apk = a(p, k), aqk = a(q, k);
+          a(p, k) = c * apk - s * aqk;
+          a(q, k) = s * apk + c * aqk;
+        }
+        a(p, q) = a(q, p) = 0.0;
+        for (int k = 0; k < n; ++k) {
+          double vkp = V[k + (size_t)n * p], vkq = V[k + (size_t)n * q];
+          V[k + (size_t)n * p] = c * vkp - s * vkq;
+          V[k + (size_t)n * q] = s * vkp + c * vkq;
+        }
+      }
+  }
+  std::vector<int> order(n);
+  for (int i = 0; i < n; ++i) order[i] = i;
+  std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return a(x, x) < a(y, y); });
+  for (int j = 0; j < n; ++j) {
+    evals[j] = a(order[j], order[j]);
+    for (int i = 0; i < n; ++i) M[i + (size_t)n * j] = V[i + (size_t)n * order[j]];
+  }
+}
+
+// ---- big_qtensor --------------------------------------------------------------
+qtensor big_qtensor::product(qtensor& v) {
+  qtensor res;
+  if (L_) res = (*L_) * v;
+  if (res.rank > 0) res = res * mid_; else res = v * mid_;
+  if (R_) res = res * (*R_);
+  res.prime(-1);
+  return res;
+}
+
+double big_qtensor::expec(qtensor& v) {
+  qtensor res = product(v);
+  return res.contract(v);
+}
+
+size_t big_qtensor::size() const {
+  if (size_ == 0) {
+    size_ = 1;
+    if (L_)
+      for (auto& ix : L_->idx_set)
+        if (ix.level() > 0) size_ *= ix.size();
+    if (R_)
+      for (auto& ix : R_->idx_set)
+        if (ix.level() > 0) size_ *= ix.size();
+  }
+  for (auto& ix : mid_.idx_set)
+    if (ix.type() == Site) size_ *= ix.size();
+  return size_;
+}
+
+// ---- the Krylov block layout and the fused product engine -----------------
+namespace {
+
+using Presence = std::vector<uint8_t>;
+
+class ProductEngine {
+ public:
+  ProductEngine(big_qtensor& A, const qtensor& x) : A_(A), x_(x) {
+    // layout: x's blocks (x's order), then blocks the product adds, until closed
+    for (unsigned b = 0; b < x.blocks.size(); ++b) add_block(x.blocks[b]);
+    for (int it = 0; it < 8; ++it) {
+      Presence all(ublocks.size(), 1);
+      qtensor out = structure(all);
+      bool grew = false;
+      for (unsigned b = 0; b < out.blocks.size(); ++b)
+        if (uid.find(out.key_of(b)) == uid.end()) {
+          add_block(out.blocks[b]);
+          grew = true;
+        }
+      if (!grew) break;
+    }
+    build_plans();
+  }
+
+  int64_t n = 0;
+  std::vector<BlockMeta> ublocks;
+  std::unordered_map<QNKey, unsigned, QNKeyHash> uid;
+  double flops = 0.0;
+
+  Presence x_presence() const {
+    Presence p(ublocks.size(), 0);
+    for (unsigned b = 0; b < x_.blocks.size(); ++b) p[b] = 1;
+    return p;
+  }
+
+  // x's blocks copied into their places of the layout; the rest is zeroed
+  void pack(const qtensor& x, double* dst) const {
+    check(tt_memset_zero(ctx(), dst, sizeof(double) * (size_t)n), "pack zero");
+    std::vector<tt_copy_desc> d;
+    for (unsigned b = 0; b < x.blocks.size(); ++b) {
+      const BlockMeta& u = ublocks[uid.at(x.key_of(b))];
+      if (u.size != x.blocks[b].size || x.blocks[b].off + x.blocks[b].size > x.arena || u.off + u.size > n)
+        throw std::runtime_error("pack: block does not fit the Krylov layout");
+      tt_copy_desc c;
+      std::memset(&c, 0, sizeof(c));
+      c.n_modes = 1;
+      c.dims[0] = (int32_t)u.size;
+      c.src_off = x.blocks[b].off;
+      c.dst_off = u.off;
+      c.src_stride[0] = 1;
+      c.dst_stride[0] = 1;
+      d.push_back(c);
+    }
+    for (size_t i = 0; i < d.size(); i += 65535)
+      check(tt_strided_copy_batched(ctx(), d.data() + i, (int)std::min<size_t>(65535, d.size() - i),
+                                    x.data->get(), dst),
+            "pack");
+  }
+
+  // y = H_eff * v on the whole layout (absent blocks of v are zero)
+  void apply(const double* v, double* y) {
+    check(tt_contract_exec(ctx(), p1_->get(), L_data(), v, i1_->get(), 1.0), "heff L*v");
+    check(tt_contract_exec(ctx(), p2_->get(), i1_->get(), A_.mid().data->get(), i2_->get(), 1.0), "heff *mid");
+    check(tt_contract_exec(ctx(), p3_->get(), i2_->get(), A_.right()->data->get(), y, 1.0), "heff *R");
+    for (auto& r : zero_ranges_)
+      check(tt_memset_zero(ctx(), y + r.first, sizeof(double) * (size_t)r.second), "heff zero");
+  }
+
+  // block presence of product(v) given the presence of v (structure only)
+  Presence product_presence(const Presence& p) {
+    auto it = pcache_.find(p);
+    if (it != pcache_.end()) return it->second;
+    qtensor out = structure(p);
+    Presence r(ublocks.size(), 0);
+    for (unsigned b = 0; b < out.blocks.size(); ++b) r[uid.at(out.key_of(b))] = 1;
+    pcache_[p] = r;
+    return r;
+  }
+
+  // the caller's tensor with the blocks present in `p`, data in `d`
+  qtensor materialize(const Presence& p, DevPtr d) const {
+    qtensor t(x_.idx_set);
+    t._initted = true;
+    for (unsigned b = 0; b < ublocks.size(); ++b)
+      if (p[b]) {
+        unsigned id = t.add_block_meta(ublocks[b].qn, ublocks[b].qi, ublocks[b].qd);
+        t.blocks[id].off = ublocks[b].off;
+      }
+    t.data = d;
+    t.arena = n;
+    return t;
+  }
+
+ private:
+  big_qtensor& A_;
+  const qtensor& x_;
+  std::shared_ptr<PlanHandle> p1_, p2_, p3_;
+  DevPtr i1_, i2_;
+  std::vector<std::pair<int64_t, int64_t>> zero_ranges_;
+  std::map<Presence, Presence> pcache_;
+
+  const double* L_data() const { return A_.left()->data->get(); }
+
+  void add_block(const BlockMeta& b) {
+    BlockMeta m = b;
+    m.off = n;
+    n += m.size;
+    QNKey k(m.qn.size());
+    for (size_t j = 0; j < m.qn.size(); ++j) k[j] = m.qn[j].pack();
+    uid[k] = (unsigned)ublocks.size();
+    ublocks.push_back(std::move(m));
+  }
+
+  qtensor meta(const Presence& p) const {
+    qtensor t(x_.idx_set);
+    t._initted = true;
+    for (unsigned b = 0; b < ublocks.size(); ++b)
+      if (p[b]) {
+        unsigned id = t.add_block_meta(ublocks[b].qn, ublocks[b].qi, ublocks[b].qd);
+        t.blocks[id].off = ublocks[b].off;
+      }
+    t.arena = n;
+    return t;
+  }
+
+  qtensor structure(const Presence& p) const {
+    if (!A_.left() || !A_.right()) throw std::runtime_error("tensor_davidsonIT: L and R must be set");
+    qtensor v = meta(p);
+    ContractStructure c1, c2, c3;
+    contract_structure(*A_.left(), v, c1);
+    contract_structure(c1.C, A_.mid(), c2);
+    contract_structure(c2.C, *A_.right(), c3);
+    c3.C.prime(-1);
+    return std::move(c3.C);
+  }
+
+  void build_plans() {
+    Presence all(ublocks.size(), 1);
+    qtensor v = meta(all);
+    ContractStructure c1, c2, c3;
+    contract_structure(*A_.left(), v, c1);
+    contract_structure(c1.C, A_.mid(), c2);
+    contract_structure(c2.C, *A_.right(), c3);
+    c3.C.prime(-1);
+    for (unsigned i = 0; i < x_.rank; ++i)
+      if (!c3.C.idx_set.at(i).same_tag(x_.idx_set[i]))
+        throw std::runtime_error("product: H_eff*x index order differs from x");
+    std::vector<uint8_t> produced(ublocks.size(), 0);
+    for (unsigned b = 0; b < c3.C.blocks.size(); ++b) {
+      unsigned u = uid.at(c3.C.key_of(b));
+      c3.outs[b].c_off = ublocks[u].off;  // write straight into the Krylov layout
+      produced[u] = 1;
+    }
+    for (unsigned u = 0; u < ublocks.size(); ++u)
+      if (!produced[u]) zero_ranges_.push_back({ublocks[u].off, ublocks[u].size});
+    c3.C.arena = n;  // outputs now address the Krylov layout
+    flops = c1.flops + c2.flops + c3.flops;
+    p1_ = make_plan(c1);
+    p2_ = make_plan(c2);
+    p3_ = make_plan(c3);
+    i1_ = dev_alloc(std::max<int64_t>(c1.C.arena, 2));
+    i2_ = dev_alloc(std::max<int64_t>(c2.C.arena, 2));
+  }
+};
+
+struct KVec {
+  DevPtr d;
+  Presence p;
+};
+
+double read1(double* d) {
+  double h;
+  check(tt_memcpy_d2h(ctx(), &h, d, sizeof(double)), "d2h");
+  return h;
+}
+
+}  // namespace
+
+// ---- tensor_davidsonIT -----------------------------------------------------
+double tensor_davidsonIT(big_qtensor& A, qtensor& x, int m, int max_restart, double tol, char mode,
+                         DavidsonStats* stats) {
+  (void)m;
+  (void)mode;
+  if (!(m >= 1 && max_restart >= 1 && tol > 0)) throw std::runtime_error("tensor_davidsonIT: bad arguments");
+  double x_norm = x.norm();
+  x *= 1.0 / x_norm;
+  int maxsize = (int)A.size();
+  int actual_maxiter = std::min(max_restart, maxsize - 1);
+  if (actual_maxiter + 2 > 16)
+    throw std::runtime_error("tensor_davidsonIT: at most 14 iterations (16 Krylov vectors) are supported");
+  ProductEngine eng(A, x);
+  const int64_t n = eng.n;
+  const int nsz = actual_maxiter + 2;
+  std::vector<KVec> v(nsz), va(nsz);
+  auto newvec = [&]() {
+    KVec k;
+    k.d = dev_alloc(n);
+    return k;
+  };
+  void* ev0 = nullptr;
+  void* ev1 = nullptr;
+  check(tt_event_create(ctx(), &ev0), "event");
+  check(tt_event_create(ctx(), &ev1), "event");
+  double heff_ms = 0.0;
+  auto product = [&](const KVec& in) {
+    KVec out = newvec();
+    check(tt_event_record(ctx(), ev0), "event");
+    eng.apply(in.d->get(), out.d->get());
+    check(tt_event_record(ctx(), ev1), "event");
+    float ms = 0.f;
+    check(tt_event_elapsed_ms(ev0, ev1, &ms), "event");
+    heff_ms += ms;
+    out.p = eng.product_presence(in.p);
+    if (stats) {
+      stats->matvecs++;
+      stats->heff_flops += eng.flops;
+    }
+    return out;
+  };
+  auto nrm = [&](const KVec& a) {
+    check(tt_vec_nrm2(ctx(), n, a.d->get(), scalar_slot(0)), "norm");
+    return read1(scalar_slot(0));
+  };
+  auto multidot = [&](const std::vector<const double*>& xs, const double* y) {
+    std::vector<double> r(xs.size());
+    check(tt_vec_multidot(ctx(), n, (int)xs.size(), xs.data(), y, scalar_slot(0)), "multidot");
+    check(tt_memcpy_d2h(ctx(), r.data(), scalar_slot(0), sizeof(double) * r.size()), "d2h");
+    return r;
+  };
+  auto por = [](Presence a, const Presence& b) {
+    for (size_t i = 0; i < a.size(); ++i) a[i] |= b[i];
+    return a;
+  };
+  // coefficients for linear combinations live in scalar slots kCoefSlot..+15
+  auto lincomb = [&](KVec& y, const std::vector<const double*>& xs, const std::vector<double>& c,
+                     bool accumulate) {
+    if (xs.size() != c.size() || xs.size() > 16) throw std::runtime_error("lincomb: 1..16 vectors");
+    check(tt_memcpy_h2d(ctx(), scalar_slot(kCoefSlot), c.data(), sizeof(double) * c.size()), "coef h2d");
+    check(tt_vec_lincomb_dev(ctx(), n, (int)xs.size(), xs.data(), scalar_slot(kCoefSlot), 1.0, accumulate ? 1 : 0,
+                             y.d->get()),
+          "lincomb");
+  };
+
+  std::vector<double> M((size_t)nsz * nsz, 0.0), Mnext((size_t)nsz * nsz, 0.0), evals(nsz, 0.0);
+  double last_lambda = 1000.0;
+  const double Approx0 = 1e-12;
+  v[0] = newvec();
+  eng.pack(x, v[0].d->get());
+  v[0].p = eng.x_presence();
+  va[0] = product(v[0]);
+  double initEn = multidot({v[0].d->get()}, va[0].d->get())[0];
+  double lambda = 0.0;
+  KVec xv;  // the Ritz vector once an iteration has produced one
+  bool have_x = false;
+  for (int ii = 0; ii < actual_maxiter + 1; ++ii) {
+    const int ni = ii + 1;
+    KVec q = newvec();
+    if (ii == 0) {
+      lambda = initEn;
+      M[0] = lambda;
+      Mnext[0] = lambda;
+      // q = va[0] - lambda v[0]
+      lincomb(q, {va[0].d->get(), v[0].d->get()}, {1.0, -lambda}, false);
+      q.p = por(va[0].p, v[0].p);
+    } else {
+      for (int mi = 0; mi < ni; ++mi)
+        for (int mj = 0; mj <= mi; ++mj) {
+          Mnext[mj + mi * (ni + 1)] = M[mj + mi * ni];
+          Mnext[mi + mj * (ni + 1)] = M[mi + mj * ni];
+        }
+      DIAG(ni, M.data(), evals.data());
+      lambda = evals[0];
+      const double sgn = (M[0] < 0.0) ? -1.0 : 1.0;  // sign stabilisation (:265-268)
+      KVec xn = newvec();
+      std::vector<const double*> xs;
+      std::vector<double> c;
+      Presence px(v[0].p.size(), 0), pq(v[0].p.size(), 0);
+      for (int k = 0; k <= ii; ++k) {
+        xs.push_back(v[k].d->get());
+        c.push_back(sgn * M[k]);
+        px = por(px, v[k].p);
+      }
+      lincomb(xn, xs, c, false);
+      xn.p = px;
+      // q = sum_k M[k] va[k] - lambda x  (same sign flip)
+      xs.clear();
+      c.clear();
+      for (int k = 0; k <= ii; ++k) {
+        xs.push_back(va[k].d->get());
+        c.push_back(sgn * M[k]);
+        pq = por(pq, va[k].p);
+      }
+      xs.push_back(xn.d->get());
+      c.push_back(-lambda);
+      lincomb(q, xs, c, false);
+      q.p = por(pq, px);
+      xv = xn;
+      have_x = true;
+    }
+    double qnorm = nrm(q);
+    bool converged = (qnorm < tol && std::fabs(lambda - last_lambda) < tol) || qnorm < std::max(Approx0, tol * 1e-3);
+    last_lambda = lambda;
+    if (stats) stats->iters = ii;
+    v[ni] = q;
+    if (qnorm < 1e-20 || (converged && ii >= 1) || ii == actual_maxiter) break;
+    // Gram-Schmidt, one pass, random refill on failure (:285-320)
+    const int Npass = 1;
+    int pass = 1, tot_pass = 0;
+    bool done = false;
+    while (pass <= Npass) {
+      ++tot_pass;
+      std::vector<const double*> vs;
+      for (int k = 0; k < ni; ++k) vs.push_back(v[k].d->get());
+      std::vector<double> Vq = multidot(vs, v[ni].d->get());
+      std::vector<double> c(ni);
+      for (int k = 0; k < ni; ++k) c[k] = -Vq[k];
+      lincomb(v[ni], vs, c, true);
+      for (int k = 0; k < ni; ++k) v[ni].p = por(v[ni].p, v[k].p);
+      double qnrm = nrm(v[ni]);
+      if (qnrm < 1e-10) {
+        KVec r = newvec();
+        r.p = v[ni - 1].p;
+        std::vector<int64_t> ranges;
+        for (unsigned b = 0; b < eng.ublocks.size(); ++b)
+          if (r.p[b]) {
+            ranges.push_back(eng.ublocks[b].off);
+            ranges.push_back(eng.ublocks[b].off + eng.ublocks[b].size);
+          }
+        DevBuf dr((int64_t)ranges.size() + 1);  // one int64 per 8-byte slot
+        check(tt_memcpy_h2d(ctx(), dr.get(), ranges.data(), sizeof(int64_t) * ranges.size()), "ranges");
+        check(tt_vec_fill_random(ctx(), n, r.d->get(), (int)ranges.size() / 2, (const int64_t*)dr.get(),
+                                 rt().rng_counter++),
+              "random refill");
+        check(tt_ctx_synchronize(ctx()), "sync");
+        v[ni] = r;
+        if (stats) stats->randomized++;
+        qnrm = nrm(v[ni]);
+        --pass;
+        if (ni >= maxsize || tot_pass > Npass * 3) {
+          done = true;
+          break;
+        }
+      }
+      check(tt_vec_scal(ctx(), n, 1.0 / qnrm, v[ni].d->get()), "scale");
+      ++pass;
+    }
+    if (done) break;
+    va[ni] = product(v[ni]);
+    std::swap(M, Mnext);
+    std::vector<const double*> vs;
+    for (int k = 0; k <= ni; ++k) vs.push_back(v[k].d->get());
+    std::vector<double> row = multidot(vs, va[ni].d->get());
+    const int l = ni;
+    for (int k = 0; k < ni + 1; ++k) {
+      M[l + k * (ni + 1)] = row[k];
+      M[k + l * (ni + 1)] = row[k];
+    }
+  }
+  tt_event_destroy(ev0);
+  tt_event_destroy(ev1);
+  if (have_x) {
+    x = eng.materialize(xv.p, xv.d);
+  }
+  x.normalize();
+  if (stats) stats->heff_flops = stats->heff_flops;  // kept
+  rt().last_heff_ms = heff_ms;
+  return lambda;
+}
+
+// ---- spin-1/2 sites and MPS/MPO construction ------------------------------
+double spin_half_op(unsigned bra, const std::string& op, unsigned ket) {
+  const unsigned Dn = 0, Up = 1;
+  if (op == "Id" || op == "I") return ket == bra ? 1.0 : 0.0;
+  if (op == "Sz") {
+    if (ket == Dn && bra == Dn) return -0.5;
+    if (ket == Up && bra == Up) return 0.5;
+    return 0.0;
+  }
+  if (op == "Sx") return ket != bra ? 0.5 : 0.0;
+  if (op == "S+" || op == "Sp") return (ket == Dn && bra == Up) ? 1.0 : 0.0;
+  if (op == "S-" || op == "Sm") return (ket == Up && bra == Dn) ? 1.0 : 0.0;
+  throw std::runtime_error("spinhalf: unsupported operator " + op);
+}
+
+qMPS make_product_qmps(unsigned L, const std::vector<QN>& phy_qn, const std::vector<unsigned>& state,
+                       unsigned id) {
+  if (state.size() != L || L < 3) throw std::runtime_error("make_product_qmps: bad length");
+  qMPS psi;
+  psi.length = L;
+  psi.id = id;
+  psi.phy_qn = phy_qn;
+  psi.bond_dims.assign(L + 1, 1);
+  QN tot(0, 0);
+  for (unsigned s : state) tot += phy_qn.at(s);
+  psi.totalQ = tot;
+  std::vector<std::set<QN>> link(L + 1);
+  link[0].insert(QN(0, 0));
+  link[L].insert(tot);
+  for (unsigned j = 1; j < L; ++j)
+    for (const QN& q : link[j - 1])
+      for (const QN& p : phy_qn) link[j].insert(q + p);
+  for (unsigned j = L - 1; j > 0; --j) {
+    std::vector<QN> rm;
+    for (const QN& q : link[j]) {
+      bool ok = false;
+      for (const QN& p : phy_qn)
+        if (link[j + 1].count(q + p)) { ok = true; break; }
+      if (!ok) rm.push_back(q);
+    }
+    for (auto& q : rm) link[j].erase(q);
+  }
+  for (unsigned i = 0; i < L; ++i) {
+    qtensor T({qtensor_index(Inward, psi.link_name(i), Link, 0),
+               qtensor_index(Inward, "Site" + std::to_string(i), Site, 0),
+               qtensor_index(Outward, psi.link_name(i + 1), Link, 0)});
+    for (const QN& q : link[i]) T.idx_set[0].addQN(q, 1);
+    for (const QN& p : phy_qn) T.idx_set[1].addQN(p, 1);
+    for (const QN& q : link[i + 1]) T.idx_set[2].addQN(q, 1);
+    T.initBlock();
+    psi.A.push_back(std::move(T));
+  }
+  QN last(0, 0);
+  for (unsigned i = 0; i < L; ++i) {
+    QN p = phy_qn[state[i]];
+    QNKey k{last.pack(), p.pack(), (last + p).pack()};
+    last += p;
+    int b = psi.A[i].find_block(k);
+    if (b < 0) throw std::runtime_error("make_product_qmps: product block missing");
+    double one = 1.0;
+    psi.A[i].set_block((unsigned)b, &one);
+  }
+  psi.center = (int)L - 1;
+  return psi;
+}
+
+qMPO make_heisenberg_qmpo(unsigned L, const double* dh, double tE, unsigned id) {
+  qMPO H;
+  H.length = L;
+  H.id = id;
+  H.phy_qn = {QN(-1), QN(1)};
+  std::string pref = "ID" + std::to_string(id) + "Link";
+  std::vector<std::vector<std::vector<double>>> host(L);
+  for (unsigned i = 0; i < L; ++i) {
+    qtensor T({qtensor_index(Inward, pref + std::to_string(i), Link, 0),
+               qtensor_index(Outward, "Site" + std::to_string(i), Site, 0),
+               qtensor_index(Inward, "Site" + std::to_string(i), Site, 1),
+               qtensor_index(Outward, pref + std::to_string(i + 1), Link, 0)});
+    if (i == 0) {
+      T.idx_set[0].addQN(QN(0), 1);
+    } else {
+      T.idx_set[0].addQN(QN(0), 3);
+      T.idx_set[0].addQN(QN(-2), 1);
+      T.idx_set[0].addQN(QN(2), 1);
+    }
+    for (auto& p : H.phy_qn) T.idx_set[1].addQN(p, 1);
+    for (auto& p : H.phy_qn) T.idx_set[2].addQN(p, 1);
+    if (i == L - 1) {
+      T.idx_set[3].addQN(QN(0), 1);
+    } else {
+      T.idx_set[3].addQN(QN(0), 3);
+      T.idx_set[3].addQN(QN(-2), 1);
+      T.idx_set[3].addQN(QN(2), 1);
+    }
+    T.initBlock();
+    host[i].resize(T.blocks.size());
+    for (unsigned b = 0; b < T.blocks.size(); ++b) host[i][b].assign((size_t)T.blocks[b].size, 0.0);
+    H.A.push_back(std::move(T));
+  }
+  // addOperators for qMPO (models/hams/Heisenberg.cpp:152-196)
+  auto add = [&](unsigned site, unsigned r, unsigned c, const std::string& op, double val, int Qi, int Qo) {
+    qtensor& T = H.A[site];
+    bool added = false;
+    for (unsigned k = 0; k < 2; ++k)
+      for (unsigned b = 0; b < 2; ++b) {
+        QNKey key{QN(Qi).pack(), H.phy_qn[k].pack(), H.phy_qn[b].pack(), QN(Qo).pack()};
+        int blk = T.find_block(key);
+        if (blk < 0) continue;
+        added = true;
+        const BlockMeta& bm = T.blocks[blk];
+        int64_t s3 = (int64_t)bm.qd[0] * bm.qd[1] * bm.qd[2];
+        int64_t off = (site == 0) ? s3 * c : (int64_t)r + s3 * c;
+        host[site][blk][(size_t)off] = val * spin_half_op(b, op, k);
+      }
+    if (!added) throw std::runtime_error("heisenberg qMPO: operator block missing");
+  };
+  for (unsigned site = 0; site < L; ++site) {
+    bool last = site == L - 1;
+    if (site > 0) add(site, 0, 0, "Id", 1.0, 0, 0);
+    if (!last) add(site, 1, 1, "Id", 1.0, 0, 0);
+    if (dh) add(site, 1, 0, "Sz", dh[site], 0, 0);
+    if (tE != 0) add(site, 1, 0, "Id", -tE / L, 0, 0);
+    if (site > 0) add(site, 2, 0, "Sz", 1.0, 0, 0);
+    if (!last) add(site, 1, 2, "Sz", 1.0, 0, 0);
+    if (site > 0) add(site, 0, 0, "S+", 1.0, -2, 0);
+    if (site > 0) add(site, 0, 0, "S-", 1.0, 2, 0);
+    if (!last) add(site, 1, 0, "S-", 0.5, 0, -2);
+    if (!last) add(site, 1, 0, "S+", 0.5, 0, 2);
+  }
+  for (unsigned i = 0; i < L; ++i)
+    for (unsigned b = 0; b < H.A[i].blocks.size(); ++b) H.A[i].set_block(b, host[i][b].data());
+  return H;
+}
+
+// ---- canonical centre ------------------------------------------------------
+double qMPS::position(int site) {
+  // mps/qtt.cpp:932-994
+  if (center == -1) {
+    center = (int)length - 1;  // rc(): sweep the centre from the right end
+    while (center > 0) position(center - 1);
+  }
+  qtensor U, V, S;
+  bool moved = false;
+  while (center != site) {
+    std::vector<qtensor_index> left, right;
+    qtensor_index mid;
+    if (center > site) {
+      std::string ln = link_name((unsigned)center);
+      for (auto& ix : A[center].idx_set) {
+        if (ix.name() == ln) { left.push_back(ix); mid = ix; } else right.push_back(ix);
+      }
+      svd(A[center], left, right, U, V, S, MoveFromRight);
+      bond_dims[center] = (unsigned)S.total_size();
+      A[center] = std::move(V);
+      A[center].idx_set[0].rename(mid.name());
+      A[center].idx_set[0].prime((int)mid.level() - (int)A[center].idx_set[0].level());
+      A[center - 1] = A[center - 1] * U;
+      A[center - 1].idx_set.back().rename(mid.name());
+      A[center - 1].idx_set.back().prime((int)mid.level() - (int)A[center - 1].idx_set.back().level());
+      --center;
+    } else {
+      std::string ln = link_name((unsigned)center + 1);
+      for (auto& ix : A[center].idx_set) {
+        if (ix.name() == ln) { right.push_back(ix); mid = ix; } else left.push_back(ix);
+      }
+      svd(A[center], left, right, U, V, S, MoveFromLeft);
+      bond_dims[center + 1] = (unsigned)S.total_size();
+      A[center] = std::move(U);
+      A[center].idx_set.back().rename(mid.name());
+      A[center].idx_set.back().prime((int)mid.level() - (int)A[center].idx_set.back().level());
+      A[center + 1] = V * A[center + 1];
+      A[center + 1].idx_set[0].rename(mid.name());
+      A[center + 1].idx_set[0].prime((int)mid.level() - (int)A[center + 1].idx_set[0].level());
+      ++center;
+    }
+    moved = true;
+  }
+  if (!moved) return 0.0;
+  return calcEntropy(S);
+}
+
+void qMPS::normalize() {
+  // mps/qtt.cpp:899-909 (centre form)
+  double nm = A[center].norm();
+  A[center] /= nm;
+}
+
+// ---- environments, site update, sweep ---------------------------------------
+static qtensor boundary(const qtensor_index& psi_ix, const qtensor_index& h_ix) {
+  qtensor T({psi_ix, h_ix, psi_ix});
+  T.idx_set[0].prime();  // primeLink
+  T.idx_set[0].dag();
+  T.initBlock();
+  T.setOne();
+  T.dag();
+  return T;
+}
+
+static qtensor env_step(const qtensor& env, const qtensor& Ai, const qtensor& W) {
+  qtensor t1 = shallow(Ai);
+  t1.conj();
+  t1.dag();
+  t1.prime();
+  qtensor t4 = t1 * env;
+  qtensor t5 = t4 * W;
+  return t5 * Ai;
+}
+
+void buildEnv(qMPS& psi, qMPO& H, std::vector<qtensor>& TR, std::vector<qtensor>& TL) {
+  // algos/dmrg/dmrg.cpp:56-85
+  const unsigned L = psi.length;
+  TL[0] = boundary(psi.A[0].idx_set[0], H.A[0].idx_set[0]);
+  TR[L - 1] = boundary(psi.A[L - 1].idx_set.back(), H.A[L - 1].idx_set.back());
+  for (unsigned i = L - 1; i > 0; --i) TR[i - 1] = env_step(TR[i], psi.A[i], H.A[i]);
+}
+
+void updateSite(qMPS& psi, qMPO& H, std::vector<qtensor>& TR, std::vector<qtensor>& TL, unsigned site,
+                double& energy, int direction, int max_bd, double cutoff, char mode, int search_space_size,
+                int max_restart, DmrgLog* log) {
+  // algos/dmrg/dmrg.cpp:300-372
+  unsigned l, r;
+  if (direction == MoveFromLeft) { l = site; r = site + 1; } else { l = site - 1; r = site; }
+  big_qtensor A;
+  A.setLeft(&TL[l]);
+  A.addMid(&H.A[l]);
+  A.addMid(&H.A[r]);
+  A.setRight(&TR[r]);
+  qtensor x = psi.A[l] * psi.A[r];
+  DavidsonStats st;
+  energy = tensor_davidsonIT(A, x, search_space_size, max_restart, 1e-12, mode, &st);
+  std::string ln = psi.link_name(r);
+  qtensor_index mid;
+  for (auto& ix : psi.A[l].idx_set)
+    if (ix.name() == ln) { mid = ix; break; }
+  qtensor S;
+  TruncInfo info;
+  svd_bond(x, psi.A[l], psi.A[r], mid, S, direction, cutoff, (unsigned long)max_bd, &info);
+  psi.bond_dims[r] = (unsigned)S.total_size();
+  psi.center = (int)(direction == MoveFromLeft ? r : l);
+  if (log) {
+    StepLog s;
+    s.site = (int)site;
+    s.direction = direction;
+    s.energy = energy;
+    s.trunc_err = info.trunc_err;
+    s.kept = info.kept;
+    s.matvecs = st.matvecs;
+    s.randomized = st.randomized;
+    s.heff_flops = st.heff_flops;
+    s.sector_qn = info.sector_qn;
+    s.kept_per_sector = info.kept_per_sector;
+    log->steps.push_back(std::move(s));
+    log->heff_flops += st.heff_flops;
+    log->heff_seconds += rt().last_heff_ms * 1e-3;
+    bool mid_bond = direction == MoveFromLeft ? (site == psi.length / 2 - 1) : (site == psi.length / 2);
+    if (mid_bond) log->entropy.push_back(calcEntropy(S));
+  }
+}
+
+void updateEnv(qMPS& psi, qMPO& H, std::vector<qtensor>& TR, std::vector<qtensor>& TL, unsigned site,
+               int direction) {
+  // algos/dmrg/dmrg.cpp:491-509
+  if (direction == MoveFromLeft)
+    TL[site + 1] = env_step(TL[site], psi.A[site], H.A[site]);
+  else
+    TR[site - 1] = env_step(TR[site], psi.A[site], H.A[site]);
+}
+
+void dmrg_prepare(qMPS& psi, qMPO& H, DmrgState& st, DmrgLog* log) {
+  const unsigned L = H.length;
+  psi.position(0);
+  psi.normalize();
+  st.TR.assign(L, qtensor());
+  st.TL.assign(L, qtensor());
+  buildEnv(psi, H, st.TR, st.TL);
+  st.envs_built = true;
+  st.sweeps_done = 0;
+  big_qtensor A;  // initial energy of the one-site problem (dmrg.cpp:716-723)
+  A.setLeft(&st.TL[0]);
+  A.addMid(&H.A[0]);
+  A.setRight(&st.TR[0]);
+  double e = A.expec(psi.A[0]);
+  if (log) log->initial_energy = e;
+}
+
+double dmrg_sweep(qMPS& psi, qMPO& H, DmrgState& st, int max_bd, double cutoff, int max_restart,
+                  DmrgLog* log) {
+  const unsigned L = H.length;
+  double energy = 0.0;
+  auto t0 = std::chrono::steady_clock::now();
+  for (int half = 0; half < 2; ++half) {
+    int direction = half == 0 ? MoveFromLeft : MoveFromRight;
+    for (unsigned i = 0; i < L - 1; ++i) {
+      unsigned site = direction == MoveFromLeft ? i : L - 1 - i;
+      updateSite(psi, H, st.TR, st.TL, site, energy, direction, max_bd, cutoff, 'S', 3, max_restart, log);
+      updateEnv(psi, H, st.TR, st.TL, site, direction);
+    }
+  }
+  psi.normalize();
+  check(tt_ctx_synchronize(ctx()), "sweep sync");
+  auto t1 = std::chrono::steady_clock::now();
+  if (log) {
+    log->sweep_energy.push_back(energy);
+    log->sweep_seconds.push_back(std::chrono::duration<double>(t1 - t0).count());
+  }
+  st.sweeps_done++;
+  return energy;
+}
+
+void dmrg_finish(qMPS& psi) { psi.position(0); }
+
+double dmrg(qMPS& psi, qMPO& H, int num_sweeps, const std::vector<int>& max_bd,
+            const std::vector<double>& cutoff, const std::vector<int>& max_restart, DmrgLog* log) {
+  DmrgState st;
+  dmrg_prepare(psi, H, st, log);
+  double energy = 0.0;
+  for (int sweep = 0; sweep < num_sweeps; ++sweep) {
+    int lbd = sweep % (int)max_bd.size();
+    int lc = sweep % (int)cutoff.size();
+    int lmr = sweep % (int)max_restart.size();
+    energy = dmrg_sweep(psi, H, st, max_bd[lbd], cutoff[lc], max_restart[lmr], log);
+  }
+  dmrg_finish(psi);
+  return energy;
+}
+
+}  // namespace ttb

@@ -1,0 +1,68 @@
+// Internal runtime shared by the sm_100a kernels and the C ABI entry points.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstdio>
+#include <string>
+#include <vector>
+
+#include "../../include/tt_b200.h"
+
+struct tt_ctx {
+  int device = 0;
+  int num_sms = 148;
+  cudaStream_t stream = nullptr;
+  cudaMemPool_t pool = nullptr;
+  int64_t launches = 0;
+  // small pinned staging buffer for scalar reads
+  double* h_scalars = nullptr;
+  // device scratch for two-pass reductions
+  double* d_partials = nullptr;
+  int partials_cap = 0;
+};
+
+namespace tt {
+
+void set_error(const std::string& msg);
+int fail(int code, const std::string& msg);
+int cuda_fail(cudaError_t e, const char* what, const char* file, int line);
+
+// Launch bookkeeping: every kernel launch goes through this so the context
+// can report how many of its kernels ran.
+inline void count_launch(tt_ctx* ctx) { ctx->launches++; }
+
+template <class T>
+inline T* pool_alloc(tt_ctx* ctx, size_t n) {
+  void* p = nullptr;
+  if (n == 0) n = 1;
+  if (cudaMallocAsync(&p, n * sizeof(T), ctx->stream) != cudaSuccess) return nullptr;
+  return static_cast<T*>(p);
+}
+inline void pool_free(tt_ctx* ctx, void* p) {
+  if (p) cudaFreeAsync(p, ctx->stream);
+}
+
+// Reduction scratch of at least n doubles (grown on demand).
+double* partials(tt_ctx* ctx, int n);
+
+}  // namespace tt
+
+#define TT_CUDA(expr)                                                   \
+  do {                                                                  \
+    cudaError_t _e = (expr);                                            \
+    if (_e != cudaSuccess) return tt::cuda_fail(_e, #expr, __FILE__, __LINE__); \
+  } while (0)
+
+#define TT_LAUNCH_CHECK(ctx)                                             \
+  do {                                                                   \
+    tt::count_launch(ctx);                                               \
+    cudaError_t _e = cudaGetLastError();                                 \
+    if (_e != cudaSuccess) return tt::cuda_fail(_e, "kernel launch", __FILE__, __LINE__); \
+  } while (0)
+
+#define TT_REQUIRE(cond, msg)                                            \
+  do {                                                                   \
+    if (!(cond)) return tt::fail(TT_ERR_INVALID, msg);                   \
+  } while (0)

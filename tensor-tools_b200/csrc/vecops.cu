@@ -1,0 +1,267 @@
+// Davidson vector kernels over flat block-sparse vectors (qtensor/qtensor.cpp
+// :1031-1179,1606-1647): dot, multi-dot, norm, axpy, scale, linear
+// combinations with device-side coefficients, masked random fill and the
+// diagonal preconditioner.  All are HBM-bound streaming kernels: 16-byte
+// vector loads, a fixed grid (a multiple of the SM count) and a two-pass
+// deterministic reduction (same summation order on every run).
+#include <cmath>
+#include <vector>
+
+#include "tt_internal.h"
+
+namespace {
+
+constexpr int RT = 256;       // threads per reduction block
+constexpr int MAXVEC = 16;    // vectors per multi-dot / linear combination
+
+inline int red_blocks(tt_ctx* ctx, int64_t n) {
+  int64_t want = (n + RT * 4 - 1) / (RT * 4);
+  int cap = ctx->num_sms * 4;
+  if (want < 1) want = 1;
+  return (int)(want < cap ? want : cap);
+}
+
+template <int NV>
+__device__ __forceinline__ void block_reduce_store(double (&v)[NV], double* out, int stride) {
+  __shared__ double sh[NV][RT / 32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+  for (int j = 0; j < NV; ++j) {
+    double x = v[j];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+    if (lane == 0) sh[j][w] = x;
+  }
+  __syncthreads();
+  if (threadIdx.x < NV) {
+    double s = 0.0;
+    for (int i = 0; i < RT / 32; ++i) s += sh[threadIdx.x][i];
+    out[threadIdx.x * stride + blockIdx.x] = s;
+  }
+}
+
+// partial sums of sum_i xs[j][i]*y[i] for j < nv
+struct PtrPack {
+  const double* p[MAXVEC];
+};
+
+template <int NV>
+__global__ void __launch_bounds__(RT) multidot_pass1(int64_t n, PtrPack xs,
+                                                     const double* __restrict__ y,
+                                                     double* part, int nv) {
+  double acc[NV];
+#pragma unroll
+  for (int j = 0; j < NV; ++j) acc[j] = 0.0;
+  const int64_t n2 = n / 2;
+  const double2* y2 = reinterpret_cast<const double2*>(y);
+  for (int64_t i = blockIdx.x * (int64_t)RT + threadIdx.x; i < n2; i += (int64_t)gridDim.x * RT) {
+    double2 b = y2[i];
+#pragma unroll
+    for (int j = 0; j < NV; ++j) {
+      if (j < nv) {
+        double2 a = reinterpret_cast<const double2*>(xs.p[j])[i];
+        acc[j] = fma(a.x, b.x, acc[j]);
+        acc[j] = fma(a.y, b.y, acc[j]);
+      }
+    }
+  }
+  if ((n & 1) && blockIdx.x == 0 && threadIdx.x == 0) {
+#pragma unroll
+    for (int j = 0; j < NV; ++j)
+      if (j < nv) acc[j] = fma(xs.p[j][n - 1], y[n - 1], acc[j]);
+  }
+  block_reduce_store<NV>(acc, part, gridDim.x);
+}
+
+__global__ void reduce_pass2(const double* part, int nblk, int nv, double* out, int do_sqrt) {
+  // one warp per output, fixed order
+  const int j = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (j >= nv) return;
+  double s = 0.0;
+  for (int i = lane; i < nblk; i += 32) s += part[j * nblk + i];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+  if (lane == 0) out[j] = do_sqrt ? sqrt(s) : s;
+}
+
+__global__ void axpy_kernel(int64_t n, double a, const double* __restrict__ x, double* __restrict__ y) {
+  const int64_t n2 = n / 2;
+  const double2* x2 = reinterpret_cast<const double2*>(x);
+  double2* y2 = reinterpret_cast<double2*>(y);
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n2; i += (int64_t)gridDim.x * blockDim.x) {
+    double2 u = x2[i], v = y2[i];
+    v.x = fma(a, u.x, v.x);
+    v.y = fma(a, u.y, v.y);
+    y2[i] = v;
+  }
+  if ((n & 1) && blockIdx.x == 0 && threadIdx.x == 0) y[n - 1] = fma(a, x[n - 1], y[n - 1]);
+}
+
+__global__ void scal_kernel(int64_t n, double a, const double* d_nrm, double* __restrict__ x) {
+  if (d_nrm) a = 1.0 / d_nrm[0];
+  const int64_t n2 = n / 2;
+  double2* x2 = reinterpret_cast<double2*>(x);
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n2; i += (int64_t)gridDim.x * blockDim.x) {
+    double2 v = x2[i];
+    v.x *= a;
+    v.y *= a;
+    x2[i] = v;
+  }
+  if ((n & 1) && blockIdx.x == 0 && threadIdx.x == 0) x[n - 1] *= a;
+}
+
+__global__ void lincomb_kernel(int64_t n, int nv, PtrPack xs, const double* __restrict__ coef,
+                               double sign, int accumulate, double* __restrict__ y) {
+  __shared__ double c[MAXVEC];
+  if (threadIdx.x < nv) c[threadIdx.x] = sign * coef[threadIdx.x];
+  __syncthreads();
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    double s = accumulate ? y[i] : 0.0;
+    for (int j = 0; j < nv; ++j) s = fma(c[j], xs.p[j][i], s);
+    y[i] = s;
+  }
+}
+
+__device__ __forceinline__ uint64_t splitmix64(uint64_t z) {
+  z += 0x9E3779B97F4A7C15ull;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+__global__ void fill_random_kernel(int64_t n, double* x, int nranges, const int64_t* ranges, uint64_t seed) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    // binary search: is i inside one of the sorted [begin,end) ranges?
+    int lo = 0, hi = nranges;
+    while (lo < hi) {
+      int mid = (lo + hi) >> 1;
+      if (ranges[2 * mid + 1] <= i) lo = mid + 1; else hi = mid;
+    }
+    bool in = lo < nranges && ranges[2 * lo] <= i;
+    double v = 0.0;
+    if (in) v = (double)(splitmix64(seed ^ (uint64_t)i * 0xD1B54A32D192ED03ull) >> 11) * 0x1.0p-53;
+    x[i] = v;
+  }
+}
+
+__global__ void precondition_kernel(int64_t n, double* __restrict__ x, const double* __restrict__ D, double theta) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    double d = D[i];
+    if (d != theta) x[i] = x[i] / (d - theta);
+  }
+}
+
+inline int stream_blocks(tt_ctx* ctx, int64_t n) {
+  int64_t want = (n + 511) / 512;
+  int cap = ctx->num_sms * 8;
+  if (want < 1) want = 1;
+  return (int)(want < cap ? want : cap);
+}
+
+bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; }
+
+int launch_multidot(tt_ctx* ctx, int64_t n, int nv, const double* const* xs, const double* y,
+                    double* d_out, int do_sqrt) {
+  PtrPack pk;
+  for (int j = 0; j < nv; ++j) {
+    if (!aligned16(xs[j])) return tt::fail(TT_ERR_INVALID, "vectors must be 16-byte aligned");
+    pk.p[j] = xs[j];
+  }
+  int nb = red_blocks(ctx, n);
+  double* part = tt::partials(ctx, nb * nv);
+  if (!part) return tt::fail(TT_ERR_OOM, "reduction scratch");
+  if (nv <= 1)
+    multidot_pass1<1><<<nb, RT, 0, ctx->stream>>>(n, pk, y, part, nv);
+  else if (nv <= 4)
+    multidot_pass1<4><<<nb, RT, 0, ctx->stream>>>(n, pk, y, part, nv);
+  else
+    multidot_pass1<MAXVEC><<<nb, RT, 0, ctx->stream>>>(n, pk, y, part, nv);
+  TT_LAUNCH_CHECK(ctx);
+  reduce_pass2<<<1, 32 * nv, 0, ctx->stream>>>(part, nb, nv, d_out, do_sqrt);
+  TT_LAUNCH_CHECK(ctx);
+  return TT_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int tt_vec_multidot(tt_ctx* ctx, int64_t n, int nvec, const double* const* xs, const double* y,
+                    double* d_out) {
+  TT_REQUIRE(ctx && xs && y && d_out, "tt_vec_multidot: null argument");
+  TT_REQUIRE(nvec >= 1 && nvec <= MAXVEC, "tt_vec_multidot: 1..16 vectors");
+  TT_REQUIRE(aligned16(y), "tt_vec_multidot: vectors must be 16-byte aligned");
+  return launch_multidot(ctx, n, nvec, xs, y, d_out, 0);
+}
+
+int tt_vec_dot(tt_ctx* ctx, int64_t n, const double* x, const double* y, double* d_out) {
+  TT_REQUIRE(ctx && x && y && d_out, "tt_vec_dot: null argument");
+  TT_REQUIRE(aligned16(y), "tt_vec_dot: vectors must be 16-byte aligned");
+  const double* xs[1] = {x};
+  return launch_multidot(ctx, n, 1, xs, y, d_out, 0);
+}
+
+int tt_vec_nrm2(tt_ctx* ctx, int64_t n, const double* x, double* d_out) {
+  TT_REQUIRE(ctx && x && d_out, "tt_vec_nrm2: null argument");
+  TT_REQUIRE(aligned16(x), "tt_vec_nrm2: vectors must be 16-byte aligned");
+  const double* xs[1] = {x};
+  return launch_multidot(ctx, n, 1, xs, x, d_out, 1);
+}
+
+int tt_vec_axpy(tt_ctx* ctx, int64_t n, double a, const double* x, double* y) {
+  TT_REQUIRE(ctx && x && y, "tt_vec_axpy: null argument");
+  TT_REQUIRE(aligned16(x) && aligned16(y), "tt_vec_axpy: vectors must be 16-byte aligned");
+  if (n <= 0) return TT_OK;
+  axpy_kernel<<<stream_blocks(ctx, n), 256, 0, ctx->stream>>>(n, a, x, y);
+  TT_LAUNCH_CHECK(ctx);
+  return TT_OK;
+}
+
+int tt_vec_scal(tt_ctx* ctx, int64_t n, double a, double* x) {
+  TT_REQUIRE(ctx && x, "tt_vec_scal: null argument");
+  TT_REQUIRE(aligned16(x), "tt_vec_scal: vectors must be 16-byte aligned");
+  if (n <= 0) return TT_OK;
+  scal_kernel<<<stream_blocks(ctx, n), 256, 0, ctx->stream>>>(n, a, nullptr, x);
+  TT_LAUNCH_CHECK(ctx);
+  return TT_OK;
+}
+
+int tt_vec_scal_inv_dev(tt_ctx* ctx, int64_t n, const double* d_nrm, double* x) {
+  TT_REQUIRE(ctx && x && d_nrm, "tt_vec_scal_inv_dev: null argument");
+  TT_REQUIRE(aligned16(x), "tt_vec_scal_inv_dev: vectors must be 16-byte aligned");
+  if (n <= 0) return TT_OK;
+  scal_kernel<<<stream_blocks(ctx, n), 256, 0, ctx->stream>>>(n, 1.0, d_nrm, x);
+  TT_LAUNCH_CHECK(ctx);
+  return TT_OK;
+}
+
+int tt_vec_lincomb_dev(tt_ctx* ctx, int64_t n, int nvec, const double* const* xs,
+                       const double* d_coef, double sign, int accumulate, double* y) {
+  TT_REQUIRE(ctx && xs && d_coef && y, "tt_vec_lincomb_dev: null argument");
+  TT_REQUIRE(nvec >= 0 && nvec <= MAXVEC, "tt_vec_lincomb_dev: 0..16 vectors");
+  PtrPack pk;
+  for (int j = 0; j < nvec; ++j) pk.p[j] = xs[j];
+  if (n <= 0) return TT_OK;
+  lincomb_kernel<<<stream_blocks(ctx, n), 256, 0, ctx->stream>>>(n, nvec, pk, d_coef, sign, accumulate, y);
+  TT_LAUNCH_CHECK(ctx);
+  return TT_OK;
+}
+
+int tt_vec_fill_random(tt_ctx* ctx, int64_t n, double* x, int nranges, const int64_t* d_ranges,
+                       uint64_t seed) {
+  TT_REQUIRE(ctx && x && (nranges == 0 || d_ranges), "tt_vec_fill_random: null argument");
+  if (n <= 0) return TT_OK;
+  fill_random_kernel<<<stream_blocks(ctx, n), 256, 0, ctx->stream>>>(n, x, nranges, d_ranges, seed);
+  TT_LAUNCH_CHECK(ctx);
+  return TT_OK;
+}
+
+int tt_vec_precondition(tt_ctx* ctx, int64_t n, double* x, const double* D, double theta) {
+  TT_REQUIRE(ctx && x && D, "tt_vec_precondition: null argument");
+  if (n <= 0) return TT_OK;
+  precondition_kernel<<<stream_blocks(ctx, n), 256, 0, ctx->stream>>>(n, x, D, theta);
+  TT_LAUNCH_CHECK(ctx);
+  return TT_OK;
+}
+
+}  // extern "C"

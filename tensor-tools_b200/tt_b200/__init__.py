@@ -1,0 +1,506 @@
+"""Python binding of the B200 two-site DMRG C ABI (include/tt_b200.h, include/tt_dmrg.h).
+
+The binding is a thin ctypes layer: every object lives in the C++ host layer
+of ``lib/libtt_b200.so`` and every number is computed by its sm_100a kernels.
+There is no CPU fallback -- importing works without a GPU (the library only
+needs the CUDA runtime to load), but creating a ``Context`` requires a B200.
+
+Names follow tensor-tools: ``QTensor`` (qtensor), ``BigQTensor``
+(big_qtensor), ``svd``/``svd_bond``, ``QMPS``/``QMPO``, ``QDMRG`` (the
+schedule overload of ``dmrg``).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import re
+from typing import List, Optional, Sequence, Tuple
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.dirname(HERE)
+ROOT = os.path.dirname(PKG)
+LIB_PATH = os.path.join(PKG, "lib", "libtt_b200.so")
+HEADERS = [os.path.join(ROOT, "include", "tt_b200.h"), os.path.join(ROOT, "include", "tt_dmrg.h")]
+
+TT_OK = 0
+MoveFromLeft, MoveFromRight = 0, 1
+Inward, Outward = 0, 1
+Link, Site = 0, 1
+
+
+class TTError(RuntimeError):
+    pass
+
+
+def _load():
+    if not os.path.exists(LIB_PATH):
+        raise ImportError("libtt_b200.so not built: run tensor-tools_b200/build.py (%s)" % LIB_PATH)
+    return C.CDLL(LIB_PATH)
+
+
+lib = _load()
+
+P = C.c_void_p
+I32 = C.c_int32
+I64 = C.c_int64
+D = C.c_double
+PI32 = C.POINTER(C.c_int32)
+PI64 = C.POINTER(C.c_int64)
+PD = C.POINTER(C.c_double)
+PP = C.POINTER(C.c_void_p)
+
+
+class IndexDesc(C.Structure):
+    _fields_ = [("arrow", I32), ("type", I32), ("level", I32), ("n_sectors", I32),
+                ("name", C.c_char_p), ("qn", PI32), ("qdim", PI32)]
+
+
+def _proto(name, *args):
+    f = getattr(lib, name)
+    f.restype = C.c_int
+    f.argtypes = list(args)
+    return f
+
+
+_proto("tt_ctx_create", C.c_int, PP)
+_proto("tt_ctx_destroy", P)
+_proto("tt_ctx_synchronize", P)
+_proto("tt_ctx_stream", P, PP)
+_proto("tt_ctx_launch_count", P, PI64)
+lib.tt_get_last_error.restype = C.c_char_p
+lib.tt_get_last_error.argtypes = []
+_proto("tt_dmrg_bind", P)
+_proto("tt_dmrg_unbind")
+_proto("tt_device_alloc", P, C.c_size_t, PP)
+_proto("tt_device_free", P, P)
+_proto("tt_memcpy_h2d", P, P, P, C.c_size_t)
+_proto("tt_memcpy_d2h", P, P, P, C.c_size_t)
+_proto("tt_memset_zero", P, P, C.c_size_t)
+_proto("tt_vec_dot", P, I64, P, P, P)
+_proto("tt_vec_nrm2", P, I64, P, P)
+_proto("tt_vec_axpy", P, I64, D, P, P)
+_proto("tt_vec_scal", P, I64, D, P)
+_proto("tt_vec_multidot", P, I64, C.c_int, PP, P, P)
+_proto("tt_vec_lincomb_dev", P, I64, C.c_int, PP, P, D, C.c_int, P)
+_proto("tt_vec_fill_random", P, I64, P, C.c_int, P, C.c_uint64)
+_proto("tt_vec_precondition", P, I64, P, P, D)
+_proto("tt_qtensor_create", C.c_int, C.POINTER(IndexDesc), PP)
+_proto("tt_qtensor_init_blocks", P)
+_proto("tt_qtensor_set_blocks", P, C.c_int, PI32)
+_proto("tt_qtensor_destroy", P)
+_proto("tt_qtensor_copy", P, PP)
+_proto("tt_qtensor_rank", P, C.POINTER(C.c_int))
+_proto("tt_qtensor_index", P, C.c_int, PI32, PI32, PI32, PI32, C.c_char_p, C.c_int, PI32, PI32, C.c_int)
+_proto("tt_qtensor_num_blocks", P, C.POINTER(C.c_int))
+_proto("tt_qtensor_block_info", P, C.c_int, PI32, PI32, PI32, PI64)
+_proto("tt_qtensor_find_block", P, PI32, C.POINTER(C.c_int))
+_proto("tt_qtensor_get_block", P, C.c_int, PD)
+_proto("tt_qtensor_set_block", P, C.c_int, PD)
+_proto("tt_qtensor_prime", P, C.c_int)
+_proto("tt_qtensor_dag", P)
+_proto("tt_qtensor_contract", P, P, PP)
+_proto("tt_qtensor_norm", P, PD)
+_proto("tt_qtensor_scale", P, D)
+_proto("tt_qtensor_add", P, P, D)
+_proto("tt_qtensor_inner_product", P, P, PD)
+_proto("tt_qtensor_svd", P, C.c_int, C.POINTER(C.c_int), C.c_int, D, C.c_uint, PP, PP, PP, PD,
+       C.POINTER(C.c_uint))
+_proto("tt_qtensor_svd_bond", P, P, P, C.c_int, C.c_int, D, C.c_ulong, PP, PD, C.POINTER(C.c_uint))
+_proto("tt_bigq_create", P, P, P, P, PP)
+_proto("tt_bigq_product", P, P, PP)
+_proto("tt_bigq_size", P, C.POINTER(C.c_uint64))
+_proto("tt_bigq_davidson", P, P, C.c_int, D, PD, C.POINTER(C.c_int))
+_proto("tt_bigq_destroy", P)
+_proto("tt_qmps_product_spinhalf", C.c_int, C.POINTER(C.c_int), C.c_uint, PP)
+_proto("tt_qmps_destroy", P)
+_proto("tt_qmps_length", P, C.POINTER(C.c_int))
+_proto("tt_qmps_bond_dims", P, C.POINTER(C.c_int))
+_proto("tt_qmps_center", P, C.POINTER(C.c_int))
+_proto("tt_qmps_position", P, C.c_int)
+_proto("tt_qmps_tensor", P, C.c_int, PP)
+_proto("tt_qmps_data_size", P, PI64)
+_proto("tt_qmps_get_data", P, PD)
+_proto("tt_qmps_set_data", P, PD)
+_proto("tt_qdmrg_env", P, C.c_int, C.c_int, PP)
+_proto("tt_qmpo_heisenberg", C.c_int, PD, D, C.c_uint, PP)
+_proto("tt_qmpo_destroy", P)
+_proto("tt_qmpo_tensor", P, C.c_int, PP)
+_proto("tt_qdmrg_create", P, P, PP)
+_proto("tt_qdmrg_sweep", P, C.c_int, D, C.c_int, PD)
+_proto("tt_qdmrg_finish", P)
+_proto("tt_qdmrg_destroy", P)
+_proto("tt_qdmrg_run", P, P, C.c_int, C.POINTER(C.c_int), C.c_int, PD, C.c_int, C.POINTER(C.c_int),
+       C.c_int, PD, PP)
+_proto("tt_qdmrg_num_steps", P, C.POINTER(C.c_int))
+_proto("tt_qdmrg_step", P, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), PD, PD, C.POINTER(C.c_uint),
+       C.POINTER(C.c_int), PD)
+_proto("tt_qdmrg_step_sectors", P, C.c_int, C.POINTER(C.c_int), PI32, C.POINTER(C.c_uint32), C.c_int)
+_proto("tt_qdmrg_stats", P, PD, PD, PD)
+_proto("tt_qdmrg_num_sweeps", P, C.POINTER(C.c_int))
+_proto("tt_qdmrg_sweep_info", P, C.c_int, PD, PD)
+
+
+def _chk(rc, what=""):
+    if rc != TT_OK:
+        msg = lib.tt_get_last_error().decode(errors="replace")
+        raise TTError("%s failed (status %d): %s" % (what, rc, msg))
+
+
+def declared_symbols() -> List[str]:
+    """Every entry point the public headers declare."""
+    names = []
+    for h in HEADERS:
+        src = open(h).read()
+        src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+        names += re.findall(r"\b(?:int|const char\*)\s+(tt_\w+)\s*\(", src)
+    return sorted(set(names))
+
+
+class Context:
+    """One device context (stream, pool); binds itself to the calling thread."""
+
+    def __init__(self, device: int = 0):
+        self.h = P()
+        _chk(lib.tt_ctx_create(device, C.byref(self.h)), "tt_ctx_create")
+        _chk(lib.tt_dmrg_bind(self.h), "tt_dmrg_bind")
+
+    def sync(self):
+        _chk(lib.tt_ctx_synchronize(self.h), "sync")
+
+    def stream(self) -> int:
+        s = P()
+        _chk(lib.tt_ctx_stream(self.h, C.byref(s)), "stream")
+        return s.value or 0
+
+    def launches(self) -> int:
+        n = I64()
+        _chk(lib.tt_ctx_launch_count(self.h, C.byref(n)), "launch count")
+        return n.value
+
+    def close(self):
+        if self.h:
+            lib.tt_dmrg_unbind()
+            lib.tt_ctx_destroy(self.h)
+            self.h = P()
+
+
+# ---------------------------------------------------------------------------
+# qtensor handles <-> oracle-style numpy block tensors
+# ---------------------------------------------------------------------------
+class QTensor:
+    """Handle of a device qtensor (qtensor/qtensor.h:47-164)."""
+
+    def __init__(self, handle):
+        self.h = handle
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            try:
+                lib.tt_qtensor_destroy(self.h)
+            except Exception:
+                pass
+            self.h = None
+
+    @staticmethod
+    def _descs(indices):
+        keep = []
+        descs = (IndexDesc * len(indices))()
+        for i, ix in enumerate(indices):
+            qn = np.array([v for (q, _) in ix.qns for v in q], dtype=np.int32)
+            qd = np.array([d for (_, d) in ix.qns], dtype=np.int32)
+            name = ix.name.encode()
+            keep += [qn, qd, name]
+            descs[i] = IndexDesc(ix.arrow, ix.type, ix.level, len(ix.qns), name,
+                                 qn.ctypes.data_as(PI32), qd.ctypes.data_as(PI32))
+        return descs, keep
+
+    @classmethod
+    def create(cls, indices, init_blocks: bool = True) -> "QTensor":
+        descs, keep = cls._descs(indices)
+        h = P()
+        _chk(lib.tt_qtensor_create(len(indices), descs, C.byref(h)), "tt_qtensor_create")
+        t = cls(h)
+        if init_blocks:
+            _chk(lib.tt_qtensor_init_blocks(h), "init_blocks")
+        return t
+
+    @classmethod
+    def from_oracle(cls, T) -> "QTensor":
+        descs, keep = cls._descs(T.idx)
+        h = P()
+        _chk(lib.tt_qtensor_create(T.rank, descs, C.byref(h)), "tt_qtensor_create")
+        t = cls(h)
+        qi = np.array([p for q in T.bqi for p in q], dtype=np.int32)
+        _chk(lib.tt_qtensor_set_blocks(h, len(T.blocks), qi.ctypes.data_as(PI32)), "set_blocks")
+        for b, blk in enumerate(T.blocks):
+            data = np.asfortranarray(blk).ravel(order="F").astype(np.float64)
+            _chk(lib.tt_qtensor_set_block(h, b, data.ctypes.data_as(PD)), "set_block")
+        return t
+
+    @property
+    def rank(self) -> int:
+        r = C.c_int()
+        _chk(lib.tt_qtensor_rank(self.h, C.byref(r)), "rank")
+        return r.value
+
+    def index_info(self, i):
+        a, t, l, n = I32(), I32(), I32(), I32()
+        name = C.create_string_buffer(256)
+        cap = 512
+        qn = (I32 * (2 * cap))()
+        qd = (I32 * cap)()
+        _chk(lib.tt_qtensor_index(self.h, i, C.byref(a), C.byref(t), C.byref(l), C.byref(n), name, 256,
+                                  qn, qd, cap), "index")
+        sectors = [((qn[2 * s], qn[2 * s + 1]), qd[s]) for s in range(n.value)]
+        return dict(arrow=a.value, type=t.value, level=l.value, name=name.value.decode(), qns=sectors)
+
+    def num_blocks(self) -> int:
+        n = C.c_int()
+        _chk(lib.tt_qtensor_num_blocks(self.h, C.byref(n)), "num_blocks")
+        return n.value
+
+    def blocks(self):
+        """[(qn tuple, qi tuple, ndarray)] with axes in the tensor's index order."""
+        r = self.rank
+        out = []
+        for b in range(self.num_blocks()):
+            qn = (I32 * (2 * r))()
+            qi = (I32 * r)()
+            qd = (I32 * r)()
+            sz = I64()
+            _chk(lib.tt_qtensor_block_info(self.h, b, qn, qi, qd, C.byref(sz)), "block_info")
+            data = np.empty(sz.value, dtype=np.float64)
+            _chk(lib.tt_qtensor_get_block(self.h, b, data.ctypes.data_as(PD)), "get_block")
+            dims = tuple(qd[j] for j in range(r))
+            out.append((tuple((qn[2 * j], qn[2 * j + 1]) for j in range(r)),
+                        tuple(qi[j] for j in range(r)), data.reshape(dims, order="F")))
+        return out
+
+    def to_oracle(self):
+        from oracle.qtensor import QIndex, QTensor as OQ
+        idx = []
+        for i in range(self.rank):
+            inf = self.index_info(i)
+            ix = QIndex(inf["arrow"], inf["name"], inf["type"], inf["level"])
+            ix.qns = list(inf["qns"])
+            idx.append(ix)
+        T = OQ(idx)
+        T.initted = True
+        for qn, qi, data in self.blocks():
+            T._append_block(qn, qi, data.shape, data.copy())
+        return T
+
+    def copy(self) -> "QTensor":
+        h = P()
+        _chk(lib.tt_qtensor_copy(self.h, C.byref(h)), "copy")
+        return QTensor(h)
+
+    def prime(self, inc=1):
+        _chk(lib.tt_qtensor_prime(self.h, inc), "prime")
+
+    def dag(self):
+        _chk(lib.tt_qtensor_dag(self.h), "dag")
+
+    def __mul__(self, other: "QTensor") -> "QTensor":
+        h = P()
+        _chk(lib.tt_qtensor_contract(self.h, other.h, C.byref(h)), "contract")
+        return QTensor(h)
+
+    def norm(self) -> float:
+        v = D()
+        _chk(lib.tt_qtensor_norm(self.h, C.byref(v)), "norm")
+        return v.value
+
+    def scale(self, c: float):
+        _chk(lib.tt_qtensor_scale(self.h, c), "scale")
+
+    def add(self, other: "QTensor", c: float = 1.0):
+        _chk(lib.tt_qtensor_add(self.h, other.h, c), "add")
+
+    def inner_product(self, other: "QTensor") -> float:
+        v = D()
+        _chk(lib.tt_qtensor_inner_product(self.h, other.h, C.byref(v)), "inner_product")
+        return v.value
+
+
+def svd(A: QTensor, left_axes: Sequence[int], direction: int, cutoff: float = 0.0, K: int = 0):
+    """svd(A, left, right, U, V, S, direction, cutoff, K) -> (U, V, S, trunc_err, kept)."""
+    la = (C.c_int * len(left_axes))(*left_axes)
+    U, V, S = P(), P(), P()
+    te = D()
+    kept = C.c_uint()
+    _chk(lib.tt_qtensor_svd(A.h, len(left_axes), la, direction, cutoff, K, C.byref(U), C.byref(V),
+                            C.byref(S), C.byref(te), C.byref(kept)), "svd")
+    return QTensor(U), QTensor(V), QTensor(S), te.value, kept.value
+
+
+def svd_bond(combined: QTensor, A_left: QTensor, A_right: QTensor, mid_axis: int, direction: int,
+             cutoff: float = 0.0, K: int = 0):
+    S = P()
+    te = D()
+    kept = C.c_uint()
+    _chk(lib.tt_qtensor_svd_bond(combined.h, A_left.h, A_right.h, mid_axis, direction, cutoff, K, C.byref(S),
+                                 C.byref(te), C.byref(kept)), "svd_bond")
+    return QTensor(S), te.value, kept.value
+
+
+class BigQTensor:
+    """big_qtensor: L, pre-contracted W1*W2 and R (qtensor/big_qtensor.{h,cpp})."""
+
+    def __init__(self, L: QTensor, W1: QTensor, W2: Optional[QTensor], R: QTensor):
+        self.h = P()
+        _chk(lib.tt_bigq_create(L.h, W1.h, W2.h if W2 is not None else None, R.h, C.byref(self.h)), "bigq")
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib.tt_bigq_destroy(self.h)
+            self.h = None
+
+    def product(self, v: QTensor) -> QTensor:
+        h = P()
+        _chk(lib.tt_bigq_product(self.h, v.h, C.byref(h)), "product")
+        return QTensor(h)
+
+    def size(self) -> int:
+        s = C.c_uint64()
+        _chk(lib.tt_bigq_size(self.h, C.byref(s)), "size")
+        return s.value
+
+    def davidson(self, x: QTensor, max_restart: int, tol: float = 1e-12) -> Tuple[float, int]:
+        e = D()
+        mv = C.c_int()
+        _chk(lib.tt_bigq_davidson(self.h, x.h, max_restart, tol, C.byref(e), C.byref(mv)), "davidson")
+        return e.value, mv.value
+
+
+class QMPS:
+    def __init__(self, L: int, state: Sequence[int], mps_id: int = 1):
+        st = (C.c_int * L)(*state)
+        self.L = L
+        self.h = P()
+        _chk(lib.tt_qmps_product_spinhalf(L, st, mps_id, C.byref(self.h)), "qmps")
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib.tt_qmps_destroy(self.h)
+            self.h = None
+
+    def bond_dims(self) -> List[int]:
+        out = (C.c_int * (self.L + 1))()
+        _chk(lib.tt_qmps_bond_dims(self.h, out), "bond_dims")
+        return list(out)
+
+    def center(self) -> int:
+        c = C.c_int()
+        _chk(lib.tt_qmps_center(self.h, C.byref(c)), "center")
+        return c.value
+
+    def position(self, site: int):
+        _chk(lib.tt_qmps_position(self.h, site), "position")
+
+    def tensor(self, i: int) -> QTensor:
+        h = P()
+        _chk(lib.tt_qmps_tensor(self.h, i, C.byref(h)), "qmps tensor")
+        return QTensor(h)
+
+    def data_size(self) -> int:
+        n = I64()
+        _chk(lib.tt_qmps_data_size(self.h, C.byref(n)), "data_size")
+        return n.value
+
+    def get_data(self, host: np.ndarray):
+        """All block data into ``host`` (float64, data_size() elements; pin it for bandwidth)."""
+        _chk(lib.tt_qmps_get_data(self.h, host.ctypes.data_as(PD)), "get_data")
+
+    def set_data(self, host: np.ndarray):
+        _chk(lib.tt_qmps_set_data(self.h, host.ctypes.data_as(PD)), "set_data")
+
+
+class QMPO:
+    def __init__(self, L: int, dh: Optional[Sequence[float]] = None, tE: float = 0.0, mpo_id: int = 2):
+        self.L = L
+        self.h = P()
+        arr = (D * L)(*dh) if dh is not None else None
+        _chk(lib.tt_qmpo_heisenberg(L, arr, tE, mpo_id, C.byref(self.h)), "qmpo")
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib.tt_qmpo_destroy(self.h)
+            self.h = None
+
+    def tensor(self, i: int) -> QTensor:
+        h = P()
+        _chk(lib.tt_qmpo_tensor(self.h, i, C.byref(h)), "qmpo tensor")
+        return QTensor(h)
+
+
+class QDMRG:
+    """Step-wise driver of dmrg(psi, H, nsweeps, maxm[], cutoff[], max_restart[])."""
+
+    def __init__(self, psi: QMPS, H: QMPO):
+        self.psi, self.H = psi, H
+        self.h = P()
+        _chk(lib.tt_qdmrg_create(psi.h, H.h, C.byref(self.h)), "qdmrg create")
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib.tt_qdmrg_destroy(self.h)
+            self.h = None
+
+    def sweep(self, max_bd: int, cutoff: float, max_restart: int) -> float:
+        e = D()
+        _chk(lib.tt_qdmrg_sweep(self.h, max_bd, cutoff, max_restart, C.byref(e)), "sweep")
+        return e.value
+
+    def finish(self):
+        _chk(lib.tt_qdmrg_finish(self.h), "finish")
+
+    def run(self, nsweeps, maxm, cutoff, max_restart) -> float:
+        e = 0.0
+        for s in range(nsweeps):
+            e = self.sweep(maxm[s % len(maxm)], cutoff[s % len(cutoff)], max_restart[s % len(max_restart)])
+        self.finish()
+        return e
+
+    def steps(self):
+        n = C.c_int()
+        _chk(lib.tt_qdmrg_num_steps(self.h, C.byref(n)), "num_steps")
+        out = []
+        for i in range(n.value):
+            site, d, mv = C.c_int(), C.c_int(), C.c_int()
+            e, te, fl = D(), D(), D()
+            kept = C.c_uint()
+            _chk(lib.tt_qdmrg_step(self.h, i, C.byref(site), C.byref(d), C.byref(e), C.byref(te),
+                                   C.byref(kept), C.byref(mv), C.byref(fl)), "step")
+            ns = C.c_int()
+            cap = 256
+            qn = (I32 * (2 * cap))()
+            kp = (C.c_uint32 * cap)()
+            _chk(lib.tt_qdmrg_step_sectors(self.h, i, C.byref(ns), qn, kp, cap), "step sectors")
+            sec = tuple(((qn[2 * j], qn[2 * j + 1]), kp[j]) for j in range(min(ns.value, cap)))
+            out.append(dict(site=site.value, direction=d.value, energy=e.value, trunc_err=te.value,
+                            kept=kept.value, matvecs=mv.value, heff_flops=fl.value, sectors=sec))
+        return out
+
+    def env(self, which: int, i: int) -> QTensor:
+        """Copy of TL[i] (which=0) or TR[i] (which=1)."""
+        h = P()
+        _chk(lib.tt_qdmrg_env(self.h, which, i, C.byref(h)), "env")
+        return QTensor(h)
+
+    def stats(self):
+        f, s, e0 = D(), D(), D()
+        _chk(lib.tt_qdmrg_stats(self.h, C.byref(f), C.byref(s), C.byref(e0)), "stats")
+        return dict(heff_flops=f.value, heff_seconds=s.value, initial_energy=e0.value)
+
+    def sweeps(self):
+        n = C.c_int()
+        _chk(lib.tt_qdmrg_num_sweeps(self.h, C.byref(n)), "num_sweeps")
+        out = []
+        for i in range(n.value):
+            e, s = D(), D()
+            _chk(lib.tt_qdmrg_sweep_info(self.h, i, C.byref(e), C.byref(s)), "sweep info")
+            out.append((e.value, s.value))
+        return out

@@ -131,6 +131,21 @@ int tt_vec_dot(tt_ctx* ctx, int64_t n, const double* x, const double* y, double*
  * HOST array of nvec device pointers. */
 int tt_vec_multidot(tt_ctx* ctx, int64_t n, int nvec, const double* const* xs,
                     const double* y, double* d_out);
+/* Allocation-free tt_vec_multidot (no counterpart in the reference).  For
+ * callers that cannot allocate device memory -- and therefore cannot create a
+ * tt_ctx -- such as an application that reserves the whole GPU for its own
+ * memory pool, or a plugin host that only lends out buffers it owns.  The
+ * caller passes the inputs, the output (d_out, nvec doubles on the device) and
+ * a CUDA stream (cudaStream_t as void*, 0 for the legacy default stream) on
+ * the current device; nothing is allocated.  Partial sums live in a fixed
+ * 16 x 1024-double (128 KiB) array inside the library that every GPU loading
+ * it holds until the process exits, so nvec is limited to 1..16 (larger is
+ * rejected with TT_ERR_INVALID); n is not limited.  The first call on a device
+ * looks up that array's device address (cudaGetSymbolAddress) and should come
+ * before any stream capture.  All calls share the array: calls that overlap
+ * on the GPU (different streams, or host threads without ordering) race. */
+int tt_vec_multidot_noalloc(void* stream, int64_t n, int nvec, const double* const* xs,
+                            const double* y, double* d_out);
 int tt_vec_nrm2(tt_ctx* ctx, int64_t n, const double* x, double* d_out);
 int tt_vec_axpy(tt_ctx* ctx, int64_t n, double a, const double* x, double* y);
 int tt_vec_scal(tt_ctx* ctx, int64_t n, double a, double* x);

@@ -4,7 +4,9 @@
 // diagonal preconditioner.  All are HBM-bound streaming kernels: 16-byte
 // vector loads, a fixed grid (a multiple of the SM count) and a two-pass
 // deterministic reduction (same summation order on every run).
+#include <algorithm>
 #include <cmath>
+#include <mutex>
 #include <vector>
 
 #include "tt_internal.h"
@@ -182,9 +184,72 @@ int launch_multidot(tt_ctx* ctx, int64_t n, int nv, const double* const* xs, con
   return TT_OK;
 }
 
+// ---- allocation-free multi-dot (tt_vec_multidot_noalloc) --------------------
+// Some callers cannot allocate device memory: an application that reserves the
+// whole device for its own pool and forbids further allocations, or a plugin
+// host that only lends out buffers it owns.  Such a caller cannot create a
+// tt_ctx (that allocates its stream, pool and scratch), so this variant keeps
+// the reduction partials in a fixed array inside the library instead.
+constexpr int NOALLOC_MAX_VEC = MAXVEC;      // at most 16 vectors per call
+constexpr int NOALLOC_MAX_BLOCKS = 1024;     // partial sums per vector
+// 16 x 1024 doubles = 128 KiB; every GPU that loads the library holds it until exit.
+static __device__ __align__(256) double g_noalloc_partials[NOALLOC_MAX_VEC * NOALLOC_MAX_BLOCKS];
+
+struct NoAllocDevice {
+  std::once_flag once;
+  double* partials = nullptr;   // device address of g_noalloc_partials on this device
+  int num_sms = 0;
+  cudaError_t status = cudaSuccess;
+};
+constexpr int NOALLOC_MAX_DEVICES = 64;
+NoAllocDevice g_noalloc_dev[NOALLOC_MAX_DEVICES];
+
 }  // namespace
 
 extern "C" {
+
+int tt_vec_multidot_noalloc(void* stream, int64_t n, int nvec, const double* const* xs, const double* y,
+                            double* d_out) {
+  TT_REQUIRE(xs && y && d_out, "tt_vec_multidot_noalloc: null argument");
+  TT_REQUIRE(n >= 0, "tt_vec_multidot_noalloc: negative length");
+  if (nvec < 1 || nvec > NOALLOC_MAX_VEC)
+    return tt::fail(TT_ERR_INVALID, "tt_vec_multidot_noalloc: nvec must be 1..16 (fixed scratch of 16 x 1024 "
+                                    "partial sums)");
+  TT_REQUIRE(aligned16(y), "tt_vec_multidot_noalloc: vectors must be 16-byte aligned");
+  int dev = 0;
+  TT_CUDA(cudaGetDevice(&dev));
+  TT_REQUIRE(dev >= 0 && dev < NOALLOC_MAX_DEVICES, "tt_vec_multidot_noalloc: device ordinal too large");
+  NoAllocDevice& D = g_noalloc_dev[dev];
+  // once per device, with that device current: the host needs the array's
+  // device address (its host-side name is only a stand-in)
+  std::call_once(D.once, [&D, dev]() {
+    void* p = nullptr;
+    D.status = cudaGetSymbolAddress(&p, g_noalloc_partials);
+    if (D.status == cudaSuccess) D.status = cudaDeviceGetAttribute(&D.num_sms, cudaDevAttrMultiProcessorCount, dev);
+    if (D.status == cudaSuccess) D.partials = static_cast<double*>(p);
+  });
+  if (D.status != cudaSuccess) return tt::cuda_fail(D.status, "tt_vec_multidot_noalloc set-up", __FILE__, __LINE__);
+  PtrPack pk;
+  for (int j = 0; j < nvec; ++j) {
+    TT_REQUIRE(xs[j] && aligned16(xs[j]), "tt_vec_multidot_noalloc: vectors must be 16-byte aligned");
+    pk.p[j] = xs[j];
+  }
+  int64_t want = (n + RT * 4 - 1) / (RT * 4);
+  int64_t cap = std::min<int64_t>(4 * (int64_t)D.num_sms, NOALLOC_MAX_BLOCKS);
+  int nb = (int)std::max<int64_t>(1, std::min(want, cap));
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  // every partial that pass 2 reads is written by pass 1 first: nothing needs zeroing
+  if (nvec <= 1)
+    multidot_pass1<1><<<nb, RT, 0, s>>>(n, pk, y, D.partials, nvec);
+  else if (nvec <= 4)
+    multidot_pass1<4><<<nb, RT, 0, s>>>(n, pk, y, D.partials, nvec);
+  else
+    multidot_pass1<MAXVEC><<<nb, RT, 0, s>>>(n, pk, y, D.partials, nvec);
+  TT_CUDA(cudaGetLastError());
+  reduce_pass2<<<1, 32 * nvec, 0, s>>>(D.partials, nb, nvec, d_out, 0);
+  TT_CUDA(cudaGetLastError());
+  return TT_OK;
+}
 
 int tt_vec_multidot(tt_ctx* ctx, int64_t n, int nvec, const double* const* xs, const double* y,
                     double* d_out) {

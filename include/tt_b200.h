@@ -197,6 +197,21 @@ typedef struct {
 int tt_sym_eig_batched(tt_ctx* ctx, const tt_eig_problem* probs, int n_probs,
                        double* G, double* Z, double* w, const double* A);
 
+/* Two-phase eigensolver used by the block SVD (n <= 2048 per problem).
+ * Phase 1: Householder tridiagonalisation of each G_p in place (reflectors
+ * below the subdiagonal), d/e/tau of T_p in T[3*w_off .. 3*w_off + 3n), and
+ * every eigenvalue in DESCENDING order in w[w_off ..] (bisection).  Phase 2:
+ * the eigenvectors of the nvec[p] largest eigenvalues as the first nvec[p]
+ * columns of Z + g_off (leading dimension n), by inverse iteration on T_p,
+ * Gram-Schmidt inside clusters of close eigenvalues, and back-transformation
+ * with the reflectors left in G; work holds 3*n*n doubles per problem at
+ * 3*g_off.  TT_EIG_ROW_1X2 problems follow the 1x2 rule described above. */
+int tt_sym_eigvals_batched(tt_ctx* ctx, const tt_eig_problem* probs, int n_probs, double* G,
+                           double* T, double* w, const double* A);
+int tt_sym_eigvecs_batched(tt_ctx* ctx, const tt_eig_problem* probs, int n_probs, const int* nvec,
+                           const double* G, const double* T, const double* w, double* Z,
+                           double* work, const double* A);
+
 #ifdef __cplusplus
 }
 #endif

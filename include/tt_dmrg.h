@@ -146,6 +146,10 @@ int tt_qdmrg_num_steps(const tt_qdmrg* run, int* n);
 int tt_qdmrg_step(const tt_qdmrg* run, int i, int* site, int* direction, double* energy, double* trunc_err,
                   unsigned* kept, int* matvecs, double* heff_flops);
 int tt_qdmrg_step_sectors(const tt_qdmrg* run, int i, int* n, int32_t* qn, uint32_t* kept, int cap);
+/* per-step profile: largest sector density matrix of the SVD and host wall
+ * seconds of the Davidson, SVD and environment-update phases */
+int tt_qdmrg_step_profile(const tt_qdmrg* run, int i, int* gram_max, double* t_davidson, double* t_svd,
+                          double* t_env);
 int tt_qdmrg_stats(const tt_qdmrg* run, double* heff_flops, double* heff_seconds, double* initial_energy);
 /* copy of the left (which = 0, TL[i]) or right (which = 1, TR[i]) environment */
 int tt_qdmrg_env(const tt_qdmrg* run, int which, int i, tt_qtensor** out);

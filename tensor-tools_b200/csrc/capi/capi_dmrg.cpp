@@ -492,6 +492,18 @@ int tt_qdmrg_step_sectors(const tt_qdmrg* run, int i, int* n, int32_t* qn, uint3
   });
 }
 
+int tt_qdmrg_step_profile(const tt_qdmrg* run, int i, int* gram_max, double* t_davidson, double* t_svd,
+                          double* t_env) {
+  TT_ARG(run && i >= 0 && i < (int)run->log.steps.size());
+  TT_GUARD({
+    const ttb::StepLog& s = run->log.steps[i];
+    if (gram_max) *gram_max = s.gram_max;
+    if (t_davidson) *t_davidson = s.t_davidson;
+    if (t_svd) *t_svd = s.t_svd;
+    if (t_env) *t_env = s.t_env;
+  });
+}
+
 int tt_qdmrg_stats(const tt_qdmrg* run, double* heff_flops, double* heff_seconds, double* initial_energy) {
   TT_ARG(run);
   TT_GUARD({

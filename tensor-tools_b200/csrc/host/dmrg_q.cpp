@@ -701,6 +701,7 @@ void updateSite(qMPS& psi, qMPO& H, std::vector<qtensor>& TR, std::vector<qtenso
   // algos/dmrg/dmrg.cpp:300-372
   unsigned l, r;
   if (direction == MoveFromLeft) { l = site; r = site + 1; } else { l = site - 1; r = site; }
+  auto t0 = std::chrono::steady_clock::now();
   big_qtensor A;
   A.setLeft(&TL[l]);
   A.addMid(&H.A[l]);
@@ -709,6 +710,8 @@ void updateSite(qMPS& psi, qMPO& H, std::vector<qtensor>& TR, std::vector<qtenso
   qtensor x = psi.A[l] * psi.A[r];
   DavidsonStats st;
   energy = tensor_davidsonIT(A, x, search_space_size, max_restart, 1e-12, mode, &st);
+  check(tt_ctx_synchronize(ctx()), "sync");
+  auto t1 = std::chrono::steady_clock::now();
   std::string ln = psi.link_name(r);
   qtensor_index mid;
   for (auto& ix : psi.A[l].idx_set)
@@ -716,6 +719,7 @@ void updateSite(qMPS& psi, qMPO& H, std::vector<qtensor>& TR, std::vector<qtenso
   qtensor S;
   TruncInfo info;
   svd_bond(x, psi.A[l], psi.A[r], mid, S, direction, cutoff, (unsigned long)max_bd, &info);
+  auto t2 = std::chrono::steady_clock::now();
   psi.bond_dims[r] = (unsigned)S.total_size();
   psi.center = (int)(direction == MoveFromLeft ? r : l);
   if (log) {
@@ -730,6 +734,9 @@ void updateSite(qMPS& psi, qMPO& H, std::vector<qtensor>& TR, std::vector<qtenso
     s.heff_flops = st.heff_flops;
     s.sector_qn = info.sector_qn;
     s.kept_per_sector = info.kept_per_sector;
+    s.gram_max = info.gram_max;
+    s.t_davidson = std::chrono::duration<double>(t1 - t0).count();
+    s.t_svd = std::chrono::duration<double>(t2 - t1).count();
     log->steps.push_back(std::move(s));
     log->heff_flops += st.heff_flops;
     log->heff_seconds += rt().last_heff_ms * 1e-3;
@@ -774,7 +781,13 @@ double dmrg_sweep(qMPS& psi, qMPO& H, DmrgState& st, int max_bd, double cutoff, 
     for (unsigned i = 0; i < L - 1; ++i) {
       unsigned site = direction == MoveFromLeft ? i : L - 1 - i;
       updateSite(psi, H, st.TR, st.TL, site, energy, direction, max_bd, cutoff, 'S', 3, max_restart, log);
+      auto te0 = std::chrono::steady_clock::now();
       updateEnv(psi, H, st.TR, st.TL, site, direction);
+      if (log && !log->steps.empty()) {
+        check(tt_ctx_synchronize(ctx()), "sync");
+        log->steps.back().t_env =
+            std::chrono::duration<double>(std::chrono::steady_clock::now() - te0).count();
+      }
     }
   }
   psi.normalize();

@@ -94,6 +94,10 @@ struct StepLog {
   double heff_flops = 0.0;
   std::vector<QN> sector_qn;
   std::vector<unsigned> kept_per_sector;
+  int gram_max = 0;          // largest per-sector density matrix of the SVD
+  double t_davidson = 0.0;   // host wall seconds of the phases of this step
+  double t_svd = 0.0;
+  double t_env = 0.0;
 };
 struct DmrgLog {
   std::vector<StepLog> steps;

@@ -257,9 +257,12 @@ void svd(const qtensor& A, const std::vector<qtensor_index>& left,
     PlanHandle ph(plan);
     check(tt_contract_exec(ctx(), plan, A.data->get(), A.data->get(), G->get(), 1.0), "svd gram");
   }
-  check(tt_sym_eig_batched(ctx(), probs.data(), (int)probs.size(), G->get(), Z->get(), W->get(),
-                           packed ? packed->get() : nullptr),
-        "svd eig");
+  // phase 1: tridiagonal form and every eigenvalue; vectors only once the
+  // truncation below has fixed how many states each sector keeps
+  DevPtr Tt = dev_alloc(std::max<int64_t>(3 * wtot, 1));
+  check(tt_sym_eigvals_batched(ctx(), probs.data(), (int)probs.size(), G->get(), Tt->get(), W->get(),
+                               packed ? packed->get() : nullptr),
+        "svd eigenvalues");
   std::vector<double> w((size_t)std::max<int64_t>(wtot, 1));
   check(tt_memcpy_d2h(ctx(), w.data(), W->get(), sizeof(double) * (size_t)wtot), "svd eigenvalues");
 
@@ -295,6 +298,8 @@ void svd(const qtensor& A, const std::vector<qtensor_index>& left,
     if ((1 - cumsum < cutoff && cutoff != 0.0) || (acc >= K && K != 0)) break;
   }
   if (info) {
+    info->gram_max = 0;
+    for (auto& s : sec) info->gram_max = std::max<int>(info->gram_max, (int)s.g);
     info->trunc_err = std::max(1 - cumsum, 0.0);
     info->kept = (unsigned)acc;
     info->sector_qn.clear();
@@ -303,6 +308,16 @@ void svd(const qtensor& A, const std::vector<qtensor_index>& left,
       info->sector_qn.push_back(sec[ii].q);
       info->kept_per_sector.push_back(new_dim[ii]);
     }
+  }
+
+  // phase 2: eigenvectors of the kept states only
+  {
+    std::vector<int> nvec(sec.size());
+    for (unsigned ii = 0; ii < sec.size(); ++ii) nvec[ii] = (int)new_dim[ii];
+    DevPtr work = dev_alloc(std::max<int64_t>(3 * gtot, 1));
+    check(tt_sym_eigvecs_batched(ctx(), probs.data(), (int)probs.size(), nvec.data(), G->get(), Tt->get(),
+                                 W->get(), Z->get(), work->get(), packed ? packed->get() : nullptr),
+          "svd eigenvectors");
   }
 
   // ---- U, V, S structure (:1302-1438) ----------------------------------

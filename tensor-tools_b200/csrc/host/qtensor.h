@@ -230,6 +230,7 @@ std::shared_ptr<PlanHandle> make_plan(const ContractStructure& cs);
 struct TruncInfo {
   double trunc_err = 0.0;
   unsigned kept = 0;
+  int gram_max = 0;
   std::vector<QN> sector_qn;
   std::vector<unsigned> kept_per_sector;
 };

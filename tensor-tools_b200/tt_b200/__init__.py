@@ -138,6 +138,8 @@ _proto("tt_qdmrg_step", P, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), PD, 
        C.POINTER(C.c_int), PD)
 _proto("tt_qdmrg_step_sectors", P, C.c_int, C.POINTER(C.c_int), PI32, C.POINTER(C.c_uint32), C.c_int)
 _proto("tt_qdmrg_stats", P, PD, PD, PD)
+_proto("tt_qdmrg_step_profile", P, C.c_int, C.POINTER(C.c_int), PD, PD, PD)
+_proto("tt_sym_eig_batched", P, C.c_void_p, C.c_int, P, P, P, P)
 _proto("tt_qdmrg_num_sweeps", P, C.POINTER(C.c_int))
 _proto("tt_qdmrg_sweep_info", P, C.c_int, PD, PD)
 
@@ -482,6 +484,18 @@ class QDMRG:
             sec = tuple(((qn[2 * j], qn[2 * j + 1]), kp[j]) for j in range(min(ns.value, cap)))
             out.append(dict(site=site.value, direction=d.value, energy=e.value, trunc_err=te.value,
                             kept=kept.value, matvecs=mv.value, heff_flops=fl.value, sectors=sec))
+        return out
+
+    def profile(self):
+        """Per step: (largest SVD sector, Davidson s, SVD s, env-update s)."""
+        n = C.c_int()
+        _chk(lib.tt_qdmrg_num_steps(self.h, C.byref(n)), "num_steps")
+        out = []
+        for i in range(n.value):
+            g = C.c_int()
+            a, b, c = D(), D(), D()
+            _chk(lib.tt_qdmrg_step_profile(self.h, i, C.byref(g), C.byref(a), C.byref(b), C.byref(c)), "profile")
+            out.append((g.value, a.value, b.value, c.value))
         return out
 
     def env(self, which: int, i: int) -> QTensor:

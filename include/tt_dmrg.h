@@ -64,6 +64,12 @@ typedef struct {
 
 int tt_dmrg_bind(tt_ctx* ctx);
 int tt_dmrg_unbind(void);
+/* on != 0: synchronise between the phases of each two-site step so that
+ * tt_qdmrg_step_profile reports per-phase times (slower; off by default) */
+int tt_dmrg_set_profiling(int on);
+/* host-side planning counters of this thread: seconds and calls spent in
+ * block-structure computation and in contraction-plan creation */
+int tt_dmrg_planning_counters(double* t_structure, int64_t* n_structure, double* t_plan, int64_t* n_plan);
 
 /* ---- qtensor ------------------------------------------------------------- */
 int tt_qtensor_create(int rank, const tt_index_desc* idx, tt_qtensor** out);
@@ -149,7 +155,7 @@ int tt_qdmrg_step_sectors(const tt_qdmrg* run, int i, int* n, int32_t* qn, uint3
 /* per-step profile: largest sector density matrix of the SVD and host wall
  * seconds of the Davidson, SVD and environment-update phases */
 int tt_qdmrg_step_profile(const tt_qdmrg* run, int i, int* gram_max, double* t_davidson, double* t_svd,
-                          double* t_env);
+                          double* t_env, double* t_engine);
 int tt_qdmrg_stats(const tt_qdmrg* run, double* heff_flops, double* heff_seconds, double* initial_energy);
 /* copy of the left (which = 0, TL[i]) or right (which = 1, TR[i]) environment */
 int tt_qdmrg_env(const tt_qdmrg* run, int which, int i, tt_qtensor** out);

@@ -79,6 +79,17 @@ int tt_dmrg_bind(tt_ctx* ctx) {
 
 int tt_dmrg_unbind(void) { TT_GUARD(ttb::unbind_context()); }
 
+int tt_dmrg_set_profiling(int on) { TT_GUARD(ttb::rt().profile = on != 0); }
+
+int tt_dmrg_planning_counters(double* t_structure, int64_t* n_structure, double* t_plan, int64_t* n_plan) {
+  TT_GUARD({
+    if (t_structure) *t_structure = ttb::rt().t_structure;
+    if (n_structure) *n_structure = ttb::rt().n_structure;
+    if (t_plan) *t_plan = ttb::rt().t_plan;
+    if (n_plan) *n_plan = ttb::rt().n_plan;
+  });
+}
+
 // ---- qtensor -------------------------------------------------------------
 int tt_qtensor_create(int rank, const tt_index_desc* idx, tt_qtensor** out) {
   TT_ARG(out && rank >= 0 && (rank == 0 || idx));
@@ -493,7 +504,7 @@ int tt_qdmrg_step_sectors(const tt_qdmrg* run, int i, int* n, int32_t* qn, uint3
 }
 
 int tt_qdmrg_step_profile(const tt_qdmrg* run, int i, int* gram_max, double* t_davidson, double* t_svd,
-                          double* t_env) {
+                          double* t_env, double* t_engine) {
   TT_ARG(run && i >= 0 && i < (int)run->log.steps.size());
   TT_GUARD({
     const ttb::StepLog& s = run->log.steps[i];
@@ -501,6 +512,7 @@ int tt_qdmrg_step_profile(const tt_qdmrg* run, int i, int* gram_max, double* t_d
     if (t_davidson) *t_davidson = s.t_davidson;
     if (t_svd) *t_svd = s.t_svd;
     if (t_env) *t_env = s.t_env;
+    if (t_engine) *t_engine = s.t_engine;
   });
 }
 

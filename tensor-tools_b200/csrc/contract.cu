@@ -337,18 +337,16 @@ int tt_contract_plan(tt_ctx* ctx, const tt_out_block* outs, int n_out,
     return tt::fail(TT_ERR_OOM, "tt_contract_plan: device allocation failed");
   }
   cudaStream_t s = ctx->stream;
-  TT_CUDA(cudaMemcpyAsync(plan->d_tasks, tsorted.data(), sizeof(TaskDev) * tsorted.size(),
-                          cudaMemcpyHostToDevice, s));
-  TT_CUDA(cudaMemcpyAsync(plan->d_outs, ho.data(), sizeof(OutDev) * ho.size(), cudaMemcpyHostToDevice, s));
-  TT_CUDA(cudaMemcpyAsync(plan->d_pairs, hp.data(), sizeof(PairDev) * hp.size(), cudaMemcpyHostToDevice, s));
-  TT_CUDA(cudaMemcpyAsync(d_jobs, jobs.data(), sizeof(TableJob) * jobs.size(), cudaMemcpyHostToDevice, s));
+  // staged copies: the host vectors may die at return without stalling the stream
+  TT_CUDA(tt::h2d_async(ctx, plan->d_tasks, tsorted.data(), sizeof(TaskDev) * tsorted.size()));
+  TT_CUDA(tt::h2d_async(ctx, plan->d_outs, ho.data(), sizeof(OutDev) * ho.size()));
+  TT_CUDA(tt::h2d_async(ctx, plan->d_pairs, hp.data(), sizeof(PairDev) * hp.size()));
+  TT_CUDA(tt::h2d_async(ctx, d_jobs, jobs.data(), sizeof(TableJob) * jobs.size()));
   if (!jobs.empty()) {
     expand_tables<<<(unsigned)jobs.size(), 128, 0, s>>>(d_jobs, (int)jobs.size(), plan->d_tab);
     TT_LAUNCH_CHECK(ctx);
   }
-  // host staging vectors die at return: make the copies complete first
-  TT_CUDA(cudaStreamSynchronize(s));
-  tt::pool_free(ctx, d_jobs);
+  tt::pool_free(ctx, d_jobs);  // stream-ordered: freed after expand_tables ran
   *plan_out = plan;
   return TT_OK;
 }

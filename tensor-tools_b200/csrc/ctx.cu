@@ -36,6 +36,22 @@ double* partials(tt_ctx* ctx, int n) {
   return ctx->d_partials;
 }
 
+cudaError_t h2d_async(tt_ctx* ctx, void* dst, const void* src, size_t bytes) {
+  if (bytes == 0) return cudaSuccess;
+  const size_t need = (bytes + 255) & ~(size_t)255;
+  if (!ctx->stage || need > ctx->stage_cap)
+    return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, ctx->stream);
+  if (ctx->stage_head + need > ctx->stage_cap) {
+    cudaError_t e = cudaStreamSynchronize(ctx->stream);  // every staged copy has landed
+    if (e != cudaSuccess) return e;
+    ctx->stage_head = 0;
+  }
+  char* p = ctx->stage + ctx->stage_head;
+  std::memcpy(p, src, bytes);
+  ctx->stage_head += need;
+  return cudaMemcpyAsync(dst, p, bytes, cudaMemcpyHostToDevice, ctx->stream);
+}
+
 }  // namespace tt
 
 extern "C" {
@@ -62,6 +78,8 @@ int tt_ctx_create(int device, tt_ctx** out) {
   uint64_t thresh = UINT64_MAX;  // keep freed blocks cached in the pool
   TT_CUDA(cudaMemPoolSetAttribute(ctx->pool, cudaMemPoolAttrReleaseThreshold, &thresh));
   TT_CUDA(cudaMallocHost(&ctx->h_scalars, 4096 * sizeof(double)));
+  ctx->stage_cap = (size_t)64 << 20;
+  TT_CUDA(cudaMallocHost(&ctx->stage, ctx->stage_cap));
   if (!tt::partials(ctx, 16 * 4 * ctx->num_sms + 64)) {
     delete ctx;
     return tt::fail(TT_ERR_OOM, "tt_ctx_create: scratch allocation failed");
@@ -76,6 +94,7 @@ int tt_ctx_destroy(tt_ctx* ctx) {
   cudaStreamSynchronize(ctx->stream);
   if (ctx->d_partials) cudaFree(ctx->d_partials);
   if (ctx->h_scalars) cudaFreeHost(ctx->h_scalars);
+  if (ctx->stage) cudaFreeHost(ctx->stage);
   cudaStreamDestroy(ctx->stream);
   delete ctx;
   return TT_OK;
@@ -142,7 +161,13 @@ int tt_device_free(tt_ctx* ctx, void* dptr) {
 int tt_memcpy_h2d(tt_ctx* ctx, void* dst, const void* src, size_t bytes) {
   TT_REQUIRE(ctx, "null context");
   if (bytes == 0) return TT_OK;
-  TT_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, ctx->stream));
+  if (bytes < ((size_t)1 << 20)) {
+    TT_CUDA(tt::h2d_async(ctx, dst, src, bytes));  // staged: the source may be reused at once
+  } else {
+    // bulk data straight from the caller's buffer (pin it for full bandwidth;
+    // a pinned source must stay untouched until the stream is synchronised)
+    TT_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, ctx->stream));
+  }
   return TT_OK;
 }
 

@@ -279,14 +279,12 @@ int tt_strided_copy_batched(tt_ctx* ctx, const tt_copy_desc* descs, int n, const
   TT_REQUIRE(n <= 65535, "tt_strided_copy_batched: too many descriptors");
   tt_copy_desc* dd = tt::pool_alloc<tt_copy_desc>(ctx, n);
   if (!dd) return tt::fail(TT_ERR_OOM, "tt_strided_copy_batched: allocation failed");
-  TT_CUDA(cudaMemcpyAsync(dd, descs, sizeof(tt_copy_desc) * n, cudaMemcpyHostToDevice, ctx->stream));
+  TT_CUDA(tt::h2d_async(ctx, dd, descs, sizeof(tt_copy_desc) * n));  // staged: descs may be reused
   int gx = (int)((maxe + 255) / 256);
   if (gx > 64) gx = 64;
   dim3 grid(gx, n);
   strided_copy<<<grid, 256, 0, ctx->stream>>>(dd, src, dst);
   TT_LAUNCH_CHECK(ctx);
-  // descs is host memory owned by the caller: complete the copy before returning
-  TT_CUDA(cudaStreamSynchronize(ctx->stream));
   tt::pool_free(ctx, dd);
   return TT_OK;
 }

@@ -118,11 +118,12 @@ using Presence = std::vector<uint8_t>;
 class ProductEngine {
  public:
   ProductEngine(big_qtensor& A, const qtensor& x) : A_(A), x_(x) {
-    // layout: x's blocks (x's order), then blocks the product adds, until closed
+    if (!A_.left() || !A_.right()) throw std::runtime_error("tensor_davidsonIT: L and R must be set");
+    // the block set: x's blocks, then the blocks the product adds, until closed
     for (unsigned b = 0; b < x.blocks.size(); ++b) add_block(x.blocks[b]);
+    qtensor out;
     for (int it = 0; it < 8; ++it) {
-      Presence all(ublocks.size(), 1);
-      qtensor out = structure(all);
+      out = structure(Presence(ublocks.size(), 1));
       bool grew = false;
       for (unsigned b = 0; b < out.blocks.size(); ++b)
         if (uid.find(out.key_of(b)) == uid.end()) {
@@ -131,7 +132,20 @@ class ProductEngine {
         }
       if (!grew) break;
     }
-    build_plans();
+    // final layout: the product's own output blocks at their output offsets
+    // (so the cached *R plan writes straight into the Krylov vectors), then
+    // any block of the set the product does not produce
+    std::vector<BlockMeta> set = std::move(ublocks);
+    ublocks.clear();
+    uid.clear();
+    n = 0;
+    for (unsigned b = 0; b < out.blocks.size(); ++b) add_block(out.blocks[b]);
+    for (auto& b : set) {
+      QNKey k(b.qn.size());
+      for (size_t j = 0; j < b.qn.size(); ++j) k[j] = b.qn[j].pack();
+      if (uid.find(k) == uid.end()) add_block(b);
+    }
+    build_plans(out.arena);
   }
 
   int64_t n = 0;
@@ -141,7 +155,7 @@ class ProductEngine {
 
   Presence x_presence() const {
     Presence p(ublocks.size(), 0);
-    for (unsigned b = 0; b < x_.blocks.size(); ++b) p[b] = 1;
+    for (unsigned b = 0; b < x_.blocks.size(); ++b) p[uid.at(x_.key_of(b))] = 1;
     return p;
   }
 
@@ -171,9 +185,11 @@ class ProductEngine {
 
   // y = H_eff * v on the whole layout (absent blocks of v are zero)
   void apply(const double* v, double* y) {
-    check(tt_contract_exec(ctx(), p1_->get(), L_data(), v, i1_->get(), 1.0), "heff L*v");
-    check(tt_contract_exec(ctx(), p2_->get(), i1_->get(), A_.mid().data->get(), i2_->get(), 1.0), "heff *mid");
-    check(tt_contract_exec(ctx(), p3_->get(), i2_->get(), A_.right()->data->get(), y, 1.0), "heff *R");
+    if (c1_->plan) check(tt_contract_exec(ctx(), c1_->plan->get(), L_data(), v, i1_->get(), 1.0), "heff L*v");
+    if (c2_->plan)
+      check(tt_contract_exec(ctx(), c2_->plan->get(), i1_->get(), A_.mid().data->get(), i2_->get(), 1.0), "heff *mid");
+    if (c3_->plan)
+      check(tt_contract_exec(ctx(), c3_->plan->get(), i2_->get(), A_.right()->data->get(), y, 1.0), "heff *R");
     for (auto& r : zero_ranges_)
       check(tt_memset_zero(ctx(), y + r.first, sizeof(double) * (size_t)r.second), "heff zero");
   }
@@ -206,7 +222,7 @@ class ProductEngine {
  private:
   big_qtensor& A_;
   const qtensor& x_;
-  std::shared_ptr<PlanHandle> p1_, p2_, p3_;
+  std::shared_ptr<const CachedContraction> c1_, c2_, c3_;
   DevPtr i1_, i2_;
   std::vector<std::pair<int64_t, int64_t>> zero_ranges_;
   std::map<Presence, Presence> pcache_;
@@ -235,43 +251,39 @@ class ProductEngine {
     return t;
   }
 
+  // product(v) structure for the block set `p` (metadata only; cached)
   qtensor structure(const Presence& p) const {
-    if (!A_.left() || !A_.right()) throw std::runtime_error("tensor_davidsonIT: L and R must be set");
     qtensor v = meta(p);
-    ContractStructure c1, c2, c3;
-    contract_structure(*A_.left(), v, c1);
-    contract_structure(c1.C, A_.mid(), c2);
-    contract_structure(c2.C, *A_.right(), c3);
-    c3.C.prime(-1);
-    return std::move(c3.C);
+    auto c1 = contract_cached(*A_.left(), v, false);
+    auto c2 = contract_cached(c1->cs.C, A_.mid(), false);
+    auto c3 = contract_cached(c2->cs.C, *A_.right(), false);
+    qtensor out = c3->cs.C;
+    out.prime(-1);
+    return out;
   }
 
-  void build_plans() {
-    Presence all(ublocks.size(), 1);
-    qtensor v = meta(all);
-    ContractStructure c1, c2, c3;
-    contract_structure(*A_.left(), v, c1);
-    contract_structure(c1.C, A_.mid(), c2);
-    contract_structure(c2.C, *A_.right(), c3);
-    c3.C.prime(-1);
+  void build_plans(int64_t produced_size) {
+    qtensor v = meta(Presence(ublocks.size(), 1));
+    c1_ = contract_cached(*A_.left(), v, true);
+    c2_ = contract_cached(c1_->cs.C, A_.mid(), true);
+    c3_ = contract_cached(c2_->cs.C, *A_.right(), true);
+    const qtensor& o = c3_->cs.C;
     for (unsigned i = 0; i < x_.rank; ++i)
-      if (!c3.C.idx_set.at(i).same_tag(x_.idx_set[i]))
+      if (o.idx_set.size() != x_.rank || o.idx_set[i].level() != x_.idx_set[i].level() + 1 ||
+          o.idx_set[i].name() != x_.idx_set[i].name() || o.idx_set[i].arrow() != x_.idx_set[i].arrow() ||
+          o.idx_set[i].sectors() != x_.idx_set[i].sectors())
         throw std::runtime_error("product: H_eff*x index order differs from x");
-    std::vector<uint8_t> produced(ublocks.size(), 0);
-    for (unsigned b = 0; b < c3.C.blocks.size(); ++b) {
-      unsigned u = uid.at(c3.C.key_of(b));
-      c3.outs[b].c_off = ublocks[u].off;  // write straight into the Krylov layout
-      produced[u] = 1;
-    }
-    for (unsigned u = 0; u < ublocks.size(); ++u)
-      if (!produced[u]) zero_ranges_.push_back({ublocks[u].off, ublocks[u].size});
-    c3.C.arena = n;  // outputs now address the Krylov layout
-    flops = c1.flops + c2.flops + c3.flops;
-    p1_ = make_plan(c1);
-    p2_ = make_plan(c2);
-    p3_ = make_plan(c3);
-    i1_ = dev_alloc(std::max<int64_t>(c1.C.arena, 2));
-    i2_ = dev_alloc(std::max<int64_t>(c2.C.arena, 2));
+    // the product output must sit exactly at the start of the layout
+    if (o.arena != produced_size || o.blocks.size() > ublocks.size())
+      throw std::runtime_error("product: output layout mismatch");
+    for (unsigned b = 0; b < o.blocks.size(); ++b)
+      if (o.blocks[b].off != ublocks[b].off || o.blocks[b].qn != ublocks[b].qn)
+        throw std::runtime_error("product: output layout mismatch");
+    for (unsigned u = (unsigned)o.blocks.size(); u < ublocks.size(); ++u)
+      zero_ranges_.push_back({ublocks[u].off, ublocks[u].size});
+    flops = c1_->cs.flops + c2_->cs.flops + c3_->cs.flops;
+    i1_ = dev_alloc(std::max<int64_t>(c1_->cs.C.arena, 2));
+    i2_ = dev_alloc(std::max<int64_t>(c2_->cs.C.arena, 2));
   }
 };
 
@@ -300,7 +312,11 @@ double tensor_davidsonIT(big_qtensor& A, qtensor& x, int m, int max_restart, dou
   int actual_maxiter = std::min(max_restart, maxsize - 1);
   if (actual_maxiter + 2 > 16)
     throw std::runtime_error("tensor_davidsonIT: at most 14 iterations (16 Krylov vectors) are supported");
+  auto tb0 = std::chrono::steady_clock::now();
   ProductEngine eng(A, x);
+  if (rt().profile) check(tt_ctx_synchronize(ctx()), "sync");
+  auto tb1 = std::chrono::steady_clock::now();
+  if (stats) stats->t_engine = std::chrono::duration<double>(tb1 - tb0).count();
   const int64_t n = eng.n;
   const int nsz = actual_maxiter + 2;
   std::vector<KVec> v(nsz), va(nsz);
@@ -309,25 +325,27 @@ double tensor_davidsonIT(big_qtensor& A, qtensor& x, int m, int max_restart, dou
     k.d = dev_alloc(n);
     return k;
   };
-  void* ev0 = nullptr;
-  void* ev1 = nullptr;
-  check(tt_event_create(ctx(), &ev0), "event");
-  check(tt_event_create(ctx(), &ev1), "event");
-  double heff_ms = 0.0;
+  // events bracket every product; their times are read once, at the end
+  std::vector<std::pair<void*, void*>> evs;
+  std::vector<bool> ev_kept;
   auto product = [&](const KVec& in) {
     KVec out = newvec();
-    check(tt_event_record(ctx(), ev0), "event");
+    std::pair<void*, void*> e{nullptr, nullptr};
+    check(tt_event_create(ctx(), &e.first), "event");
+    check(tt_event_create(ctx(), &e.second), "event");
+    check(tt_event_record(ctx(), e.first), "event");
     eng.apply(in.d->get(), out.d->get());
-    check(tt_event_record(ctx(), ev1), "event");
-    float ms = 0.f;
-    check(tt_event_elapsed_ms(ev0, ev1, &ms), "event");
-    heff_ms += ms;
+    check(tt_event_record(ctx(), e.second), "event");
+    evs.push_back(e);
+    ev_kept.push_back(true);
     out.p = eng.product_presence(in.p);
+    return out;
+  };
+  auto count_product = [&]() {
     if (stats) {
       stats->matvecs++;
       stats->heff_flops += eng.flops;
     }
-    return out;
   };
   auto nrm = [&](const KVec& a) {
     check(tt_vec_nrm2(ctx(), n, a.d->get(), scalar_slot(0)), "norm");
@@ -360,6 +378,7 @@ double tensor_davidsonIT(big_qtensor& A, qtensor& x, int m, int max_restart, dou
   eng.pack(x, v[0].d->get());
   v[0].p = eng.x_presence();
   va[0] = product(v[0]);
+  count_product();
   double initEn = multidot({v[0].d->get()}, va[0].d->get())[0];
   double lambda = 0.0;
   KVec xv;  // the Ritz vector once an iteration has produced one
@@ -415,21 +434,40 @@ double tensor_davidsonIT(big_qtensor& A, qtensor& x, int m, int max_restart, dou
     if (stats) stats->iters = ii;
     v[ni] = q;
     if (qnorm < 1e-20 || (converged && ii >= 1) || ii == actual_maxiter) break;
-    // Gram-Schmidt, one pass, random refill on failure (:285-320)
+    // Gram-Schmidt, one pass, random refill on failure (:285-320).  The
+    // overlaps never leave the device; the new vector's norm is read together
+    // with the next row of M, because its product is issued right away (and
+    // discarded in the rare case that the orthogonalisation failed).
     const int Npass = 1;
+    const int kNormSlot = 20;
     int pass = 1, tot_pass = 0;
     bool done = false;
+    std::vector<double> row;
     while (pass <= Npass) {
       ++tot_pass;
       std::vector<const double*> vs;
       for (int k = 0; k < ni; ++k) vs.push_back(v[k].d->get());
-      std::vector<double> Vq = multidot(vs, v[ni].d->get());
-      std::vector<double> c(ni);
-      for (int k = 0; k < ni; ++k) c[k] = -Vq[k];
-      lincomb(v[ni], vs, c, true);
+      check(tt_vec_multidot(ctx(), n, ni, vs.data(), v[ni].d->get(), scalar_slot(0)), "GS overlaps");
+      check(tt_vec_lincomb_dev(ctx(), n, ni, vs.data(), scalar_slot(0), -1.0, 1, v[ni].d->get()), "GS update");
       for (int k = 0; k < ni; ++k) v[ni].p = por(v[ni].p, v[k].p);
-      double qnrm = nrm(v[ni]);
-      if (qnrm < 1e-10) {
+      check(tt_vec_nrm2(ctx(), n, v[ni].d->get(), scalar_slot(kNormSlot)), "GS norm");
+      check(tt_vec_scal_inv_dev(ctx(), n, scalar_slot(kNormSlot), v[ni].d->get()), "GS scale");
+      KVec va_new = product(v[ni]);
+      std::vector<const double*> vs2(vs);
+      vs2.push_back(v[ni].d->get());
+      check(tt_vec_multidot(ctx(), n, ni + 1, vs2.data(), va_new.d->get(), scalar_slot(0)), "M row");
+      std::vector<double> h(kNormSlot + 1);
+      check(tt_memcpy_d2h(ctx(), h.data(), scalar_slot(0), sizeof(double) * h.size()), "d2h");
+      double qnrm = h[kNormSlot];
+      if (qnrm >= 1e-10) {
+        va[ni] = va_new;
+        count_product();
+        row.assign(h.begin(), h.begin() + ni + 1);
+        ++pass;
+        continue;
+      }
+      ev_kept.back() = false;  // the speculative product is discarded
+      {
         KVec r = newvec();
         r.p = v[ni - 1].p;
         std::vector<int64_t> ranges;
@@ -457,25 +495,29 @@ double tensor_davidsonIT(big_qtensor& A, qtensor& x, int m, int max_restart, dou
       ++pass;
     }
     if (done) break;
-    va[ni] = product(v[ni]);
     std::swap(M, Mnext);
-    std::vector<const double*> vs;
-    for (int k = 0; k <= ni; ++k) vs.push_back(v[k].d->get());
-    std::vector<double> row = multidot(vs, va[ni].d->get());
     const int l = ni;
     for (int k = 0; k < ni + 1; ++k) {
       M[l + k * (ni + 1)] = row[k];
       M[k + l * (ni + 1)] = row[k];
     }
   }
-  tt_event_destroy(ev0);
-  tt_event_destroy(ev1);
   if (have_x) {
     x = eng.materialize(xv.p, xv.d);
   }
-  x.normalize();
-  if (stats) stats->heff_flops = stats->heff_flops;  // kept
+  x.normalize();  // synchronises: every recorded event has completed
+  double heff_ms = 0.0;
+  for (size_t i = 0; i < evs.size(); ++i) {
+    float ms = 0.f;
+    if (ev_kept[i]) {
+      check(tt_event_elapsed_ms(evs[i].first, evs[i].second, &ms), "event");
+      heff_ms += ms;
+    }
+    tt_event_destroy(evs[i].first);
+    tt_event_destroy(evs[i].second);
+  }
   rt().last_heff_ms = heff_ms;
+  if (stats) stats->t_loop = std::chrono::duration<double>(std::chrono::steady_clock::now() - tb1).count();
   return lambda;
 }
 
@@ -710,7 +752,7 @@ void updateSite(qMPS& psi, qMPO& H, std::vector<qtensor>& TR, std::vector<qtenso
   qtensor x = psi.A[l] * psi.A[r];
   DavidsonStats st;
   energy = tensor_davidsonIT(A, x, search_space_size, max_restart, 1e-12, mode, &st);
-  check(tt_ctx_synchronize(ctx()), "sync");
+  if (rt().profile) check(tt_ctx_synchronize(ctx()), "sync");
   auto t1 = std::chrono::steady_clock::now();
   std::string ln = psi.link_name(r);
   qtensor_index mid;
@@ -736,6 +778,7 @@ void updateSite(qMPS& psi, qMPO& H, std::vector<qtensor>& TR, std::vector<qtenso
     s.kept_per_sector = info.kept_per_sector;
     s.gram_max = info.gram_max;
     s.t_davidson = std::chrono::duration<double>(t1 - t0).count();
+    s.t_engine = st.t_engine;
     s.t_svd = std::chrono::duration<double>(t2 - t1).count();
     log->steps.push_back(std::move(s));
     log->heff_flops += st.heff_flops;
@@ -784,7 +827,7 @@ double dmrg_sweep(qMPS& psi, qMPO& H, DmrgState& st, int max_bd, double cutoff, 
       auto te0 = std::chrono::steady_clock::now();
       updateEnv(psi, H, st.TR, st.TL, site, direction);
       if (log && !log->steps.empty()) {
-        check(tt_ctx_synchronize(ctx()), "sync");
+        if (rt().profile) check(tt_ctx_synchronize(ctx()), "sync");
         log->steps.back().t_env =
             std::chrono::duration<double>(std::chrono::steady_clock::now() - te0).count();
       }

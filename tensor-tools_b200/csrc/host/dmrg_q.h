@@ -47,6 +47,8 @@ struct DavidsonStats {
   int iters = 0;
   int randomized = 0;
   double heff_flops = 0.0;   // algorithmic flops of the H_eff*x products
+  double t_engine = 0.0;     // host seconds: Krylov layout + product plans
+  double t_loop = 0.0;       // host seconds: the iterations
 };
 
 // tensor_davidsonIT for big_qtensor (linalg/tensor_davidson.cpp:193-347).
@@ -98,6 +100,7 @@ struct StepLog {
   double t_davidson = 0.0;   // host wall seconds of the phases of this step
   double t_svd = 0.0;
   double t_env = 0.0;
+  double t_engine = 0.0;     // part of t_davidson: Krylov layout and product plans
 };
 struct DmrgLog {
   std::vector<StepLog> steps;

@@ -506,7 +506,7 @@ void svd(const qtensor& A, const std::vector<qtensor_index>& left,
   for (unsigned ii = 0; ii < sec.size(); ++ii)
     for (unsigned j = 0; j < new_dim[ii]; ++j) hs.push_back(svals[ii][j]);
   if (!hs.empty()) check(tt_memcpy_h2d(ctx(), S.data->get(), hs.data(), sizeof(double) * hs.size()), "svd S");
-  check(tt_ctx_synchronize(ctx()), "svd sync");
+  // no synchronisation: the caller orders later work on the same stream
 }
 
 void svd_bond(const qtensor& combined, qtensor& A_left, qtensor& A_right, const qtensor_index& mid,

@@ -2,6 +2,7 @@
 #include "qtensor.h"
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstring>
 #include <numeric>
@@ -23,11 +24,13 @@ void check(int status, const char* what) {
 }
 
 void bind_context(tt_ctx* c) {
+  clear_contraction_cache();  // cached plans belong to the previous context
   rt().scalars.reset();
   rt().ctx = c;
   if (c) rt().scalars = std::make_shared<DevBuf>(kScalarSlots);
 }
 void unbind_context() {
+  clear_contraction_cache();
   rt().scalars.reset();
   rt().ctx = nullptr;
 }
@@ -372,7 +375,7 @@ std::vector<int64_t> colmajor_strides(const std::vector<int>& qd) {
 
 }  // namespace
 
-void contract_structure(const qtensor& A, const qtensor& B, ContractStructure& out) {
+static void contract_structure_impl(const qtensor& A, const qtensor& B, ContractStructure& out) {
   // mark repeated indices (qtensor.cpp:540-555)
   std::vector<std::pair<qtensor_index, int>> marker;
   auto find = [&](const qtensor_index& ix) -> int* {
@@ -574,7 +577,104 @@ void validate_pairs(const std::vector<tt_out_block>& outs, const std::vector<tt_
   }
 }
 
+void contract_structure(const qtensor& A, const qtensor& B, ContractStructure& out) {
+  auto t0 = std::chrono::steady_clock::now();
+  contract_structure_impl(A, B, out);
+  rt().t_structure += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  rt().n_structure++;
+}
+
+namespace {
+
+void serialize(const qtensor& T, std::vector<int64_t>& k) {
+  k.push_back(T.rank);
+  for (const auto& ix : T.idx_set) {
+    k.push_back(((int64_t)ix.arrow() << 40) | ((int64_t)ix.type() << 32) | ix.level());
+    k.push_back((int64_t)ix.name().size());
+    int64_t w = 0;
+    int nb = 0;
+    for (char ch : ix.name()) {
+      w = (w << 8) | (unsigned char)ch;
+      if (++nb == 8) { k.push_back(w); w = 0; nb = 0; }
+    }
+    if (nb) k.push_back(w);
+    k.push_back((int64_t)ix.size());
+    for (const auto& s : ix.sectors()) {
+      k.push_back(s.first.pack());
+      k.push_back(s.second);
+    }
+  }
+  k.push_back((int64_t)T.blocks.size());
+  k.push_back(T.arena);
+  for (const auto& b : T.blocks) {
+    for (const QN& q : b.qn) k.push_back(q.pack());
+    for (int d : b.qd) k.push_back(d);
+    for (unsigned i : b.qi) k.push_back(i);
+    k.push_back(b.off);
+  }
+}
+
+struct CacheEntry {
+  std::vector<int64_t> key;
+  std::shared_ptr<CachedContraction> val;
+};
+struct ContractionCache {
+  std::unordered_map<uint64_t, std::vector<CacheEntry>> map;
+  size_t entries = 0;
+};
+ContractionCache& cache() {
+  static thread_local ContractionCache c;
+  return c;
+}
+constexpr size_t kCacheMax = 16384;
+
+}  // namespace
+
+void clear_contraction_cache() {
+  cache().map.clear();
+  cache().entries = 0;
+}
+
+size_t contraction_cache_size() { return cache().entries; }
+
+std::shared_ptr<const CachedContraction> contract_cached(const qtensor& A, const qtensor& B, bool need_plan) {
+  std::vector<int64_t> key;
+  key.reserve(64 + 8 * (A.blocks.size() + B.blocks.size()) * (A.rank + B.rank));
+  serialize(A, key);
+  key.push_back(-1);
+  serialize(B, key);
+  uint64_t h = 1469598103934665603ull;
+  for (int64_t v : key) h = (h ^ (uint64_t)v) * 1099511628211ull;
+  auto& bucket = cache().map[h];
+  std::shared_ptr<CachedContraction> val;
+  for (auto& e : bucket)
+    if (e.key == key) {
+      val = e.val;
+      break;
+    }
+  if (!val) {
+    if (cache().entries >= kCacheMax) {
+      clear_contraction_cache();
+      return contract_cached(A, B, need_plan);
+    }
+    val = std::make_shared<CachedContraction>();
+    contract_structure(A, B, val->cs);
+    cache().map[h].push_back(CacheEntry{std::move(key), val});
+    cache().entries++;
+  }
+  if (need_plan && !val->plan && !val->cs.outs.empty()) val->plan = make_plan(val->cs);
+  return val;
+}
+
 std::shared_ptr<PlanHandle> make_plan(const ContractStructure& cs) {
+  auto t0 = std::chrono::steady_clock::now();
+  struct Acc {
+    std::chrono::steady_clock::time_point t0;
+    ~Acc() {
+      rt().t_plan += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+      rt().n_plan++;
+    }
+  } acc{t0};
   validate_pairs(cs.outs, cs.pairs, cs.a_size, cs.b_size, cs.C.arena);
   tt_plan* p = nullptr;
   check(tt_contract_plan(ctx(), cs.outs.data(), (int)cs.outs.size(), cs.pairs.data(), (int)cs.pairs.size(),
@@ -587,14 +687,11 @@ qtensor operator*(const qtensor& A, const qtensor& B) {
   if (!A._initted && !B._initted) throw std::runtime_error("operator*: both operands uninitialised");
   if (A._initted && !B._initted) return qtensor(A);
   if (B._initted && !A._initted) return qtensor(B);
-  ContractStructure cs;
-  contract_structure(A, B, cs);
-  std::shared_ptr<PlanHandle> plan;
-  if (!cs.outs.empty()) plan = make_plan(cs);
-  qtensor C = std::move(cs.C);
+  auto cc = contract_cached(A, B, true);
+  qtensor C = cc->cs.C;  // metadata only (C has no data yet)
   C.data = dev_alloc(C.arena);
-  if (plan)
-    check(tt_contract_exec(ctx(), plan->get(), A.data->get(), B.data->get(), C.data->get(), 1.0),
+  if (cc->plan)
+    check(tt_contract_exec(ctx(), cc->plan->get(), A.data->get(), B.data->get(), C.data->get(), 1.0),
           "contract exec");
   return C;
 }

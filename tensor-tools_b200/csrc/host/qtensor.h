@@ -32,6 +32,11 @@ struct Runtime {
   uint64_t rng_counter = 0x5eed;
   std::shared_ptr<DevBuf> scalars;  // 16 device doubles for reductions
   double last_heff_ms = 0.0;        // device time of the last Davidson's H_eff*x launches
+  bool profile = false;             // synchronise between step phases to time them
+  // host-side planning counters (always on; cheap)
+  double t_structure = 0.0;         // seconds in contract_structure
+  double t_plan = 0.0;              // seconds in plan creation (validation + tt_contract_plan)
+  int64_t n_structure = 0, n_plan = 0;
 };
 Runtime& rt();
 // Bind / unbind the device context used by every host object on this thread.
@@ -211,6 +216,20 @@ struct ContractStructure {
   int64_t a_size = 0, b_size = 0;       // operand arenas (doubles), for validation
 };
 void contract_structure(const qtensor& A, const qtensor& B, ContractStructure& out);
+
+// Cached form: the structure of A*B (and, on first use, its device plan) is
+// kept in a per-thread cache keyed by the complete block metadata of both
+// operands (index tags, block QNs, dims and arena offsets), compared exactly.
+// DMRG repeats the same contractions sweep after sweep once the bond
+// dimensions settle, so steady-state sweeps plan nothing.
+struct CachedContraction {
+  ContractStructure cs;
+  std::shared_ptr<class PlanHandle> plan;  // null when cs has no output blocks
+};
+std::shared_ptr<const CachedContraction> contract_cached(const qtensor& A, const qtensor& B,
+                                                         bool need_plan);
+void clear_contraction_cache();
+size_t contraction_cache_size();
 
 // A cached contraction plan on the device.
 class PlanHandle {

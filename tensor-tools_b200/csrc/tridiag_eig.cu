@@ -432,7 +432,7 @@ int tt_sym_eigvals_batched(tt_ctx* ctx, const tt_eig_problem* probs, int n_probs
   std::vector<EigDev> hp = to_dev(probs, n_probs, nullptr);
   EigDev* dp = tt::pool_alloc<EigDev>(ctx, n_probs);
   if (!dp) return tt::fail(TT_ERR_OOM, "tt_sym_eigvals_batched: allocation failed");
-  TT_CUDA(cudaMemcpyAsync(dp, hp.data(), sizeof(EigDev) * n_probs, cudaMemcpyHostToDevice, ctx->stream));
+  TT_CUDA(tt::h2d_async(ctx, dp, hp.data(), sizeof(EigDev) * n_probs));
   static bool attr = false;
   if (!attr) {
     TT_CUDA(cudaFuncSetAttribute(tridiag_eigvals, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)vals_smem()));
@@ -440,7 +440,6 @@ int tt_sym_eigvals_batched(tt_ctx* ctx, const tt_eig_problem* probs, int n_probs
   }
   tridiag_eigvals<<<n_probs, TT, vals_smem(), ctx->stream>>>(dp, G, T, w, A);
   TT_LAUNCH_CHECK(ctx);
-  TT_CUDA(cudaStreamSynchronize(ctx->stream));  // hp dies at return
   tt::pool_free(ctx, dp);
   return TT_OK;
 }
@@ -460,10 +459,9 @@ int tt_sym_eigvecs_batched(tt_ctx* ctx, const tt_eig_problem* probs, int n_probs
   std::vector<EigDev> hp = to_dev(probs, n_probs, nvec);
   EigDev* dp = tt::pool_alloc<EigDev>(ctx, n_probs);
   if (!dp) return tt::fail(TT_ERR_OOM, "tt_sym_eigvecs_batched: allocation failed");
-  TT_CUDA(cudaMemcpyAsync(dp, hp.data(), sizeof(EigDev) * n_probs, cudaMemcpyHostToDevice, ctx->stream));
+  TT_CUDA(tt::h2d_async(ctx, dp, hp.data(), sizeof(EigDev) * n_probs));
   tridiag_eigvecs<<<n_probs, TT, 0, ctx->stream>>>(dp, G, T, w, Z, work, A);
   TT_LAUNCH_CHECK(ctx);
-  TT_CUDA(cudaStreamSynchronize(ctx->stream));
   tt::pool_free(ctx, dp);
   return TT_OK;
 }

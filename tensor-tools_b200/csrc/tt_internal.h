@@ -21,6 +21,10 @@ struct tt_ctx {
   // device scratch for two-pass reductions
   double* d_partials = nullptr;
   int partials_cap = 0;
+  // pinned staging ring for host->device copies that must not stall the stream
+  char* stage = nullptr;
+  size_t stage_cap = 0;
+  size_t stage_head = 0;
 };
 
 namespace tt {
@@ -46,6 +50,14 @@ inline void pool_free(tt_ctx* ctx, void* p) {
 
 // Reduction scratch of at least n doubles (grown on demand).
 double* partials(tt_ctx* ctx, int n);
+
+// Asynchronous host->device copy on the context's stream.  The source is
+// first copied into the pinned staging ring, so the caller may release it on
+// return and the stream is not serialised (pageable sources would be).  When
+// the ring wraps, the stream is synchronised once so no staged bytes still in
+// flight are overwritten.  Copies larger than the ring fall back to a plain
+// (pageable) cudaMemcpyAsync.
+cudaError_t h2d_async(tt_ctx* ctx, void* dst, const void* src, size_t bytes);
 
 }  // namespace tt
 

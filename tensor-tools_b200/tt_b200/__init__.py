@@ -138,7 +138,9 @@ _proto("tt_qdmrg_step", P, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), PD, 
        C.POINTER(C.c_int), PD)
 _proto("tt_qdmrg_step_sectors", P, C.c_int, C.POINTER(C.c_int), PI32, C.POINTER(C.c_uint32), C.c_int)
 _proto("tt_qdmrg_stats", P, PD, PD, PD)
-_proto("tt_qdmrg_step_profile", P, C.c_int, C.POINTER(C.c_int), PD, PD, PD)
+_proto("tt_qdmrg_step_profile", P, C.c_int, C.POINTER(C.c_int), PD, PD, PD, PD)
+_proto("tt_dmrg_set_profiling", C.c_int)
+_proto("tt_dmrg_planning_counters", PD, PI64, PD, PI64)
 _proto("tt_sym_eig_batched", P, C.c_void_p, C.c_int, P, P, P, P)
 _proto("tt_qdmrg_num_sweeps", P, C.POINTER(C.c_int))
 _proto("tt_qdmrg_sweep_info", P, C.c_int, PD, PD)
@@ -493,9 +495,10 @@ class QDMRG:
         out = []
         for i in range(n.value):
             g = C.c_int()
-            a, b, c = D(), D(), D()
-            _chk(lib.tt_qdmrg_step_profile(self.h, i, C.byref(g), C.byref(a), C.byref(b), C.byref(c)), "profile")
-            out.append((g.value, a.value, b.value, c.value))
+            a, b, c, e = D(), D(), D(), D()
+            _chk(lib.tt_qdmrg_step_profile(self.h, i, C.byref(g), C.byref(a), C.byref(b), C.byref(c), C.byref(e)),
+                 "profile")
+            out.append((g.value, a.value, b.value, c.value, e.value))
         return out
 
     def env(self, which: int, i: int) -> QTensor:

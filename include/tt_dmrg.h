@@ -162,6 +162,22 @@ int tt_qdmrg_env(const tt_qdmrg* run, int which, int i, tt_qtensor** out);
 int tt_qdmrg_num_sweeps(const tt_qdmrg* run, int* n);
 int tt_qdmrg_sweep_info(const tt_qdmrg* run, int i, double* energy, double* seconds);
 
+/* ---- dense (no QN) MPS / MPO / DMRG ------------------------------------------ */
+typedef struct tt_dmps tt_dmps;
+typedef struct tt_dmpo tt_dmpo;
+/* MPS(sites, product string): 1 on the chosen spin, DBL_EPSILON elsewhere */
+int tt_dmps_product_spinhalf(int L, const int* state, unsigned id, tt_dmps** out);
+int tt_dmps_destroy(tt_dmps* psi);
+int tt_dmps_bond_dims(const tt_dmps* psi, int* out);  /* L+1 entries */
+/* hand-written Heisenberg MPO, bond dimension 5 */
+int tt_dmpo_heisenberg(int L, const double* dh, double tE, unsigned id, tt_dmpo** out);
+int tt_dmpo_destroy(tt_dmpo* H);
+/* dmrg(MPS&, MPO&, nsweeps, maxm[], cutoff[], max_restart[]); sweep_energy
+ * (nsweeps entries) and step_kept (2*(L-1)*nsweeps entries) may be NULL */
+int tt_ddmrg_run(tt_dmps* psi, tt_dmpo* H, int nsweeps, const int* maxm, int n_maxm, const double* cutoff,
+                 int n_cutoff, const int* max_restart, int n_mr, double* energy, double* sweep_energy,
+                 int* step_kept);
+
 #ifdef __cplusplus
 }
 #endif

@@ -548,3 +548,65 @@ int tt_qdmrg_sweep_info(const tt_qdmrg* run, int i, double* energy, double* seco
 }
 
 }  // extern "C"
+
+// ---- dense path ------------------------------------------------------------------
+#include "../host/dmrg_d.h"
+
+struct tt_dmps {
+  ttb::MPS psi;
+};
+struct tt_dmpo {
+  ttb::MPO H;
+};
+
+extern "C" {
+
+int tt_dmps_product_spinhalf(int L, const int* state, unsigned id, tt_dmps** out) {
+  TT_ARG(L >= 3 && state && out);
+  TT_GUARD({
+    std::vector<unsigned> st(state, state + L);
+    tt_dmps* h = new tt_dmps();
+    h->psi = ttb::make_product_mps((unsigned)L, st, id);
+    *out = h;
+  });
+}
+
+int tt_dmps_destroy(tt_dmps* psi) { TT_GUARD(delete psi); }
+
+int tt_dmps_bond_dims(const tt_dmps* psi, int* out) {
+  TT_ARG(psi && out);
+  TT_GUARD({
+    for (size_t i = 0; i < psi->psi.bond_dims.size(); ++i) out[i] = (int)psi->psi.bond_dims[i];
+  });
+}
+
+int tt_dmpo_heisenberg(int L, const double* dh, double tE, unsigned id, tt_dmpo** out) {
+  TT_ARG(L >= 3 && out);
+  TT_GUARD({
+    tt_dmpo* h = new tt_dmpo();
+    h->H = ttb::make_heisenberg_mpo((unsigned)L, dh, tE, id);
+    *out = h;
+  });
+}
+
+int tt_dmpo_destroy(tt_dmpo* H) { TT_GUARD(delete H); }
+
+int tt_ddmrg_run(tt_dmps* psi, tt_dmpo* H, int nsweeps, const int* maxm, int n_maxm, const double* cutoff,
+                 int n_cutoff, const int* max_restart, int n_mr, double* energy, double* sweep_energy,
+                 int* step_kept) {
+  TT_ARG(psi && H && maxm && cutoff && max_restart && n_maxm > 0 && n_cutoff > 0 && n_mr > 0 && nsweeps >= 0);
+  TT_ARG(psi->psi.length == H->H.length);
+  TT_GUARD({
+    ttb::DenseDmrgLog log;
+    double e = ttb::dmrg(psi->psi, H->H, nsweeps, std::vector<int>(maxm, maxm + n_maxm),
+                         std::vector<double>(cutoff, cutoff + n_cutoff),
+                         std::vector<int>(max_restart, max_restart + n_mr), &log);
+    if (energy) *energy = e;
+    if (sweep_energy)
+      for (size_t i = 0; i < log.sweep_energy.size(); ++i) sweep_energy[i] = log.sweep_energy[i];
+    if (step_kept)
+      for (size_t i = 0; i < log.steps.size(); ++i) step_kept[i] = (int)log.steps[i].kept;
+  });
+}
+
+}  // extern "C"

@@ -25,12 +25,14 @@ void check(int status, const char* what) {
 
 void bind_context(tt_ctx* c) {
   clear_contraction_cache();  // cached plans belong to the previous context
+  rt().dense_plans.clear();
   rt().scalars.reset();
   rt().ctx = c;
   if (c) rt().scalars = std::make_shared<DevBuf>(kScalarSlots);
 }
 void unbind_context() {
   clear_contraction_cache();
+  rt().dense_plans.clear();
   rt().scalars.reset();
   rt().ctx = nullptr;
 }

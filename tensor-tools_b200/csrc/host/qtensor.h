@@ -37,6 +37,8 @@ struct Runtime {
   double t_structure = 0.0;         // seconds in contract_structure
   double t_plan = 0.0;              // seconds in plan creation (validation + tt_contract_plan)
   int64_t n_structure = 0, n_plan = 0;
+  // plans of dense (single-block) contractions, keyed by their pair description
+  std::map<std::vector<int64_t>, std::shared_ptr<class PlanHandle>> dense_plans;
 };
 Runtime& rt();
 // Bind / unbind the device context used by every host object on this thread.

@@ -124,6 +124,13 @@ _proto("tt_qmps_data_size", P, PI64)
 _proto("tt_qmps_get_data", P, PD)
 _proto("tt_qmps_set_data", P, PD)
 _proto("tt_qdmrg_env", P, C.c_int, C.c_int, PP)
+_proto("tt_dmps_product_spinhalf", C.c_int, C.POINTER(C.c_int), C.c_uint, PP)
+_proto("tt_dmps_destroy", P)
+_proto("tt_dmps_bond_dims", P, C.POINTER(C.c_int))
+_proto("tt_dmpo_heisenberg", C.c_int, PD, D, C.c_uint, PP)
+_proto("tt_dmpo_destroy", P)
+_proto("tt_ddmrg_run", P, P, C.c_int, C.POINTER(C.c_int), C.c_int, PD, C.c_int, C.POINTER(C.c_int), C.c_int,
+       PD, PD, C.POINTER(C.c_int))
 _proto("tt_qmpo_heisenberg", C.c_int, PD, D, C.c_uint, PP)
 _proto("tt_qmpo_destroy", P)
 _proto("tt_qmpo_tensor", P, C.c_int, PP)
@@ -521,3 +528,51 @@ class QDMRG:
             _chk(lib.tt_qdmrg_sweep_info(self.h, i, C.byref(e), C.byref(s)), "sweep info")
             out.append((e.value, s.value))
         return out
+
+
+# ---------------------------------------------------------------------------
+# dense (dtensor) path
+# ---------------------------------------------------------------------------
+class DMPS:
+    """MPS(sites, product string) of the dense path (mps/tt.cpp:225-262)."""
+
+    def __init__(self, L: int, state: Sequence[int], mps_id: int = 1):
+        self.L = L
+        self.h = P()
+        _chk(lib.tt_dmps_product_spinhalf(L, (C.c_int * L)(*state), mps_id, C.byref(self.h)), "dmps")
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib.tt_dmps_destroy(self.h)
+            self.h = None
+
+    def bond_dims(self) -> List[int]:
+        out = (C.c_int * (self.L + 1))()
+        _chk(lib.tt_dmps_bond_dims(self.h, out), "bond_dims")
+        return list(out)
+
+
+class DMPO:
+    """Hand-written dense Heisenberg MPO, D=5 (models/hams/Heisenberg.cpp:185-208)."""
+
+    def __init__(self, L: int, dh: Optional[Sequence[float]] = None, tE: float = 0.0, mpo_id: int = 2):
+        self.L = L
+        self.h = P()
+        arr = (D * L)(*dh) if dh is not None else None
+        _chk(lib.tt_dmpo_heisenberg(L, arr, tE, mpo_id, C.byref(self.h)), "dmpo")
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib.tt_dmpo_destroy(self.h)
+            self.h = None
+
+
+def ddmrg_run(psi: DMPS, H: DMPO, nsweeps: int, maxm, cutoff, max_restart):
+    """dmrg(MPS&, MPO&, nsweeps, maxm[], cutoff[], max_restart[]) -> (energy, sweep energies, kept per step)."""
+    e = D()
+    se = (D * max(1, nsweeps))()
+    kept = (C.c_int * max(1, 2 * (psi.L - 1) * nsweeps))()
+    _chk(lib.tt_ddmrg_run(psi.h, H.h, nsweeps, (C.c_int * len(maxm))(*maxm), len(maxm),
+                          (D * len(cutoff))(*cutoff), len(cutoff), (C.c_int * len(max_restart))(*max_restart),
+                          len(max_restart), C.byref(e), se, kept), "ddmrg")
+    return e.value, list(se)[:nsweeps], list(kept)

@@ -27,6 +27,14 @@
  *   tt_qdmrg_*               buildEnv / updateSite / updateEnv / dmrg (schedule overload)
  *                                                            algos/dmrg/dmrg.cpp:56-85,300-372,
  *                                                            491-509,702-755
+ *   tt_autompo_*             AutoMPO, HTerm, SiteTerm         models/hams/AutoMPO.{h,cpp}
+ *   tt_qmpo_from_autompo     Heisenberg<T>::buildHam(AutoMPO&, qMPO&)
+ *                                                            models/hams/Heisenberg.cpp:412-635
+ *   tt_dmpo_from_autompo     Heisenberg<T>::buildHam(AutoMPO&, MPO&)
+ *                                                            models/hams/Heisenberg.cpp:213-330
+ *   tt_lattice               squareLattice / squareNextNeighbor / triangularLattice
+ *                                                            models/lattice/square.h:25-103,
+ *                                                            models/lattice/triangular.h:25-64
  *   tt_ddmrg_*               the dense dtensor / big_dtensor path and its dmrg
  *                                                            dtensor/dtensor.cpp, dtensor/big_dtensor.cpp,
  *                                                            dtensor/dtensor_op.cpp,
@@ -177,6 +185,37 @@ int tt_dmpo_destroy(tt_dmpo* H);
 int tt_ddmrg_run(tt_dmps* psi, tt_dmpo* H, int nsweeps, const int* maxm, int n_maxm, const double* cutoff,
                  int n_cutoff, const int* max_restart, int n_mr, double* energy, double* sweep_energy,
                  int* step_kept);
+
+/* ---- AutoMPO and lattices ------------------------------------------------------ */
+typedef struct tt_autompo tt_autompo;
+int tt_autompo_create(tt_autompo** out);
+int tt_autompo_destroy(tt_autompo* a);
+/* ampo += coef, ops[0], sites[0], ...: operators are kept in site order, a zero
+ * coefficient is dropped and a repeated operator list sums its coefficient */
+int tt_autompo_add(tt_autompo* a, double coef, int nops, const char* const* ops, const int* sites);
+int tt_autompo_size(const tt_autompo* a, int* n);
+/* term k in the accumulator's order (operator lists sorted by length, then by
+ * (site, name)); op names are copied NUL-terminated into names[16*j] for
+ * j < min(*nops, cap), and their sites into sites[j] */
+int tt_autompo_term(const tt_autompo* a, int k, double* coef, int* nops, char* names, int* sites, int cap);
+/* MPO bond dimensions of the finite-state layout for N sites (N+1 entries);
+ * with_charges selects the U(1) layout, which needs Sz / S+ / S- / Id only */
+int tt_autompo_link_dims(const tt_autompo* a, int N, int with_charges, int* dims);
+int tt_qmpo_from_autompo(const tt_autompo* a, int N, unsigned id, tt_qmpo** out);
+int tt_dmpo_from_autompo(const tt_autompo* a, int N, unsigned id, tt_dmpo** out);
+/* dims (4 entries) and, when data is not NULL, the column-major values of the
+ * dense MPO tensor on site i (left link, ket site, bra site, right link) */
+int tt_dmpo_tensor(const tt_dmpo* H, int i, int64_t* dims, double* data, int64_t cap);
+
+enum { TT_LATTICE_SQUARE = 0, TT_LATTICE_SQUARE_NEXT_NEIGHBOR = 1, TT_LATTICE_TRIANGULAR = 2 };
+/* 1-based sites, y fastest; type 0 unset, 1 nearest, 2 next-nearest neighbour;
+ * coordinates are 0 where the reference records none (triangular) */
+typedef struct {
+  int s1, s2, type;
+  double x1, y1, x2, y2;
+} tt_lattice_bond;
+/* writes min(*n_bonds, cap) bonds; *n_bonds is the full count */
+int tt_lattice(int kind, int Nx, int Ny, int yperiodic, tt_lattice_bond* bonds, int cap, int* n_bonds);
 
 #ifdef __cplusplus
 }

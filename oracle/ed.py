@@ -68,3 +68,49 @@ def ground_energy(L: int, bonds: Sequence[Tuple[int, int, float]], n_up: Optiona
 
 def chain_bonds(L: int, J: float = 1.0) -> List[Tuple[int, int, float]]:
     return [(i, i + 1, J) for i in range(L - 1)]
+
+
+_OP_ACTION = {
+    # op -> {ket bit: (bra bit, amplitude)} for spin-1/2 (Dn = 0, Up = 1)
+    "Id": {0: (0, 1.0), 1: (1, 1.0)},
+    "Sz": {0: (0, -0.5), 1: (1, 0.5)},
+    "Sx": {0: (1, 0.5), 1: (0, 0.5)},
+    "S+": {0: (1, 1.0)},
+    "S-": {1: (0, 1.0)},
+}
+
+
+def terms_hamiltonian(L: int, terms, n_up: Optional[int] = None):
+    """Sparse H = sum_t coef_t prod_j op_j(site_j) for terms given as
+    (coef, ((site, op), ...)); over the full 2^L space, or the sector with
+    n_up up spins when every term conserves Sz."""
+    basis = np.arange(2 ** L, dtype=np.int64) if n_up is None else sector_basis(L, n_up)
+    index = {int(s): i for i, s in enumerate(basis)}
+    rows, cols, vals = [], [], []
+    for a, s in enumerate(basis):
+        s = int(s)
+        for coef, ops in terms:
+            t, amp = s, coef
+            for i, op in reversed(ops):
+                act = _OP_ACTION[op].get((t >> i) & 1)
+                if act is None:
+                    amp = 0.0
+                    break
+                t = (t & ~(1 << i)) | (act[0] << i)
+                amp *= act[1]
+            if amp == 0.0:
+                continue
+            if t not in index:
+                raise ValueError("term leaves the Sz sector")
+            rows.append(index[t])
+            cols.append(a)
+            vals.append(amp)
+    n = len(basis)
+    return sp.csr_matrix((vals, (rows, cols)), shape=(n, n))
+
+
+def terms_ground_energy(L: int, terms, n_up: Optional[int] = None) -> float:
+    H = terms_hamiltonian(L, terms, n_up)
+    if H.shape[0] <= 400:
+        return float(np.linalg.eigvalsh(H.toarray())[0])
+    return float(spla.eigsh(H, k=1, which="SA", tol=1e-14, maxiter=100000)[0][0])

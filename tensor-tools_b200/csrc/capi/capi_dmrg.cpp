@@ -610,3 +610,125 @@ int tt_ddmrg_run(tt_dmps* psi, tt_dmpo* H, int nsweeps, const int* maxm, int n_m
 }
 
 }  // extern "C"
+
+// ---- AutoMPO and lattices (host-side; only the MPO builders touch the device) ----
+#include "../host/autompo.h"
+
+struct tt_autompo {
+  ttb::AutoMPO a;
+};
+
+extern "C" {
+
+int tt_autompo_create(tt_autompo** out) {
+  TT_ARG(out);
+  TT_GUARD(*out = new tt_autompo());
+}
+
+int tt_autompo_destroy(tt_autompo* a) { TT_GUARD(delete a); }
+
+int tt_autompo_add(tt_autompo* a, double coef, int nops, const char* const* ops, const int* sites) {
+  TT_ARG(a && nops > 0 && ops && sites);
+  for (int j = 0; j < nops; ++j) TT_ARG(ops[j] && sites[j] >= 0);
+  TT_GUARD({
+    ttb::HTerm t;
+    for (int j = 0; j < nops; ++j) t.add(ops[j], sites[j]);
+    t.coef *= coef;
+    a->a.add(t);
+  });
+}
+
+int tt_autompo_size(const tt_autompo* a, int* n) {
+  TT_ARG(a && n);
+  TT_GUARD(*n = a->a.size());
+}
+
+int tt_autompo_term(const tt_autompo* a, int k, double* coef, int* nops, char* names, int* sites, int cap) {
+  TT_ARG(a && k >= 0 && k < a->a.size() && cap >= 0);
+  TT_GUARD({
+    auto it = a->a.terms().begin();
+    std::advance(it, k);
+    if (coef) *coef = it->coef;
+    if (nops) *nops = it->Nops();
+    for (int j = 0; j < it->Nops() && j < cap; ++j) {
+      if (names) {
+        std::strncpy(names + 16 * j, it->ops[j].op.c_str(), 15);
+        names[16 * j + 15] = '\0';
+      }
+      if (sites) sites[j] = it->ops[j].i;
+    }
+  });
+}
+
+int tt_autompo_link_dims(const tt_autompo* a, int N, int with_charges, int* dims) {
+  TT_ARG(a && N >= 2 && dims);
+  TT_GUARD({
+    auto links = ttb::automp_links(a->a, (unsigned)N, with_charges != 0);
+    for (int n = 0; n <= N; ++n) dims[n] = (int)links[n].states.size();
+  });
+}
+
+int tt_qmpo_from_autompo(const tt_autompo* a, int N, unsigned id, tt_qmpo** out) {
+  TT_ARG(a && N >= 2 && out);
+  TT_GUARD({
+    tt_qmpo* h = new tt_qmpo();
+    try {
+      h->H = ttb::build_qmpo(a->a, (unsigned)N, id);
+    } catch (...) {
+      delete h;
+      throw;
+    }
+    *out = h;
+  });
+}
+
+int tt_dmpo_from_autompo(const tt_autompo* a, int N, unsigned id, tt_dmpo** out) {
+  TT_ARG(a && N >= 2 && out);
+  TT_GUARD({
+    tt_dmpo* h = new tt_dmpo();
+    try {
+      h->H = ttb::build_mpo(a->a, (unsigned)N, id);
+    } catch (...) {
+      delete h;
+      throw;
+    }
+    *out = h;
+  });
+}
+
+int tt_dmpo_tensor(const tt_dmpo* H, int i, int64_t* dims, double* data, int64_t cap) {
+  TT_ARG(H && dims && i >= 0 && i < (int)H->H.length);
+  TT_GUARD({
+    const ttb::dtensor& T = H->H.A[i];
+    int64_t n = 1;
+    for (int j = 0; j < 4; ++j) {
+      dims[j] = T.idx_set[j].size;
+      n *= dims[j];
+    }
+    if (data) {
+      if (cap < n) throw std::runtime_error("tt_dmpo_tensor: buffer too small");
+      std::vector<double> h = T.get();
+      std::memcpy(data, h.data(), sizeof(double) * (size_t)n);
+    }
+  });
+}
+
+int tt_lattice(int kind, int Nx, int Ny, int yperiodic, tt_lattice_bond* bonds, int cap, int* n_bonds) {
+  TT_ARG(Nx >= 1 && Ny >= 1 && n_bonds && cap >= 0 && (bonds || cap == 0));
+  TT_GUARD({
+    std::vector<ttb::LatticeBond> g;
+    if (kind == TT_LATTICE_SQUARE)
+      g = ttb::square_lattice(Nx, Ny, yperiodic != 0);
+    else if (kind == TT_LATTICE_SQUARE_NEXT_NEIGHBOR)
+      g = ttb::square_next_neighbor(Nx, Ny, yperiodic != 0);
+    else if (kind == TT_LATTICE_TRIANGULAR)
+      g = ttb::triangular_lattice(Nx, Ny, yperiodic != 0);
+    else
+      throw std::runtime_error("tt_lattice: unknown lattice kind");
+    *n_bonds = (int)g.size();
+    for (int j = 0; j < (int)g.size() && j < cap; ++j)
+      bonds[j] = tt_lattice_bond{g[j].s1, g[j].s2, g[j].type, g[j].x1, g[j].y1, g[j].x2, g[j].y2};
+  });
+}
+
+}  // extern "C"

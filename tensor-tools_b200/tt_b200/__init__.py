@@ -132,6 +132,15 @@ _proto("tt_dmpo_destroy", P)
 _proto("tt_ddmrg_run", P, P, C.c_int, C.POINTER(C.c_int), C.c_int, PD, C.c_int, C.POINTER(C.c_int), C.c_int,
        PD, PD, C.POINTER(C.c_int))
 _proto("tt_qmpo_heisenberg", C.c_int, PD, D, C.c_uint, PP)
+_proto("tt_autompo_create", PP)
+_proto("tt_autompo_destroy", P)
+_proto("tt_autompo_add", P, D, C.c_int, C.POINTER(C.c_char_p), C.POINTER(C.c_int))
+_proto("tt_autompo_size", P, C.POINTER(C.c_int))
+_proto("tt_autompo_term", P, C.c_int, PD, C.POINTER(C.c_int), C.c_char_p, C.POINTER(C.c_int), C.c_int)
+_proto("tt_autompo_link_dims", P, C.c_int, C.c_int, C.POINTER(C.c_int))
+_proto("tt_qmpo_from_autompo", P, C.c_int, C.c_uint, PP)
+_proto("tt_dmpo_from_autompo", P, C.c_int, C.c_uint, PP)
+_proto("tt_dmpo_tensor", P, C.c_int, PI64, PD, I64)
 _proto("tt_qmpo_destroy", P)
 _proto("tt_qmpo_tensor", P, C.c_int, PP)
 _proto("tt_qdmrg_create", P, P, PP)
@@ -430,11 +439,24 @@ class QMPS:
 
 
 class QMPO:
-    def __init__(self, L: int, dh: Optional[Sequence[float]] = None, tE: float = 0.0, mpo_id: int = 2):
+    """U(1) qMPO: the hand-written Heisenberg chain (models/hams/Heisenberg.cpp:333-402),
+    or any spin-1/2 AutoMPO through ``QMPO.from_autompo``."""
+
+    def __init__(self, L: int, dh: Optional[Sequence[float]] = None, tE: float = 0.0, mpo_id: int = 2,
+                 _handle=None):
         self.L = L
         self.h = P()
+        if _handle is not None:
+            self.h = _handle
+            return
         arr = (D * L)(*dh) if dh is not None else None
         _chk(lib.tt_qmpo_heisenberg(L, arr, tE, mpo_id, C.byref(self.h)), "qmpo")
+
+    @classmethod
+    def from_autompo(cls, ampo: "AutoMPO", N: int, mpo_id: int = 2) -> "QMPO":
+        h = P()
+        _chk(lib.tt_qmpo_from_autompo(ampo.h, N, mpo_id, C.byref(h)), "qmpo from autompo")
+        return cls(N, _handle=h)
 
     def __del__(self):
         if getattr(self, "h", None):
@@ -553,13 +575,33 @@ class DMPS:
 
 
 class DMPO:
-    """Hand-written dense Heisenberg MPO, D=5 (models/hams/Heisenberg.cpp:185-208)."""
+    """Dense MPO: the hand-written Heisenberg chain, D=5 (models/hams/Heisenberg.cpp:185-208),
+    or any spin-1/2 AutoMPO through ``DMPO.from_autompo``."""
 
-    def __init__(self, L: int, dh: Optional[Sequence[float]] = None, tE: float = 0.0, mpo_id: int = 2):
+    def __init__(self, L: int, dh: Optional[Sequence[float]] = None, tE: float = 0.0, mpo_id: int = 2,
+                 _handle=None):
         self.L = L
         self.h = P()
+        if _handle is not None:
+            self.h = _handle
+            return
         arr = (D * L)(*dh) if dh is not None else None
         _chk(lib.tt_dmpo_heisenberg(L, arr, tE, mpo_id, C.byref(self.h)), "dmpo")
+
+    @classmethod
+    def from_autompo(cls, ampo: "AutoMPO", N: int, mpo_id: int = 2) -> "DMPO":
+        h = P()
+        _chk(lib.tt_dmpo_from_autompo(ampo.h, N, mpo_id, C.byref(h)), "dmpo from autompo")
+        return cls(N, _handle=h)
+
+    def tensor(self, i: int) -> np.ndarray:
+        """Site tensor as an array (left link, ket, bra, right link)."""
+        dims = (I64 * 4)()
+        _chk(lib.tt_dmpo_tensor(self.h, i, dims, None, 0), "dmpo tensor")
+        n = int(np.prod(list(dims)))
+        out = np.zeros(n)
+        _chk(lib.tt_dmpo_tensor(self.h, i, dims, out.ctypes.data_as(PD), n), "dmpo tensor")
+        return out.reshape(list(dims), order="F")
 
     def __del__(self):
         if getattr(self, "h", None):
@@ -576,3 +618,97 @@ def ddmrg_run(psi: DMPS, H: DMPO, nsweeps: int, maxm, cutoff, max_restart):
                           (D * len(cutoff))(*cutoff), len(cutoff), (C.c_int * len(max_restart))(*max_restart),
                           len(max_restart), C.byref(e), se, kept), "ddmrg")
     return e.value, list(se)[:nsweeps], list(kept)
+
+
+class AutoMPO:
+    """AutoMPO term accumulator (models/hams/AutoMPO.{h,cpp}); host-side only.
+
+    ``ampo.add(0.5, "S+", i, "S-", j)`` or ``ampo += (0.5, "S+", i, "S-", j)``
+    mirrors the reference's ``ampo += 0.5, "S+", i, "S-", j;``."""
+
+    def __init__(self):
+        self.h = P()
+        _chk(lib.tt_autompo_create(C.byref(self.h)), "autompo create")
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib.tt_autompo_destroy(self.h)
+            self.h = None
+
+    def add(self, *args):
+        coef, ops, sites, pending = 1.0, [], [], None
+        for a in args:
+            if isinstance(a, str):
+                if pending is not None:
+                    raise ValueError("Invalid input to AutoMPO (two strings in a row?)")
+                pending = a
+            elif pending is not None:
+                ops.append(pending.encode())
+                sites.append(int(a))
+                pending = None
+            else:
+                coef *= float(a)
+        if pending is not None:
+            raise ValueError("Invalid input to AutoMPO (missing site number?)")
+        if not ops:
+            raise ValueError("No operators in HTerm")
+        _chk(lib.tt_autompo_add(self.h, coef, len(ops), (C.c_char_p * len(ops))(*ops),
+                                (C.c_int * len(sites))(*sites)), "autompo add")
+        return self
+
+    def __iadd__(self, term):
+        return self.add(*(term if isinstance(term, tuple) else (term,)))
+
+    def __len__(self):
+        n = C.c_int()
+        _chk(lib.tt_autompo_size(self.h, C.byref(n)), "autompo size")
+        return n.value
+
+    def terms(self):
+        """[(coef, ((site, op), ...))] in the accumulator's order."""
+        out = []
+        for k in range(len(self)):
+            coef, nops = D(), C.c_int()
+            names = C.create_string_buffer(16 * 8)
+            sites = (C.c_int * 8)()
+            _chk(lib.tt_autompo_term(self.h, k, C.byref(coef), C.byref(nops), names, sites, 8), "autompo term")
+            ops = tuple((sites[j], names.raw[16 * j:16 * j + 16].split(b"\0")[0].decode())
+                        for j in range(min(nops.value, 8)))
+            out.append((coef.value, ops))
+        return out
+
+    def link_dims(self, N: int, with_charges: bool = True) -> List[int]:
+        dims = (C.c_int * (N + 1))()
+        _chk(lib.tt_autompo_link_dims(self.h, N, int(with_charges), dims), "autompo link dims")
+        return list(dims)
+
+
+class LatticeBond(C.Structure):
+    _fields_ = [("s1", C.c_int), ("s2", C.c_int), ("type", C.c_int), ("x1", D), ("y1", D), ("x2", D), ("y2", D)]
+
+
+_proto("tt_lattice", C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(LatticeBond), C.c_int, C.POINTER(C.c_int))
+TT_LATTICE_SQUARE, TT_LATTICE_SQUARE_NEXT_NEIGHBOR, TT_LATTICE_TRIANGULAR = 0, 1, 2
+
+
+def _lattice(kind, Nx, Ny, yperiodic):
+    n = C.c_int()
+    _chk(lib.tt_lattice(kind, Nx, Ny, int(yperiodic), None, 0, C.byref(n)), "lattice")
+    buf = (LatticeBond * max(1, n.value))()
+    _chk(lib.tt_lattice(kind, Nx, Ny, int(yperiodic), buf, n.value, C.byref(n)), "lattice")
+    return [(b.s1, b.s2, b.type, b.x1, b.y1, b.x2, b.y2) for b in buf[:n.value]]
+
+
+def square_lattice(Nx: int, Ny: int, yperiodic: bool = False):
+    """squareLattice (models/lattice/square.h:25-58): (s1, s2, type, x1, y1, x2, y2), 1-based sites."""
+    return _lattice(TT_LATTICE_SQUARE, Nx, Ny, yperiodic)
+
+
+def square_next_neighbor(Nx: int, Ny: int, yperiodic: bool = False):
+    """squareNextNeighbor (models/lattice/square.h:60-103); type 1 nearest, 2 next nearest."""
+    return _lattice(TT_LATTICE_SQUARE_NEXT_NEIGHBOR, Nx, Ny, yperiodic)
+
+
+def triangular_lattice(Nx: int, Ny: int, yperiodic: bool = True):
+    """triangularLattice (models/lattice/triangular.h:25-64)."""
+    return _lattice(TT_LATTICE_TRIANGULAR, Nx, Ny, yperiodic)

@@ -342,7 +342,10 @@ def run_ours(args):
                          "achieved": achieved, "peak": peak64, "unit": "TFLOP/s",
                          "frac": achieved / peak64 if peak64 else None,
                          "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (FP64 tensor path)",
-                         "traffic": None},
+                         # dram__bytes_read.sum + dram__bytes_write.sum per grouped_dgemm
+                         # launch: mean of three launches captured mid-sweep by ncu on this
+                         # workload (profiles/grouped_dgemm_heisenberg_L100_maxdim512.md)
+                         "traffic": 364544, "traffic_unit": "bytes per launch"},
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_val, "unit": "s/sweep", "h2d_bytes_per_step": int(n * 8),
                     "d2h_bytes_per_step": int(n * 8),

@@ -151,6 +151,11 @@ int tt_vec_axpy(tt_ctx* ctx, int64_t n, double a, const double* x, double* y);
 int tt_vec_scal(tt_ctx* ctx, int64_t n, double a, double* x);
 /* x *= 1/ *d_nrm, with the norm read on the device. */
 int tt_vec_scal_inv_dev(tt_ctx* ctx, int64_t n, const double* d_nrm, double* x);
+/* x[i + inner*(m + mid*o)] *= scale[m] (scale: mid <= TT_SCALE_MODE_MAX host
+ * values): a diagonal one-site operator such as Sz applied to one mode of a
+ * column-major block; no alignment requirement */
+#define TT_SCALE_MODE_MAX 8
+int tt_vec_scale_mode(tt_ctx* ctx, int64_t inner, int mid, int64_t outer, const double* scale, double* x);
 /* y = sum_j sign * coef[j] * xs[j] (+ y if accumulate), coefficients on the
  * device: the Gram-Schmidt projection and Ritz-vector build in one pass.
  * xs is a HOST array of nvec (0..16) device pointers. */

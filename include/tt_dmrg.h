@@ -27,6 +27,18 @@
  *   tt_qdmrg_*               buildEnv / updateSite / updateEnv / dmrg (schedule overload)
  *                                                            algos/dmrg/dmrg.cpp:56-85,300-372,
  *                                                            491-509,702-755
+ *   tt_qmps_overlap / tt_dmps_overlap
+ *                            psiphi(qMPS&, qMPS&) / psiphi(MPS&, MPS&)
+ *                                                            mps/observables.cpp:382-450
+ *   tt_qmps_expectation / tt_dmps_expectation
+ *                            psiHphi(psi, H, phi)            mps/observables.cpp:25-103
+ *   tt_qmps_measure_sz / tt_dmps_measure_sz
+ *                            <Sz_i>, <Sz_i Sz_j> (no reference counterpart; the
+ *                            reference offers only psiHphi / psiphi)
+ *   tt_qmps_save / tt_qmps_load, tt_dmps_save / tt_dmps_load
+ *                            qTensorTrain::save/load, TensorTrain::save/load
+ *                                                            mps/qtt.cpp:678-771, mps/tt.cpp,
+ *                                                            dtensor/dtensor.cpp:610-713
  *   tt_autompo_*             AutoMPO, HTerm, SiteTerm         models/hams/AutoMPO.{h,cpp}
  *   tt_qmpo_from_autompo     Heisenberg<T>::buildHam(AutoMPO&, qMPO&)
  *                                                            models/hams/Heisenberg.cpp:412-635
@@ -177,6 +189,7 @@ typedef struct tt_dmpo tt_dmpo;
 int tt_dmps_product_spinhalf(int L, const int* state, unsigned id, tt_dmps** out);
 int tt_dmps_destroy(tt_dmps* psi);
 int tt_dmps_bond_dims(const tt_dmps* psi, int* out);  /* L+1 entries */
+int tt_dmps_length(const tt_dmps* psi, int* L);
 /* hand-written Heisenberg MPO, bond dimension 5 */
 int tt_dmpo_heisenberg(int L, const double* dh, double tE, unsigned id, tt_dmpo** out);
 int tt_dmpo_destroy(tt_dmpo* H);
@@ -185,6 +198,28 @@ int tt_dmpo_destroy(tt_dmpo* H);
 int tt_ddmrg_run(tt_dmps* psi, tt_dmpo* H, int nsweeps, const int* maxm, int n_maxm, const double* cutoff,
                  int n_cutoff, const int* max_restart, int n_mr, double* energy, double* sweep_energy,
                  int* step_kept);
+
+/* ---- observables ----------------------------------------------------------------- */
+/* <psi|phi> and <psi|H|phi> (unnormalised, as the reference) */
+int tt_qmps_overlap(const tt_qmps* psi, const tt_qmps* phi, double* out);
+int tt_qmps_expectation(const tt_qmps* psi, const tt_qmpo* H, const tt_qmps* phi, double* out);
+/* <Sz_i> (L entries) and <Sz_i Sz_j> (L*L, row-major, symmetric), normalised
+ * by <psi|psi>; either output may be NULL */
+int tt_qmps_measure_sz(const tt_qmps* psi, double* sz, double* szsz);
+int tt_dmps_overlap(const tt_dmps* psi, const tt_dmps* phi, double* out);
+int tt_dmps_expectation(const tt_dmps* psi, const tt_dmpo* H, const tt_dmps* phi, double* out);
+int tt_dmps_measure_sz(const tt_dmps* psi, double* sz, double* szsz);
+
+/* ---- checkpoints ------------------------------------------------------------------ */
+/* Metadata to fn + ".ttmps" (text: MPS attributes, indices, per-block sector
+ * tuples and byte offsets); block data, dense column-major doubles back to
+ * back in site and block order, to wfn (NULL: fn + "__T.bin"). */
+int tt_qmps_save(const tt_qmps* psi, const char* fn, const char* wfn);
+/* fn: the ".ttmps" file; data_prefix (may be NULL) is prepended to the
+ * recorded raw file name */
+int tt_qmps_load(const char* fn, const char* data_prefix, tt_qmps** out);
+int tt_dmps_save(const tt_dmps* psi, const char* fn, const char* wfn);
+int tt_dmps_load(const char* fn, const char* data_prefix, tt_dmps** out);
 
 /* ---- AutoMPO and lattices ------------------------------------------------------ */
 typedef struct tt_autompo tt_autompo;

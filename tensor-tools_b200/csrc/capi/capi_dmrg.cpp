@@ -580,6 +580,11 @@ int tt_dmps_bond_dims(const tt_dmps* psi, int* out) {
   });
 }
 
+int tt_dmps_length(const tt_dmps* psi, int* L) {
+  TT_ARG(psi && L);
+  TT_GUARD(*L = (int)psi->psi.length);
+}
+
 int tt_dmpo_heisenberg(int L, const double* dh, double tE, unsigned id, tt_dmpo** out) {
   TT_ARG(L >= 3 && out);
   TT_GUARD({
@@ -728,6 +733,90 @@ int tt_lattice(int kind, int Nx, int Ny, int yperiodic, tt_lattice_bond* bonds, 
     *n_bonds = (int)g.size();
     for (int j = 0; j < (int)g.size() && j < cap; ++j)
       bonds[j] = tt_lattice_bond{g[j].s1, g[j].s2, g[j].type, g[j].x1, g[j].y1, g[j].x2, g[j].y2};
+  });
+}
+
+}  // extern "C"
+
+// ---- observables ------------------------------------------------------------------
+#include "../host/observables.h"
+
+namespace {
+template <class Psi>
+void copy_sz(const Psi& psi, double* sz, double* szsz) {
+  std::vector<double> a, b;
+  ttb::measure_sz(psi, a, b);
+  if (sz) std::memcpy(sz, a.data(), sizeof(double) * a.size());
+  if (szsz) std::memcpy(szsz, b.data(), sizeof(double) * b.size());
+}
+}  // namespace
+
+extern "C" {
+
+int tt_qmps_overlap(const tt_qmps* psi, const tt_qmps* phi, double* out) {
+  TT_ARG(psi && phi && out);
+  TT_GUARD(*out = ttb::psiphi(psi->psi, phi->psi));
+}
+
+int tt_qmps_expectation(const tt_qmps* psi, const tt_qmpo* H, const tt_qmps* phi, double* out) {
+  TT_ARG(psi && H && phi && out);
+  TT_GUARD(*out = ttb::psiHphi(psi->psi, H->H, phi->psi));
+}
+
+int tt_qmps_measure_sz(const tt_qmps* psi, double* sz, double* szsz) {
+  TT_ARG(psi);
+  TT_GUARD(copy_sz(psi->psi, sz, szsz));
+}
+
+int tt_dmps_overlap(const tt_dmps* psi, const tt_dmps* phi, double* out) {
+  TT_ARG(psi && phi && out);
+  TT_GUARD(*out = ttb::psiphi(psi->psi, phi->psi));
+}
+
+int tt_dmps_expectation(const tt_dmps* psi, const tt_dmpo* H, const tt_dmps* phi, double* out) {
+  TT_ARG(psi && H && phi && out);
+  TT_GUARD(*out = ttb::psiHphi(psi->psi, H->H, phi->psi));
+}
+
+int tt_dmps_measure_sz(const tt_dmps* psi, double* sz, double* szsz) {
+  TT_ARG(psi);
+  TT_GUARD(copy_sz(psi->psi, sz, szsz));
+}
+
+}  // extern "C"
+
+// ---- checkpoints -------------------------------------------------------------------
+#include "../host/checkpoint.h"
+
+extern "C" {
+
+int tt_qmps_save(const tt_qmps* psi, const char* fn, const char* wfn) {
+  TT_ARG(psi && fn && *fn);
+  TT_GUARD(ttb::save(psi->psi, fn, wfn ? wfn : ""));
+}
+
+int tt_qmps_load(const char* fn, const char* data_prefix, tt_qmps** out) {
+  TT_ARG(fn && out);
+  TT_GUARD({
+    ttb::qMPS p = ttb::load_qmps(fn, data_prefix ? data_prefix : "");
+    tt_qmps* h = new tt_qmps();
+    h->psi = std::move(p);
+    *out = h;
+  });
+}
+
+int tt_dmps_save(const tt_dmps* psi, const char* fn, const char* wfn) {
+  TT_ARG(psi && fn && *fn);
+  TT_GUARD(ttb::save(psi->psi, fn, wfn ? wfn : ""));
+}
+
+int tt_dmps_load(const char* fn, const char* data_prefix, tt_dmps** out) {
+  TT_ARG(fn && out);
+  TT_GUARD({
+    ttb::MPS p = ttb::load_mps(fn, data_prefix ? data_prefix : "");
+    tt_dmps* h = new tt_dmps();
+    h->psi = std::move(p);
+    *out = h;
   });
 }
 

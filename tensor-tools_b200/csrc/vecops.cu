@@ -99,6 +99,18 @@ __global__ void axpy_kernel(int64_t n, double a, const double* __restrict__ x, d
   if ((n & 1) && blockIdx.x == 0 && threadIdx.x == 0) y[n - 1] = fma(a, x[n - 1], y[n - 1]);
 }
 
+struct ModeScale {
+  double v[TT_SCALE_MODE_MAX];
+};
+
+// x[i + inner*(m + mid*o)] *= scale[m]: a diagonal operator on one mode of a
+// column-major tensor (no alignment requirement: blocks of a qtensor arena
+// start at arbitrary element offsets).
+__global__ void scale_mode_kernel(int64_t inner, int mid, int64_t total, ModeScale s, double* __restrict__ x) {
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x)
+    x[e] *= s.v[(int)((e / inner) % mid)];
+}
+
 __global__ void scal_kernel(int64_t n, double a, const double* d_nrm, double* __restrict__ x) {
   if (d_nrm) a = 1.0 / d_nrm[0];
   const int64_t n2 = n / 2;
@@ -287,6 +299,18 @@ int tt_vec_scal(tt_ctx* ctx, int64_t n, double a, double* x) {
   TT_REQUIRE(aligned16(x), "tt_vec_scal: vectors must be 16-byte aligned");
   if (n <= 0) return TT_OK;
   scal_kernel<<<stream_blocks(ctx, n), 256, 0, ctx->stream>>>(n, a, nullptr, x);
+  TT_LAUNCH_CHECK(ctx);
+  return TT_OK;
+}
+
+int tt_vec_scale_mode(tt_ctx* ctx, int64_t inner, int mid, int64_t outer, const double* scale, double* x) {
+  TT_REQUIRE(ctx && x && scale, "tt_vec_scale_mode: null argument");
+  TT_REQUIRE(inner >= 0 && outer >= 0 && mid >= 1 && mid <= TT_SCALE_MODE_MAX, "tt_vec_scale_mode: bad extents");
+  int64_t total = inner * mid * outer;
+  if (total == 0) return TT_OK;
+  ModeScale s{};
+  for (int m = 0; m < mid; ++m) s.v[m] = scale[m];
+  scale_mode_kernel<<<stream_blocks(ctx, total), 256, 0, ctx->stream>>>(inner, mid, total, s, x);
   TT_LAUNCH_CHECK(ctx);
   return TT_OK;
 }

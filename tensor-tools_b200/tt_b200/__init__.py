@@ -141,9 +141,17 @@ _proto("tt_autompo_link_dims", P, C.c_int, C.c_int, C.POINTER(C.c_int))
 _proto("tt_qmpo_from_autompo", P, C.c_int, C.c_uint, PP)
 _proto("tt_dmpo_from_autompo", P, C.c_int, C.c_uint, PP)
 _proto("tt_dmpo_tensor", P, C.c_int, PI64, PD, I64)
+for _pre in ("tt_qmps", "tt_dmps"):
+    _proto(_pre + "_save", P, C.c_char_p, C.c_char_p)
+    _proto(_pre + "_length", P, C.POINTER(C.c_int))
+    _proto(_pre + "_load", C.c_char_p, C.c_char_p, PP)
+    _proto(_pre + "_overlap", P, P, PD)
+    _proto(_pre + "_expectation", P, P, P, PD)
+    _proto(_pre + "_measure_sz", P, PD, PD)
 _proto("tt_qmpo_destroy", P)
 _proto("tt_qmpo_tensor", P, C.c_int, PP)
 _proto("tt_qdmrg_create", P, P, PP)
+_proto("tt_vec_scale_mode", P, I64, C.c_int, I64, PD, P)
 _proto("tt_qdmrg_sweep", P, C.c_int, D, C.c_int, PD)
 _proto("tt_qdmrg_finish", P)
 _proto("tt_qdmrg_destroy", P)
@@ -396,11 +404,46 @@ class BigQTensor:
 
 
 class QMPS:
-    def __init__(self, L: int, state: Sequence[int], mps_id: int = 1):
-        st = (C.c_int * L)(*state)
+    def __init__(self, L: int, state: Sequence[int] = None, mps_id: int = 1, _handle=None):
         self.L = L
         self.h = P()
+        if _handle is not None:
+            self.h = _handle
+            return
+        st = (C.c_int * L)(*state)
         _chk(lib.tt_qmps_product_spinhalf(L, st, mps_id, C.byref(self.h)), "qmps")
+
+    def save(self, fn: str, wfn: Optional[str] = None):
+        """qTensorTrain::save: metadata to fn + '.ttmps', blocks to wfn (default fn + '__T.bin')."""
+        _chk(lib.tt_qmps_save(self.h, fn.encode(), wfn.encode() if wfn else None), "qmps save")
+
+    @classmethod
+    def load(cls, fn: str, data_prefix: str = "") -> "QMPS":
+        """qTensorTrain::load(fn, dataPrefix) from a '.ttmps' metadata file."""
+        h = P()
+        _chk(lib.tt_qmps_load(fn.encode(), data_prefix.encode(), C.byref(h)), "qmps load")
+        n = C.c_int()
+        _chk(lib.tt_qmps_length(h, C.byref(n)), "qmps length")
+        return cls(n.value, _handle=h)
+
+    def overlap(self, other=None) -> float:
+        """psiphi(self, other) (mps/observables.cpp:382-450); other defaults to self."""
+        out = D()
+        _chk(lib.tt_qmps_overlap(self.h, (other or self).h, C.byref(out)), "overlap")
+        return out.value
+
+    def expectation(self, H, other=None) -> float:
+        """psiHphi(self, H, other) (mps/observables.cpp:25-103), unnormalised."""
+        out = D()
+        _chk(lib.tt_qmps_expectation(self.h, H.h, (other or self).h, C.byref(out)), "expectation")
+        return out.value
+
+    def measure_sz(self):
+        """(<Sz_i> as an (L,) array, <Sz_i Sz_j> as an (L, L) array), normalised by <psi|psi>."""
+        sz = np.zeros(self.L)
+        szsz = np.zeros((self.L, self.L))
+        _chk(lib.tt_qmps_measure_sz(self.h, sz.ctypes.data_as(PD), szsz.ctypes.data_as(PD)), "measure_sz")
+        return sz, szsz
 
     def __del__(self):
         if getattr(self, "h", None):
@@ -490,9 +533,11 @@ class QDMRG:
     def finish(self):
         _chk(lib.tt_qdmrg_finish(self.h), "finish")
 
-    def run(self, nsweeps, maxm, cutoff, max_restart) -> float:
+    def run(self, nsweeps, maxm, cutoff, max_restart, start_sweep: int = 0) -> float:
+        """Sweeps start_sweep .. nsweeps-1 of the schedule (maxm[s % len] ...),
+        then the final position(0); start_sweep > 0 resumes a loaded checkpoint."""
         e = 0.0
-        for s in range(nsweeps):
+        for s in range(start_sweep, nsweeps):
             e = self.sweep(maxm[s % len(maxm)], cutoff[s % len(cutoff)], max_restart[s % len(max_restart)])
         self.finish()
         return e
@@ -558,10 +603,24 @@ class QDMRG:
 class DMPS:
     """MPS(sites, product string) of the dense path (mps/tt.cpp:225-262)."""
 
-    def __init__(self, L: int, state: Sequence[int], mps_id: int = 1):
+    def __init__(self, L: int, state: Sequence[int] = None, mps_id: int = 1, _handle=None):
         self.L = L
         self.h = P()
+        if _handle is not None:
+            self.h = _handle
+            return
         _chk(lib.tt_dmps_product_spinhalf(L, (C.c_int * L)(*state), mps_id, C.byref(self.h)), "dmps")
+
+    def save(self, fn: str, wfn: Optional[str] = None):
+        _chk(lib.tt_dmps_save(self.h, fn.encode(), wfn.encode() if wfn else None), "dmps save")
+
+    @classmethod
+    def load(cls, fn: str, data_prefix: str = "") -> "DMPS":
+        h = P()
+        _chk(lib.tt_dmps_load(fn.encode(), data_prefix.encode(), C.byref(h)), "dmps load")
+        n = C.c_int()
+        _chk(lib.tt_dmps_length(h, C.byref(n)), "dmps length")
+        return cls(n.value, _handle=h)
 
     def __del__(self):
         if getattr(self, "h", None):
@@ -572,6 +631,25 @@ class DMPS:
         out = (C.c_int * (self.L + 1))()
         _chk(lib.tt_dmps_bond_dims(self.h, out), "bond_dims")
         return list(out)
+
+    def overlap(self, other=None) -> float:
+        """psiphi(self, other) (mps/observables.cpp:382-450); other defaults to self."""
+        out = D()
+        _chk(lib.tt_dmps_overlap(self.h, (other or self).h, C.byref(out)), "overlap")
+        return out.value
+
+    def expectation(self, H, other=None) -> float:
+        """psiHphi(self, H, other) (mps/observables.cpp:25-103), unnormalised."""
+        out = D()
+        _chk(lib.tt_dmps_expectation(self.h, H.h, (other or self).h, C.byref(out)), "expectation")
+        return out.value
+
+    def measure_sz(self):
+        """(<Sz_i> as an (L,) array, <Sz_i Sz_j> as an (L, L) array), normalised by <psi|psi>."""
+        sz = np.zeros(self.L)
+        szsz = np.zeros((self.L, self.L))
+        _chk(lib.tt_dmps_measure_sz(self.h, sz.ctypes.data_as(PD), szsz.ctypes.data_as(PD)), "measure_sz")
+        return sz, szsz
 
 
 class DMPO:

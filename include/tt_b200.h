@@ -50,6 +50,9 @@ extern "C" {
 
 /* ---- precision of the block contractions -------------------------------- */
 #define TT_PREC_FP64       0  /* DMMA f64 tensor-core tiles                  */
+#define TT_PREC_TF32       1  /* tcgen05 kind::tf32, FP32 accumulator in TMEM */
+#define TT_PREC_TF32X3     2  /* tcgen05 kind::tf32 on hi/lo splits of the FP64
+                                 operands (hi*hi + hi*lo + lo*hi), FP32 accumulator */
 
 #define TT_MAX_MODES       6  /* tensor modes per GEMM dimension of a pair   */
 
@@ -119,6 +122,10 @@ int tt_contract_exec(tt_ctx* ctx, const tt_plan* plan, const double* A,
 int tt_plan_destroy(tt_ctx* ctx, tt_plan* plan);
 /* Algorithmic work of one exec: sum over pairs of 2*m*n*k. */
 int tt_plan_flops(const tt_plan* plan, double* flops);
+/* Device status of the plan's tensor-core launches since the plan was built:
+ * TT_OK, or TT_ERR_TIMEOUT when a bounded wait on the MMA completion barrier
+ * gave up (the tile was then skipped).  Synchronises the context's stream. */
+int tt_plan_device_status(tt_ctx* ctx, const tt_plan* plan, int* status);
 
 /* ---- Davidson vector kernels (flat, deterministic reductions) -----------
  * Vectors are contiguous FP64 arrays of n elements (all blocks of a

@@ -91,6 +91,13 @@ int tt_dmrg_set_profiling(int on);
  * block-structure computation and in contraction-plan creation */
 int tt_dmrg_planning_counters(double* t_structure, int64_t* n_structure, double* t_plan, int64_t* n_plan);
 
+/* Precisions (TT_PREC_*) on this thread: op -- qtensor/dtensor contractions
+ * (operator*); heff -- the H_eff*x products inside Davidson; env -- the
+ * environment updates of a sweep.  Gram-Schmidt, the Rayleigh-Ritz problem,
+ * the SVD and the two-site tensor stay FP64; with heff != TT_PREC_FP64 the
+ * last step of every sweep re-evaluates its energy with an FP64 product. */
+int tt_dmrg_set_precision(int op, int heff, int env);
+
 /* ---- qtensor ------------------------------------------------------------- */
 int tt_qtensor_create(int rank, const tt_index_desc* idx, tt_qtensor** out);
 int tt_qtensor_init_blocks(tt_qtensor* t);

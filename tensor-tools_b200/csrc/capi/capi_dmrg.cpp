@@ -79,6 +79,16 @@ int tt_dmrg_bind(tt_ctx* ctx) {
 
 int tt_dmrg_unbind(void) { TT_GUARD(ttb::unbind_context()); }
 
+int tt_dmrg_set_precision(int op, int heff, int env) {
+  auto ok = [](int p) { return p == TT_PREC_FP64 || p == TT_PREC_TF32 || p == TT_PREC_TF32X3; };
+  TT_ARG(ok(op) && ok(heff) && ok(env));
+  TT_GUARD({
+    ttb::rt().precision = op;
+    ttb::rt().heff_precision = heff;
+    ttb::rt().env_precision = env;
+  });
+}
+
 int tt_dmrg_set_profiling(int on) { TT_GUARD(ttb::rt().profile = on != 0); }
 
 int tt_dmrg_planning_counters(double* t_structure, int64_t* n_structure, double* t_plan, int64_t* n_plan) {

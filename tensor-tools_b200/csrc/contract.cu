@@ -212,10 +212,340 @@ grouped_dgemm(const TaskDev* __restrict__ tasks, const OutDev* __restrict__ outs
   }
 }
 
+// ---------------------------------------------------------------------------
+// Mixed-precision path: tcgen05 (5th-generation tensor cores), kind::tf32.
+//
+// One CTA of eight warps computes a TC_BM x TC_BN tile of an output block
+// with an FP32 accumulator in tensor memory (128 lanes = tile rows, TC_BN
+// columns).  For every k-chunk of TC_BK elements each thread first issues its
+// TC_LOADS gathered FP64 loads of A and of B (the same offset tables as the
+// FP64 kernel), then -- once the MMAs that last read the stage have completed
+// -- splits each value into TF32 hi and lo parts (x = hi + lo, both rounded
+// to nearest) and stores them K-major with the 128-byte swizzle.  Thread 0
+// issues the tcgen05.mma instructions of the chunk (hi*hi, and for the split
+// form hi*lo and lo*hi as well) and commits them to the stage's mbarrier.  The
+// gather is software-pipelined: the loads of chunk c+1 are issued before chunk
+// c is converted, and run while the MMAs of chunk c execute.  The
+// epilogue reads the accumulator with tcgen05.ld (warp w reads TMEM lanes
+// 32(w%4).. and column half w/4) and writes alpha * acc as FP64.  Every wait
+// is bounded: on timeout the CTA records TT_ERR_TIMEOUT in the plan's status
+// word, drains what it issued (again bounded), frees its tensor memory and
+// returns.
+constexpr int TC_BM = 128;
+constexpr int TC_BN = 128;
+constexpr int TC_BK = 32;                        // fp32 elements = one 128-byte swizzle row
+constexpr int TC_THREADS = 256;
+constexpr int TC_LOADS = TC_BM * TC_BK / TC_THREADS;  // per operand and thread: 16
+constexpr int TC_A_BYTES = TC_BM * TC_BK * 4;    // 16 KB
+constexpr int TC_B_BYTES = TC_BN * TC_BK * 4;    // 16 KB
+constexpr int TC_STAGE_BYTES = 2 * TC_A_BYTES + 2 * TC_B_BYTES;  // hi and lo of A and B
+constexpr int TC_STAGES = 2;
+constexpr size_t TC_SMEM_BYTES = (size_t)TC_STAGES * TC_STAGE_BYTES + 1024;  // + alignment slack
+constexpr uint32_t TC_TMEM_COLS = TC_BN;         // FP32 accumulator: TC_BN columns x 128 lanes
+constexpr uint32_t TC_WAIT_LIMIT = 1u << 26;
+static_assert(TC_BM * TC_BK % TC_THREADS == 0 && TC_BN * TC_BK % TC_THREADS == 0, "tile / thread mismatch");
+static_assert(TC_BN == TC_BM, "the load mappings assume square tiles");
+
+// Instruction descriptor: D f32, A/B tf32, both K-major, N = TC_BN, M = TC_BM.
+constexpr uint32_t TC_IDESC = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(TC_BN >> 3) << 17) |
+                              ((uint32_t)(TC_BM >> 4) << 24);
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+// Shared-memory matrix descriptor, K-major with 128-byte swizzle: rows of 128
+// bytes, 8-row groups 1024 bytes apart (stride byte offset), version 1.
+__device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
+  uint64_t d = (uint64_t)((saddr >> 4) & 0x3FFFu);
+  d |= (uint64_t)1 << 16;              // leading byte offset (unused for swizzled K-major)
+  d |= (uint64_t)(1024 >> 4) << 32;    // stride byte offset
+  d |= (uint64_t)1 << 46;              // descriptor version
+  d |= (uint64_t)2 << 61;              // SWIZZLE_128B
+  return d;
+}
+
+// Byte offset of element (row r, k) in a K-major 128B-swizzled tile.
+__device__ __forceinline__ uint32_t sw128_off(int r, int k) {
+  return (uint32_t)((r >> 3) * 1024 + (r & 7) * 128 + ((((k >> 2) ^ (r & 7))) << 4) + (k & 3) * 4);
+}
+
+__device__ __forceinline__ void st_shared_u32(uint32_t addr, uint32_t v) {
+  asm volatile("st.shared.u32 [%0], %1;" ::"r"(addr), "r"(v));
+}
+
+__device__ __forceinline__ uint32_t to_tf32(float x) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+  return r;
+}
+
+// x -> TF32 hi (and lo = TF32(x - hi) for the split form) stored at addr / addr + lo_delta
+template <bool SPLIT>
+__device__ __forceinline__ void put_tf32(uint32_t addr, uint32_t lo_delta, double x) {
+  const uint32_t hi = to_tf32(__double2float_rn(x));
+  st_shared_u32(addr, hi);
+  if (SPLIT) st_shared_u32(addr + lo_delta, to_tf32(__double2float_rn(x - (double)__uint_as_float(hi))));
+}
+
+__device__ __forceinline__ void mbar_init(uint32_t addr, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(addr), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint32_t addr, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}\n"
+      : "=r"(ok)
+      : "r"(addr), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// bounded wait for the phase with the given parity; false on timeout
+__device__ __forceinline__ bool mbar_wait_bounded(uint32_t addr, uint32_t parity) {
+  for (uint32_t it = 0; it < TC_WAIT_LIMIT; ++it)
+    if (mbar_try_wait(addr, parity)) return true;
+  return false;
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+__device__ __forceinline__ void mma_tf32(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %3, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %4, p;\n\t}\n" ::"r"(tmem_d),
+      "l"(da), "l"(db), "r"(accumulate), "r"(TC_IDESC)
+      : "memory");
+}
+
+__device__ __forceinline__ void mma_commit(uint32_t mbar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(mbar)
+               : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int j = 0; j < 16; ++j) v[j] = __uint_as_float(r[j]);
+}
+
+template <bool SPLIT>
+__global__ void __launch_bounds__(TC_THREADS, 1)
+grouped_tc(const TaskDev* __restrict__ tasks, const OutDev* __restrict__ outs,
+           const PairDev* __restrict__ pairs, const int32_t* __restrict__ tab,
+           const double* __restrict__ A, const double* __restrict__ B,
+           double* __restrict__ C, double alpha, int* __restrict__ status) {
+  extern __shared__ uint8_t tc_smem_raw[];
+  __shared__ __align__(8) uint64_t mbar[TC_STAGES];
+  __shared__ uint32_t tmem_slot;
+  __shared__ int flag;  // 1 after a timeout
+  __shared__ int32_t rowA_s[TC_BM];
+  __shared__ int32_t colB_s[TC_BN];
+
+  const uint32_t sbase = (smem_u32(tc_smem_raw) + 1023u) & ~1023u;
+  const TaskDev task = tasks[blockIdx.x];
+  const OutDev out = outs[task.out];
+  const int tid = threadIdx.x;
+  const int warp = tid >> 5;
+  const int lane = tid & 31;
+
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_slot)),
+                 "r"(TC_TMEM_COLS)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  if (tid == 0) {
+    mbar_init(smem_u32(&mbar[0]), 1);
+    mbar_init(smem_u32(&mbar[1]), 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    flag = 0;
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = tmem_slot;
+
+  uint32_t phase[TC_STAGES] = {0, 0};
+  bool pending[TC_STAGES] = {false, false};
+  bool any_mma = false;
+  int gc = 0;  // chunk counter over all pairs of the task
+
+  for (int p = task.p_begin; p < task.p_end && !flag; ++p) {
+    const PairDev P = pairs[p];
+    __syncthreads();
+    if (tid < TC_BM) {
+      const int m = task.m0 + tid;
+      rowA_s[tid] = m < P.m ? tab[P.rowA + m] : 0;
+    } else if (tid - TC_BM < TC_BN) {
+      const int n = task.n0 + tid - TC_BM;
+      colB_s[tid - TC_BM] = n < P.n ? tab[P.colB + n] : 0;
+    }
+    __syncthreads();
+    const double* Ab = A + P.a_off;
+    const double* Bb = B + P.b_off;
+    const int K = P.k;
+    const int nchunks = (K + TC_BK - 1) / TC_BK;
+    // gathered FP64 loads of one chunk into registers
+    auto gather = [&](int c, double (&xa)[TC_LOADS], double (&xb)[TC_LOADS]) {
+      const int k0 = c * TC_BK;
+      if (P.a_mfast) {
+        const int m = tid & (TC_BM - 1);
+        const bool mok = task.m0 + m < P.m;
+        const int32_t rm = rowA_s[m];
+#pragma unroll
+        for (int i = 0; i < TC_LOADS; ++i) {
+          const int gk = k0 + (tid >> 7) + 2 * i;
+          xa[i] = (mok && gk < K) ? Ab[rm + tab[P.colA + gk]] : 0.0;
+        }
+      } else {
+        const int gk = k0 + lane;
+        const int32_t ck = gk < K ? tab[P.colA + gk] : 0;
+#pragma unroll
+        for (int i = 0; i < TC_LOADS; ++i) {
+          const int m = warp + 8 * i;
+          xa[i] = (task.m0 + m < P.m && gk < K) ? Ab[rowA_s[m] + ck] : 0.0;
+        }
+      }
+      if (P.b_kfast) {
+        const int gk = k0 + lane;
+        const int32_t rk = gk < K ? tab[P.rowB + gk] : 0;
+#pragma unroll
+        for (int i = 0; i < TC_LOADS; ++i) {
+          const int n = warp + 8 * i;
+          xb[i] = (task.n0 + n < P.n && gk < K) ? Bb[rk + colB_s[n]] : 0.0;
+        }
+      } else {
+        const int n = tid & (TC_BN - 1);
+        const bool nok = task.n0 + n < P.n;
+        const int32_t cn = colB_s[n];
+#pragma unroll
+        for (int i = 0; i < TC_LOADS; ++i) {
+          const int gk = k0 + (tid >> 7) + 2 * i;
+          xb[i] = (nok && gk < K) ? Bb[tab[P.rowB + gk] + cn] : 0.0;
+        }
+      }
+    };
+    double xa[TC_LOADS], xb[TC_LOADS], ya[TC_LOADS], yb[TC_LOADS];
+    gather(0, xa, xb);
+    for (int c = 0; c < nchunks; ++c, ++gc) {
+      const int s = gc & 1;
+      // 1. the next chunk's loads go out before this chunk is converted
+      if (c + 1 < nchunks) gather(c + 1, ya, yb);
+      // 2. the MMAs that last read this stage must have completed
+      if (pending[s]) {
+        if (tid == 0 && !mbar_wait_bounded(smem_u32(&mbar[s]), phase[s])) flag = 1;
+        __syncthreads();
+        phase[s] ^= 1;
+        pending[s] = false;
+        if (flag) break;
+      }
+      // 3. split and store (K-major, 128-byte swizzle)
+      const uint32_t a_hi = sbase + s * TC_STAGE_BYTES;
+      const uint32_t b_hi = a_hi + 2 * TC_A_BYTES;
+      if (P.a_mfast) {
+        const int m = tid & (TC_BM - 1);
+#pragma unroll
+        for (int i = 0; i < TC_LOADS; ++i)
+          put_tf32<SPLIT>(a_hi + sw128_off(m, (tid >> 7) + 2 * i), TC_A_BYTES, xa[i]);
+      } else {
+#pragma unroll
+        for (int i = 0; i < TC_LOADS; ++i) put_tf32<SPLIT>(a_hi + sw128_off(warp + 8 * i, lane), TC_A_BYTES, xa[i]);
+      }
+      if (P.b_kfast) {
+#pragma unroll
+        for (int i = 0; i < TC_LOADS; ++i) put_tf32<SPLIT>(b_hi + sw128_off(warp + 8 * i, lane), TC_B_BYTES, xb[i]);
+      } else {
+        const int n = tid & (TC_BN - 1);
+#pragma unroll
+        for (int i = 0; i < TC_LOADS; ++i)
+          put_tf32<SPLIT>(b_hi + sw128_off(n, (tid >> 7) + 2 * i), TC_B_BYTES, xb[i]);
+      }
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      __syncthreads();
+      // 4. one thread issues the chunk's MMAs
+      if (tid == 0) {
+        tc_fence_after();
+        const uint32_t ah = a_hi, al = a_hi + TC_A_BYTES, bh = b_hi, bl = b_hi + TC_B_BYTES;
+#pragma unroll
+        for (int kk = 0; kk < TC_BK / 8; ++kk) {  // K = 8 tf32 (32 bytes) per instruction
+          const uint32_t adv = 32u * kk;
+          if (SPLIT) {
+            mma_tf32(tmem, sw128_desc(al + adv), sw128_desc(bh + adv), any_mma || kk > 0 ? 1u : 0u);
+            mma_tf32(tmem, sw128_desc(ah + adv), sw128_desc(bl + adv), 1u);
+            mma_tf32(tmem, sw128_desc(ah + adv), sw128_desc(bh + adv), 1u);
+          } else {
+            mma_tf32(tmem, sw128_desc(ah + adv), sw128_desc(bh + adv), any_mma || kk > 0 ? 1u : 0u);
+          }
+        }
+        mma_commit(smem_u32(&mbar[s]));
+      }
+      pending[s] = true;
+      any_mma = true;
+#pragma unroll
+      for (int i = 0; i < TC_LOADS; ++i) {
+        xa[i] = ya[i];
+        xb[i] = yb[i];
+      }
+    }
+  }
+  // drain: every committed stage completes before TMEM is read or freed
+  for (int s = 0; s < TC_STAGES; ++s)
+    if (pending[s]) {
+      if (tid == 0 && !mbar_wait_bounded(smem_u32(&mbar[s]), phase[s])) flag = 1;
+      phase[s] ^= 1;
+    }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (flag) {
+    if (tid == 0) atomicExch(status, TT_ERR_TIMEOUT);
+  } else {
+    double* Cb = C + out.c_off;
+    const int quarter = warp & 3;         // TMEM lanes 32*quarter .. +31 = tile rows
+    const int col0 = (warp >> 2) * (TC_BN / 2);
+    const int m = task.m0 + quarter * 32 + lane;
+#pragma unroll
+    for (int c16 = 0; c16 < TC_BN / 32; ++c16) {
+      float v[16];
+      if (any_mma) {
+        tmem_ld16(tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(col0 + c16 * 16), v);
+      } else {
+#pragma unroll
+        for (int j = 0; j < 16; ++j) v[j] = 0.f;
+      }
+      if (m < out.m) {
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+          const int n = task.n0 + col0 + c16 * 16 + j;
+          if (n < out.n) Cb[m + (int64_t)out.ldc * n] = alpha * (double)v[j];
+        }
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TC_TMEM_COLS) : "memory");
+}
+
 }  // namespace
 
 struct tt_plan {
   int precision = TT_PREC_FP64;
+  int* d_status = nullptr;  // tensor-core path: TT_OK or TT_ERR_TIMEOUT
   int n_tasks = 0;
   int n_pairs = 0;
   int n_out = 0;
@@ -233,7 +563,10 @@ int tt_contract_plan(tt_ctx* ctx, const tt_out_block* outs, int n_out,
                      tt_plan** plan_out) {
   TT_REQUIRE(ctx && plan_out, "tt_contract_plan: null argument");
   TT_REQUIRE(n_out >= 0 && n_pairs >= 0, "tt_contract_plan: negative count");
-  TT_REQUIRE(precision == TT_PREC_FP64, "tt_contract_plan: unsupported precision");
+  TT_REQUIRE(precision == TT_PREC_FP64 || precision == TT_PREC_TF32 || precision == TT_PREC_TF32X3,
+             "tt_contract_plan: unsupported precision");
+  const bool tc = precision != TT_PREC_FP64;
+  const int tile_m = tc ? TC_BM : BM, tile_n = tc ? TC_BN : BN;
   *plan_out = nullptr;
   // pairs grouped by output block (stable: keeps the reference's accumulation order)
   std::vector<int> order(n_pairs);
@@ -305,8 +638,8 @@ int tt_contract_plan(tt_ctx* ctx, const tt_out_block* outs, int n_out,
   for (int o = 0; o < n_out; ++o) {
     TT_REQUIRE(outs[o].m >= 0 && outs[o].n >= 0 && outs[o].ldc >= outs[o].m,
                "tt_contract_plan: bad output block");
-    for (int m0 = 0; m0 < outs[o].m; m0 += BM)
-      for (int n0 = 0; n0 < outs[o].n; n0 += BN) {
+    for (int m0 = 0; m0 < outs[o].m; m0 += tile_m)
+      for (int n0 = 0; n0 < outs[o].n; n0 += tile_n) {
         TaskDev t{o, m0, n0, first[o], first[o + 1]};
         tasks.push_back(t);
         tcost.push_back(work[o] + 1);
@@ -330,13 +663,15 @@ int tt_contract_plan(tt_ctx* ctx, const tt_out_block* outs, int n_out,
   plan->d_outs = tt::pool_alloc<OutDev>(ctx, ho.size());
   plan->d_pairs = tt::pool_alloc<PairDev>(ctx, hp.size());
   plan->d_tab = tt::pool_alloc<int32_t>(ctx, (size_t)tab_len);
+  plan->d_status = tt::pool_alloc<int>(ctx, 1);
   TableJob* d_jobs = tt::pool_alloc<TableJob>(ctx, jobs.size());
-  if (!plan->d_tasks || !plan->d_outs || !plan->d_pairs || !plan->d_tab || !d_jobs) {
+  if (!plan->d_tasks || !plan->d_outs || !plan->d_pairs || !plan->d_tab || !plan->d_status || !d_jobs) {
     tt_plan_destroy(ctx, plan);
     tt::pool_free(ctx, d_jobs);
     return tt::fail(TT_ERR_OOM, "tt_contract_plan: device allocation failed");
   }
   cudaStream_t s = ctx->stream;
+  TT_CUDA(cudaMemsetAsync(plan->d_status, 0, sizeof(int), s));
   // staged copies: the host vectors may die at return without stalling the stream
   TT_CUDA(tt::h2d_async(ctx, plan->d_tasks, tsorted.data(), sizeof(TaskDev) * tsorted.size()));
   TT_CUDA(tt::h2d_async(ctx, plan->d_outs, ho.data(), sizeof(OutDev) * ho.size()));
@@ -359,10 +694,22 @@ int tt_contract_exec(tt_ctx* ctx, const tt_plan* plan, const double* A, const do
   if (!attr_set) {
     TT_CUDA(cudaFuncSetAttribute(grouped_dgemm, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)SMEM_BYTES));
+    TT_CUDA(cudaFuncSetAttribute(grouped_tc<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)TC_SMEM_BYTES));
+    TT_CUDA(cudaFuncSetAttribute(grouped_tc<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)TC_SMEM_BYTES));
     attr_set = true;
   }
-  grouped_dgemm<<<plan->n_tasks, THREADS, SMEM_BYTES, ctx->stream>>>(
-      plan->d_tasks, plan->d_outs, plan->d_pairs, plan->d_tab, A, B, C, alpha);
+  if (plan->precision == TT_PREC_FP64) {
+    grouped_dgemm<<<plan->n_tasks, THREADS, SMEM_BYTES, ctx->stream>>>(
+        plan->d_tasks, plan->d_outs, plan->d_pairs, plan->d_tab, A, B, C, alpha);
+  } else if (plan->precision == TT_PREC_TF32X3) {
+    grouped_tc<true><<<plan->n_tasks, TC_THREADS, TC_SMEM_BYTES, ctx->stream>>>(
+        plan->d_tasks, plan->d_outs, plan->d_pairs, plan->d_tab, A, B, C, alpha, plan->d_status);
+  } else {
+    grouped_tc<false><<<plan->n_tasks, TC_THREADS, TC_SMEM_BYTES, ctx->stream>>>(
+        plan->d_tasks, plan->d_outs, plan->d_pairs, plan->d_tab, A, B, C, alpha, plan->d_status);
+  }
   TT_LAUNCH_CHECK(ctx);
   return TT_OK;
 }
@@ -374,8 +721,18 @@ int tt_plan_destroy(tt_ctx* ctx, tt_plan* plan) {
     tt::pool_free(ctx, plan->d_outs);
     tt::pool_free(ctx, plan->d_pairs);
     tt::pool_free(ctx, plan->d_tab);
+    tt::pool_free(ctx, plan->d_status);
   }
   delete plan;
+  return TT_OK;
+}
+
+int tt_plan_device_status(tt_ctx* ctx, const tt_plan* plan, int* status) {
+  TT_REQUIRE(ctx && plan && status, "tt_plan_device_status: null argument");
+  int h = 0;
+  TT_CUDA(cudaMemcpyAsync(&h, plan->d_status, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  TT_CUDA(cudaStreamSynchronize(ctx->stream));
+  *status = h;
   return TT_OK;
 }
 

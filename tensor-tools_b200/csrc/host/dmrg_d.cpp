@@ -2,6 +2,7 @@
 // (reference lines in dmrg_d.h).  Every dense contraction is one grouped-GEMM
 // pair over strided modes; plans depend only on shapes and are cached.
 #include "dmrg_d.h"
+#include "observables.h"
 
 #include <algorithm>
 #include <cfloat>
@@ -55,8 +56,9 @@ int put_modes(const std::vector<Ax>& ax, int32_t* dims, int64_t* st1, int64_t* s
 // A plan for C(M x N) = A(M x K) B(K x N) with the given strided views; cached
 // by the complete pair description (dense blocks start at offset 0).
 std::shared_ptr<PlanHandle> dense_plan(const tt_block_pair& p, int64_t M, int64_t N, int64_t a_size,
-                                       int64_t b_size, int64_t ldc) {
+                                       int64_t b_size, int64_t ldc, int precision = TT_PREC_FP64) {
   std::vector<int64_t> key;
+  key.push_back(precision);
   key.push_back(M);
   key.push_back(N);
   key.push_back(ldc);
@@ -79,7 +81,7 @@ std::shared_ptr<PlanHandle> dense_plan(const tt_block_pair& p, int64_t M, int64_
   std::vector<tt_block_pair> pairs{p};
   validate_pairs(outs, pairs, a_size, b_size, ldc * std::max<int64_t>(N, 1));
   tt_plan* h = nullptr;
-  check(tt_contract_plan(ctx(), outs.data(), 1, pairs.data(), 1, TT_PREC_FP64, &h), "dense plan");
+  check(tt_contract_plan(ctx(), outs.data(), 1, pairs.data(), 1, precision, &h), "dense plan");
   auto ph = std::make_shared<PlanHandle>(h);
   if (cache.size() > 4096) cache.clear();
   cache[key] = ph;
@@ -264,7 +266,7 @@ dtensor operator*(const dtensor& A, const dtensor& B) {
   p.n_k = put_modes(km, p.k_dims, p.a_k_stride, p.b_k_stride);
   p.n_n = put_modes(nm, p.n_dims, p.b_n_stride, nullptr);
   dtensor C(cidx, false);
-  auto plan = dense_plan(p, M, N, A.size, B.size, std::max<int64_t>(M, 1));
+  auto plan = dense_plan(p, M, N, A.size, B.size, std::max<int64_t>(M, 1), rt().precision);
   check(tt_contract_exec(ctx(), plan->get(), A.data->get(), B.data->get(), C.data->get(), 1.0), "dense contract");
   return C;
 }
@@ -689,7 +691,15 @@ double dmrg(MPS& psi, MPO& H, int num_sweeps, const std::vector<int>& max_bd, co
         A.setRight(&TR[r]);
         dtensor x = psi.A[l] * psi.A[r];
         DavidsonStats st;
-        energy = tensor_davidson(A, x, 3, max_restart[lmr], 1e-12, 'S', &st);
+        {
+          PrecisionScope prec(rt().heff_precision);
+          energy = tensor_davidson(A, x, 3, max_restart[lmr], 1e-12, 'S', &st);
+        }
+        if (rt().heff_precision != TT_PREC_FP64 && half == 1 && i == L - 2) {
+          // mixed precision: the sweep's energy is the FP64 Rayleigh quotient
+          dtensor y = A.product(x);
+          energy = x.inner_product(y) / x.inner_product(x);
+        }
         dtensor_index mid;
         for (auto& ix : psi.A[l].idx_set)
           if (ix.name == psi.link_name(r)) { mid = ix; break; }
@@ -697,12 +707,21 @@ double dmrg(MPS& psi, MPO& H, int num_sweeps, const std::vector<int>& max_bd, co
         dsvd_bond(x, psi.A[l], psi.A[r], mid, S, direction, cutoff[lc], (unsigned long)max_bd[lbd]);
         psi.bond_dims[r] = (unsigned)S.size;
         psi.center = (int)(direction == MoveFromLeft ? r : l);
-        if (direction == MoveFromLeft)
-          TL[site + 1] = denv_step(TL[site], psi.A[site], H.A[site]);
-        else
-          TR[site - 1] = denv_step(TR[site], psi.A[site], H.A[site]);
+        {
+          PrecisionScope prec(rt().env_precision);
+          if (direction == MoveFromLeft)
+            TL[site + 1] = denv_step(TL[site], psi.A[site], H.A[site]);
+          else
+            TR[site - 1] = denv_step(TR[site], psi.A[site], H.A[site]);
+        }
         if (log) log->steps.push_back(DenseStepLog{(int)site, direction, st.matvecs, energy, (unsigned)S.size});
       }
+    }
+    if (rt().env_precision != TT_PREC_FP64) {
+      // mixed-precision environments bias the Ritz value to first order: the
+      // sweep energy is <psi|H|psi> / <psi|psi> contracted in FP64
+      PrecisionScope prec(TT_PREC_FP64);
+      energy = psiHphi(psi, H, psi) / psiphi(psi, psi);
     }
     if (log) {
       log->sweep_energy.push_back(energy);

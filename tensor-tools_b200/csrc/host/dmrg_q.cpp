@@ -1,6 +1,7 @@
 // big_qtensor, device-resident tensor_davidsonIT, qMPS/qMPO and the U(1)
 // two-site DMRG driver (see dmrg_q.h for the reference lines followed).
 #include "dmrg_q.h"
+#include "observables.h"
 
 #include <algorithm>
 #include <chrono>
@@ -184,12 +185,13 @@ class ProductEngine {
   }
 
   // y = H_eff * v on the whole layout (absent blocks of v are zero)
-  void apply(const double* v, double* y) {
-    if (c1_->plan) check(tt_contract_exec(ctx(), c1_->plan->get(), L_data(), v, i1_->get(), 1.0), "heff L*v");
-    if (c2_->plan)
-      check(tt_contract_exec(ctx(), c2_->plan->get(), i1_->get(), A_.mid().data->get(), i2_->get(), 1.0), "heff *mid");
-    if (c3_->plan)
-      check(tt_contract_exec(ctx(), c3_->plan->get(), i2_->get(), A_.right()->data->get(), y, 1.0), "heff *R");
+  void apply(const double* v, double* y, int precision = TT_PREC_FP64) {
+    if (tt_plan* p = c1_->plan_for(precision))
+      check(tt_contract_exec(ctx(), p, L_data(), v, i1_->get(), 1.0), "heff L*v");
+    if (tt_plan* p = c2_->plan_for(precision))
+      check(tt_contract_exec(ctx(), p, i1_->get(), A_.mid().data->get(), i2_->get(), 1.0), "heff *mid");
+    if (tt_plan* p = c3_->plan_for(precision))
+      check(tt_contract_exec(ctx(), p, i2_->get(), A_.right()->data->get(), y, 1.0), "heff *R");
     for (auto& r : zero_ranges_)
       check(tt_memset_zero(ctx(), y + r.first, sizeof(double) * (size_t)r.second), "heff zero");
   }
@@ -264,9 +266,9 @@ class ProductEngine {
 
   void build_plans(int64_t produced_size) {
     qtensor v = meta(Presence(ublocks.size(), 1));
-    c1_ = contract_cached(*A_.left(), v, true);
-    c2_ = contract_cached(c1_->cs.C, A_.mid(), true);
-    c3_ = contract_cached(c2_->cs.C, *A_.right(), true);
+    c1_ = contract_cached(*A_.left(), v, false);
+    c2_ = contract_cached(c1_->cs.C, A_.mid(), false);
+    c3_ = contract_cached(c2_->cs.C, *A_.right(), false);
     const qtensor& o = c3_->cs.C;
     for (unsigned i = 0; i < x_.rank; ++i)
       if (o.idx_set.size() != x_.rank || o.idx_set[i].level() != x_.idx_set[i].level() + 1 ||
@@ -334,7 +336,7 @@ double tensor_davidsonIT(big_qtensor& A, qtensor& x, int m, int max_restart, dou
     check(tt_event_create(ctx(), &e.first), "event");
     check(tt_event_create(ctx(), &e.second), "event");
     check(tt_event_record(ctx(), e.first), "event");
-    eng.apply(in.d->get(), out.d->get());
+    eng.apply(in.d->get(), out.d->get(), rt().heff_precision);
     check(tt_event_record(ctx(), e.second), "event");
     evs.push_back(e);
     ev_kept.push_back(true);
@@ -502,10 +504,19 @@ double tensor_davidsonIT(big_qtensor& A, qtensor& x, int m, int max_restart, dou
       M[k + l * (ni + 1)] = row[k];
     }
   }
+  const KVec& xfin = have_x ? xv : v[0];
   if (have_x) {
     x = eng.materialize(xv.p, xv.d);
   }
   x.normalize();  // synchronises: every recorded event has completed
+  if (rt().heff_precision != TT_PREC_FP64 && rt().energy_fp64) {
+    // mixed precision: the reported energy is the FP64 Rayleigh quotient of
+    // the final (normalised) vector, its error second order in the vector's
+    KVec y = newvec();
+    eng.apply(xfin.d->get(), y.d->get(), TT_PREC_FP64);
+    check(tt_vec_dot(ctx(), n, xfin.d->get(), y.d->get(), scalar_slot(0)), "fp64 energy");
+    lambda = read1(scalar_slot(0));
+  }
   double heff_ms = 0.0;
   for (size_t i = 0; i < evs.size(); ++i) {
     float ms = 0.f;
@@ -790,7 +801,8 @@ void updateSite(qMPS& psi, qMPO& H, std::vector<qtensor>& TR, std::vector<qtenso
 
 void updateEnv(qMPS& psi, qMPO& H, std::vector<qtensor>& TR, std::vector<qtensor>& TL, unsigned site,
                int direction) {
-  // algos/dmrg/dmrg.cpp:491-509
+  // algos/dmrg/dmrg.cpp:491-509; contractions at the environment precision
+  PrecisionScope prec(rt().env_precision);
   if (direction == MoveFromLeft)
     TL[site + 1] = env_step(TL[site], psi.A[site], H.A[site]);
   else
@@ -823,7 +835,10 @@ double dmrg_sweep(qMPS& psi, qMPO& H, DmrgState& st, int max_bd, double cutoff, 
     int direction = half == 0 ? MoveFromLeft : MoveFromRight;
     for (unsigned i = 0; i < L - 1; ++i) {
       unsigned site = direction == MoveFromLeft ? i : L - 1 - i;
+      // the sweep's energy (its last step) is evaluated in FP64 in mixed precision
+      rt().energy_fp64 = half == 1 && i == L - 2;
       updateSite(psi, H, st.TR, st.TL, site, energy, direction, max_bd, cutoff, 'S', 3, max_restart, log);
+      rt().energy_fp64 = false;
       auto te0 = std::chrono::steady_clock::now();
       updateEnv(psi, H, st.TR, st.TL, site, direction);
       if (log && !log->steps.empty()) {
@@ -834,6 +849,13 @@ double dmrg_sweep(qMPS& psi, qMPO& H, DmrgState& st, int max_bd, double cutoff, 
     }
   }
   psi.normalize();
+  if (rt().env_precision != TT_PREC_FP64) {
+    // environments built in mixed precision bias the Ritz value to first
+    // order in their error, while the state itself keeps FP64 quality: the
+    // sweep energy is <psi|H|psi> / <psi|psi> contracted in FP64
+    PrecisionScope prec(TT_PREC_FP64);
+    energy = psiHphi(psi, H, psi) / psiphi(psi, psi);
+  }
   check(tt_ctx_synchronize(ctx()), "sweep sync");
   auto t1 = std::chrono::steady_clock::now();
   if (log) {

@@ -664,11 +664,21 @@ std::shared_ptr<const CachedContraction> contract_cached(const qtensor& A, const
     cache().map[h].push_back(CacheEntry{std::move(key), val});
     cache().entries++;
   }
-  if (need_plan && !val->plan && !val->cs.outs.empty()) val->plan = make_plan(val->cs);
+  if (need_plan) val->plan_for(rt().precision);
   return val;
 }
 
-std::shared_ptr<PlanHandle> make_plan(const ContractStructure& cs) {
+tt_plan* CachedContraction::plan_for(int precision) const {
+  if (precision < 0 || precision > 2) throw std::runtime_error("plan_for: bad precision");
+  if (cs.outs.empty()) return nullptr;
+  if (!plans[precision]) plans[precision] = make_plan(cs, precision);
+  return plans[precision]->get();
+}
+
+PrecisionScope::PrecisionScope(int p) : saved(rt().precision) { rt().precision = p; }
+PrecisionScope::~PrecisionScope() { rt().precision = saved; }
+
+std::shared_ptr<PlanHandle> make_plan(const ContractStructure& cs, int precision) {
   auto t0 = std::chrono::steady_clock::now();
   struct Acc {
     std::chrono::steady_clock::time_point t0;
@@ -680,7 +690,7 @@ std::shared_ptr<PlanHandle> make_plan(const ContractStructure& cs) {
   validate_pairs(cs.outs, cs.pairs, cs.a_size, cs.b_size, cs.C.arena);
   tt_plan* p = nullptr;
   check(tt_contract_plan(ctx(), cs.outs.data(), (int)cs.outs.size(), cs.pairs.data(), (int)cs.pairs.size(),
-                         TT_PREC_FP64, &p),
+                         precision, &p),
         "contract plan");
   return std::make_shared<PlanHandle>(p);
 }
@@ -689,12 +699,11 @@ qtensor operator*(const qtensor& A, const qtensor& B) {
   if (!A._initted && !B._initted) throw std::runtime_error("operator*: both operands uninitialised");
   if (A._initted && !B._initted) return qtensor(A);
   if (B._initted && !A._initted) return qtensor(B);
-  auto cc = contract_cached(A, B, true);
+  auto cc = contract_cached(A, B, false);
   qtensor C = cc->cs.C;  // metadata only (C has no data yet)
   C.data = dev_alloc(C.arena);
-  if (cc->plan)
-    check(tt_contract_exec(ctx(), cc->plan->get(), A.data->get(), B.data->get(), C.data->get(), 1.0),
-          "contract exec");
+  if (tt_plan* p = cc->plan_for(rt().precision))
+    check(tt_contract_exec(ctx(), p, A.data->get(), B.data->get(), C.data->get(), 1.0), "contract exec");
   return C;
 }
 

@@ -39,6 +39,14 @@ struct Runtime {
   int64_t n_structure = 0, n_plan = 0;
   // plans of dense (single-block) contractions, keyed by their pair description
   std::map<std::vector<int64_t>, std::shared_ptr<class PlanHandle>> dense_plans;
+  // precision of qtensor operator* (TT_PREC_FP64 unless a mixed-precision sweep
+  // is updating environments); H_eff products take theirs from the sweep
+  int precision = TT_PREC_FP64;
+  // precisions of a DMRG sweep: H_eff*x in Davidson and the environment
+  // updates; GS, Rayleigh-Ritz and the SVD always run in FP64
+  int heff_precision = TT_PREC_FP64;
+  int env_precision = TT_PREC_FP64;
+  bool energy_fp64 = false;  // set by the sweep driver for its last step
 };
 Runtime& rt();
 // Bind / unbind the device context used by every host object on this thread.
@@ -226,8 +234,12 @@ void contract_structure(const qtensor& A, const qtensor& B, ContractStructure& o
 // dimensions settle, so steady-state sweeps plan nothing.
 struct CachedContraction {
   ContractStructure cs;
-  std::shared_ptr<class PlanHandle> plan;  // null when cs has no output blocks
+  // device plans by precision (TT_PREC_FP64 / TF32 / TF32X3), built on first
+  // use; null when cs has no output blocks
+  mutable std::shared_ptr<class PlanHandle> plans[3];
+  tt_plan* plan_for(int precision) const;
 };
+// need_plan builds the plan of rt().precision right away.
 std::shared_ptr<const CachedContraction> contract_cached(const qtensor& A, const qtensor& B,
                                                          bool need_plan);
 void clear_contraction_cache();
@@ -245,7 +257,14 @@ class PlanHandle {
  private:
   tt_plan* p_ = nullptr;
 };
-std::shared_ptr<PlanHandle> make_plan(const ContractStructure& cs);
+std::shared_ptr<PlanHandle> make_plan(const ContractStructure& cs, int precision = TT_PREC_FP64);
+
+// Scoped change of rt().precision, the precision of operator* contractions.
+struct PrecisionScope {
+  int saved;
+  explicit PrecisionScope(int p);
+  ~PrecisionScope();
+};
 
 // ---- block SVD (qtensor_op.cpp:1097-1544) ---------------------------------
 struct TruncInfo {

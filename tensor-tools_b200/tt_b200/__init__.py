@@ -34,6 +34,10 @@ class TTError(RuntimeError):
     pass
 
 
+TT_PREC_FP64, TT_PREC_TF32, TT_PREC_TF32X3 = 0, 1, 2
+PRECISIONS = {"fp64": TT_PREC_FP64, "tf32": TT_PREC_TF32, "tf32x3": TT_PREC_TF32X3}
+
+
 def _load():
     if not os.path.exists(LIB_PATH):
         raise ImportError("libtt_b200.so not built: run tensor-tools_b200/build.py (%s)" % LIB_PATH)
@@ -72,6 +76,8 @@ _proto("tt_ctx_launch_count", P, PI64)
 lib.tt_get_last_error.restype = C.c_char_p
 lib.tt_get_last_error.argtypes = []
 _proto("tt_dmrg_bind", P)
+_proto("tt_dmrg_set_precision", C.c_int, C.c_int, C.c_int)
+_proto("tt_plan_device_status", P, P, C.POINTER(C.c_int))
 _proto("tt_dmrg_unbind")
 _proto("tt_device_alloc", P, C.c_size_t, PP)
 _proto("tt_device_free", P, P)
@@ -790,3 +796,11 @@ def square_next_neighbor(Nx: int, Ny: int, yperiodic: bool = False):
 def triangular_lattice(Nx: int, Ny: int, yperiodic: bool = True):
     """triangularLattice (models/lattice/triangular.h:25-64)."""
     return _lattice(TT_LATTICE_TRIANGULAR, Nx, Ny, yperiodic)
+
+
+def set_precision(op: str = "fp64", heff: str = "fp64", env: str = "fp64"):
+    """Contraction precisions on this thread ("fp64", "tf32", "tf32x3"): op for
+    QTensor/dense contractions, heff for the Davidson H_eff*x products, env for
+    the environment updates.  The mixed form of the DMRG sweep is
+    set_precision(heff="tf32x3", env="tf32x3")."""
+    _chk(lib.tt_dmrg_set_precision(PRECISIONS[op], PRECISIONS[heff], PRECISIONS[env]), "set_precision")

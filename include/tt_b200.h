@@ -17,6 +17,8 @@
  *                                                       dtensor/dtensor.cpp:792-849
  *   tt_vec_fill_random       qtensor<T>::setRandom      qtensor/qtensor.cpp:381-388
  *   tt_vec_precondition      elemWiseDivide             linalg/tensor_davidson.cpp:25-36
+ *   tt_dav_*                 tensor_davidsonIT control  linalg/tensor_davidson.cpp:193-347,
+ *                            DIAG                       linalg/lapack_wrapper.cpp:40-54
  *   tt_sym_eig_batched       CTF Matrix::svd per QN sector (ScaLAPACK pdgesvd)
  *                                                       qtensor/qtensor_op.cpp:1269,
  *                                                       dtensor/dtensor_op.cpp:175
@@ -55,6 +57,7 @@ extern "C" {
                                  operands (hi*hi + hi*lo + lo*hi), FP32 accumulator */
 
 #define TT_MAX_MODES       6  /* tensor modes per GEMM dimension of a pair   */
+#define TT_DAV_MAX        16  /* Krylov vectors of the device-resident Davidson */
 
 typedef struct tt_ctx tt_ctx;
 typedef struct tt_plan tt_plan;
@@ -67,6 +70,9 @@ int tt_ctx_destroy(tt_ctx* ctx);
 int tt_ctx_synchronize(tt_ctx* ctx);
 /* cudaStream_t of the context, as an opaque pointer (for event timing). */
 int tt_ctx_stream(tt_ctx* ctx, void** stream);
+/* Host wall seconds spent blocked in synchronisations of this context's
+ * stream (device-to-host reads, tt_ctx_synchronize) and how many there were. */
+int tt_ctx_wait_stats(tt_ctx* ctx, double* seconds, int64_t* count);
 const char* tt_get_last_error(void);
 
 int tt_device_alloc(tt_ctx* ctx, size_t bytes, void** dptr);
@@ -174,6 +180,32 @@ int tt_vec_fill_random(tt_ctx* ctx, int64_t n, double* x, int nranges,
                        const int64_t* d_ranges, uint64_t seed);
 /* x[i] = x[i] / (D[i] - theta) where D[i] != theta. */
 int tt_vec_precondition(tt_ctx* ctx, int64_t n, double* x, const double* D, double theta);
+
+/* ---- device-resident Davidson control (tensor_davidsonIT) -----------------
+ * The decisions of the Davidson loop (linalg/tensor_davidson.cpp:193-347) run
+ * on the device so that a caller can enqueue every iteration without reading
+ * scalars back: tt_dav_begin takes the initial Rayleigh quotient, tt_dav_ritz
+ * diagonalises the projected matrix (DIAG: dsyev semantics, <= TT_DAV_MAX) and
+ * writes the Ritz coefficients (tt_dav_coefficients gives their device
+ * addresses, for tt_vec_lincomb_dev), tt_dav_converged applies the
+ * convergence test to the residual norm, tt_dav_add_row adds the new row of
+ * the projected matrix unless Gram-Schmidt failed (norm < 1e-10).  After the
+ * loop has ended every control call is a no-op; tt_dav_read synchronises and
+ * returns where it ended (final_ii, or -2 with fail_ii for a Gram-Schmidt
+ * failure that the caller finishes on the host). */
+typedef struct tt_dav_state tt_dav_state;
+typedef struct {
+  int done, final_ii, fail_ii, iters;
+  double lambda;
+} tt_dav_result;
+int tt_dav_state_create(tt_ctx* ctx, tt_dav_state** st);
+int tt_dav_state_destroy(tt_ctx* ctx, tt_dav_state* st);
+int tt_dav_coefficients(tt_dav_state* st, double** coef_x, double** coef_q);
+int tt_dav_begin(tt_ctx* ctx, tt_dav_state* st, const double* d_init_energy);
+int tt_dav_ritz(tt_ctx* ctx, tt_dav_state* st, int ii);
+int tt_dav_converged(tt_ctx* ctx, tt_dav_state* st, int ii, int maxiter, double tol, const double* d_qnorm);
+int tt_dav_add_row(tt_ctx* ctx, tt_dav_state* st, int ii, const double* d_row, const double* d_gsnorm);
+int tt_dav_read(tt_ctx* ctx, const tt_dav_state* st, tt_dav_result* out);
 
 /* ---- strided copies ------------------------------------------------------
  * dst[dst_off + sum_i j_i*dst_stride[i]] = src[src_off + sum_i j_i*src_stride[i]]

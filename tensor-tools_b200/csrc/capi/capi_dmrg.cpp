@@ -79,6 +79,15 @@ int tt_dmrg_bind(tt_ctx* ctx) {
 
 int tt_dmrg_unbind(void) { TT_GUARD(ttb::unbind_context()); }
 
+int tt_dmrg_set_profile_step(int step) { TT_GUARD(ttb::rt().profile_step = step); }
+
+int tt_dmrg_set_davidson(int device_control) { TT_GUARD(ttb::rt().dav_device = device_control != 0); }
+
+int tt_dmrg_davidson_fallbacks(int64_t* n) {
+  TT_ARG(n);
+  TT_GUARD(*n = ttb::rt().dav_fallbacks);
+}
+
 int tt_dmrg_set_precision(int op, int heff, int env) {
   auto ok = [](int p) { return p == TT_PREC_FP64 || p == TT_PREC_TF32 || p == TT_PREC_TF32X3; };
   TT_ARG(ok(op) && ok(heff) && ok(env));

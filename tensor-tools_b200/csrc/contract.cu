@@ -236,6 +236,7 @@ constexpr int TC_BN = 128;
 constexpr int TC_BK = 32;                        // fp32 elements = one 128-byte swizzle row
 constexpr int TC_THREADS = 256;
 constexpr int TC_LOADS = TC_BM * TC_BK / TC_THREADS;  // per operand and thread: 16
+constexpr int TC_QUADS = TC_LOADS / 4;                // 16-byte swizzle units per operand and thread
 constexpr int TC_A_BYTES = TC_BM * TC_BK * 4;    // 16 KB
 constexpr int TC_B_BYTES = TC_BN * TC_BK * 4;    // 16 KB
 constexpr int TC_STAGE_BYTES = 2 * TC_A_BYTES + 2 * TC_B_BYTES;  // hi and lo of A and B
@@ -270,8 +271,8 @@ __device__ __forceinline__ uint32_t sw128_off(int r, int k) {
   return (uint32_t)((r >> 3) * 1024 + (r & 7) * 128 + ((((k >> 2) ^ (r & 7))) << 4) + (k & 3) * 4);
 }
 
-__device__ __forceinline__ void st_shared_u32(uint32_t addr, uint32_t v) {
-  asm volatile("st.shared.u32 [%0], %1;" ::"r"(addr), "r"(v));
+__device__ __forceinline__ void st_shared_v4(uint32_t addr, uint32_t a, uint32_t b, uint32_t c, uint32_t d) {
+  asm volatile("st.shared.v4.u32 [%0], {%1, %2, %3, %4};" ::"r"(addr), "r"(a), "r"(b), "r"(c), "r"(d));
 }
 
 __device__ __forceinline__ uint32_t to_tf32(float x) {
@@ -280,12 +281,18 @@ __device__ __forceinline__ uint32_t to_tf32(float x) {
   return r;
 }
 
-// x -> TF32 hi (and lo = TF32(x - hi) for the split form) stored at addr / addr + lo_delta
+// four consecutive-k values -> TF32 hi (and lo = TF32(x - hi) for the split
+// form) as one 16-byte unit at addr (and addr + lo_delta)
 template <bool SPLIT>
-__device__ __forceinline__ void put_tf32(uint32_t addr, uint32_t lo_delta, double x) {
-  const uint32_t hi = to_tf32(__double2float_rn(x));
-  st_shared_u32(addr, hi);
-  if (SPLIT) st_shared_u32(addr + lo_delta, to_tf32(__double2float_rn(x - (double)__uint_as_float(hi))));
+__device__ __forceinline__ void put_quad(uint32_t addr, uint32_t lo_delta, const double (&x)[4]) {
+  uint32_t h[4], l[4];
+#pragma unroll
+  for (int e = 0; e < 4; ++e) {
+    h[e] = to_tf32(__double2float_rn(x[e]));
+    if (SPLIT) l[e] = to_tf32(__double2float_rn(x[e] - (double)__uint_as_float(h[e])));
+  }
+  st_shared_v4(addr, h[0], h[1], h[2], h[3]);
+  if (SPLIT) st_shared_v4(addr + lo_delta, l[0], l[1], l[2], l[3]);
 }
 
 __device__ __forceinline__ void mbar_init(uint32_t addr, uint32_t count) {
@@ -397,47 +404,38 @@ grouped_tc(const TaskDev* __restrict__ tasks, const OutDev* __restrict__ outs,
     const double* Bb = B + P.b_off;
     const int K = P.k;
     const int nchunks = (K + TC_BK - 1) / TC_BK;
-    // gathered FP64 loads of one chunk into registers
-    auto gather = [&](int c, double (&xa)[TC_LOADS], double (&xb)[TC_LOADS]) {
+    // Gathered FP64 loads of one chunk into registers.  A thread owns
+    // TC_QUADS quads (row r, k = 4q..4q+3): one 16-byte swizzle unit each.
+    //   unit-stride rows (A m-fast / B with n fast): r = tid % 128, q = tid / 128 + 2i
+    //   unit-stride k (A k-fast / B k-fast):          q = tid % 8,   r = tid / 8 + 32i
+    auto gather = [&](int c, double (&xa)[TC_QUADS][4], double (&xb)[TC_QUADS][4]) {
       const int k0 = c * TC_BK;
-      if (P.a_mfast) {
-        const int m = tid & (TC_BM - 1);
-        const bool mok = task.m0 + m < P.m;
-        const int32_t rm = rowA_s[m];
 #pragma unroll
-        for (int i = 0; i < TC_LOADS; ++i) {
-          const int gk = k0 + (tid >> 7) + 2 * i;
-          xa[i] = (mok && gk < K) ? Ab[rm + tab[P.colA + gk]] : 0.0;
-        }
-      } else {
-        const int gk = k0 + lane;
-        const int32_t ck = gk < K ? tab[P.colA + gk] : 0;
+      for (int i = 0; i < TC_QUADS; ++i) {
+        const int r = P.a_mfast ? (tid & (TC_BM - 1)) : ((tid >> 3) + 32 * i);
+        const int q = P.a_mfast ? ((tid >> 7) + 2 * i) : (tid & 7);
+        const bool rok = task.m0 + r < P.m;
+        const int32_t rr = rowA_s[r];
 #pragma unroll
-        for (int i = 0; i < TC_LOADS; ++i) {
-          const int m = warp + 8 * i;
-          xa[i] = (task.m0 + m < P.m && gk < K) ? Ab[rowA_s[m] + ck] : 0.0;
+        for (int e = 0; e < 4; ++e) {
+          const int gk = k0 + 4 * q + e;
+          xa[i][e] = (rok && gk < K) ? Ab[rr + tab[P.colA + gk]] : 0.0;
         }
       }
-      if (P.b_kfast) {
-        const int gk = k0 + lane;
-        const int32_t rk = gk < K ? tab[P.rowB + gk] : 0;
 #pragma unroll
-        for (int i = 0; i < TC_LOADS; ++i) {
-          const int n = warp + 8 * i;
-          xb[i] = (task.n0 + n < P.n && gk < K) ? Bb[rk + colB_s[n]] : 0.0;
-        }
-      } else {
-        const int n = tid & (TC_BN - 1);
-        const bool nok = task.n0 + n < P.n;
-        const int32_t cn = colB_s[n];
+      for (int i = 0; i < TC_QUADS; ++i) {
+        const int r = P.b_kfast ? ((tid >> 3) + 32 * i) : (tid & (TC_BN - 1));
+        const int q = P.b_kfast ? (tid & 7) : ((tid >> 7) + 2 * i);
+        const bool rok = task.n0 + r < P.n;
+        const int32_t cr = colB_s[r];
 #pragma unroll
-        for (int i = 0; i < TC_LOADS; ++i) {
-          const int gk = k0 + (tid >> 7) + 2 * i;
-          xb[i] = (nok && gk < K) ? Bb[tab[P.rowB + gk] + cn] : 0.0;
+        for (int e = 0; e < 4; ++e) {
+          const int gk = k0 + 4 * q + e;
+          xb[i][e] = (rok && gk < K) ? Bb[tab[P.rowB + gk] + cr] : 0.0;
         }
       }
     };
-    double xa[TC_LOADS], xb[TC_LOADS], ya[TC_LOADS], yb[TC_LOADS];
+    double xa[TC_QUADS][4], xb[TC_QUADS][4], ya[TC_QUADS][4], yb[TC_QUADS][4];
     gather(0, xa, xb);
     for (int c = 0; c < nchunks; ++c, ++gc) {
       const int s = gc & 1;
@@ -451,26 +449,20 @@ grouped_tc(const TaskDev* __restrict__ tasks, const OutDev* __restrict__ outs,
         pending[s] = false;
         if (flag) break;
       }
-      // 3. split and store (K-major, 128-byte swizzle)
+      // 3. split and store (K-major, 128-byte swizzle, one 16-byte unit per quad)
       const uint32_t a_hi = sbase + s * TC_STAGE_BYTES;
       const uint32_t b_hi = a_hi + 2 * TC_A_BYTES;
-      if (P.a_mfast) {
-        const int m = tid & (TC_BM - 1);
 #pragma unroll
-        for (int i = 0; i < TC_LOADS; ++i)
-          put_tf32<SPLIT>(a_hi + sw128_off(m, (tid >> 7) + 2 * i), TC_A_BYTES, xa[i]);
-      } else {
-#pragma unroll
-        for (int i = 0; i < TC_LOADS; ++i) put_tf32<SPLIT>(a_hi + sw128_off(warp + 8 * i, lane), TC_A_BYTES, xa[i]);
+      for (int i = 0; i < TC_QUADS; ++i) {
+        const int r = P.a_mfast ? (tid & (TC_BM - 1)) : ((tid >> 3) + 32 * i);
+        const int q = P.a_mfast ? ((tid >> 7) + 2 * i) : (tid & 7);
+        put_quad<SPLIT>(a_hi + sw128_off(r, 4 * q), TC_A_BYTES, xa[i]);
       }
-      if (P.b_kfast) {
 #pragma unroll
-        for (int i = 0; i < TC_LOADS; ++i) put_tf32<SPLIT>(b_hi + sw128_off(warp + 8 * i, lane), TC_B_BYTES, xb[i]);
-      } else {
-        const int n = tid & (TC_BN - 1);
-#pragma unroll
-        for (int i = 0; i < TC_LOADS; ++i)
-          put_tf32<SPLIT>(b_hi + sw128_off(n, (tid >> 7) + 2 * i), TC_B_BYTES, xb[i]);
+      for (int i = 0; i < TC_QUADS; ++i) {
+        const int r = P.b_kfast ? ((tid >> 3) + 32 * i) : (tid & (TC_BN - 1));
+        const int q = P.b_kfast ? (tid & 7) : ((tid >> 7) + 2 * i);
+        put_quad<SPLIT>(b_hi + sw128_off(r, 4 * q), TC_B_BYTES, xb[i]);
       }
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       __syncthreads();
@@ -494,10 +486,12 @@ grouped_tc(const TaskDev* __restrict__ tasks, const OutDev* __restrict__ outs,
       pending[s] = true;
       any_mma = true;
 #pragma unroll
-      for (int i = 0; i < TC_LOADS; ++i) {
-        xa[i] = ya[i];
-        xb[i] = yb[i];
-      }
+      for (int i = 0; i < TC_QUADS; ++i)
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          xa[i][e] = ya[i][e];
+          xb[i][e] = yb[i][e];
+        }
     }
   }
   // drain: every committed stage completes before TMEM is read or freed

@@ -2,6 +2,8 @@
 #include <cstring>
 #include <string>
 
+#include <chrono>
+
 #include "tt_internal.h"
 
 namespace tt {
@@ -54,6 +56,18 @@ cudaError_t h2d_async(tt_ctx* ctx, void* dst, const void* src, size_t bytes) {
 
 }  // namespace tt
 
+namespace {
+constexpr size_t kBounceBytes = (size_t)1 << 20;  // pinned bounce buffer for small reads
+
+cudaError_t timed_sync(tt_ctx* ctx) {
+  auto t0 = std::chrono::steady_clock::now();
+  cudaError_t e = cudaStreamSynchronize(ctx->stream);
+  ctx->wait_seconds += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  ctx->waits++;
+  return e;
+}
+}  // namespace
+
 extern "C" {
 
 const char* tt_get_last_error(void) { return tt::g_last_error.c_str(); }
@@ -77,7 +91,7 @@ int tt_ctx_create(int device, tt_ctx** out) {
   TT_CUDA(cudaDeviceGetDefaultMemPool(&ctx->pool, device));
   uint64_t thresh = UINT64_MAX;  // keep freed blocks cached in the pool
   TT_CUDA(cudaMemPoolSetAttribute(ctx->pool, cudaMemPoolAttrReleaseThreshold, &thresh));
-  TT_CUDA(cudaMallocHost(&ctx->h_scalars, 4096 * sizeof(double)));
+  TT_CUDA(cudaMallocHost(&ctx->h_scalars, kBounceBytes));
   ctx->stage_cap = (size_t)64 << 20;
   TT_CUDA(cudaMallocHost(&ctx->stage, ctx->stage_cap));
   if (!tt::partials(ctx, 16 * 4 * ctx->num_sms + 64)) {
@@ -100,9 +114,17 @@ int tt_ctx_destroy(tt_ctx* ctx) {
   return TT_OK;
 }
 
+
 int tt_ctx_synchronize(tt_ctx* ctx) {
   TT_REQUIRE(ctx, "null context");
-  TT_CUDA(cudaStreamSynchronize(ctx->stream));
+  TT_CUDA(timed_sync(ctx));
+  return TT_OK;
+}
+
+int tt_ctx_wait_stats(tt_ctx* ctx, double* seconds, int64_t* count) {
+  TT_REQUIRE(ctx, "null context");
+  if (seconds) *seconds = ctx->wait_seconds;
+  if (count) *count = ctx->waits;
   return TT_OK;
 }
 
@@ -174,8 +196,20 @@ int tt_memcpy_h2d(tt_ctx* ctx, void* dst, const void* src, size_t bytes) {
 int tt_memcpy_d2h(tt_ctx* ctx, void* dst, const void* src, size_t bytes) {
   TT_REQUIRE(ctx, "null context");
   if (bytes == 0) return TT_OK;
-  TT_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, ctx->stream));
-  TT_CUDA(cudaStreamSynchronize(ctx->stream));
+  if (bytes <= kBounceBytes) {
+    // small reads (Davidson scalars, SVD spectra) bounce through pinned memory:
+    // a copy into pageable memory is staged by the driver at a much higher cost
+    TT_CUDA(cudaMemcpyAsync(ctx->h_scalars, src, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+    TT_CUDA(timed_sync(ctx));
+    std::memcpy(dst, ctx->h_scalars, bytes);
+    return TT_OK;
+  }
+  auto t0 = std::chrono::steady_clock::now();
+  cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, ctx->stream);  // blocks if pageable
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  ctx->wait_seconds += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  ctx->waits++;
+  TT_CUDA(e);
   return TT_OK;
 }
 

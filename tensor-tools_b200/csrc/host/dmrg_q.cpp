@@ -3,6 +3,8 @@
 #include "dmrg_q.h"
 #include "observables.h"
 
+#include <cuda_profiler_api.h>
+
 #include <algorithm>
 #include <chrono>
 #include <cmath>
@@ -303,8 +305,167 @@ double read1(double* d) {
 }  // namespace
 
 // ---- tensor_davidsonIT -----------------------------------------------------
+// Device-resident form: every iteration is enqueued up front and the loop's
+// decisions run in the tt_dav_* control kernels, so the whole call
+// synchronises once.  Returns false (x untouched apart from its
+// normalisation) when Gram-Schmidt failed before the loop ended; the host
+// loop below then redoes the call, with its random refill.
+static bool davidson_device(big_qtensor& A, qtensor& x, int max_restart, double tol, DavidsonStats* stats,
+                            double& lambda_out) {
+  int maxsize = (int)A.size();
+  int actual_maxiter = std::min(max_restart, maxsize - 1);
+  if (actual_maxiter < 0 || actual_maxiter + 2 > TT_DAV_MAX || x.arena == 0) return false;
+  if (!rt().dav) check(tt_dav_state_create(ctx(), &rt().dav), "davidson state");
+  tt_dav_state* st = rt().dav;
+  double *coef_x = nullptr, *coef_q = nullptr;
+  check(tt_dav_coefficients(st, &coef_x, &coef_q), "davidson coefficients");
+  // x /= |x| on the device (tensor_davidson.cpp:205-206)
+  check(tt_vec_nrm2(ctx(), x.arena, x.data->get(), scalar_slot(0)), "norm");
+  check(tt_vec_scal_inv_dev(ctx(), x.arena, scalar_slot(0), x.data->get()), "normalize");
+  auto tb0 = std::chrono::steady_clock::now();
+  ProductEngine eng(A, x);
+  auto tb1 = std::chrono::steady_clock::now();
+  if (stats) stats->t_engine = std::chrono::duration<double>(tb1 - tb0).count();
+  const int64_t n = eng.n;
+  const int nsz = actual_maxiter + 2;
+  std::vector<KVec> v(nsz), va(nsz), xs(nsz);
+  auto newvec = [&]() {
+    KVec k;
+    k.d = dev_alloc(n);
+    return k;
+  };
+  auto por = [](Presence a, const Presence& b) {
+    for (size_t i = 0; i < a.size(); ++i) a[i] |= b[i];
+    return a;
+  };
+  std::vector<std::pair<void*, void*>> evs;
+  auto product = [&](const KVec& in) {
+    KVec out = newvec();
+    std::pair<void*, void*> e{nullptr, nullptr};
+    check(tt_event_create(ctx(), &e.first), "event");
+    check(tt_event_create(ctx(), &e.second), "event");
+    check(tt_event_record(ctx(), e.first), "event");
+    eng.apply(in.d->get(), out.d->get(), rt().heff_precision);
+    check(tt_event_record(ctx(), e.second), "event");
+    evs.push_back(e);
+    out.p = eng.product_presence(in.p);
+    return out;
+  };
+  auto lincomb = [&](KVec& y, const std::vector<const double*>& vs, const double* coef, double scale, int acc) {
+    check(tt_vec_lincomb_dev(ctx(), n, (int)vs.size(), vs.data(), coef, scale, acc, y.d->get()), "lincomb");
+  };
+  const int kQnormSlot = 24, kNormSlot = 20;
+  v[0] = newvec();
+  eng.pack(x, v[0].d->get());
+  v[0].p = eng.x_presence();
+  va[0] = product(v[0]);
+  {
+    const double* p0 = v[0].d->get();
+    check(tt_vec_multidot(ctx(), n, 1, &p0, va[0].d->get(), scalar_slot(0)), "initial energy");
+  }
+  check(tt_dav_begin(ctx(), st, scalar_slot(0)), "davidson begin");
+  for (int ii = 0; ii < actual_maxiter + 1; ++ii) {
+    const int ni = ii + 1;
+    KVec q = newvec();
+    if (ii == 0) {
+      lincomb(q, {va[0].d->get(), v[0].d->get()}, coef_q, 1.0, 0);
+      q.p = por(va[0].p, v[0].p);
+    } else {
+      check(tt_dav_ritz(ctx(), st, ii), "davidson ritz");
+      KVec xn = newvec();
+      std::vector<const double*> vv, vq;
+      Presence px(v[0].p.size(), 0), pq(v[0].p.size(), 0);
+      for (int k = 0; k <= ii; ++k) {
+        vv.push_back(v[k].d->get());
+        px = por(px, v[k].p);
+        vq.push_back(va[k].d->get());
+        pq = por(pq, va[k].p);
+      }
+      lincomb(xn, vv, coef_x, 1.0, 0);
+      xn.p = px;
+      vq.push_back(xn.d->get());
+      lincomb(q, vq, coef_q, 1.0, 0);
+      q.p = por(pq, px);
+      xs[ii] = xn;
+    }
+    check(tt_vec_nrm2(ctx(), n, q.d->get(), scalar_slot(kQnormSlot)), "residual norm");
+    check(tt_dav_converged(ctx(), st, ii, actual_maxiter, tol, scalar_slot(kQnormSlot)), "davidson test");
+    v[ni] = q;
+    if (ii == actual_maxiter) break;
+    // one Gram-Schmidt pass (:285-320) with device-side overlaps and norm
+    std::vector<const double*> vs;
+    for (int k = 0; k < ni; ++k) {
+      vs.push_back(v[k].d->get());
+      v[ni].p = por(v[ni].p, v[k].p);
+    }
+    check(tt_vec_multidot(ctx(), n, ni, vs.data(), v[ni].d->get(), scalar_slot(0)), "GS overlaps");
+    check(tt_vec_lincomb_dev(ctx(), n, ni, vs.data(), scalar_slot(0), -1.0, 1, v[ni].d->get()), "GS update");
+    check(tt_vec_nrm2(ctx(), n, v[ni].d->get(), scalar_slot(kNormSlot)), "GS norm");
+    check(tt_vec_scal_inv_dev(ctx(), n, scalar_slot(kNormSlot), v[ni].d->get()), "GS scale");
+    va[ni] = product(v[ni]);
+    vs.push_back(v[ni].d->get());
+    check(tt_vec_multidot(ctx(), n, ni + 1, vs.data(), va[ni].d->get(), scalar_slot(0)), "M row");
+    check(tt_dav_add_row(ctx(), st, ii, scalar_slot(0), scalar_slot(kNormSlot)), "davidson row");
+  }
+  tt_dav_result res;
+  check(tt_dav_read(ctx(), st, &res), "davidson read");  // the call's one synchronisation
+  if (res.final_ii == -2 || !res.done) {
+    for (auto& e : evs) {
+      tt_event_destroy(e.first);
+      tt_event_destroy(e.second);
+    }
+    return false;
+  }
+  const int f = res.final_ii;
+  if (f >= 1) x = eng.materialize(xs[f].p, xs[f].d);
+  x.normalize();
+  double heff_ms = 0.0;
+  for (size_t i = 0; i < evs.size(); ++i) {
+    if ((int)i <= f) {  // products of the iterations that ran: the initial one and f more
+      float ms = 0.f;
+      check(tt_event_elapsed_ms(evs[i].first, evs[i].second, &ms), "event");
+      heff_ms += ms;
+    }
+    tt_event_destroy(evs[i].first);
+    tt_event_destroy(evs[i].second);
+  }
+  rt().last_heff_ms = heff_ms;
+  double lambda = res.lambda;
+  if (rt().heff_precision != TT_PREC_FP64 && rt().energy_fp64) {
+    KVec y = newvec();
+    const KVec& xf = f >= 1 ? xs[f] : v[0];
+    eng.apply(xf.d->get(), y.d->get(), TT_PREC_FP64);
+    check(tt_vec_dot(ctx(), n, xf.d->get(), y.d->get(), scalar_slot(0)), "fp64 energy");
+    lambda = read1(scalar_slot(0));
+  }
+  if (stats) {
+    stats->matvecs = f + 1;
+    stats->heff_flops = (f + 1) * eng.flops;
+    stats->iters = res.iters;
+    stats->t_loop = std::chrono::duration<double>(std::chrono::steady_clock::now() - tb1).count();
+  }
+  lambda_out = lambda;
+  return true;
+}
+
+static double davidson_host(big_qtensor& A, qtensor& x, int m, int max_restart, double tol, char mode,
+                            DavidsonStats* stats);
+
 double tensor_davidsonIT(big_qtensor& A, qtensor& x, int m, int max_restart, double tol, char mode,
                          DavidsonStats* stats) {
+  if (!(m >= 1 && max_restart >= 1 && tol > 0)) throw std::runtime_error("tensor_davidsonIT: bad arguments");
+  if (rt().dav_device) {
+    double lambda = 0.0;
+    if (davidson_device(A, x, max_restart, tol, stats, lambda)) return lambda;
+    rt().dav_fallbacks++;
+    if (stats) *stats = DavidsonStats();
+  }
+  return davidson_host(A, x, m, max_restart, tol, mode, stats);
+}
+
+// Host-controlled form: the loop's decisions read scalars back every iteration.
+static double davidson_host(big_qtensor& A, qtensor& x, int m, int max_restart, double tol, char mode,
+                            DavidsonStats* stats) {
   (void)m;
   (void)mode;
   if (!(m >= 1 && max_restart >= 1 && tol > 0)) throw std::runtime_error("tensor_davidsonIT: bad arguments");
@@ -837,10 +998,16 @@ double dmrg_sweep(qMPS& psi, qMPO& H, DmrgState& st, int max_bd, double cutoff, 
       unsigned site = direction == MoveFromLeft ? i : L - 1 - i;
       // the sweep's energy (its last step) is evaluated in FP64 in mixed precision
       rt().energy_fp64 = half == 1 && i == L - 2;
+      const bool prof = rt().profile_step == (int)(half * (L - 1) + i);
+      if (prof) cudaProfilerStart();
       updateSite(psi, H, st.TR, st.TL, site, energy, direction, max_bd, cutoff, 'S', 3, max_restart, log);
       rt().energy_fp64 = false;
       auto te0 = std::chrono::steady_clock::now();
       updateEnv(psi, H, st.TR, st.TL, site, direction);
+      if (prof) {
+        check(tt_ctx_synchronize(ctx()), "sync");
+        cudaProfilerStop();
+      }
       if (log && !log->steps.empty()) {
         if (rt().profile) check(tt_ctx_synchronize(ctx()), "sync");
         log->steps.back().t_env =

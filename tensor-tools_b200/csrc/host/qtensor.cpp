@@ -23,10 +23,16 @@ void check(int status, const char* what) {
   }
 }
 
+static void drop_dav_state() {
+  if (rt().dav) tt_dav_state_destroy(rt().ctx, rt().dav);
+  rt().dav = nullptr;
+}
+
 void bind_context(tt_ctx* c) {
   clear_contraction_cache();  // cached plans belong to the previous context
   rt().dense_plans.clear();
   rt().scalars.reset();
+  drop_dav_state();
   rt().ctx = c;
   if (c) rt().scalars = std::make_shared<DevBuf>(kScalarSlots);
 }
@@ -34,6 +40,7 @@ void unbind_context() {
   clear_contraction_cache();
   rt().dense_plans.clear();
   rt().scalars.reset();
+  drop_dav_state();
   rt().ctx = nullptr;
 }
 double* scalar_slot(int i) { return rt().scalars->get() + i; }

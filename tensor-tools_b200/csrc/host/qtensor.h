@@ -47,6 +47,11 @@ struct Runtime {
   int heff_precision = TT_PREC_FP64;
   int env_precision = TT_PREC_FP64;
   bool energy_fp64 = false;  // set by the sweep driver for its last step
+  // device-resident Davidson control state (created on first use)
+  ::tt_dav_state* dav = nullptr;
+  bool dav_device = true;    // run tensor_davidsonIT's control on the device
+  int64_t dav_fallbacks = 0; // Gram-Schmidt failures finished by the host loop
+  int profile_step = -1;      // two-site step of a sweep bracketed by the CUDA profiler range
 };
 Runtime& rt();
 // Bind / unbind the device context used by every host object on this thread.

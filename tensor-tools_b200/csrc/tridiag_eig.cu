@@ -15,6 +15,7 @@
 //   (gap <= 1e-3 ||T||, the clustering rule of LAPACK's inverse iteration);
 //   back-transformation z = Q y with the stored reflectors.
 // The matrix sits in shared memory when n <= 160, otherwise in global memory.
+#include <algorithm>
 #include <cfloat>
 #include <cmath>
 #include <vector>
@@ -264,7 +265,8 @@ __device__ __forceinline__ double hash_unit(uint64_t z) {
 
 __global__ void __launch_bounds__(TT)
 tridiag_eigvecs(const EigDev* __restrict__ probs, const double* G, const double* Tg, const double* W, double* Zg,
-                double* work, const double* Amat) {
+                double* work, const double* Amat, int smem_cap) {
+  extern __shared__ double zsm[];  // n*nvec eigenvector block + n reflector, when they fit
   __shared__ double red[33];
   __shared__ double coef[MAX_N / 2];
   __shared__ int cstart[MAX_N / 2];
@@ -272,8 +274,13 @@ tridiag_eigvecs(const EigDev* __restrict__ probs, const double* G, const double*
   const int n = P.n, nvec = P.nvec;
   const int tid = threadIdx.x;
   if (n <= 0 || nvec <= 0) return;
-  double* Z = Zg + P.g_off;  // n x nvec, leading dimension n
+  double* Zout = Zg + P.g_off;  // n x nvec, leading dimension n
+  // the iterations run on a shared-memory copy when it fits
+  const bool in_smem = (int64_t)n * nvec + n <= (int64_t)smem_cap;
+  double* Z = in_smem ? zsm : Zout;
+  double* vk = in_smem ? zsm + (int64_t)n * nvec : nullptr;
   if (P.flags & TT_EIG_ROW_1X2) {
+    Z = Zout;
     if (tid == 0) {
       double a = Amat[P.a_off], b = Amat[P.a_off + 1];
       double dd = sqrt(a * a + b * b), z0, z1;
@@ -379,10 +386,16 @@ tridiag_eigvecs(const EigDev* __restrict__ probs, const double* G, const double*
     if (tk == 0.0) continue;
     const int m = n - k - 1;
     const int warp = tid >> 5, lane = tid & 31, nw = blockDim.x >> 5;
+    const double* refl = Gp + (k + 1) + (int64_t)n * k;  // v[1:] = refl[1:], v[0] = 1
+    if (vk) {
+      for (int i = tid; i < m; i += blockDim.x) vk[i] = (i == 0) ? 1.0 : refl[i];
+      __syncthreads();
+      refl = vk;
+    }
     for (int j = warp; j < nvec; j += nw) {
       const double* y = Z + (int64_t)n * j + (k + 1);
       double s = (lane == 0) ? y[0] : 0.0;  // v_0 = 1
-      for (int i = 1 + lane; i < m; i += 32) s += Gp[(k + 1 + i) + (int64_t)n * k] * y[i];
+      for (int i = 1 + lane; i < m; i += 32) s += refl[i] * y[i];
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
       if (lane == 0) coef[j] = tk * s;
@@ -390,7 +403,7 @@ tridiag_eigvecs(const EigDev* __restrict__ probs, const double* G, const double*
     __syncthreads();
     for (int el = tid; el < m * nvec; el += blockDim.x) {
       int i = el % m, j = el / m;
-      double vi = (i == 0) ? 1.0 : Gp[(k + 1 + i) + (int64_t)n * k];
+      double vi = (i == 0) ? 1.0 : refl[i];
       Z[(int64_t)n * j + k + 1 + i] -= vi * coef[j];
     }
     __syncthreads();
@@ -404,6 +417,10 @@ tridiag_eigvecs(const EigDev* __restrict__ probs, const double* G, const double*
     if (y[imax] < 0.0)
       for (int i = 0; i < n; ++i) y[i] = -y[i];
   }
+  if (in_smem) {
+    __syncthreads();
+    for (int64_t i = tid; i < (int64_t)n * nvec; i += blockDim.x) Zout[i] = Z[i];
+  }
 }
 
 std::vector<EigDev> to_dev(const tt_eig_problem* probs, int n_probs, const int* nvec) {
@@ -415,6 +432,7 @@ std::vector<EigDev> to_dev(const tt_eig_problem* probs, int n_probs, const int* 
 }
 
 size_t vals_smem() { return sizeof(double) * ((size_t)SM_N * SM_N + 4 * (size_t)SM_N); }
+constexpr int64_t kVecsSmemCap = 25 * 1024;  // doubles (200 KB) of eigenvectors + reflector in shared memory
 
 }  // namespace
 
@@ -460,7 +478,19 @@ int tt_sym_eigvecs_batched(tt_ctx* ctx, const tt_eig_problem* probs, int n_probs
   EigDev* dp = tt::pool_alloc<EigDev>(ctx, n_probs);
   if (!dp) return tt::fail(TT_ERR_OOM, "tt_sym_eigvecs_batched: allocation failed");
   TT_CUDA(tt::h2d_async(ctx, dp, hp.data(), sizeof(EigDev) * n_probs));
-  tridiag_eigvecs<<<n_probs, TT, 0, ctx->stream>>>(dp, G, T, w, Z, work, A);
+  // shared memory for the largest problem that fits (the others iterate in global memory)
+  int64_t need = 0;
+  for (int i = 0; i < n_probs; ++i) {
+    int64_t q = (int64_t)probs[i].n * nvec[i] + probs[i].n;
+    if (q <= kVecsSmemCap) need = std::max(need, q);
+  }
+  static bool attr = false;
+  if (!attr) {
+    TT_CUDA(cudaFuncSetAttribute(tridiag_eigvecs, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)(sizeof(double) * kVecsSmemCap)));
+    attr = true;
+  }
+  tridiag_eigvecs<<<n_probs, TT, sizeof(double) * (size_t)need, ctx->stream>>>(dp, G, T, w, Z, work, A, (int)need);
   TT_LAUNCH_CHECK(ctx);
   tt::pool_free(ctx, dp);
   return TT_OK;

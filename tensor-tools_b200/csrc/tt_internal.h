@@ -25,6 +25,9 @@ struct tt_ctx {
   char* stage = nullptr;
   size_t stage_cap = 0;
   size_t stage_head = 0;
+  // host wall time spent blocked in stream synchronisations, and their count
+  double wait_seconds = 0.0;
+  int64_t waits = 0;
 };
 
 namespace tt {

@@ -72,11 +72,15 @@ _proto("tt_ctx_create", C.c_int, PP)
 _proto("tt_ctx_destroy", P)
 _proto("tt_ctx_synchronize", P)
 _proto("tt_ctx_stream", P, PP)
+_proto("tt_ctx_wait_stats", P, PD, PI64)
 _proto("tt_ctx_launch_count", P, PI64)
 lib.tt_get_last_error.restype = C.c_char_p
 lib.tt_get_last_error.argtypes = []
 _proto("tt_dmrg_bind", P)
 _proto("tt_dmrg_set_precision", C.c_int, C.c_int, C.c_int)
+_proto("tt_dmrg_set_davidson", C.c_int)
+_proto("tt_dmrg_set_profile_step", C.c_int)
+_proto("tt_dmrg_davidson_fallbacks", PI64)
 _proto("tt_plan_device_status", P, P, C.POINTER(C.c_int))
 _proto("tt_dmrg_unbind")
 _proto("tt_device_alloc", P, C.c_size_t, PP)
@@ -207,6 +211,12 @@ class Context:
         s = P()
         _chk(lib.tt_ctx_stream(self.h, C.byref(s)), "stream")
         return s.value or 0
+
+    def wait_stats(self):
+        """(host seconds blocked in stream synchronisations, number of them)."""
+        s, n = D(), I64()
+        _chk(lib.tt_ctx_wait_stats(self.h, C.byref(s), C.byref(n)), "wait stats")
+        return s.value, n.value
 
     def launches(self) -> int:
         n = I64()
@@ -804,3 +814,15 @@ def set_precision(op: str = "fp64", heff: str = "fp64", env: str = "fp64"):
     the environment updates.  The mixed form of the DMRG sweep is
     set_precision(heff="tf32x3", env="tf32x3")."""
     _chk(lib.tt_dmrg_set_precision(PRECISIONS[op], PRECISIONS[heff], PRECISIONS[env]), "set_precision")
+
+
+def set_davidson_control(device: bool = True):
+    """tensor_davidsonIT control on the device (one synchronisation per call,
+    host loop on Gram-Schmidt failure) or on the host (reads back every iteration)."""
+    _chk(lib.tt_dmrg_set_davidson(int(device)), "set_davidson")
+
+
+def davidson_fallbacks() -> int:
+    n = I64()
+    _chk(lib.tt_dmrg_davidson_fallbacks(C.byref(n)), "davidson_fallbacks")
+    return n.value

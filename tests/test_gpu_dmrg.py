@@ -65,3 +65,28 @@ def test_dmrg_heisenberg_matches_ed(ctx):
     assert gpsi.center() == 0
     st = run.stats()
     assert st["heff_flops"] > 0 and st["heff_seconds"] > 0
+
+
+def test_device_and_host_davidson_control_agree(ctx):
+    """The device-resident Davidson control (one synchronisation per call) and
+    the host loop run the same algorithm: same kept states per sector at every
+    step, energies within round-off."""
+    import tt_b200
+    L = 12
+    h = list(np.random.default_rng(23).uniform(-0.1, 0.1, L))
+    sched = ([8, 16, 32, 32, 32], [1e-10], [6])
+    out = {}
+    for mode in (False, True):
+        tt_b200.set_davidson_control(mode)
+        try:
+            psi = tt_b200.QMPS(L, qdmrg.neel(L))
+            run = tt_b200.QDMRG(psi, tt_b200.QMPO(L, dh=h))
+            e = run.run(5, *sched)
+            out[mode] = (e, [(s["kept"], s["sectors"]) for s in run.steps()], [s["energy"] for s in run.steps()])
+        finally:
+            tt_b200.set_davidson_control(True)
+    (eh, kh, sh), (ed_, kd, sd) = out[False], out[True]
+    assert abs(eh - ed_) <= 1e-12 * abs(eh)
+    assert kh == kd
+    for a, b in zip(sh, sd):
+        assert abs(a - b) <= 1e-10 * abs(a)

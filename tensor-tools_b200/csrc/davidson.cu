@@ -30,66 +30,108 @@ struct tt_dav_state {
 
 namespace {
 
-// DIAG (linalg/lapack_wrapper.cpp:40-54, dsyev semantics): cyclic Jacobi on
-// the n x n column-major A (overwritten), eigenvalues ascending in ev,
-// eigenvectors in the columns of M.  Same rotation order and stopping rule as
-// the host DIAG.
-__device__ void dav_diag(int n, double* M, double* ev) {
-  // working copies in shared memory (local arrays would live in slow local memory)
+// DIAG (linalg/lapack_wrapper.cpp:40-54, dsyev semantics) for one warp:
+// parallel cyclic Jacobi with the round-robin ordering (every round rotates
+// n/2 disjoint index pairs at once; Golub & Van Loan, "Matrix Computations",
+// 4th ed., sec. 8.5.5), stopping when the off-diagonal mass falls below
+// 1e-32 of the total, as the host DIAG does.  Eigenvalues ascending in ev,
+// eigenvectors in the columns of M (column-major, n x n).  All 32 lanes call it.
+__device__ void dav_diag_warp(int n, double* M, double* ev) {
   __shared__ double A[TT_DAV_MAX * TT_DAV_MAX], V[TT_DAV_MAX * TT_DAV_MAX];
-  for (int i = 0; i < n * n; ++i) {
+  __shared__ double cs[TT_DAV_MAX / 2], sn[TT_DAV_MAX / 2];
+  __shared__ int pp[TT_DAV_MAX / 2], qq[TT_DAV_MAX / 2];
+  __shared__ int order[TT_DAV_MAX];
+  const int lane = threadIdx.x & 31;
+  for (int i = lane; i < n * n; i += 32) {
     A[i] = M[i];
-    V[i] = 0.0;
+    V[i] = (i % n == i / n) ? 1.0 : 0.0;
   }
-  for (int i = 0; i < n; ++i) V[i + n * i] = 1.0;
+  __syncwarp();
+  const int N = n + (n & 1);  // even number of players; index n is a bye when n is odd
+  const int npair = N / 2;
   for (int sweep = 0; sweep < 100; ++sweep) {
     double off = 0.0, fro = 0.0;
-    for (int j = 0; j < n; ++j)
-      for (int i = 0; i < n; ++i) {
-        fro += A[i + n * j] * A[i + n * j];
-        if (i != j) off += A[i + n * j] * A[i + n * j];
-      }
-    if (off <= 1e-32 * fro || off == 0.0) break;
-    for (int p = 0; p < n - 1; ++p)
-      for (int q = p + 1; q < n; ++q) {
-        const double apq = A[p + n * q];
-        if (apq == 0.0) continue;
-        const double tau = (A[q + n * q] - A[p + n * p]) / (2.0 * apq);
-        const double t = (tau >= 0.0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
-        const double c = 1.0 / sqrt(1.0 + t * t), s = t * c;
-        for (int k = 0; k < n; ++k) {
-          const double akp = A[k + n * p], akq = A[k + n * q];
-          A[k + n * p] = c * akp - s * akq;
-          A[k + n * q] = s * akp + c * akq;
-        }
-        for (int k = 0; k < n; ++k) {
-          const double apk = A[p + n * k], aqk = A[q + n * k];
-          A[p + n * k] = c * apk - s * aqk;
-          A[q + n * k] = s * apk + c * aqk;
-        }
-        A[p + n * q] = A[q + n * p] = 0.0;
-        for (int k = 0; k < n; ++k) {
-          const double vkp = V[k + n * p], vkq = V[k + n * q];
-          V[k + n * p] = c * vkp - s * vkq;
-          V[k + n * q] = s * vkp + c * vkq;
-        }
-      }
-  }
-  int order[TT_DAV_MAX];
-  for (int i = 0; i < n; ++i) order[i] = i;
-  for (int i = 1; i < n; ++i) {  // stable insertion sort by eigenvalue
-    const int o = order[i];
-    int j = i - 1;
-    while (j >= 0 && A[order[j] + n * order[j]] > A[o + n * o]) {
-      order[j + 1] = order[j];
-      --j;
+    for (int i = lane; i < n * n; i += 32) {
+      const double a2 = A[i] * A[i];
+      fro += a2;
+      if (i % n != i / n) off += a2;
     }
-    order[j + 1] = o;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      off += __shfl_down_sync(0xffffffffu, off, o);
+      fro += __shfl_down_sync(0xffffffffu, fro, o);
+    }
+    off = __shfl_sync(0xffffffffu, off, 0);  // lane 0's sums decide for the whole warp
+    fro = __shfl_sync(0xffffffffu, fro, 0);
+    if (off <= 1e-32 * fro || off == 0.0) break;
+    for (int r = 0; r < N - 1; ++r) {
+      if (lane < npair) {
+        // round-robin: player 0 fixed, the others rotate by r
+        auto player = [&](int i) { return i == 0 ? 0 : ((i - 1 + r) % (N - 1)) + 1; };
+        int a = player(lane), b = player(N - 1 - lane);
+        int p = a < b ? a : b, q = a < b ? b : a;
+        double c = 1.0, sv = 0.0;
+        if (q < n) {
+          const double apq = A[p + n * q];
+          if (apq != 0.0) {
+            const double tau = (A[q + n * q] - A[p + n * p]) / (2.0 * apq);
+            const double t = (tau >= 0.0 ? 1.0 : -1.0) / (fabs(tau) + sqrt(1.0 + tau * tau));
+            c = 1.0 / sqrt(1.0 + t * t);
+            sv = t * c;
+          }
+        } else {
+          q = p;  // bye: identity rotation
+        }
+        pp[lane] = p;
+        qq[lane] = q;
+        cs[lane] = c;
+        sn[lane] = sv;
+      }
+      __syncwarp();
+      // A <- A J and V <- V J (columns p, q of every pair), then A <- J^T A (rows)
+      for (int it = lane; it < npair * n; it += 32) {
+        const int t = it / n, k = it % n;
+        const int p = pp[t], q = qq[t];
+        if (p == q || sn[t] == 0.0) continue;
+        const double c = cs[t], sv = sn[t];
+        const double akp = A[k + n * p], akq = A[k + n * q];
+        A[k + n * p] = c * akp - sv * akq;
+        A[k + n * q] = sv * akp + c * akq;
+        const double vkp = V[k + n * p], vkq = V[k + n * q];
+        V[k + n * p] = c * vkp - sv * vkq;
+        V[k + n * q] = sv * vkp + c * vkq;
+      }
+      __syncwarp();
+      for (int it = lane; it < npair * n; it += 32) {
+        const int t = it / n, k = it % n;
+        const int p = pp[t], q = qq[t];
+        if (p == q || sn[t] == 0.0) continue;
+        const double c = cs[t], sv = sn[t];
+        const double apk = A[p + n * k], aqk = A[q + n * k];
+        A[p + n * k] = c * apk - sv * aqk;
+        A[q + n * k] = sv * apk + c * aqk;
+      }
+      __syncwarp();
+      if (lane < npair && pp[lane] != qq[lane] && sn[lane] != 0.0) A[pp[lane] + n * qq[lane]] = A[qq[lane] + n * pp[lane]] = 0.0;
+      __syncwarp();
+    }
   }
-  for (int j = 0; j < n; ++j) {
-    ev[j] = A[order[j] + n * order[j]];
-    for (int i = 0; i < n; ++i) M[i + n * j] = V[i + n * order[j]];
+  if (lane == 0) {  // stable insertion sort by eigenvalue
+    for (int i = 0; i < n; ++i) order[i] = i;
+    for (int i = 1; i < n; ++i) {
+      const int o = order[i];
+      int j = i - 1;
+      while (j >= 0 && A[order[j] + n * order[j]] > A[o + n * o]) {
+        order[j + 1] = order[j];
+        --j;
+      }
+      order[j + 1] = o;
+    }
   }
+  __syncwarp();
+  for (int j = lane; j < n; j += 32) ev[j] = A[order[j] + n * order[j]];
+  for (int i = lane; i < n * n; i += 32) M[i] = V[(i % n) + n * order[i / n]];
+  __syncwarp();
 }
 
 __global__ void dav_begin_kernel(tt_dav_state* st, const double* init_en) {
@@ -109,24 +151,30 @@ __global__ void dav_begin_kernel(tt_dav_state* st, const double* init_en) {
 }
 
 __global__ void dav_ritz_kernel(tt_dav_state* st, int ii) {
-  if (threadIdx.x != 0 || st->done) return;
+  if (st->done) return;  // uniform: read before anything is written
+  const int lane = threadIdx.x & 31;
   const int ni = ii + 1;
   double* M = st->buf[st->cur];
   double* Mn = st->buf[1 - st->cur];
-  for (int mi = 0; mi < ni; ++mi)
-    for (int mj = 0; mj <= mi; ++mj) {
+  for (int e = lane; e < ni * ni; e += 32) {
+    const int mi = e / ni, mj = e % ni;
+    if (mj <= mi) {
       Mn[mj + mi * (ni + 1)] = M[mj + mi * ni];
       Mn[mi + mj * (ni + 1)] = M[mi + mj * ni];
     }
-  dav_diag(ni, M, st->evals);
-  const double lam = st->evals[0];
-  st->lambda = lam;
-  const double sgn = (M[0] < 0.0) ? -1.0 : 1.0;  // sign stabilisation (:265-268)
-  for (int k = 0; k <= ii; ++k) {
-    st->coef_x[k] = sgn * M[k];
-    st->coef_q[k] = sgn * M[k];
   }
-  st->coef_q[ii + 1] = -lam;
+  __syncwarp();
+  dav_diag_warp(ni, M, st->evals);
+  if (lane == 0) {
+    const double lam = st->evals[0];
+    st->lambda = lam;
+    const double sgn = (M[0] < 0.0) ? -1.0 : 1.0;  // sign stabilisation (:265-268)
+    for (int k = 0; k <= ii; ++k) {
+      st->coef_x[k] = sgn * M[k];
+      st->coef_q[k] = sgn * M[k];
+    }
+    st->coef_q[ii + 1] = -lam;
+  }
 }
 
 __global__ void dav_conv_kernel(tt_dav_state* st, int ii, int maxiter, double tol, const double* qnorm) {

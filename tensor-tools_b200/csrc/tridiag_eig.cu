@@ -192,13 +192,41 @@ tridiag_eigvals(const EigDev* __restrict__ probs, double* G, double* Tg, double*
     for (int j = tid; j < n; j += blockDim.x) Wp[j] = 0.0;
     return;
   }
-  for (int j = tid; j < n; j += blockDim.x) {  // j-th smallest eigenvalue
+  // Bisection for the j-th smallest eigenvalue, two levels per round: three
+  // lanes of a group evaluate the Sturm count at the midpoint and at the
+  // midpoints of both halves, so a round takes the same two steps (same
+  // points, same tests) as two rounds of plain bisection.
+  auto open_interval = [&](double lo, double hi) {
+    return hi - lo > fmax(atol, 2.0 * DBL_EPSILON * fmax(fabs(lo), fabs(hi)));
+  };
+  const int lane = tid & 31, wid = tid >> 5, nwarp = blockDim.x >> 5;
+  const int grp = lane < 30 ? lane / 3 : 0, sub = lane % 3;
+  for (int base = wid * 10; base < n; base += nwarp * 10) {
+    const int j = base + grp;
+    const bool active = lane < 30 && j < n;
     double lo = gl - atol, hi = gu + atol;
-    for (int it = 0; it < 128 && hi - lo > fmax(atol, 2.0 * DBL_EPSILON * fmax(fabs(lo), fabs(hi))); ++it) {
-      double mid = 0.5 * (lo + hi);
-      if (sturm_count(d, e2, n, mid, pivmin) > j) hi = mid; else lo = mid;
+    int it = 0;
+    bool work = active && open_interval(lo, hi);
+    while (__any_sync(0xffffffffu, work)) {
+      const double mid = 0.5 * (lo + hi), lm = 0.5 * (lo + mid), rm = 0.5 * (mid + hi);
+      const double x = sub == 0 ? mid : (sub == 1 ? lm : rm);
+      const int c = work ? sturm_count(d, e2, n, x, pivmin) : 0;
+      const int cm = __shfl_sync(0xffffffffu, c, 3 * grp);
+      const int cl = __shfl_sync(0xffffffffu, c, 3 * grp + 1);
+      const int cr = __shfl_sync(0xffffffffu, c, 3 * grp + 2);
+      if (work) {
+        const bool left = cm > j;
+        if (left) hi = mid; else lo = mid;
+        ++it;
+        if (it < 128 && open_interval(lo, hi)) {
+          const double x2 = left ? lm : rm;
+          if ((left ? cl : cr) > j) hi = x2; else lo = x2;
+          ++it;
+        }
+        work = it < 128 && open_interval(lo, hi);
+      }
     }
-    Wp[n - 1 - j] = 0.5 * (lo + hi);  // descending order
+    if (active && sub == 0) Wp[n - 1 - j] = 0.5 * (lo + hi);  // descending order
   }
 }
 
@@ -305,7 +333,10 @@ tridiag_eigvecs(const EigDev* __restrict__ probs, const double* G, const double*
   const double* tau = e + n;
   const double* lam = W + P.w_off;  // descending
   const double* Gp = G + P.g_off;
-  double* U = work + 3 * P.g_off;   // 3n scratch per eigenvector (3 n*n per problem)
+  // 3n scratch per eigenvector (3 n*n per problem in global memory), in shared
+  // memory after the eigenvectors and the reflector when it fits
+  const bool u_smem = in_smem && 4 * (int64_t)n * nvec + n <= (int64_t)smem_cap;
+  double* U = u_smem ? zsm + (int64_t)n * nvec + n : work + 3 * P.g_off;
   // ||T||_1 for the pivot floor and the cluster tolerance
   double loc = 0.0;
   for (int i = tid; i < n; i += blockDim.x)
@@ -481,8 +512,10 @@ int tt_sym_eigvecs_batched(tt_ctx* ctx, const tt_eig_problem* probs, int n_probs
   // shared memory for the largest problem that fits (the others iterate in global memory)
   int64_t need = 0;
   for (int i = 0; i < n_probs; ++i) {
-    int64_t q = (int64_t)probs[i].n * nvec[i] + probs[i].n;
-    if (q <= kVecsSmemCap) need = std::max(need, q);
+    const int64_t with_u = 4 * (int64_t)probs[i].n * nvec[i] + probs[i].n;  // Z, reflector and LU scratch
+    const int64_t z_only = (int64_t)probs[i].n * nvec[i] + probs[i].n;
+    if (with_u <= kVecsSmemCap) need = std::max(need, with_u);
+    else if (z_only <= kVecsSmemCap) need = std::max(need, z_only);
   }
   static bool attr = false;
   if (!attr) {

@@ -178,6 +178,11 @@ int tt_qmpo_tensor(const tt_qmpo* H, int i, tt_qtensor** out);
 /* Step-wise driver: create = position(0), normalize, buildEnv, initial energy. */
 int tt_qdmrg_create(tt_qmps* psi, tt_qmpo* H, tt_qdmrg** out);
 /* one full sweep (L->R, R->L, normalize) with this sweep's schedule entries */
+/* Noise for the following sweeps: the kept side's density matrix of every
+ * truncation becomes rho + noise * rho_P / tr(rho_P), rho_P the reduced
+ * density matrix of (half of H_eff) x (White, PRB 72, 180403 (2005)); the
+ * reference has no noise term, 0 restores its update exactly. */
+int tt_qdmrg_set_noise(tt_qdmrg* run, double noise);
 int tt_qdmrg_sweep(tt_qdmrg* run, int max_bd, double cutoff, int max_restart, double* energy);
 int tt_qdmrg_finish(tt_qdmrg* run);                          /* psi.position(0) */
 int tt_qdmrg_destroy(tt_qdmrg* run);

@@ -454,6 +454,11 @@ int tt_qdmrg_create(tt_qmps* psi, tt_qmpo* H, tt_qdmrg** out) {
   });
 }
 
+int tt_qdmrg_set_noise(tt_qdmrg* run, double noise) {
+  TT_ARG(run && noise >= 0.0);
+  TT_GUARD(run->st.noise = noise);
+}
+
 int tt_qdmrg_sweep(tt_qdmrg* run, int max_bd, double cutoff, int max_restart, double* energy) {
   TT_ARG(run && max_restart >= 1);
   TT_GUARD({

@@ -911,7 +911,7 @@ void buildEnv(qMPS& psi, qMPO& H, std::vector<qtensor>& TR, std::vector<qtensor>
 
 void updateSite(qMPS& psi, qMPO& H, std::vector<qtensor>& TR, std::vector<qtensor>& TL, unsigned site,
                 double& energy, int direction, int max_bd, double cutoff, char mode, int search_space_size,
-                int max_restart, DmrgLog* log) {
+                int max_restart, DmrgLog* log, double noise) {
   // algos/dmrg/dmrg.cpp:300-372
   unsigned l, r;
   if (direction == MoveFromLeft) { l = site; r = site + 1; } else { l = site - 1; r = site; }
@@ -932,7 +932,17 @@ void updateSite(qMPS& psi, qMPO& H, std::vector<qtensor>& TR, std::vector<qtenso
     if (ix.name() == ln) { mid = ix; break; }
   qtensor S;
   TruncInfo info;
-  svd_bond(x, psi.A[l], psi.A[r], mid, S, direction, cutoff, (unsigned long)max_bd, &info);
+  if (noise > 0.0) {
+    // density-matrix perturbation from the half of H_eff on the kept side:
+    // (TL W1) x left to right, x (W2 TR) right to left
+    qtensor P = direction == MoveFromLeft ? (TL[l] * x) * H.A[l] : (x * H.A[r]) * TR[r];
+    NoiseTerm nt;
+    nt.P = &P;
+    nt.weight = noise;
+    svd_bond(x, psi.A[l], psi.A[r], mid, S, direction, cutoff, (unsigned long)max_bd, &info, &nt);
+  } else {
+    svd_bond(x, psi.A[l], psi.A[r], mid, S, direction, cutoff, (unsigned long)max_bd, &info);
+  }
   auto t2 = std::chrono::steady_clock::now();
   psi.bond_dims[r] = (unsigned)S.total_size();
   psi.center = (int)(direction == MoveFromLeft ? r : l);
@@ -1000,7 +1010,7 @@ double dmrg_sweep(qMPS& psi, qMPO& H, DmrgState& st, int max_bd, double cutoff, 
       rt().energy_fp64 = half == 1 && i == L - 2;
       const bool prof = rt().profile_step == (int)(half * (L - 1) + i);
       if (prof) cudaProfilerStart();
-      updateSite(psi, H, st.TR, st.TL, site, energy, direction, max_bd, cutoff, 'S', 3, max_restart, log);
+      updateSite(psi, H, st.TR, st.TL, site, energy, direction, max_bd, cutoff, 'S', 3, max_restart, log, st.noise);
       rt().energy_fp64 = false;
       auto te0 = std::chrono::steady_clock::now();
       updateEnv(psi, H, st.TR, st.TL, site, direction);

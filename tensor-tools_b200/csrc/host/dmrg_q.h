@@ -115,7 +115,7 @@ struct DmrgLog {
 void buildEnv(qMPS& psi, qMPO& H, std::vector<qtensor>& TR, std::vector<qtensor>& TL);
 void updateSite(qMPS& psi, qMPO& H, std::vector<qtensor>& TR, std::vector<qtensor>& TL, unsigned site,
                 double& energy, int direction, int max_bd, double cutoff, char mode,
-                int search_space_size, int max_restart, DmrgLog* log);
+                int search_space_size, int max_restart, DmrgLog* log, double noise = 0.0);
 void updateEnv(qMPS& psi, qMPO& H, std::vector<qtensor>& TR, std::vector<qtensor>& TL, unsigned site,
                int direction);
 // dmrg schedule overload (algos/dmrg/dmrg.cpp:702-755)
@@ -127,6 +127,7 @@ struct DmrgState {
   std::vector<qtensor> TR, TL;
   bool envs_built = false;
   int sweeps_done = 0;
+  double noise = 0.0;  // density-matrix perturbation of the following sweeps (0: the reference's update)
 };
 // One full sweep (L->R then R->L) of the schedule overload, starting from a
 // state prepared by dmrg_prepare (position(0), normalize, buildEnv).

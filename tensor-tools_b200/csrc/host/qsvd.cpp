@@ -14,6 +14,8 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <map>
+#include <set>
 
 #include "qtensor.h"
 
@@ -66,11 +68,119 @@ struct Sector {
   int keep = 0;
 };
 
+// rho_q += weight / tr(P P^T) * (P P^T)_q over the sectors of the decomposition
+void add_noise(const NoiseTerm& nz, const std::vector<Sector>& sec, const std::vector<qtensor_index>& left,
+               const std::vector<qtensor_index>& right, int direction, int64_t gtot, const DevPtr& G) {
+  const qtensor& P = *nz.P;
+  const std::vector<qtensor_index>& side = direction == MoveFromLeft ? left : right;
+  const unsigned ns = (unsigned)side.size();
+  // the axes of P that carry the kept side's indices (matched by name and type)
+  std::vector<int> row_ax(ns, -1);
+  for (unsigned j = 0; j < ns; ++j)
+    for (unsigned a = 0; a < P.rank; ++a)
+      if (P.idx_set[a].name() == side[j].name() && P.idx_set[a].type() == side[j].type() &&
+          P.idx_set[a].sectors() == side[j].sectors())
+        row_ax[j] = (int)a;
+  for (int a : row_ax)
+    if (a < 0) throw std::runtime_error("svd noise: perturbation lacks an index of the kept side");
+  std::vector<unsigned> col_ax;
+  for (unsigned a = 0; a < P.rank; ++a)
+    if (std::find(row_ax.begin(), row_ax.end(), (int)a) == row_ax.end()) col_ax.push_back(a);
+  // blocks by (row tuple, column tuple)
+  std::map<std::vector<unsigned>, std::map<std::vector<unsigned>, unsigned>> by_row;
+  for (unsigned b = 0; b < P.blocks.size(); ++b) {
+    std::vector<unsigned> rq, cq;
+    for (int a : row_ax) rq.push_back(P.blocks[b].qi[a]);
+    for (unsigned a : col_ax) cq.push_back(P.blocks[b].qi[a]);
+    by_row[rq][cq] = b;
+  }
+  std::vector<tt_out_block> outs;
+  std::vector<tt_block_pair> pairs;
+  for (const Sector& s : sec) {
+    if (s.g == 0 || (direction == MoveFromRight && s.rows == 1 && s.cols == 2)) continue;
+    const auto& tup = direction == MoveFromLeft ? s.lq : s.rq;
+    const auto& off = direction == MoveFromLeft ? s.loff : s.roff;
+    const auto& sz = direction == MoveFromLeft ? s.lsz : s.rsz;
+    for (size_t i = 0; i < tup.size(); ++i) {
+      auto ri = by_row.find(tup[i]);
+      if (ri == by_row.end()) continue;
+      for (size_t j = 0; j < tup.size(); ++j) {
+        auto rj = by_row.find(tup[j]);
+        if (rj == by_row.end()) continue;
+        int ob = -1;
+        for (auto& kv : ri->second) {
+          auto cj = rj->second.find(kv.first);
+          if (cj == rj->second.end()) continue;
+          const BlockMeta& bi = P.blocks[kv.second];
+          const BlockMeta& bj = P.blocks[cj->second];
+          if (ob < 0) {
+            outs.push_back(tt_out_block{s.g_off + off[i] + s.g * off[j], (int32_t)sz[i], (int32_t)sz[j],
+                                        (int32_t)s.g});
+            ob = (int)outs.size() - 1;
+          }
+          auto si = cm_strides(bi.qd), sj = cm_strides(bj.qd);
+          tt_block_pair p;
+          std::memset(&p, 0, sizeof(p));
+          p.out_block = ob;
+          p.a_off = bi.off;
+          p.b_off = bj.off;
+          std::vector<Ax> ax;
+          for (int a : row_ax) ax.push_back({bi.qd[a], si[a], 0});
+          p.n_m = fill_modes(ax, p.m_dims, p.a_m_stride, nullptr);
+          ax.clear();
+          for (unsigned a : col_ax) ax.push_back({bi.qd[a], si[a], sj[a]});
+          p.n_k = fill_modes(ax, p.k_dims, p.a_k_stride, p.b_k_stride);
+          ax.clear();
+          for (int a : row_ax) ax.push_back({bj.qd[a], sj[a], 0});
+          p.n_n = fill_modes(ax, p.n_dims, p.b_n_stride, nullptr);
+          pairs.push_back(p);
+        }
+      }
+    }
+  }
+  if (outs.empty()) return;
+  // rho_P written block by block into a zeroed buffer of the same layout as G
+  DevPtr GP = dev_alloc(gtot);
+  GP->zero();
+  validate_pairs(outs, pairs, P.arena, P.arena, gtot);
+  tt_plan* plan = nullptr;
+  check(tt_contract_plan(ctx(), outs.data(), (int)outs.size(), pairs.data(), (int)pairs.size(), TT_PREC_FP64,
+                         &plan),
+        "svd noise plan");
+  PlanHandle ph(plan);
+  check(tt_contract_exec(ctx(), plan, P.data->get(), P.data->get(), GP->get(), 1.0), "svd noise gram");
+  // tr(rho_P): the diagonals of its sector blocks
+  std::vector<tt_copy_desc> diag;
+  int64_t nd = 0;
+  for (const Sector& s : sec) {
+    if (s.g == 0) continue;
+    tt_copy_desc d;
+    std::memset(&d, 0, sizeof(d));
+    d.n_modes = 1;
+    d.dims[0] = (int32_t)s.g;
+    d.src_off = s.g_off;
+    d.src_stride[0] = s.g + 1;
+    d.dst_off = nd;
+    d.dst_stride[0] = 1;
+    diag.push_back(d);
+    nd += s.g;
+  }
+  DevPtr D = dev_alloc(std::max<int64_t>(nd, 2));
+  D->zero();
+  check(tt_strided_copy_batched(ctx(), diag.data(), (int)diag.size(), GP->get(), D->get()), "svd noise trace");
+  std::vector<double> dh((size_t)nd);
+  check(tt_memcpy_d2h(ctx(), dh.data(), D->get(), sizeof(double) * dh.size()), "svd noise trace");
+  double tr = 0.0;
+  for (double v : dh) tr += v;
+  if (!(tr > 0.0)) return;
+  check(tt_vec_axpy(ctx(), gtot, nz.weight / tr, GP->get(), G->get()), "svd noise add");
+}
+
 }  // namespace
 
 void svd(const qtensor& A, const std::vector<qtensor_index>& left,
          const std::vector<qtensor_index>& right, qtensor& U, qtensor& V, qtensor& S,
-         int direction, double cutoff, unsigned K, TruncInfo* info) {
+         int direction, double cutoff, unsigned K, TruncInfo* info, const NoiseTerm* noise) {
   S = qtensor();
   std::vector<qtensor_index> new_idx(left);
   new_idx.insert(new_idx.end(), right.begin(), right.end());
@@ -257,6 +367,7 @@ void svd(const qtensor& A, const std::vector<qtensor_index>& left,
     PlanHandle ph(plan);
     check(tt_contract_exec(ctx(), plan, A.data->get(), A.data->get(), G->get(), 1.0), "svd gram");
   }
+  if (noise && noise->P && noise->weight > 0.0 && gtot > 0) add_noise(*noise, sec, left, right, direction, gtot, G);
   // phase 1: tridiagonal form and every eigenvalue; vectors only once the
   // truncation below has fixed how many states each sector keeps
   DevPtr Tt = dev_alloc(std::max<int64_t>(3 * wtot, 1));
@@ -510,7 +621,7 @@ void svd(const qtensor& A, const std::vector<qtensor_index>& left,
 }
 
 void svd_bond(const qtensor& combined, qtensor& A_left, qtensor& A_right, const qtensor_index& mid,
-              qtensor& S, int direction, double cutoff, unsigned long K, TruncInfo* info) {
+              qtensor& S, int direction, double cutoff, unsigned long K, TruncInfo* info, const NoiseTerm* noise) {
   qtensor U, V;
   qtensor_index dag_mid = mid;
   dag_mid.dag();
@@ -519,7 +630,7 @@ void svd_bond(const qtensor& combined, qtensor& A_left, qtensor& A_right, const 
     if (!ix.same_tag(mid)) left.push_back(ix);
   for (auto& ix : A_right.idx_set)
     if (!ix.same_tag(dag_mid)) right.push_back(ix);
-  svd(combined, left, right, U, V, S, direction, cutoff, (unsigned)K, info);
+  svd(combined, left, right, U, V, S, direction, cutoff, (unsigned)K, info, noise);
   qtensor_index& u = U.idx_set.back();
   u.rename(mid.name());
   u.retype(mid.type());

@@ -279,12 +279,23 @@ struct TruncInfo {
   std::vector<QN> sector_qn;
   std::vector<unsigned> kept_per_sector;
 };
+// Density-matrix perturbation ("noise", White, PRB 72, 180403 (2005)): the
+// density matrix of the kept side becomes rho + weight * rho_P / tr(rho_P),
+// rho_P = P P^T over the rows of P that carry the kept side's indices (found
+// by name; other axes are summed), restricted to the QN sectors of A.  The
+// kept basis diagonalises the perturbed rho; the other factor is still the
+// projection of A itself.  No counterpart in the reference.
+struct NoiseTerm {
+  const qtensor* P = nullptr;
+  double weight = 0.0;
+};
 void svd(const qtensor& A, const std::vector<qtensor_index>& left,
          const std::vector<qtensor_index>& right, qtensor& U, qtensor& V, qtensor& S,
-         int direction, double cutoff = 0.0, unsigned K = 0, TruncInfo* info = nullptr);
+         int direction, double cutoff = 0.0, unsigned K = 0, TruncInfo* info = nullptr,
+         const NoiseTerm* noise = nullptr);
 void svd_bond(const qtensor& combined, qtensor& A_left, qtensor& A_right,
               const qtensor_index& mid, qtensor& S, int direction, double cutoff = 0.0,
-              unsigned long K = 0, TruncInfo* info = nullptr);
+              unsigned long K = 0, TruncInfo* info = nullptr, const NoiseTerm* noise = nullptr);
 double calcEntropy(const qtensor& S, double cutoff = 1e-24);
 
 // permutation from -> to (qtensor_index_op.cpp:23-37)

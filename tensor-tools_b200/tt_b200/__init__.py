@@ -163,6 +163,7 @@ _proto("tt_qmpo_tensor", P, C.c_int, PP)
 _proto("tt_qdmrg_create", P, P, PP)
 _proto("tt_vec_scale_mode", P, I64, C.c_int, I64, PD, P)
 _proto("tt_qdmrg_sweep", P, C.c_int, D, C.c_int, PD)
+_proto("tt_qdmrg_set_noise", P, D)
 _proto("tt_qdmrg_finish", P)
 _proto("tt_qdmrg_destroy", P)
 _proto("tt_qdmrg_run", P, P, C.c_int, C.POINTER(C.c_int), C.c_int, PD, C.c_int, C.POINTER(C.c_int),
@@ -541,7 +542,9 @@ class QDMRG:
             lib.tt_qdmrg_destroy(self.h)
             self.h = None
 
-    def sweep(self, max_bd: int, cutoff: float, max_restart: int) -> float:
+    def sweep(self, max_bd: int, cutoff: float, max_restart: int, noise: float = 0.0) -> float:
+        """One sweep; noise > 0 adds the density-matrix perturbation to its truncations."""
+        _chk(lib.tt_qdmrg_set_noise(self.h, noise), "set_noise")
         e = D()
         _chk(lib.tt_qdmrg_sweep(self.h, max_bd, cutoff, max_restart, C.byref(e)), "sweep")
         return e.value
@@ -549,12 +552,14 @@ class QDMRG:
     def finish(self):
         _chk(lib.tt_qdmrg_finish(self.h), "finish")
 
-    def run(self, nsweeps, maxm, cutoff, max_restart, start_sweep: int = 0) -> float:
+    def run(self, nsweeps, maxm, cutoff, max_restart, start_sweep: int = 0, noise=None) -> float:
         """Sweeps start_sweep .. nsweeps-1 of the schedule (maxm[s % len] ...),
-        then the final position(0); start_sweep > 0 resumes a loaded checkpoint."""
+        then the final position(0); start_sweep > 0 resumes a loaded checkpoint.
+        noise: per-sweep noise values (the last one repeats), default none."""
         e = 0.0
         for s in range(start_sweep, nsweeps):
-            e = self.sweep(maxm[s % len(maxm)], cutoff[s % len(cutoff)], max_restart[s % len(max_restart)])
+            nz = 0.0 if not noise else noise[min(s, len(noise) - 1)]
+            e = self.sweep(maxm[s % len(maxm)], cutoff[s % len(cutoff)], max_restart[s % len(max_restart)], nz)
         self.finish()
         return e
 

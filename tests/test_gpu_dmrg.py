@@ -90,3 +90,43 @@ def test_device_and_host_davidson_control_agree(ctx):
     assert kh == kd
     for a, b in zip(sh, sd):
         assert abs(a - b) <= 1e-10 * abs(a)
+
+
+def test_noise_schedule_converges_to_the_noise_free_ground_state(ctx):
+    """Density-matrix noise decaying to zero (as in the J1-J2 configuration)
+    on a small J1-J2 cylinder: the final energy equals exact diagonalisation
+    and the noise-free oracle's, every noisy sweep stays variational, and the
+    noise changes the kept bases while it is on."""
+    import tt_b200
+    from oracle import autompo as am
+    Nx, Ny, J2 = 4, 4, 0.5
+    N = Nx * Ny
+    terms = []
+    for s1, s2, typ, *_ in am.square_next_neighbor(Nx, Ny, True):
+        J = 1.0 if typ == 1 else J2
+        i, j = s1 - 1, s2 - 1
+        terms += [(0.5 * J, ((i, "S+"), (j, "S-"))), (0.5 * J, ((i, "S-"), (j, "S+"))), (J, ((i, "Sz"), (j, "Sz")))]
+    a, o = tt_b200.AutoMPO(), am.AutoMPO()
+    for coef, ops in terms:
+        args = [coef]
+        for i, op in ops:
+            args += [op, i]
+        a.add(*args)
+        o.add(*args)
+    maxm, cutoff, mr = [16, 32, 64, 128, 256, 256, 256, 256, 256], [1e-12], [6]
+    noise = [1e-4, 1e-5, 1e-6, 1e-8, 0.0]
+    Eed = ed.terms_ground_energy(N, terms, N // 2)
+    psi = tt_b200.QMPS(N, qdmrg.neel(N))
+    run = tt_b200.QDMRG(psi, tt_b200.QMPO.from_autompo(a, N))
+    e = run.run(9, maxm, cutoff, mr, noise=noise)
+    for se, _ in run.sweeps():
+        assert se >= Eed - 1e-9 * abs(Eed)
+    assert abs(e - Eed) <= 1e-8 * abs(Eed)
+    # the noise-free path through the same sweeps ends at the same state
+    psi0 = tt_b200.QMPS(N, qdmrg.neel(N))
+    run0 = tt_b200.QDMRG(psi0, tt_b200.QMPO.from_autompo(a, N))
+    e0 = run0.run(9, maxm, cutoff, mr)
+    assert abs(e - e0) <= 1e-8 * abs(Eed)
+    # while on, noise changes the kept bases, hence the early sweep energies
+    early = [abs(x[0] - y[0]) for x, y in zip(run.sweeps()[:3], run0.sweeps()[:3])]
+    assert max(early) > 1e-12

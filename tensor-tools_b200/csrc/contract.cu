@@ -684,7 +684,7 @@ int tt_contract_exec(tt_ctx* ctx, const tt_plan* plan, const double* A, const do
                      double* C, double alpha) {
   TT_REQUIRE(ctx && plan, "tt_contract_exec: null argument");
   if (plan->n_tasks == 0) return TT_OK;
-  static bool attr_set = false;
+  static thread_local bool attr_set = false;  // per host thread: each may drive its own device
   if (!attr_set) {
     TT_CUDA(cudaFuncSetAttribute(grouped_dgemm, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)SMEM_BYTES));

@@ -249,7 +249,7 @@ int tt_sym_eig_batched(tt_ctx* ctx, const tt_eig_problem* probs, int n_probs, do
   TT_CUDA(cudaMemcpyAsync(dp, hp.data(), sizeof(EigDev) * n_probs, cudaMemcpyHostToDevice, ctx->stream));
   TT_CUDA(cudaMemsetAsync(dstatus, 0, sizeof(int), ctx->stream));
   const size_t smem = sizeof(double) * 2 * SMEM_N * SMEM_N;
-  static bool attr = false;
+  static thread_local bool attr = false;  // per host thread: each may drive its own device
   if (!attr) {
     TT_CUDA(cudaFuncSetAttribute(jacobi_eig, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     attr = true;

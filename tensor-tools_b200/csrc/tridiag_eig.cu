@@ -482,7 +482,7 @@ int tt_sym_eigvals_batched(tt_ctx* ctx, const tt_eig_problem* probs, int n_probs
   EigDev* dp = tt::pool_alloc<EigDev>(ctx, n_probs);
   if (!dp) return tt::fail(TT_ERR_OOM, "tt_sym_eigvals_batched: allocation failed");
   TT_CUDA(tt::h2d_async(ctx, dp, hp.data(), sizeof(EigDev) * n_probs));
-  static bool attr = false;
+  static thread_local bool attr = false;  // per host thread: each may drive its own device
   if (!attr) {
     TT_CUDA(cudaFuncSetAttribute(tridiag_eigvals, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)vals_smem()));
     attr = true;
@@ -517,7 +517,7 @@ int tt_sym_eigvecs_batched(tt_ctx* ctx, const tt_eig_problem* probs, int n_probs
     if (with_u <= kVecsSmemCap) need = std::max(need, with_u);
     else if (z_only <= kVecsSmemCap) need = std::max(need, z_only);
   }
-  static bool attr = false;
+  static thread_local bool attr = false;  // per host thread: each may drive its own device
   if (!attr) {
     TT_CUDA(cudaFuncSetAttribute(tridiag_eigvecs, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)(sizeof(double) * kVecsSmemCap)));

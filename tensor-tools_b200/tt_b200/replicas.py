@@ -59,3 +59,56 @@ def run_chains(items: Sequence[Any], solve: Callable[[Any], Any]) -> List[Any]:
         return []
     flat = sorted((p for part in parts for p in part), key=lambda t: t[0])
     return [r for _, r in flat]
+
+
+
+def run_chains_concurrent(items: Sequence[Any], solve: Callable[[Any], Any], streams: int = 8,
+                          device: int = 0) -> List[Any]:
+    """Solve independent problems concurrently on one GPU.
+
+    `streams` worker threads each create their own device context (a CUDA
+    stream, the thread's plan cache and scalars), take items from a shared
+    queue, and close the context when the queue is empty -- all on the same
+    thread, since a context is bound to the thread that created it.  One DMRG
+    sweep is a chain of small dependent launches that leaves most of the GPU
+    idle, so independent chains on separate streams fill it; the C ABI
+    releases the GIL inside every call.  `solve` must return plain values (no
+    device objects, which belong to the worker's context).  Results come back
+    in item order; the first exception raised by `solve` is re-raised."""
+    import queue
+    import threading
+
+    import tt_b200
+
+    todo: "queue.Queue" = queue.Queue()
+    for k, it in enumerate(items):
+        todo.put((k, it))
+    out: List[Any] = [None] * len(items)
+    errors: List[BaseException] = []
+
+    def worker():
+        try:
+            ctx = tt_b200.Context(device)
+        except BaseException as e:  # no device: report once
+            errors.append(e)
+            return
+        try:
+            while not errors:
+                try:
+                    k, it = todo.get_nowait()
+                except queue.Empty:
+                    break
+                out[k] = solve(it)
+        except BaseException as e:
+            errors.append(e)
+        finally:
+            ctx.close()
+
+    threads = [threading.Thread(target=worker, daemon=True) for _ in range(max(1, min(streams, len(items))))]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    if errors:
+        raise errors[0]
+    return out

@@ -9,6 +9,7 @@
 // descriptors when the plan is built.
 #include <algorithm>
 #include <cstring>
+#include <map>
 #include <numeric>
 #include <vector>
 
@@ -215,37 +216,17 @@ grouped_dgemm(const TaskDev* __restrict__ tasks, const OutDev* __restrict__ outs
 // ---------------------------------------------------------------------------
 // Mixed-precision path: tcgen05 (5th-generation tensor cores), kind::tf32.
 //
-// One CTA of eight warps computes a TC_BM x TC_BN tile of an output block
-// with an FP32 accumulator in tensor memory (128 lanes = tile rows, TC_BN
-// columns).  For every k-chunk of TC_BK elements each thread first issues its
-// TC_LOADS gathered FP64 loads of A and of B (the same offset tables as the
-// FP64 kernel), then -- once the MMAs that last read the stage have completed
-// -- splits each value into TF32 hi and lo parts (x = hi + lo, both rounded
-// to nearest) and stores them K-major with the 128-byte swizzle.  Thread 0
-// issues the tcgen05.mma instructions of the chunk (hi*hi, and for the split
-// form hi*lo and lo*hi as well) and commits them to the stage's mbarrier.  The
-// gather is software-pipelined: the loads of chunk c+1 are issued before chunk
-// c is converted, and run while the MMAs of chunk c execute.  The
-// epilogue reads the accumulator with tcgen05.ld (warp w reads TMEM lanes
-// 32(w%4).. and column half w/4) and writes alpha * acc as FP64.  Every wait
-// is bounded: on timeout the CTA records TT_ERR_TIMEOUT in the plan's status
-// word, drains what it issued (again bounded), frees its tensor memory and
-// returns.
+// Two steps per contraction.  pack_tf32 converts every operand block once
+// into TF32 hi/lo tiles (x = hi + lo, both rounded to nearest) stored in the
+// exact K-major 128-byte-swizzled layout of a shared-memory MMA operand tile;
+// grouped_tc_bulk then feeds the tensor cores from those tiles with bulk
+// copies and accumulates in tensor memory (FP32), one 128 x 128 output tile
+// per CTA.  The split form issues hi*hi + hi*lo + lo*hi per k-step.
 constexpr int TC_BM = 128;
 constexpr int TC_BN = 128;
 constexpr int TC_BK = 32;                        // fp32 elements = one 128-byte swizzle row
-constexpr int TC_THREADS = 256;
-constexpr int TC_LOADS = TC_BM * TC_BK / TC_THREADS;  // per operand and thread: 16
-constexpr int TC_QUADS = TC_LOADS / 4;                // 16-byte swizzle units per operand and thread
-constexpr int TC_A_BYTES = TC_BM * TC_BK * 4;    // 16 KB
-constexpr int TC_B_BYTES = TC_BN * TC_BK * 4;    // 16 KB
-constexpr int TC_STAGE_BYTES = 2 * TC_A_BYTES + 2 * TC_B_BYTES;  // hi and lo of A and B
-constexpr int TC_STAGES = 2;
-constexpr size_t TC_SMEM_BYTES = (size_t)TC_STAGES * TC_STAGE_BYTES + 1024;  // + alignment slack
-constexpr uint32_t TC_TMEM_COLS = TC_BN;         // FP32 accumulator: TC_BN columns x 128 lanes
 constexpr uint32_t TC_WAIT_LIMIT = 1u << 26;
-static_assert(TC_BM * TC_BK % TC_THREADS == 0 && TC_BN * TC_BK % TC_THREADS == 0, "tile / thread mismatch");
-static_assert(TC_BN == TC_BM, "the load mappings assume square tiles");
+static_assert(TC_BN == TC_BM, "packed tiles are 128 rows for both operands");
 
 // Instruction descriptor: D f32, A/B tf32, both K-major, N = TC_BN, M = TC_BM.
 constexpr uint32_t TC_IDESC = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(TC_BN >> 3) << 17) |
@@ -271,28 +252,10 @@ __device__ __forceinline__ uint32_t sw128_off(int r, int k) {
   return (uint32_t)((r >> 3) * 1024 + (r & 7) * 128 + ((((k >> 2) ^ (r & 7))) << 4) + (k & 3) * 4);
 }
 
-__device__ __forceinline__ void st_shared_v4(uint32_t addr, uint32_t a, uint32_t b, uint32_t c, uint32_t d) {
-  asm volatile("st.shared.v4.u32 [%0], {%1, %2, %3, %4};" ::"r"(addr), "r"(a), "r"(b), "r"(c), "r"(d));
-}
-
 __device__ __forceinline__ uint32_t to_tf32(float x) {
   uint32_t r;
   asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
   return r;
-}
-
-// four consecutive-k values -> TF32 hi (and lo = TF32(x - hi) for the split
-// form) as one 16-byte unit at addr (and addr + lo_delta)
-template <bool SPLIT>
-__device__ __forceinline__ void put_quad(uint32_t addr, uint32_t lo_delta, const double (&x)[4]) {
-  uint32_t h[4], l[4];
-#pragma unroll
-  for (int e = 0; e < 4; ++e) {
-    h[e] = to_tf32(__double2float_rn(x[e]));
-    if (SPLIT) l[e] = to_tf32(__double2float_rn(x[e] - (double)__uint_as_float(h[e])));
-  }
-  st_shared_v4(addr, h[0], h[1], h[2], h[3]);
-  if (SPLIT) st_shared_v4(addr + lo_delta, l[0], l[1], l[2], l[3]);
 }
 
 __device__ __forceinline__ void mbar_init(uint32_t addr, uint32_t count) {
@@ -347,174 +310,199 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
   for (int j = 0; j < 16; ++j) v[j] = __uint_as_float(r[j]);
 }
 
+// ---- operand packing: FP64 blocks -> TF32 hi/lo tiles, pre-swizzled --------
+// A packed tile holds 128 rows x 32 k of one operand block as TF32 hi
+// (16 KB) followed by TF32 lo (16 KB), each laid out exactly as the K-major
+// 128-byte-swizzled shared-memory tile the MMA reads, so one bulk copy moves
+// it into shared memory unchanged.  Edges are zero-padded.  Tile (rt, kt) of
+// a block sits at base + (rt * kt_count + kt) * 32 KB.
+struct PackJob {
+  int64_t x_off;             // block offset in the operand (elements)
+  int64_t dst;               // packed block base (bytes)
+  int32_t rows, K;           // logical rows (m or n) and k
+  int32_t row_tab, k_tab;    // offset tables: element = X[x_off + tab[row_tab + r] + tab[k_tab + k]]
+  int32_t kt_count;
+  int32_t row_unit;          // rows have unit stride: walk them fastest
+};
+struct PackTile {
+  int32_t job, rt, kt;
+};
+constexpr int TC_TILE_BYTES = 2 * TC_BM * TC_BK * 4;  // hi + lo = 32 KB
+
 template <bool SPLIT>
-__global__ void __launch_bounds__(TC_THREADS, 1)
-grouped_tc(const TaskDev* __restrict__ tasks, const OutDev* __restrict__ outs,
-           const PairDev* __restrict__ pairs, const int32_t* __restrict__ tab,
-           const double* __restrict__ A, const double* __restrict__ B,
-           double* __restrict__ C, double alpha, int* __restrict__ status) {
+__global__ void __launch_bounds__(128)
+pack_tf32(const PackJob* __restrict__ jobs, const PackTile* __restrict__ tiles, const int32_t* __restrict__ tab,
+          const double* __restrict__ X, uint8_t* __restrict__ packed) {
+  const PackTile t = tiles[blockIdx.x];
+  const PackJob J = jobs[t.job];
+  const int tid = threadIdx.x;
+  uint8_t* dst = packed + J.dst + (int64_t)(t.rt * J.kt_count + t.kt) * TC_TILE_BYTES;
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    const int r = J.row_unit ? tid : (tid >> 3) + 16 * i;
+    const int q = J.row_unit ? i : (tid & 7);
+    const int gr = t.rt * TC_BM + r;
+    double x[4];
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const int gk = t.kt * TC_BK + 4 * q + e;
+      x[e] = (gr < J.rows && gk < J.K) ? X[J.x_off + tab[J.row_tab + gr] + tab[J.k_tab + gk]] : 0.0;
+    }
+    uint32_t h[4], l[4];
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      h[e] = to_tf32(__double2float_rn(x[e]));
+      l[e] = SPLIT ? to_tf32(__double2float_rn(x[e] - (double)__uint_as_float(h[e]))) : 0u;
+    }
+    const uint32_t o = sw128_off(r, 4 * q);
+    *reinterpret_cast<uint4*>(dst + o) = make_uint4(h[0], h[1], h[2], h[3]);
+    if (SPLIT) *reinterpret_cast<uint4*>(dst + TC_TILE_BYTES / 2 + o) = make_uint4(l[0], l[1], l[2], l[3]);
+  }
+}
+
+// ---- grouped tcgen05 GEMM over packed tiles ---------------------------------
+// One CTA of four warps per 128 x 128 output tile.  Thread 0 (producer)
+// streams the packed A and B tiles of every k-chunk of every block pair into
+// a TC_RING-stage ring with plain bulk copies (cp.async.bulk, completion
+// counted on the stage's full barrier); thread 32 (MMA issuer) waits for each
+// stage, issues its tcgen05.mma instructions into the TMEM accumulator and
+// commits them to the stage's empty barrier, which releases the stage to the
+// producer.  After the last chunk an accumulator barrier releases the
+// epilogue: all four warps read their 32 TMEM lanes and write alpha * acc as
+// FP64.  Every wait is bounded; on timeout the CTA records TT_ERR_TIMEOUT,
+// lets what it issued land (bounded), frees TMEM and returns.
+struct PairTC {
+  int64_t a_base, b_base;  // packed block bases (bytes)
+  int32_t kt;              // k tiles of the pair
+  int32_t pad;
+};
+constexpr int TC_RING = 3;
+constexpr int TC_RING_STAGE = 4 * TC_BM * TC_BK * 4;  // A hi, A lo, B hi, B lo: 64 KB
+constexpr size_t TC_BULK_SMEM = (size_t)TC_RING * TC_RING_STAGE + 1024;
+constexpr uint32_t TC_BULK_COLS = TC_BN;
+
+__device__ __forceinline__ void mbar_expect_tx(uint32_t mbar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mbar), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t bytes, uint32_t mbar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+               "l"(src), "r"(bytes), "r"(mbar)
+               : "memory");
+}
+
+template <bool SPLIT>
+__global__ void __launch_bounds__(128, 1)
+grouped_tc_bulk(const TaskDev* __restrict__ tasks, const OutDev* __restrict__ outs, const PairTC* __restrict__ pairs,
+                const uint8_t* __restrict__ packA, const uint8_t* __restrict__ packB, double* __restrict__ C,
+                double alpha, int* __restrict__ status) {
   extern __shared__ uint8_t tc_smem_raw[];
-  __shared__ __align__(8) uint64_t mbar[TC_STAGES];
+  __shared__ __align__(8) uint64_t full_bar[TC_RING], empty_bar[TC_RING], acc_bar;
   __shared__ uint32_t tmem_slot;
-  __shared__ int flag;  // 1 after a timeout
-  __shared__ int32_t rowA_s[TC_BM];
-  __shared__ int32_t colB_s[TC_BN];
+  __shared__ int flag, issued, consumed;
 
   const uint32_t sbase = (smem_u32(tc_smem_raw) + 1023u) & ~1023u;
   const TaskDev task = tasks[blockIdx.x];
   const OutDev out = outs[task.out];
-  const int tid = threadIdx.x;
-  const int warp = tid >> 5;
-  const int lane = tid & 31;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const uint32_t half = SPLIT ? (uint32_t)TC_TILE_BYTES : (uint32_t)(TC_TILE_BYTES / 2);  // bytes per operand tile
 
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_slot)),
-                 "r"(TC_TMEM_COLS)
+                 "r"(TC_BULK_COLS)
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
   if (tid == 0) {
-    mbar_init(smem_u32(&mbar[0]), 1);
-    mbar_init(smem_u32(&mbar[1]), 1);
+    for (int i = 0; i < TC_RING; ++i) {
+      mbar_init(smem_u32(&full_bar[i]), 1);
+      mbar_init(smem_u32(&empty_bar[i]), 1);
+    }
+    mbar_init(smem_u32(&acc_bar), 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     flag = 0;
+    issued = 0;
+    consumed = 0;
   }
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = tmem_slot;
+  int nchunks = 0;
+  for (int p = task.p_begin; p < task.p_end; ++p) nchunks += pairs[p].kt;
+  const int rt = task.m0 / TC_BM, nt = task.n0 / TC_BN;
 
-  uint32_t phase[TC_STAGES] = {0, 0};
-  bool pending[TC_STAGES] = {false, false};
-  bool any_mma = false;
-  int gc = 0;  // chunk counter over all pairs of the task
-
-  for (int p = task.p_begin; p < task.p_end && !flag; ++p) {
-    const PairDev P = pairs[p];
-    __syncthreads();
-    if (tid < TC_BM) {
-      const int m = task.m0 + tid;
-      rowA_s[tid] = m < P.m ? tab[P.rowA + m] : 0;
-    } else if (tid - TC_BM < TC_BN) {
-      const int n = task.n0 + tid - TC_BM;
-      colB_s[tid - TC_BM] = n < P.n ? tab[P.colB + n] : 0;
+  if (tid == 0) {  // producer
+    int g = 0;
+    for (int p = task.p_begin; p < task.p_end && !flag; ++p) {
+      const PairTC q = pairs[p];
+      for (int kt = 0; kt < q.kt; ++kt, ++g) {
+        const int s = g % TC_RING;
+        if (g >= TC_RING && !mbar_wait_bounded(smem_u32(&empty_bar[s]), (uint32_t)((g / TC_RING - 1) & 1))) {
+          flag = 1;
+          break;
+        }
+        const uint32_t st = sbase + s * TC_RING_STAGE;
+        mbar_expect_tx(smem_u32(&full_bar[s]), 2 * half);
+        bulk_g2s(st, packA + q.a_base + (int64_t)(rt * q.kt + kt) * TC_TILE_BYTES, half, smem_u32(&full_bar[s]));
+        bulk_g2s(st + TC_TILE_BYTES, packB + q.b_base + (int64_t)(nt * q.kt + kt) * TC_TILE_BYTES, half,
+                 smem_u32(&full_bar[s]));
+        issued = g + 1;
+      }
     }
-    __syncthreads();
-    const double* Ab = A + P.a_off;
-    const double* Bb = B + P.b_off;
-    const int K = P.k;
-    const int nchunks = (K + TC_BK - 1) / TC_BK;
-    // Gathered FP64 loads of one chunk into registers.  A thread owns
-    // TC_QUADS quads (row r, k = 4q..4q+3): one 16-byte swizzle unit each.
-    //   unit-stride rows (A m-fast / B with n fast): r = tid % 128, q = tid / 128 + 2i
-    //   unit-stride k (A k-fast / B k-fast):          q = tid % 8,   r = tid / 8 + 32i
-    auto gather = [&](int c, double (&xa)[TC_QUADS][4], double (&xb)[TC_QUADS][4]) {
-      const int k0 = c * TC_BK;
+  } else if (tid == 32) {  // MMA issuer
+    int g = 0;
+    for (; g < nchunks && !flag; ++g) {
+      const int s = g % TC_RING;
+      if (!mbar_wait_bounded(smem_u32(&full_bar[s]), (uint32_t)((g / TC_RING) & 1))) {
+        flag = 1;
+        break;
+      }
+      tc_fence_after();
+      const uint32_t ah = sbase + s * TC_RING_STAGE, al = ah + TC_TILE_BYTES / 2;
+      const uint32_t bh = ah + TC_TILE_BYTES, bl = bh + TC_TILE_BYTES / 2;
 #pragma unroll
-      for (int i = 0; i < TC_QUADS; ++i) {
-        const int r = P.a_mfast ? (tid & (TC_BM - 1)) : ((tid >> 3) + 32 * i);
-        const int q = P.a_mfast ? ((tid >> 7) + 2 * i) : (tid & 7);
-        const bool rok = task.m0 + r < P.m;
-        const int32_t rr = rowA_s[r];
-#pragma unroll
-        for (int e = 0; e < 4; ++e) {
-          const int gk = k0 + 4 * q + e;
-          xa[i][e] = (rok && gk < K) ? Ab[rr + tab[P.colA + gk]] : 0.0;
+      for (int kk = 0; kk < TC_BK / 8; ++kk) {
+        const uint32_t adv = 32u * kk;
+        const uint32_t acc = (g > 0 || kk > 0) ? 1u : 0u;
+        if (SPLIT) {
+          mma_tf32(tmem, sw128_desc(al + adv), sw128_desc(bh + adv), acc);
+          mma_tf32(tmem, sw128_desc(ah + adv), sw128_desc(bl + adv), 1u);
+          mma_tf32(tmem, sw128_desc(ah + adv), sw128_desc(bh + adv), 1u);
+        } else {
+          mma_tf32(tmem, sw128_desc(ah + adv), sw128_desc(bh + adv), acc);
         }
       }
-#pragma unroll
-      for (int i = 0; i < TC_QUADS; ++i) {
-        const int r = P.b_kfast ? ((tid >> 3) + 32 * i) : (tid & (TC_BN - 1));
-        const int q = P.b_kfast ? (tid & 7) : ((tid >> 7) + 2 * i);
-        const bool rok = task.n0 + r < P.n;
-        const int32_t cr = colB_s[r];
-#pragma unroll
-        for (int e = 0; e < 4; ++e) {
-          const int gk = k0 + 4 * q + e;
-          xb[i][e] = (rok && gk < K) ? Bb[tab[P.rowB + gk] + cr] : 0.0;
-        }
-      }
-    };
-    double xa[TC_QUADS][4], xb[TC_QUADS][4], ya[TC_QUADS][4], yb[TC_QUADS][4];
-    gather(0, xa, xb);
-    for (int c = 0; c < nchunks; ++c, ++gc) {
-      const int s = gc & 1;
-      // 1. the next chunk's loads go out before this chunk is converted
-      if (c + 1 < nchunks) gather(c + 1, ya, yb);
-      // 2. the MMAs that last read this stage must have completed
-      if (pending[s]) {
-        if (tid == 0 && !mbar_wait_bounded(smem_u32(&mbar[s]), phase[s])) flag = 1;
-        __syncthreads();
-        phase[s] ^= 1;
-        pending[s] = false;
-        if (flag) break;
-      }
-      // 3. split and store (K-major, 128-byte swizzle, one 16-byte unit per quad)
-      const uint32_t a_hi = sbase + s * TC_STAGE_BYTES;
-      const uint32_t b_hi = a_hi + 2 * TC_A_BYTES;
-#pragma unroll
-      for (int i = 0; i < TC_QUADS; ++i) {
-        const int r = P.a_mfast ? (tid & (TC_BM - 1)) : ((tid >> 3) + 32 * i);
-        const int q = P.a_mfast ? ((tid >> 7) + 2 * i) : (tid & 7);
-        put_quad<SPLIT>(a_hi + sw128_off(r, 4 * q), TC_A_BYTES, xa[i]);
-      }
-#pragma unroll
-      for (int i = 0; i < TC_QUADS; ++i) {
-        const int r = P.b_kfast ? ((tid >> 3) + 32 * i) : (tid & (TC_BN - 1));
-        const int q = P.b_kfast ? (tid & 7) : ((tid >> 7) + 2 * i);
-        put_quad<SPLIT>(b_hi + sw128_off(r, 4 * q), TC_B_BYTES, xb[i]);
-      }
-      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-      __syncthreads();
-      // 4. one thread issues the chunk's MMAs
-      if (tid == 0) {
-        tc_fence_after();
-        const uint32_t ah = a_hi, al = a_hi + TC_A_BYTES, bh = b_hi, bl = b_hi + TC_B_BYTES;
-#pragma unroll
-        for (int kk = 0; kk < TC_BK / 8; ++kk) {  // K = 8 tf32 (32 bytes) per instruction
-          const uint32_t adv = 32u * kk;
-          if (SPLIT) {
-            mma_tf32(tmem, sw128_desc(al + adv), sw128_desc(bh + adv), any_mma || kk > 0 ? 1u : 0u);
-            mma_tf32(tmem, sw128_desc(ah + adv), sw128_desc(bl + adv), 1u);
-            mma_tf32(tmem, sw128_desc(ah + adv), sw128_desc(bh + adv), 1u);
-          } else {
-            mma_tf32(tmem, sw128_desc(ah + adv), sw128_desc(bh + adv), any_mma || kk > 0 ? 1u : 0u);
-          }
-        }
-        mma_commit(smem_u32(&mbar[s]));
-      }
-      pending[s] = true;
-      any_mma = true;
-#pragma unroll
-      for (int i = 0; i < TC_QUADS; ++i)
-#pragma unroll
-        for (int e = 0; e < 4; ++e) {
-          xa[i][e] = ya[i][e];
-          xb[i][e] = yb[i][e];
-        }
+      mma_commit(smem_u32(&empty_bar[s]));
+      consumed = g + 1;
+    }
+    if (g > 0) mma_commit(smem_u32(&acc_bar));
+  }
+  __syncwarp();
+  __syncthreads();
+  if (tid == 0) {
+    if (!flag && nchunks > 0 && !mbar_wait_bounded(smem_u32(&acc_bar), 0u)) flag = 1;
+    if (flag) {
+      // let the copies that were issued but not consumed land, and the last
+      // committed MMAs finish, before shared and tensor memory are released
+      for (int g = consumed; g < issued; ++g)
+        mbar_wait_bounded(smem_u32(&full_bar[g % TC_RING]), (uint32_t)((g / TC_RING) & 1));
+      if (consumed > 0)
+        mbar_wait_bounded(smem_u32(&empty_bar[(consumed - 1) % TC_RING]), (uint32_t)(((consumed - 1) / TC_RING) & 1));
+      atomicExch(status, TT_ERR_TIMEOUT);
     }
   }
-  // drain: every committed stage completes before TMEM is read or freed
-  for (int s = 0; s < TC_STAGES; ++s)
-    if (pending[s]) {
-      if (tid == 0 && !mbar_wait_bounded(smem_u32(&mbar[s]), phase[s])) flag = 1;
-      phase[s] ^= 1;
-    }
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
-  if (flag) {
-    if (tid == 0) atomicExch(status, TT_ERR_TIMEOUT);
-  } else {
+  if (!flag) {
     double* Cb = C + out.c_off;
-    const int quarter = warp & 3;         // TMEM lanes 32*quarter .. +31 = tile rows
-    const int col0 = (warp >> 2) * (TC_BN / 2);
-    const int m = task.m0 + quarter * 32 + lane;
+    const int m = task.m0 + warp * 32 + lane;
 #pragma unroll
-    for (int c16 = 0; c16 < TC_BN / 32; ++c16) {
+    for (int c16 = 0; c16 < TC_BN / 16; ++c16) {
       float v[16];
-      if (any_mma) {
-        tmem_ld16(tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(col0 + c16 * 16), v);
+      if (nchunks > 0) {
+        tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(c16 * 16), v);
       } else {
 #pragma unroll
         for (int j = 0; j < 16; ++j) v[j] = 0.f;
@@ -522,7 +510,7 @@ grouped_tc(const TaskDev* __restrict__ tasks, const OutDev* __restrict__ outs,
       if (m < out.m) {
 #pragma unroll
         for (int j = 0; j < 16; ++j) {
-          const int n = task.n0 + col0 + c16 * 16 + j;
+          const int n = task.n0 + c16 * 16 + j;
           if (n < out.n) Cb[m + (int64_t)out.ldc * n] = alpha * (double)v[j];
         }
       }
@@ -532,7 +520,7 @@ grouped_tc(const TaskDev* __restrict__ tasks, const OutDev* __restrict__ outs,
   __syncthreads();
   tc_fence_after();
   if (warp == 0)
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TC_TMEM_COLS) : "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TC_BULK_COLS) : "memory");
 }
 
 }  // namespace
@@ -540,6 +528,16 @@ grouped_tc(const TaskDev* __restrict__ tasks, const OutDev* __restrict__ outs,
 struct tt_plan {
   int precision = TT_PREC_FP64;
   int* d_status = nullptr;  // tensor-core path: TT_OK or TT_ERR_TIMEOUT
+  // tensor-core path: packing jobs and tiles of the unique A / B blocks, the
+  // pairs in packed form, and the packed sizes (buffers are taken from the
+  // stream-ordered pool for each exec)
+  PackJob* d_jobsA = nullptr;
+  PackJob* d_jobsB = nullptr;
+  PackTile* d_tilesA = nullptr;
+  PackTile* d_tilesB = nullptr;
+  PairTC* d_pairtc = nullptr;
+  int n_tilesA = 0, n_tilesB = 0;
+  int64_t bytesA = 0, bytesB = 0;
   int n_tasks = 0;
   int n_pairs = 0;
   int n_out = 0;
@@ -647,8 +645,46 @@ int tt_contract_plan(tt_ctx* ctx, const tt_out_block* outs, int n_out,
   std::vector<OutDev> ho(n_out);
   for (int o = 0; o < n_out; ++o) ho[o] = OutDev{outs[o].c_off, outs[o].m, outs[o].n, outs[o].ldc};
 
+  // tensor-core path: one packing job per distinct operand block
+  std::vector<PackJob> ja, jb;
+  std::vector<PackTile> ta, tb;
+  std::vector<PairTC> ptc;
+  int64_t bytesA = 0, bytesB = 0;
+  if (tc) {
+    std::map<int64_t, int> ua, ub;
+    ptc.resize(n_pairs);
+    for (int ii = 0; ii < n_pairs; ++ii) {
+      const PairDev& P = hp[ii];
+      const int kt = (P.k + TC_BK - 1) / TC_BK;
+      auto ia = ua.find(P.a_off);
+      if (ia == ua.end()) {
+        const int rt = (P.m + TC_BM - 1) / TC_BM;
+        ja.push_back(PackJob{P.a_off, bytesA, P.m, P.k, P.rowA, P.colA, kt, P.a_mfast});
+        for (int r = 0; r < rt; ++r)
+          for (int k = 0; k < kt; ++k) ta.push_back(PackTile{(int32_t)ja.size() - 1, r, k});
+        bytesA += (int64_t)rt * kt * TC_TILE_BYTES;
+        ia = ua.emplace(P.a_off, (int)ja.size() - 1).first;
+      }
+      auto ib = ub.find(P.b_off);
+      if (ib == ub.end()) {
+        const int rt = (P.n + TC_BN - 1) / TC_BN;
+        jb.push_back(PackJob{P.b_off, bytesB, P.n, P.k, P.colB, P.rowB, kt, P.b_kfast ? 0 : 1});
+        for (int r = 0; r < rt; ++r)
+          for (int k = 0; k < kt; ++k) tb.push_back(PackTile{(int32_t)jb.size() - 1, r, k});
+        bytesB += (int64_t)rt * kt * TC_TILE_BYTES;
+        ib = ub.emplace(P.b_off, (int)jb.size() - 1).first;
+      }
+      ptc[ii] = PairTC{ja[ia->second].dst, jb[ib->second].dst, kt, 0};
+    }
+    TT_REQUIRE(ta.size() < (1u << 31) && tb.size() < (1u << 31), "tt_contract_plan: too many packed tiles");
+  }
+
   tt_plan* plan = new tt_plan();
   plan->precision = precision;
+  plan->n_tilesA = (int)ta.size();
+  plan->n_tilesB = (int)tb.size();
+  plan->bytesA = bytesA;
+  plan->bytesB = bytesB;
   plan->n_tasks = (int)tsorted.size();
   plan->n_pairs = n_pairs;
   plan->n_out = n_out;
@@ -659,7 +695,17 @@ int tt_contract_plan(tt_ctx* ctx, const tt_out_block* outs, int n_out,
   plan->d_tab = tt::pool_alloc<int32_t>(ctx, (size_t)tab_len);
   plan->d_status = tt::pool_alloc<int>(ctx, 1);
   TableJob* d_jobs = tt::pool_alloc<TableJob>(ctx, jobs.size());
-  if (!plan->d_tasks || !plan->d_outs || !plan->d_pairs || !plan->d_tab || !plan->d_status || !d_jobs) {
+  bool tc_ok = true;
+  if (tc) {
+    plan->d_jobsA = tt::pool_alloc<PackJob>(ctx, ja.size());
+    plan->d_jobsB = tt::pool_alloc<PackJob>(ctx, jb.size());
+    plan->d_tilesA = tt::pool_alloc<PackTile>(ctx, ta.size());
+    plan->d_tilesB = tt::pool_alloc<PackTile>(ctx, tb.size());
+    plan->d_pairtc = tt::pool_alloc<PairTC>(ctx, ptc.size());
+    tc_ok = (ja.empty() || plan->d_jobsA) && (jb.empty() || plan->d_jobsB) && (ta.empty() || plan->d_tilesA) &&
+            (tb.empty() || plan->d_tilesB) && (ptc.empty() || plan->d_pairtc);
+  }
+  if (!plan->d_tasks || !plan->d_outs || !plan->d_pairs || !plan->d_tab || !plan->d_status || !d_jobs || !tc_ok) {
     tt_plan_destroy(ctx, plan);
     tt::pool_free(ctx, d_jobs);
     return tt::fail(TT_ERR_OOM, "tt_contract_plan: device allocation failed");
@@ -671,6 +717,13 @@ int tt_contract_plan(tt_ctx* ctx, const tt_out_block* outs, int n_out,
   TT_CUDA(tt::h2d_async(ctx, plan->d_outs, ho.data(), sizeof(OutDev) * ho.size()));
   TT_CUDA(tt::h2d_async(ctx, plan->d_pairs, hp.data(), sizeof(PairDev) * hp.size()));
   TT_CUDA(tt::h2d_async(ctx, d_jobs, jobs.data(), sizeof(TableJob) * jobs.size()));
+  if (tc) {
+    TT_CUDA(tt::h2d_async(ctx, plan->d_jobsA, ja.data(), sizeof(PackJob) * ja.size()));
+    TT_CUDA(tt::h2d_async(ctx, plan->d_jobsB, jb.data(), sizeof(PackJob) * jb.size()));
+    TT_CUDA(tt::h2d_async(ctx, plan->d_tilesA, ta.data(), sizeof(PackTile) * ta.size()));
+    TT_CUDA(tt::h2d_async(ctx, plan->d_tilesB, tb.data(), sizeof(PackTile) * tb.size()));
+    TT_CUDA(tt::h2d_async(ctx, plan->d_pairtc, ptc.data(), sizeof(PairTC) * ptc.size()));
+  }
   if (!jobs.empty()) {
     expand_tables<<<(unsigned)jobs.size(), 128, 0, s>>>(d_jobs, (int)jobs.size(), plan->d_tab);
     TT_LAUNCH_CHECK(ctx);
@@ -688,23 +741,48 @@ int tt_contract_exec(tt_ctx* ctx, const tt_plan* plan, const double* A, const do
   if (!attr_set) {
     TT_CUDA(cudaFuncSetAttribute(grouped_dgemm, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)SMEM_BYTES));
-    TT_CUDA(cudaFuncSetAttribute(grouped_tc<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)TC_SMEM_BYTES));
-    TT_CUDA(cudaFuncSetAttribute(grouped_tc<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)TC_SMEM_BYTES));
+    TT_CUDA(cudaFuncSetAttribute(grouped_tc_bulk<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)TC_BULK_SMEM));
+    TT_CUDA(cudaFuncSetAttribute(grouped_tc_bulk<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)TC_BULK_SMEM));
     attr_set = true;
   }
   if (plan->precision == TT_PREC_FP64) {
     grouped_dgemm<<<plan->n_tasks, THREADS, SMEM_BYTES, ctx->stream>>>(
         plan->d_tasks, plan->d_outs, plan->d_pairs, plan->d_tab, A, B, C, alpha);
-  } else if (plan->precision == TT_PREC_TF32X3) {
-    grouped_tc<true><<<plan->n_tasks, TC_THREADS, TC_SMEM_BYTES, ctx->stream>>>(
-        plan->d_tasks, plan->d_outs, plan->d_pairs, plan->d_tab, A, B, C, alpha, plan->d_status);
-  } else {
-    grouped_tc<false><<<plan->n_tasks, TC_THREADS, TC_SMEM_BYTES, ctx->stream>>>(
-        plan->d_tasks, plan->d_outs, plan->d_pairs, plan->d_tab, A, B, C, alpha, plan->d_status);
+    TT_LAUNCH_CHECK(ctx);
+    return TT_OK;
   }
-  TT_LAUNCH_CHECK(ctx);
+  // pack both operands into tensor-core tiles (pool buffers, released in stream order)
+  const bool split = plan->precision == TT_PREC_TF32X3;
+  uint8_t* pa = tt::pool_alloc<uint8_t>(ctx, (size_t)std::max<int64_t>(plan->bytesA, 16));
+  uint8_t* pb = tt::pool_alloc<uint8_t>(ctx, (size_t)std::max<int64_t>(plan->bytesB, 16));
+  if (!pa || !pb) {
+    tt::pool_free(ctx, pa);
+    tt::pool_free(ctx, pb);
+    return tt::fail(TT_ERR_OOM, "tt_contract_exec: packed operand allocation failed");
+  }
+  if (plan->n_tilesA) {
+    if (split) pack_tf32<true><<<plan->n_tilesA, 128, 0, ctx->stream>>>(plan->d_jobsA, plan->d_tilesA, plan->d_tab, A, pa);
+    else pack_tf32<false><<<plan->n_tilesA, 128, 0, ctx->stream>>>(plan->d_jobsA, plan->d_tilesA, plan->d_tab, A, pa);
+    TT_LAUNCH_CHECK(ctx);
+  }
+  if (plan->n_tilesB) {
+    if (split) pack_tf32<true><<<plan->n_tilesB, 128, 0, ctx->stream>>>(plan->d_jobsB, plan->d_tilesB, plan->d_tab, B, pb);
+    else pack_tf32<false><<<plan->n_tilesB, 128, 0, ctx->stream>>>(plan->d_jobsB, plan->d_tilesB, plan->d_tab, B, pb);
+    TT_LAUNCH_CHECK(ctx);
+  }
+  if (split)
+    grouped_tc_bulk<true><<<plan->n_tasks, 128, TC_BULK_SMEM, ctx->stream>>>(
+        plan->d_tasks, plan->d_outs, plan->d_pairtc, pa, pb, C, alpha, plan->d_status);
+  else
+    grouped_tc_bulk<false><<<plan->n_tasks, 128, TC_BULK_SMEM, ctx->stream>>>(
+        plan->d_tasks, plan->d_outs, plan->d_pairtc, pa, pb, C, alpha, plan->d_status);
+  cudaError_t le = cudaGetLastError();
+  tt::pool_free(ctx, pa);
+  tt::pool_free(ctx, pb);
+  if (le != cudaSuccess) return tt::cuda_fail(le, "tt_contract_exec: tensor-core launch", __FILE__, __LINE__);
+  tt::count_launch(ctx);
   return TT_OK;
 }
 
@@ -716,6 +794,11 @@ int tt_plan_destroy(tt_ctx* ctx, tt_plan* plan) {
     tt::pool_free(ctx, plan->d_pairs);
     tt::pool_free(ctx, plan->d_tab);
     tt::pool_free(ctx, plan->d_status);
+    tt::pool_free(ctx, plan->d_jobsA);
+    tt::pool_free(ctx, plan->d_jobsB);
+    tt::pool_free(ctx, plan->d_tilesA);
+    tt::pool_free(ctx, plan->d_tilesB);
+    tt::pool_free(ctx, plan->d_pairtc);
   }
   delete plan;
   return TT_OK;

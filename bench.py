@@ -63,8 +63,11 @@ def parse():
     p.add_argument("--cpu-budget", type=float, default=20.0, help="seconds of CPU baseline sampling")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision (tcgen05 3xTF32) arm")
-    p.add_argument("--workload", default="heisenberg", choices=["heisenberg", "xxz-chains"],
-                   help="heisenberg: the default sweep benchmark; xxz-chains: independent chains sharing the GPU")
+    p.add_argument("--workload", default="heisenberg", choices=["heisenberg", "xxz-chains", "gemm"],
+                   help="heisenberg: the default sweep benchmark; xxz-chains: independent chains sharing the "
+                        "GPU; gemm: one single-block contraction per precision (kernel throughput)")
+    p.add_argument("--gemm-size", type=int, default=4096)
+    p.add_argument("--precisions", default="fp64,tf32x3,tf32")
     p.add_argument("--chains", type=int, default=16)
     p.add_argument("--chain-sweeps", type=int, default=3)
     p.add_argument("--streams", type=int, default=16)
@@ -458,12 +461,66 @@ def run_chains(args):
         "max_energy_difference": max(abs(a - b) for a, b in zip(seq, conc))}))
 
 
+def run_gemm(args):
+    """Throughput of the grouped contraction kernels on one large block: C(m, n)
+    = A(m, k) B(k, n), m = n = k = --gemm-size, random FP64 operands, as a
+    qtensor contraction with one sector per index; W untimed and K timed
+    launches per precision, CUDA events on the library stream.  The
+    mixed-precision times include the packing of both operands."""
+    import numpy as np
+    import torch
+    import tt_b200
+    from oracle.qtensor import QIndex, QTensor, Inward, Outward, Link, qn
+    ctx = tt_b200.Context(0)
+    stream = torch.cuda.ExternalStream(ctx.stream())
+    n = args.gemm_size
+    rng = np.random.default_rng(0)
+
+    def idx(arrow, name):
+        ix = QIndex(arrow, name, Link, 0)
+        ix.add_qn(qn(0), n)
+        return ix
+
+    i, k, j = idx(Inward, "i"), idx(Outward, "k"), idx(Inward, "j")
+    A = QTensor([i, k])
+    A.init_block()
+    A.blocks[0][...] = rng.standard_normal((n, n))
+    B = QTensor([k.dagged(), j])
+    B.init_block()
+    B.blocks[0][...] = rng.standard_normal((n, n))
+    gA, gB = tt_b200.QTensor.from_oracle(A), tt_b200.QTensor.from_oracle(B)
+    out = {}
+    for prec in args.precisions.split(","):
+        tt_b200.set_precision(op=prec)
+        for _ in range(args.warmup):
+            C = gA * gB
+        ctx.sync()
+        ms = 0.0
+        for _ in range(args.steps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            C = gA * gB
+            e1.record(stream)
+            e1.synchronize()
+            ms += e0.elapsed_time(e1)
+            del C
+        out[prec] = {"ms": ms / args.steps, "tflops": 2.0 * n ** 3 / (ms / args.steps * 1e-3) / 1e12}
+    tt_b200.set_precision()
+    print(json.dumps({"metric": "single-block contraction throughput", "unit": "TFLOP/s (algorithmic)",
+                      "config": {"workload": "C = A B, %d^3, one QN sector" % n, "steps": args.steps,
+                                 "warmup": args.warmup}, "results": out}))
+    del gA, gB
+    ctx.close()
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
     elif args.workload == "xxz-chains":
         run_chains(args)
+    elif args.workload == "gemm":
+        run_gemm(args)
     else:
         run_ours(args)
 

@@ -63,9 +63,17 @@ def parse():
     p.add_argument("--cpu-budget", type=float, default=20.0, help="seconds of CPU baseline sampling")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision (tcgen05 3xTF32) arm")
-    p.add_argument("--workload", default="heisenberg", choices=["heisenberg", "xxz-chains", "gemm"],
+    p.add_argument("--workload", default="heisenberg", choices=["heisenberg", "xxz-chains", "gemm", "j1j2"],
                    help="heisenberg: the default sweep benchmark; xxz-chains: independent chains sharing the "
-                        "GPU; gemm: one single-block contraction per precision (kernel throughput)")
+                        "GPU; gemm: one single-block contraction per precision (kernel throughput); j1j2: "
+                        "FP64 vs mixed sweeps on the J1-J2 cylinder at --maxdim")
+    p.add_argument("--maxdim", type=int, default=1024)
+    p.add_argument("--nx", type=int, default=16)
+    p.add_argument("--ny", type=int, default=6)
+    p.add_argument("--breakdown", action="store_true")
+    p.add_argument("--profile-step", type=int, default=-1,
+                   help="j1j2: bracket this two-site step of the first timed sweep with a profiler range "
+                        "(for ncu --profile-from-start off)")
     p.add_argument("--gemm-size", type=int, default=4096)
     p.add_argument("--precisions", default="fp64,tf32x3,tf32")
     p.add_argument("--chains", type=int, default=16)
@@ -261,10 +269,12 @@ def fp64_peak_tflops(torch):
 
 
 def mixed_arm(args, ctx, stream, flush, e_fp64, torch, tt_b200, qdmrg):
-    """The same schedule with H_eff*x and the environment updates on the
-    tcgen05 3xTF32 path (GS, Rayleigh-Ritz, SVD in FP64; sweep energy
-    <psi|H|psi> contracted in FP64), timed like the FP64 arm."""
-    tt_b200.set_precision(heff="tf32x3", env="tf32x3")
+    """The same schedule with H_eff*x and the environment updates in the
+    automatic mixed form (3xTF32 on tcgen05 for the contractions the cost
+    model predicts faster there, FP64 DMMA for the rest; GS, Rayleigh-Ritz,
+    SVD in FP64; sweep energy <psi|H|psi> contracted in FP64), timed like the
+    FP64 arm."""
+    tt_b200.set_precision(heff="tf32x3-auto", env="tf32x3-auto")
     try:
         psi = tt_b200.QMPS(L_SITES, qdmrg.neel(L_SITES))
         run = tt_b200.QDMRG(psi, tt_b200.QMPO(L_SITES))
@@ -289,7 +299,8 @@ def mixed_arm(args, ctx, stream, flush, e_fp64, torch, tt_b200, qdmrg):
         tt_b200.set_precision()
     fl = st1["heff_flops"] - st0["heff_flops"]
     hs = st1["heff_seconds"] - st0["heff_seconds"]
-    return {"precision": "3xTF32 tcgen05 H_eff*x and environments; FP64 GS, Rayleigh-Ritz, SVD, sweep energy",
+    return {"precision": "tf32x3-auto: 3xTF32 tcgen05 or FP64 DMMA per contraction (cost model) for H_eff*x and "
+                         "environments; FP64 GS, Rayleigh-Ritz, SVD, sweep energy",
             "value": total_ms * 1e-3 / args.steps, "unit": "s/sweep", "energy": energy,
             "dE_per_site_vs_fp64": abs(energy - e_fp64) / L_SITES, "heff_tflops": fl / hs / 1e12 if hs > 0 else 0.0,
             "bond_dims_mid": psi.bond_dims()[L_SITES // 2]}
@@ -513,6 +524,129 @@ def run_gemm(args):
     ctx.close()
 
 
+def planning_counters(tt_b200):
+    """Host seconds and calls spent in block-structure computation and in
+    contraction-plan creation on this thread so far."""
+    import ctypes as C
+    ts, tp = C.c_double(), C.c_double()
+    ns, np_ = C.c_int64(), C.c_int64()
+    tt_b200.lib.tt_dmrg_planning_counters(C.byref(ts), C.byref(ns), C.byref(tp), C.byref(np_))
+    return {"structure_s": ts.value, "structure_calls": ns.value, "plan_s": tp.value, "plan_calls": np_.value}
+
+
+def run_j1j2(args):
+    """FP64 against mixed precision at large bond dimension, on the J1-J2
+    cylinder configuration: spin-1/2 J1-J2 Heisenberg model (J1 = 1, J2 = 0.5)
+    on an Nx x Ny cylinder (periodic in y, square_next_neighbor ordering),
+    U(1) Sz = 0, Neel start, cutoff 1e-10, Davidson max 6 iterations.  One
+    FP64 ramp (maxdim doubling from 64 to --maxdim, noise 1e-6 decaying to 0
+    over its sweeps) builds the starting state, which is checkpointed; each
+    precision then loads it and runs W warm-up and K timed sweeps at
+    --maxdim (CUDA events on the library stream, L2 flushed before each).
+    With --breakdown one further sweep per precision runs with a
+    synchronisation between step phases and reports where its time goes."""
+    import torch
+    import tt_b200
+    from oracle import qdmrg
+    Nx, Ny, J2 = args.nx, args.ny, 0.5
+    N = Nx * Ny
+    a = tt_b200.AutoMPO()
+    for s1, s2, typ, *_ in tt_b200.square_next_neighbor(Nx, Ny, True):
+        J = 1.0 if typ == 1 else J2
+        a.add(0.5 * J, "S+", s1 - 1, "S-", s2 - 1)
+        a.add(0.5 * J, "S-", s1 - 1, "S+", s2 - 1)
+        a.add(J, "Sz", s1 - 1, "Sz", s2 - 1)
+    ctx = tt_b200.Context(0)
+    stream = torch.cuda.ExternalStream(ctx.stream())
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    H = tt_b200.QMPO.from_autompo(a, N)
+    cutoff, mr = 1e-10, MAX_RESTART
+    ramp = []
+    m = 64
+    while m < args.maxdim:
+        ramp.append(m)
+        m *= 2
+    noise = [1e-6 * (1.0 - k / max(1, len(ramp))) for k in range(len(ramp))]
+    t0 = time.perf_counter()
+    psi = tt_b200.QMPS(N, qdmrg.neel(N))
+    run = tt_b200.QDMRG(psi, H)
+    for m, nz in zip(ramp, noise):
+        run.sweep(m, cutoff, mr, nz)
+    run.finish()
+    t_ramp = time.perf_counter() - t0
+    tmpdir = tempfile.mkdtemp()
+    ck = os.path.join(tmpdir, "start")
+    psi.save(ck)
+    start_dims = psi.bond_dims()
+    del run, psi
+    out = {}
+    for prec in args.precisions.split(","):
+        if prec not in tt_b200.PRECISIONS:
+            continue
+        tt_b200.set_precision(heff=prec, env=prec)
+        try:
+            psi = tt_b200.QMPS.load(ck + ".ttmps")
+            run = tt_b200.QDMRG(psi, H)
+            for _ in range(args.warmup):
+                run.sweep(args.maxdim, cutoff, mr)
+            st0 = run.stats()
+            pc0 = planning_counters(tt_b200)
+            ms, e = 0.0, None
+            tt_b200.lib.tt_dmrg_set_profile_step(args.profile_step)
+            for it in range(args.steps):
+                if it == 1:
+                    tt_b200.lib.tt_dmrg_set_profile_step(-1)
+                flush.zero_()
+                torch.cuda.synchronize()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                e = run.sweep(args.maxdim, cutoff, mr)
+                e1.record(stream)
+                e1.synchronize()
+                ms += e0.elapsed_time(e1)
+            tt_b200.lib.tt_dmrg_set_profile_step(-1)
+            pc1 = planning_counters(tt_b200)
+            st1 = run.stats()
+            fl = st1["heff_flops"] - st0["heff_flops"]
+            hs = st1["heff_seconds"] - st0["heff_seconds"]
+            res = {"s_per_sweep": ms * 1e-3 / args.steps, "energy": e, "heff_tflops": fl / hs / 1e12 if hs else 0.0,
+                   "heff_s_per_sweep": hs / args.steps, "heff_tflop_per_sweep": fl / args.steps / 1e12,
+                   "max_bond_dim": max(psi.bond_dims()),
+                   "host_planning_s_per_sweep": {k: (pc1[k] - pc0[k]) / args.steps for k in pc0}}
+            if args.breakdown:
+                lib = tt_b200.lib
+                lib.tt_dmrg_set_profiling(1)
+                n0 = len(run.profile())
+                try:
+                    run.sweep(args.maxdim, cutoff, mr)
+                finally:
+                    lib.tt_dmrg_set_profiling(0)
+                prof = run.profile()[n0:]
+                res["breakdown_s"] = {"davidson": sum(p[1] for p in prof), "svd": sum(p[2] for p in prof),
+                                      "env": sum(p[3] for p in prof), "other": sum(p[4] for p in prof),
+                                      "largest_svd_sector": max(p[0] for p in prof)}
+            out[prec] = res
+            del run, psi
+        finally:
+            tt_b200.set_precision()
+    ref = out.get("fp64")
+    for prec, res in out.items():
+        if ref is not None and prec != "fp64":
+            res["dE_per_site_vs_fp64"] = abs(res["energy"] - ref["energy"]) / N
+            res["speedup_vs_fp64"] = ref["s_per_sweep"] / res["s_per_sweep"]
+    print(json.dumps({"metric": "sec/sweep: mixed precision vs FP64 at large bond dimension", "unit": "s/sweep",
+                      "higher_is_better": False, "n_gpus": 1, "data": "synthetic",
+                      "config": {"workload": "U(1) J1-J2 Heisenberg %dx%d cylinder (periodic y), J2=0.5, Sz=0 "
+                                             "Neel start, cutoff 1e-10, Davidson max 6 iters" % (Nx, Ny),
+                                 "maxdim": args.maxdim, "ramp": ramp, "ramp_noise": noise,
+                                 "ramp_seconds": t_ramp, "start_max_bond_dim": max(start_dims),
+                                 "steps": args.steps, "warmup": args.warmup,
+                                 "l2": "L2 flushed before each timed sweep"},
+                      "results": out}))
+    H = None
+    ctx.close()
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -521,6 +655,8 @@ def main():
         run_chains(args)
     elif args.workload == "gemm":
         run_gemm(args)
+    elif args.workload == "j1j2":
+        run_j1j2(args)
     else:
         run_ours(args)
 

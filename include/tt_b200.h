@@ -55,6 +55,13 @@ extern "C" {
 #define TT_PREC_TF32       1  /* tcgen05 kind::tf32, FP32 accumulator in TMEM */
 #define TT_PREC_TF32X3     2  /* tcgen05 kind::tf32 on hi/lo splits of the FP64
                                  operands (hi*hi + hi*lo + lo*hi), FP32 accumulator */
+/* Per contraction, TF32 / 3xTF32 where the plan's cost model (padded tile
+ * work, DRAM bytes including the operand packing, launches) predicts the
+ * tensor-core form to be faster than FP64 DMMA, FP64 elsewhere -- e.g. the
+ * bandwidth-bound contractions over a small MPO link.  Never less accurate
+ * than the forced kind. */
+#define TT_PREC_TF32_AUTO   3
+#define TT_PREC_TF32X3_AUTO 4
 
 #define TT_MAX_MODES       6  /* tensor modes per GEMM dimension of a pair   */
 #define TT_DAV_MAX        16  /* Krylov vectors of the device-resident Davidson */
@@ -128,6 +135,9 @@ int tt_contract_exec(tt_ctx* ctx, const tt_plan* plan, const double* A,
 int tt_plan_destroy(tt_ctx* ctx, tt_plan* plan);
 /* Algorithmic work of one exec: sum over pairs of 2*m*n*k. */
 int tt_plan_flops(const tt_plan* plan, double* flops);
+/* The precision the plan runs in (TT_PREC_FP64 / TF32 / TF32X3): an *_AUTO
+ * request resolves to one of them when the plan is built. */
+int tt_plan_precision(const tt_plan* plan, int* precision);
 /* Device status of the plan's tensor-core launches since the plan was built:
  * TT_OK, or TT_ERR_TIMEOUT when a bounded wait on the MMA completion barrier
  * gave up (the tile was then skipped).  Synchronises the context's stream. */

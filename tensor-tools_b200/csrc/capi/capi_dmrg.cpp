@@ -89,7 +89,7 @@ int tt_dmrg_davidson_fallbacks(int64_t* n) {
 }
 
 int tt_dmrg_set_precision(int op, int heff, int env) {
-  auto ok = [](int p) { return p == TT_PREC_FP64 || p == TT_PREC_TF32 || p == TT_PREC_TF32X3; };
+  auto ok = [](int p) { return p >= TT_PREC_FP64 && p <= TT_PREC_TF32X3_AUTO; };
   TT_ARG(ok(op) && ok(heff) && ok(env));
   TT_GUARD({
     ttb::rt().precision = op;

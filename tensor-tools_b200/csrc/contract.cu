@@ -523,6 +523,51 @@ grouped_tc_bulk(const TaskDev* __restrict__ tasks, const OutDev* __restrict__ ou
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TC_BULK_COLS) : "memory");
 }
 
+// Cost model of the *_AUTO precisions: predicted device time (microseconds)
+// of one exec of a contraction in `prec` (FP64 DMMA, or a tcgen05 kind with
+// its two packing launches).  Work is counted on padded tiles (an output tile
+// runs every pair of its block over k rounded up to the k-step); the grid is
+// bound by the total at the full-chip rate, by its longest tile at one SM's
+// rate, and by its DRAM bytes.  The tensor-core form moves each operand
+// element three more times (read by the packer, written packed, read packed),
+// so a contraction with a small k -- the bandwidth-bound middle contraction
+// of H_eff*x and of the environment update -- stays in FP64, which is exact
+// to more digits and no slower there.  Rates are the measured single-block
+// throughputs of the two kernels on B200 (4096^3: DMMA 26 TFLOP/s, tcgen05
+// 690 TFLOP/s of TF32 products).
+double predict_us(const tt_out_block* outs, int n_out, const std::vector<PairDev>& hp,
+                  const std::vector<int>& first, int prec, int num_sms) {
+  constexpr double kDmmaRate = 27e12, kTcRate = 650e12, kHbm = 6.0e12, kLaunchUs = 2.5;
+  const bool tc = prec != TT_PREC_FP64;
+  const int tm = tc ? TC_BM : BM, tn = tc ? TC_BN : BN, tk = tc ? TC_BK : BK;
+  const double rate = tc ? (prec == TT_PREC_TF32X3 ? kTcRate / 3.0 : kTcRate) : kDmmaRate;
+  auto up = [](int x, int t) { return (double)((x + t - 1) / t) * t; };
+  double total = 0.0, longest = 0.0, bytes = 0.0;
+  std::map<int64_t, std::pair<double, double>> ua, ub;  // distinct operand blocks: (elements, padded elements)
+  for (int o = 0; o < n_out; ++o) {
+    double kpad = 0.0;
+    for (int i = first[o]; i < first[o + 1]; ++i) {
+      const PairDev& P = hp[i];
+      kpad += up(P.k, tk);
+      ua.emplace(P.a_off, std::make_pair((double)P.m * P.k, up(P.m, tm) * up(P.k, tk)));
+      ub.emplace(P.b_off, std::make_pair((double)P.n * P.k, up(P.n, tn) * up(P.k, tk)));
+    }
+    const double tiles = up(outs[o].m, tm) / tm * (up(outs[o].n, tn) / tn);
+    const double task = 2.0 * tm * tn * kpad;
+    total += tiles * task;
+    if (tiles > 0) longest = std::max(longest, task);
+    bytes += 8.0 * outs[o].m * outs[o].n;  // C
+  }
+  // FP64 reads every operand element once from DRAM; the tensor-core form
+  // also writes the packed tiles (hi + lo: 8 bytes per padded element, TF32:
+  // 4) and reads them back
+  const double packed = prec == TT_PREC_TF32X3 ? 8.0 : 4.0;
+  for (const auto* u : {&ua, &ub})
+    for (const auto& kv : *u) bytes += 8.0 * kv.second.first + (tc ? 2.0 * packed * kv.second.second : 0.0);
+  const double t = std::max({total / rate, longest / (rate / std::max(1, num_sms)), bytes / kHbm});
+  return t * 1e6 + (tc ? 3 : 1) * kLaunchUs;
+}
+
 }  // namespace
 
 struct tt_plan {
@@ -555,10 +600,10 @@ int tt_contract_plan(tt_ctx* ctx, const tt_out_block* outs, int n_out,
                      tt_plan** plan_out) {
   TT_REQUIRE(ctx && plan_out, "tt_contract_plan: null argument");
   TT_REQUIRE(n_out >= 0 && n_pairs >= 0, "tt_contract_plan: negative count");
-  TT_REQUIRE(precision == TT_PREC_FP64 || precision == TT_PREC_TF32 || precision == TT_PREC_TF32X3,
+  TT_REQUIRE(precision >= TT_PREC_FP64 && precision <= TT_PREC_TF32X3_AUTO,
              "tt_contract_plan: unsupported precision");
-  const bool tc = precision != TT_PREC_FP64;
-  const int tile_m = tc ? TC_BM : BM, tile_n = tc ? TC_BN : BN;
+  const bool automatic = precision == TT_PREC_TF32_AUTO || precision == TT_PREC_TF32X3_AUTO;
+  if (automatic) precision = precision == TT_PREC_TF32_AUTO ? TT_PREC_TF32 : TT_PREC_TF32X3;
   *plan_out = nullptr;
   // pairs grouped by output block (stable: keeps the reference's accumulation order)
   std::vector<int> order(n_pairs);
@@ -624,6 +669,11 @@ int tt_contract_plan(tt_ctx* ctx, const tt_out_block* outs, int n_out,
   }
   TT_REQUIRE(tab_len < (1ll << 31), "tt_contract_plan: offset tables too large");
   for (int o = 0; o < n_out; ++o) first[o + 1] += first[o];
+  if (automatic && predict_us(outs, n_out, hp, first, TT_PREC_FP64, ctx->num_sms) <=
+                       predict_us(outs, n_out, hp, first, precision, ctx->num_sms))
+    precision = TT_PREC_FP64;
+  const bool tc = precision != TT_PREC_FP64;
+  const int tile_m = tc ? TC_BM : BM, tile_n = tc ? TC_BN : BN;
   // tile tasks, longest first (LPT) so heavy blocks start early
   std::vector<TaskDev> tasks;
   std::vector<int64_t> tcost;
@@ -810,6 +860,12 @@ int tt_plan_device_status(tt_ctx* ctx, const tt_plan* plan, int* status) {
   TT_CUDA(cudaMemcpyAsync(&h, plan->d_status, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
   TT_CUDA(cudaStreamSynchronize(ctx->stream));
   *status = h;
+  return TT_OK;
+}
+
+int tt_plan_precision(const tt_plan* plan, int* precision) {
+  TT_REQUIRE(plan && precision, "tt_plan_precision: null argument");
+  *precision = plan->precision;
   return TT_OK;
 }
 

@@ -943,6 +943,7 @@ void updateSite(qMPS& psi, qMPO& H, std::vector<qtensor>& TR, std::vector<qtenso
   } else {
     svd_bond(x, psi.A[l], psi.A[r], mid, S, direction, cutoff, (unsigned long)max_bd, &info);
   }
+  if (rt().profile) check(tt_ctx_synchronize(ctx()), "sync");  // the SVD's asynchronous tail counts as SVD
   auto t2 = std::chrono::steady_clock::now();
   psi.bond_dims[r] = (unsigned)S.total_size();
   psi.center = (int)(direction == MoveFromLeft ? r : l);

@@ -676,7 +676,7 @@ std::shared_ptr<const CachedContraction> contract_cached(const qtensor& A, const
 }
 
 tt_plan* CachedContraction::plan_for(int precision) const {
-  if (precision < 0 || precision > 2) throw std::runtime_error("plan_for: bad precision");
+  if (precision < TT_PREC_FP64 || precision > TT_PREC_TF32X3_AUTO) throw std::runtime_error("plan_for: bad precision");
   if (cs.outs.empty()) return nullptr;
   if (!plans[precision]) plans[precision] = make_plan(cs, precision);
   return plans[precision]->get();

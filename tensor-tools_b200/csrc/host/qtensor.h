@@ -239,9 +239,9 @@ void contract_structure(const qtensor& A, const qtensor& B, ContractStructure& o
 // dimensions settle, so steady-state sweeps plan nothing.
 struct CachedContraction {
   ContractStructure cs;
-  // device plans by precision (TT_PREC_FP64 / TF32 / TF32X3), built on first
-  // use; null when cs has no output blocks
-  mutable std::shared_ptr<class PlanHandle> plans[3];
+  // device plans by requested precision (TT_PREC_FP64 ... TT_PREC_TF32X3_AUTO),
+  // built on first use; null when cs has no output blocks
+  mutable std::shared_ptr<class PlanHandle> plans[TT_PREC_TF32X3_AUTO + 1];
   tt_plan* plan_for(int precision) const;
 };
 // need_plan builds the plan of rt().precision right away.

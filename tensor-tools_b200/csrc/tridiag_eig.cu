@@ -15,6 +15,8 @@
 //   (gap <= 1e-3 ||T||, the clustering rule of LAPACK's inverse iteration);
 //   back-transformation z = Q y with the stored reflectors.
 // The matrix sits in shared memory when n <= 160, otherwise in global memory.
+#include <cooperative_groups.h>
+
 #include <algorithm>
 #include <cfloat>
 #include <cmath>
@@ -454,6 +456,411 @@ tridiag_eigvecs(const EigDev* __restrict__ probs, const double* G, const double*
   }
 }
 
+// ---------------------------------------------------------------------------
+// Sectors with n > SM_N: one thread-block cluster (CL CTAs, distributed shared
+// memory) per sector, so a large density matrix is reduced by CL SMs at once
+// instead of one SM streaming it from L2.
+//
+// Phase 1: the columns of G are dealt out cyclically (column c to CTA c % CL)
+// and held in each CTA's shared memory when they fit (global otherwise).  For
+// column k the owner builds the reflector v and publishes it; every CTA forms
+// p = tau A22 v on its own columns and the partial p.v; after a second
+// cluster barrier every CTA gathers p and the partial dots (fixed order, so
+// every CTA holds the same w = p - (tau/2)(p.v) v) and applies the rank-2
+// update to its own columns.  Two cluster barriers per column; the published
+// buffers alternate by the parity of k, so no third barrier is needed.
+// Bisection then runs over all warps of the cluster.
+//
+// Phase 2: CTA r owns eigenvectors [r q, r q + q), q = ceil(nvec / CL).
+// Inverse iteration runs one thread per vector.  Gram-Schmidt (twice, inside
+// the clusters of close eigenvalues as in the one-CTA kernel) takes vectors
+// in order: each CTA projects the current vector y on its own earlier cluster
+// members and publishes the partial sum of projections; after a cluster
+// barrier every CTA subtracts all partial sums in CTA order.  Every CTA thus
+// holds the same iterate, decides collapse/retry identically, and one barrier
+// per projection round suffices (partial sums alternate between two buffers).
+// The back-transformation needs no communication: every CTA applies all
+// reflectors to its own vectors, staged a few at a time in shared memory.
+// Every loop bound here is the same in all CTAs of a cluster, so every CTA
+// reaches every cluster barrier.
+namespace cgx = cooperative_groups;
+
+constexpr int CL_STAGE = 4;  // reflectors staged per round of the back-transformation
+
+__device__ __forceinline__ int first_owned(int from, int rank, int CL) {
+  // smallest l with rank + CL * l >= from
+  return from <= rank ? 0 : (from - rank + CL - 1) / CL;
+}
+
+__global__ void __launch_bounds__(TT)
+tridiag_eigvals_cluster(const EigDev* __restrict__ probs, double* G, double* Tg, double* W, int cap) {
+  extern __shared__ double sm[];
+  __shared__ double red[33];
+  __shared__ double s_tau, s_beta, s_scale;
+  cgx::cluster_group cluster = cgx::this_cluster();
+  const int CL = (int)cluster.num_blocks();
+  const int rank = (int)cluster.block_rank();
+  const EigDev P = probs[blockIdx.x / CL];
+  const int n = P.n;
+  const int tid = threadIdx.x;
+  if (n <= 0) return;  // the same problem for the whole cluster
+  double* Gp = G + P.g_off;
+  double* Wp = W + P.w_off;
+  double* dg = Tg + 3 * P.w_off;
+  double* eg = dg + n;
+  double* tg = eg + n;
+  const int lcols = (n + CL - 1) / CL;
+  const int64_t extra = 4 * (int64_t)n + 2 * lcols + 8;
+  const bool in_smem = (int64_t)lcols * n + extra <= cap;
+  double* rest = in_smem ? sm + (int64_t)lcols * n : sm;
+  double* vbuf = rest;          // [2][n] reflector published by the column's owner
+  double* vloc = vbuf + 2 * n;  // this CTA's copy of v
+  double* wloc = vloc + n;      // this CTA's copy of w
+  double* pown = wloc + n;      // [2][lcols] p on the owned columns
+  double* misc = pown + 2 * lcols;  // tau[2], partial p.v[2]
+  auto col = [&](int l) -> double* {  // l-th owned column (global column rank + CL l)
+    return in_smem ? sm + (int64_t)l * n : Gp + (int64_t)(rank + CL * l) * n;
+  };
+  if (in_smem)
+    for (int l = 0; l < lcols && rank + CL * l < n; ++l)
+      for (int i = tid; i < n; i += blockDim.x) sm[(int64_t)l * n + i] = Gp[(int64_t)(rank + CL * l) * n + i];
+  __syncthreads();
+  const int warp = tid >> 5, lane = tid & 31, nw = blockDim.x >> 5;
+  for (int k = 0; k + 2 < n; ++k) {
+    const int m = n - k - 1;
+    const int par = k & 1;
+    const int owner = k % CL;
+    if (rank == owner) {
+      double* a = col(k / CL);
+      double loc = 0.0;
+      for (int i = 1 + tid; i < m; i += blockDim.x) {
+        const double t = a[k + 1 + i];
+        loc += t * t;
+      }
+      const double sigma = block_reduce(loc, red, false);
+      if (tid == 0) {
+        const double alpha = a[k + 1];
+        if (sigma == 0.0) {
+          s_tau = 0.0;
+          s_beta = alpha;
+          s_scale = 0.0;
+        } else {
+          const double mu = sqrt(alpha * alpha + sigma);
+          const double beta = alpha <= 0.0 ? mu : -mu;
+          s_tau = (beta - alpha) / beta;
+          s_scale = 1.0 / (alpha - beta);
+          s_beta = beta;
+        }
+        tg[k] = s_tau;
+        eg[k] = s_beta;
+        misc[par] = s_tau;
+      }
+      __syncthreads();
+      if (s_tau != 0.0) {
+        const double scale = s_scale;
+        for (int i = tid; i < m; i += blockDim.x) {
+          const double vi = (i == 0) ? 1.0 : a[k + 1 + i] * scale;
+          vbuf[par * n + i] = vi;
+          if (i > 0) Gp[(k + 1 + i) + (int64_t)n * k] = vi;  // reflector kept for phase 2
+        }
+      }
+    }
+    cluster.sync();
+    const double tau = *cluster.map_shared_rank(misc + par, owner);
+    if (tau == 0.0) continue;  // column already reduced (same decision in every CTA)
+    const double* ov = cluster.map_shared_rank(vbuf + par * n, owner);
+    for (int i = tid; i < m; i += blockDim.x) vloc[i] = ov[i];
+    __syncthreads();
+    // p = tau A22 v on the owned columns (A22 symmetric: column dot v), one warp per column
+    const int l0 = first_owned(k + 1, rank, CL);
+    for (int l = l0 + warp; l < lcols; l += nw) {
+      const int c = rank + CL * l;
+      if (c >= n) continue;
+      const double* a = col(l) + k + 1;
+      double s = 0.0;
+      for (int i = lane; i < m; i += 32) s += a[i] * vloc[i];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+      if (lane == 0) pown[par * lcols + l] = tau * s;
+    }
+    __syncthreads();
+    double loc = 0.0;
+    for (int l = l0 + tid; l < lcols; l += blockDim.x) {
+      const int c = rank + CL * l;
+      if (c < n) loc += pown[par * lcols + l] * vloc[c - k - 1];
+    }
+    const double part = block_reduce(loc, red, false);
+    if (tid == 0) misc[2 + par] = part;
+    cluster.sync();
+    double pv = 0.0;  // fixed CTA order: every CTA forms the same K and w
+    for (int o = 0; o < CL; ++o) pv += *cluster.map_shared_rank(misc + 2 + par, o);
+    const double K = 0.5 * tau * pv;
+    for (int i = tid; i < m; i += blockDim.x) {
+      const int c = k + 1 + i;
+      const double p = *cluster.map_shared_rank(pown + par * lcols + c / CL, c % CL);
+      wloc[i] = p - K * vloc[i];
+    }
+    __syncthreads();
+    // A22 -= v w^T + w v^T on the owned columns
+    for (int l = l0; l < lcols; ++l) {
+      const int c = rank + CL * l;
+      if (c >= n) break;
+      const double vc = vloc[c - k - 1], wc = wloc[c - k - 1];
+      double* a = col(l) + k + 1;
+      for (int i = tid; i < m; i += blockDim.x) a[i] -= vloc[i] * wc + wloc[i] * vc;
+    }
+    __syncthreads();
+  }
+  // T: diagonal from the owners, the last off-diagonal A[n-1, n-2]
+  for (int l = 0; l < lcols; ++l) {
+    const int c = rank + CL * l;
+    if (c >= n) break;
+    if (tid == 0) dg[c] = col(l)[c];
+    if (c == n - 2 && tid == 0) eg[n - 2] = col(l)[n - 1];
+  }
+  if (rank == 0 && tid == 0) {
+    eg[n - 1] = 0.0;
+    tg[n - 1] = 0.0;
+    if (n >= 2) tg[n - 2] = 0.0;
+  }
+  __threadfence();
+  cluster.sync();  // also the last access of another CTA's shared memory
+  double* d = vloc;
+  double* e2 = wloc;
+  for (int i = tid; i < n; i += blockDim.x) {
+    d[i] = dg[i];
+    e2[i] = i < n - 1 ? eg[i] * eg[i] : 0.0;
+  }
+  __syncthreads();
+  double lo_loc = DBL_MAX, hi_loc = -DBL_MAX, e2max = 0.0;
+  for (int i = tid; i < n; i += blockDim.x) {
+    const double r = (i > 0 ? fabs(eg[i - 1]) : 0.0) + (i < n - 1 ? fabs(eg[i]) : 0.0);
+    lo_loc = fmin(lo_loc, d[i] - r);
+    hi_loc = fmax(hi_loc, d[i] + r);
+    if (i < n - 1) e2max = fmax(e2max, e2[i]);
+  }
+  const double gu = block_reduce(hi_loc, red, true);
+  const double gl = -block_reduce(-lo_loc, red, true);
+  const double emax = block_reduce(e2max, red, true);
+  const double bnorm = fmax(fabs(gl), fabs(gu));
+  const double pivmin = DBL_MIN * fmax(1.0, emax);
+  const double atol = 4.0 * DBL_EPSILON * bnorm + 2.0 * pivmin;
+  if (bnorm == 0.0) {
+    for (int j = rank * (int)blockDim.x + tid; j < n; j += CL * (int)blockDim.x) Wp[j] = 0.0;
+    return;
+  }
+  // bisection as in tridiag_eigvals, over every warp of the cluster
+  auto open_interval = [&](double lo, double hi) {
+    return hi - lo > fmax(atol, 2.0 * DBL_EPSILON * fmax(fabs(lo), fabs(hi)));
+  };
+  const int grp = lane < 30 ? lane / 3 : 0, sub = lane % 3;
+  for (int base = (rank * nw + warp) * 10; base < n; base += CL * nw * 10) {
+    const int j = base + grp;
+    const bool active = lane < 30 && j < n;
+    double lo = gl - atol, hi = gu + atol;
+    int it = 0;
+    bool work = active && open_interval(lo, hi);
+    while (__any_sync(0xffffffffu, work)) {
+      const double mid = 0.5 * (lo + hi), lm = 0.5 * (lo + mid), rm = 0.5 * (mid + hi);
+      const double x = sub == 0 ? mid : (sub == 1 ? lm : rm);
+      const int c = work ? sturm_count(d, e2, n, x, pivmin) : 0;
+      const int cm = __shfl_sync(0xffffffffu, c, 3 * grp);
+      const int cl = __shfl_sync(0xffffffffu, c, 3 * grp + 1);
+      const int cr = __shfl_sync(0xffffffffu, c, 3 * grp + 2);
+      if (work) {
+        const bool left = cm > j;
+        if (left) hi = mid; else lo = mid;
+        ++it;
+        if (it < 128 && open_interval(lo, hi)) {
+          const double x2 = left ? lm : rm;
+          if ((left ? cl : cr) > j) hi = x2; else lo = x2;
+          ++it;
+        }
+        work = it < 128 && open_interval(lo, hi);
+      }
+    }
+    if (active && sub == 0) Wp[n - 1 - j] = 0.5 * (lo + hi);
+  }
+}
+
+__global__ void __launch_bounds__(TT)
+tridiag_eigvecs_cluster(const EigDev* __restrict__ probs, const double* G, const double* Tg, const double* W,
+                        double* Zg, double* work, int cap) {
+  extern __shared__ double zsm[];
+  __shared__ double red[33];
+  __shared__ double coef[MAX_N / 2];
+  __shared__ int cstart[MAX_N / 2];
+  __shared__ int hasv[2];
+  __shared__ int hv[32];
+  cgx::cluster_group cluster = cgx::this_cluster();
+  const int CL = (int)cluster.num_blocks();
+  const int rank = (int)cluster.block_rank();
+  const EigDev P = probs[blockIdx.x / CL];
+  const int n = P.n, nvec = P.nvec;
+  const int tid = threadIdx.x;
+  if (n <= 0 || nvec <= 0) return;  // the same problem for the whole cluster
+  double* Zout = Zg + P.g_off;
+  const int q = (nvec + CL - 1) / CL;
+  const int j0 = rank * q, j1 = min(nvec, j0 + q), nown = max(0, j1 - j0);
+  const bool in_smem = (int64_t)q * n + 6 * (int64_t)n <= cap;
+  double* Z = in_smem ? zsm : Zout + (int64_t)n * j0;  // own vector t at Z + n t
+  double* ybuf = in_smem ? zsm + (int64_t)q * n : zsm;  // the current Gram-Schmidt iterate
+  double* ubuf = ybuf + n;                              // [2][n] published partial projections
+  double* scr = ubuf + 2 * n;                           // 3n LU scratch
+  const double* d = Tg + 3 * P.w_off;
+  const double* e = d + n;
+  const double* tau = e + n;
+  const double* lam = W + P.w_off;  // descending
+  const double* Gp = G + P.g_off;
+  const int warp = tid >> 5, lane = tid & 31, nw = blockDim.x >> 5;
+  double loc = 0.0;
+  for (int i = tid; i < n; i += blockDim.x)
+    loc = fmax(loc, fabs(d[i]) + (i > 0 ? fabs(e[i - 1]) : 0.0) + (i + 1 < n ? fabs(e[i]) : 0.0));
+  const double tnorm = block_reduce(loc, red, true);
+  const double tiny = tnorm > 1e-250 ? fmax(DBL_EPSILON * tnorm, DBL_MIN) : 1.0;
+  const double ortol = 1e-3 * tnorm;
+  // (a) inverse iteration on the own vectors, one thread each (same start vectors as the one-CTA kernel)
+  for (int t = tid; t < nown; t += blockDim.x) {
+    const int j = j0 + t;
+    double* y = Z + (int64_t)n * t;
+    for (int i = 0; i < n; ++i) y[i] = hash_unit(((uint64_t)P.g_off << 20) ^ ((uint64_t)j << 32) ^ (uint64_t)i);
+    for (int it = 0; it < INV_ITERS; ++it) {
+      tri_solve(d, e, n, lam[j], tiny, y, work + 3 * P.g_off + (int64_t)3 * n * j, 1);
+      double s = 0.0;
+      for (int i = 0; i < n; ++i) s += y[i] * y[i];
+      const double inv = 1.0 / sqrt(s);
+      for (int i = 0; i < n; ++i) y[i] *= inv;
+    }
+  }
+  if (tid == 0) {
+    int c = 0;
+    for (int j = 0; j < nvec && j < MAX_N / 2; ++j) {
+      if (j == 0 || lam[j - 1] - lam[j] > ortol) c = j;
+      cstart[j] = c;
+    }
+  }
+  __syncthreads();
+  cluster.sync();  // every start vector is in place
+  // (b) Gram-Schmidt, vector by vector
+  int g = 0;
+  for (int j = 1; j < nvec && j < MAX_N / 2; ++j) {
+    const int c0 = cstart[j];
+    if (c0 == j) continue;
+    const int owner = j / q;
+    const double* yj = in_smem ? cluster.map_shared_rank(zsm + (int64_t)n * (j - owner * q), owner)
+                               : Zout + (int64_t)n * j;
+    for (int i = tid; i < n; i += blockDim.x) ybuf[i] = yj[i];
+    __syncthreads();
+    const int ka = max(c0, j0), kb = min(j, j1);  // own members of the cluster before j
+    for (int pass = 0; pass < 6; ++pass) {
+      for (int r = 0; r < 2; ++r) {
+        const int par = g & 1;
+        double* u = ubuf + par * n;
+        for (int k = ka + warp; k < kb; k += nw) {
+          const double* zk = Z + (int64_t)n * (k - j0);
+          double s = 0.0;
+          for (int i = lane; i < n; i += 32) s += zk[i] * ybuf[i];
+#pragma unroll
+          for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+          if (lane == 0) coef[k - ka] = s;
+        }
+        __syncthreads();
+        if (kb > ka)
+          for (int i = tid; i < n; i += blockDim.x) {
+            double s = 0.0;
+            for (int k = ka; k < kb; ++k) s += coef[k - ka] * Z[(int64_t)n * (k - j0) + i];
+            u[i] = s;
+          }
+        if (tid == 0) hasv[par] = kb > ka ? 1 : 0;
+        __syncthreads();
+        cluster.sync();
+        if (tid < CL) hv[tid] = *cluster.map_shared_rank(hasv + par, tid);
+        __syncthreads();
+        for (int i = tid; i < n; i += blockDim.x) {
+          double s = ybuf[i];
+          for (int o = 0; o < CL; ++o)
+            if (hv[o]) s -= *cluster.map_shared_rank(u + i, o);
+          ybuf[i] = s;
+        }
+        __syncthreads();
+        ++g;
+      }
+      loc = 0.0;
+      for (int i = tid; i < n; i += blockDim.x) loc += ybuf[i] * ybuf[i];
+      const double nrm = sqrt(block_reduce(loc, red, false));
+      if (nrm > 0.5 || pass == 5) {
+        const double inv = nrm > 0.0 ? 1.0 / nrm : 0.0;
+        for (int i = tid; i < n; i += blockDim.x) ybuf[i] *= inv;
+        __syncthreads();
+        break;
+      }
+      // collapsed onto earlier vectors: one more inverse iteration from the
+      // orthogonal remainder (every CTA alike), then orthogonalise again
+      if (tid == 0) {
+        const double inv = nrm > 0.0 ? 1.0 / nrm : 1.0;
+        for (int i = 0; i < n; ++i) ybuf[i] = nrm > 0.0 ? ybuf[i] * inv : hash_unit((uint64_t)(j * 7919 + i + pass));
+        tri_solve(d, e, n, lam[j], tiny, ybuf, scr, 1);
+      }
+      __syncthreads();
+    }
+    if (rank == owner)
+      for (int i = tid; i < n; i += blockDim.x) Z[(int64_t)n * (j - j0) + i] = ybuf[i];
+    __syncthreads();
+  }
+  cluster.sync();  // no CTA reads another's shared memory after this point
+  // (c) back-transformation z = H_0 H_1 ... H_{n-3} y, last reflector first
+  double* stg = ubuf;  // CL_STAGE staged reflectors (5n doubles available)
+  for (int kb = n - 3; kb >= 0; kb -= CL_STAGE) {
+    __syncthreads();
+    for (int s = 0; s < CL_STAGE && kb - s >= 0; ++s) {
+      const int k = kb - s, m = n - k - 1;
+      for (int i = tid; i < m; i += blockDim.x) stg[(int64_t)s * n + i] = (i == 0) ? 1.0 : Gp[(k + 1 + i) + (int64_t)n * k];
+    }
+    __syncthreads();
+    for (int t = warp; t < nown; t += nw) {
+      double* y = Z + (int64_t)n * t;
+      for (int s = 0; s < CL_STAGE && kb - s >= 0; ++s) {
+        const int k = kb - s, m = n - k - 1;
+        const double tk = tau[k];
+        if (tk == 0.0) continue;
+        const double* v = stg + (int64_t)s * n;
+        double acc = 0.0;
+        for (int i = lane; i < m; i += 32) acc += v[i] * y[k + 1 + i];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+        const double c = tk * acc;
+        for (int i = lane; i < m; i += 32) y[k + 1 + i] -= v[i] * c;
+        __syncwarp();
+      }
+    }
+  }
+  __syncthreads();
+  // (d) deterministic gauge: the largest-magnitude entry (first on ties) is positive
+  for (int t = warp; t < nown; t += nw) {
+    double* y = Z + (int64_t)n * t;
+    double best = -1.0;
+    int bi = n;
+    for (int i = lane; i < n; i += 32) {
+      const double a = fabs(y[i]);
+      if (a > best) { best = a; bi = i; }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+      const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+      if (ob > best || (ob == best && oi < bi)) { best = ob; bi = oi; }
+    }
+    const bool flip = bi < n && y[bi] < 0.0;
+    __syncwarp();
+    if (flip)
+      for (int i = lane; i < n; i += 32) y[i] = -y[i];
+  }
+  if (in_smem) {
+    __syncthreads();
+    for (int64_t i = tid; i < (int64_t)n * nown; i += blockDim.x) Zout[(int64_t)n * j0 + i] = Z[i];
+  }
+}
+
 std::vector<EigDev> to_dev(const tt_eig_problem* probs, int n_probs, const int* nvec) {
   std::vector<EigDev> hp(n_probs);
   for (int i = 0; i < n_probs; ++i)
@@ -464,6 +871,100 @@ std::vector<EigDev> to_dev(const tt_eig_problem* probs, int n_probs, const int* 
 
 size_t vals_smem() { return sizeof(double) * ((size_t)SM_N * SM_N + 4 * (size_t)SM_N); }
 constexpr int64_t kVecsSmemCap = 25 * 1024;  // doubles (200 KB) of eigenvectors + reflector in shared memory
+
+// Sectors above the shared-memory size of the one-CTA kernels go to the cluster kernels.
+bool is_big(const EigDev& e) { return e.n > SM_N && !(e.flags & TT_EIG_ROW_1X2); }
+
+// Cluster size and shared-memory caps of the cluster kernels on this thread's
+// device: 16 CTAs per cluster when the device can co-schedule that many with
+// the full shared-memory carve-out, else 8, else none (the one-CTA kernels
+// take every problem).
+struct ClusterPlan {
+  int device = -1;
+  int cl = 0;
+  int64_t vals_cap = 0, vecs_cap = 0;  // doubles of dynamic shared memory per CTA
+};
+
+const ClusterPlan& cluster_plan(tt_ctx* ctx) {
+  static thread_local ClusterPlan cp;
+  if (cp.device == ctx->device) return cp;
+  cp = ClusterPlan();
+  cp.device = ctx->device;
+  int optin = 0;
+  if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device) != cudaSuccess) {
+    cudaGetLastError();
+    return cp;
+  }
+  cudaFuncAttributes fa, fb;
+  if (cudaFuncGetAttributes(&fa, tridiag_eigvals_cluster) != cudaSuccess ||
+      cudaFuncGetAttributes(&fb, tridiag_eigvecs_cluster) != cudaSuccess) {
+    cudaGetLastError();
+    return cp;
+  }
+  const int64_t va = ((int64_t)optin - (int64_t)fa.sharedSizeBytes - 1024) / 8;
+  const int64_t vb = ((int64_t)optin - (int64_t)fb.sharedSizeBytes - 1024) / 8;
+  if (va < 4 * MAX_N + 1024 || vb < 6 * MAX_N) return cp;
+  const void* kernels[2] = {(const void*)tridiag_eigvals_cluster, (const void*)tridiag_eigvecs_cluster};
+  const int64_t caps[2] = {va, vb};
+  for (int k = 0; k < 2; ++k) {
+    if (cudaFuncSetAttribute(kernels[k], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(caps[k] * 8)) !=
+            cudaSuccess ||
+        cudaFuncSetAttribute(kernels[k], cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) {
+      cudaGetLastError();
+      return cp;
+    }
+  }
+  for (int cl : {16, 8}) {
+    bool ok = true;
+    for (int k = 0; k < 2 && ok; ++k) {
+      cudaLaunchConfig_t cfg = {};
+      cudaLaunchAttribute at[1];
+      at[0].id = cudaLaunchAttributeClusterDimension;
+      at[0].val.clusterDim.x = cl;
+      at[0].val.clusterDim.y = 1;
+      at[0].val.clusterDim.z = 1;
+      cfg.gridDim = dim3(cl);
+      cfg.blockDim = dim3(TT);
+      cfg.dynamicSmemBytes = (size_t)(caps[k] * 8);
+      cfg.attrs = at;
+      cfg.numAttrs = 1;
+      int nc = 0;
+      if (cudaOccupancyMaxActiveClusters(&nc, kernels[k], &cfg) != cudaSuccess) {
+        cudaGetLastError();
+        nc = 0;
+      }
+      ok = nc >= 1;
+    }
+    if (ok) {
+      cp.cl = cl;
+      break;
+    }
+  }
+  cp.vals_cap = va;
+  cp.vecs_cap = vb;
+  return cp;
+}
+
+// One cluster of `cl` CTAs per problem; `need` doubles of dynamic shared memory.
+template <class... Args>
+cudaError_t launch_cluster(tt_ctx* ctx, int cl, int n_probs, int64_t need, const void* kernel, Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = cl;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  cfg.gridDim = dim3((unsigned)(cl * n_probs));
+  cfg.blockDim = dim3(TT);
+  cfg.dynamicSmemBytes = (size_t)(need * 8);
+  cfg.stream = ctx->stream;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  void* argv[] = {(void*)&args...};
+  const cudaError_t e = cudaLaunchKernelExC(&cfg, kernel, argv);
+  tt::count_launch(ctx);
+  return e;
+}
 
 }  // namespace
 
@@ -478,17 +979,35 @@ int tt_sym_eigvals_batched(tt_ctx* ctx, const tt_eig_problem* probs, int n_probs
     if (probs[i].flags & TT_EIG_ROW_1X2)
       TT_REQUIRE(probs[i].n == 2 && A, "tt_sym_eigvals_batched: 1x2 case needs n == 2 and A");
   }
-  std::vector<EigDev> hp = to_dev(probs, n_probs, nullptr);
-  EigDev* dp = tt::pool_alloc<EigDev>(ctx, n_probs);
+  std::vector<EigDev> all = to_dev(probs, n_probs, nullptr);
+  const ClusterPlan& cp = cluster_plan(ctx);
+  std::vector<EigDev> small, big;
+  for (const EigDev& e : all) (cp.cl > 0 && is_big(e) ? big : small).push_back(e);
+  EigDev* dp = tt::pool_alloc<EigDev>(ctx, all.size());
   if (!dp) return tt::fail(TT_ERR_OOM, "tt_sym_eigvals_batched: allocation failed");
-  TT_CUDA(tt::h2d_async(ctx, dp, hp.data(), sizeof(EigDev) * n_probs));
+  small.insert(small.end(), big.begin(), big.end());  // small problems first, then the cluster ones
+  TT_CUDA(tt::h2d_async(ctx, dp, small.data(), sizeof(EigDev) * small.size()));
+  const int n_small = (int)(small.size() - big.size());
   static thread_local bool attr = false;  // per host thread: each may drive its own device
   if (!attr) {
     TT_CUDA(cudaFuncSetAttribute(tridiag_eigvals, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)vals_smem()));
     attr = true;
   }
-  tridiag_eigvals<<<n_probs, TT, vals_smem(), ctx->stream>>>(dp, G, T, w, A);
-  TT_LAUNCH_CHECK(ctx);
+  if (n_small > 0) {
+    tridiag_eigvals<<<n_small, TT, vals_smem(), ctx->stream>>>(dp, G, T, w, A);
+    TT_LAUNCH_CHECK(ctx);
+  }
+  if (!big.empty()) {
+    int64_t need = 0;  // doubles: the column slab in shared memory when it fits under the cap
+    for (const EigDev& e : big) {
+      const int64_t lcols = (e.n + cp.cl - 1) / cp.cl;
+      const int64_t extra = 4 * (int64_t)e.n + 2 * lcols + 8;
+      const int64_t full = lcols * e.n + extra;
+      need = std::max(need, full <= cp.vals_cap ? full : extra);
+    }
+    TT_CUDA(launch_cluster(ctx, cp.cl, (int)big.size(), need, (const void*)tridiag_eigvals_cluster,
+                           dp + n_small, G, T, w, (int)need));
+  }
   tt::pool_free(ctx, dp);
   return TT_OK;
 }
@@ -505,15 +1024,21 @@ int tt_sym_eigvecs_batched(tt_ctx* ctx, const tt_eig_problem* probs, int n_probs
                "tt_sym_eigvecs_batched: nvec must be 0..min(n, 1024)");
     if (probs[i].flags & TT_EIG_ROW_1X2) TT_REQUIRE(A, "tt_sym_eigvecs_batched: 1x2 case needs A");
   }
-  std::vector<EigDev> hp = to_dev(probs, n_probs, nvec);
-  EigDev* dp = tt::pool_alloc<EigDev>(ctx, n_probs);
+  std::vector<EigDev> all = to_dev(probs, n_probs, nvec);
+  const ClusterPlan& cp = cluster_plan(ctx);
+  std::vector<EigDev> small, big;
+  for (const EigDev& e : all) (cp.cl > 0 && is_big(e) ? big : small).push_back(e);
+  EigDev* dp = tt::pool_alloc<EigDev>(ctx, all.size());
   if (!dp) return tt::fail(TT_ERR_OOM, "tt_sym_eigvecs_batched: allocation failed");
-  TT_CUDA(tt::h2d_async(ctx, dp, hp.data(), sizeof(EigDev) * n_probs));
+  const int n_small = (int)small.size();
+  small.insert(small.end(), big.begin(), big.end());
+  TT_CUDA(tt::h2d_async(ctx, dp, small.data(), sizeof(EigDev) * small.size()));
   // shared memory for the largest problem that fits (the others iterate in global memory)
   int64_t need = 0;
-  for (int i = 0; i < n_probs; ++i) {
-    const int64_t with_u = 4 * (int64_t)probs[i].n * nvec[i] + probs[i].n;  // Z, reflector and LU scratch
-    const int64_t z_only = (int64_t)probs[i].n * nvec[i] + probs[i].n;
+  for (int i = 0; i < n_small; ++i) {
+    const EigDev& e = small[i];
+    const int64_t with_u = 4 * (int64_t)e.n * e.nvec + e.n;  // Z, reflector and LU scratch
+    const int64_t z_only = (int64_t)e.n * e.nvec + e.n;
     if (with_u <= kVecsSmemCap) need = std::max(need, with_u);
     else if (z_only <= kVecsSmemCap) need = std::max(need, z_only);
   }
@@ -523,8 +1048,22 @@ int tt_sym_eigvecs_batched(tt_ctx* ctx, const tt_eig_problem* probs, int n_probs
                                  (int)(sizeof(double) * kVecsSmemCap)));
     attr = true;
   }
-  tridiag_eigvecs<<<n_probs, TT, sizeof(double) * (size_t)need, ctx->stream>>>(dp, G, T, w, Z, work, A, (int)need);
-  TT_LAUNCH_CHECK(ctx);
+  if (n_small > 0) {
+    tridiag_eigvecs<<<n_small, TT, sizeof(double) * (size_t)need, ctx->stream>>>(dp, G, T, w, Z, work, A,
+                                                                                  (int)need);
+    TT_LAUNCH_CHECK(ctx);
+  }
+  if (!big.empty()) {
+    int64_t needc = 0;  // doubles: own eigenvectors in shared memory when they fit, plus 6n of buffers
+    for (const EigDev& e : big) {
+      const int64_t q = (e.nvec + cp.cl - 1) / cp.cl;
+      const int64_t extra = 6 * (int64_t)e.n;
+      const int64_t full = q * e.n + extra;
+      needc = std::max(needc, full <= cp.vecs_cap ? full : extra);
+    }
+    TT_CUDA(launch_cluster(ctx, cp.cl, (int)big.size(), needc, (const void*)tridiag_eigvecs_cluster,
+                           dp + n_small, G, T, w, Z, work, (int)needc));
+  }
   tt::pool_free(ctx, dp);
   return TT_OK;
 }

@@ -34,8 +34,11 @@ class TTError(RuntimeError):
     pass
 
 
-TT_PREC_FP64, TT_PREC_TF32, TT_PREC_TF32X3 = 0, 1, 2
-PRECISIONS = {"fp64": TT_PREC_FP64, "tf32": TT_PREC_TF32, "tf32x3": TT_PREC_TF32X3}
+TT_PREC_FP64, TT_PREC_TF32, TT_PREC_TF32X3, TT_PREC_TF32_AUTO, TT_PREC_TF32X3_AUTO = 0, 1, 2, 3, 4
+# "*-auto": per contraction, the tensor-core kind where the plan's cost model
+# predicts it faster than FP64, FP64 elsewhere
+PRECISIONS = {"fp64": TT_PREC_FP64, "tf32": TT_PREC_TF32, "tf32x3": TT_PREC_TF32X3,
+              "tf32-auto": TT_PREC_TF32_AUTO, "tf32x3-auto": TT_PREC_TF32X3_AUTO}
 
 
 def _load():
@@ -814,10 +817,12 @@ def triangular_lattice(Nx: int, Ny: int, yperiodic: bool = True):
 
 
 def set_precision(op: str = "fp64", heff: str = "fp64", env: str = "fp64"):
-    """Contraction precisions on this thread ("fp64", "tf32", "tf32x3"): op for
-    QTensor/dense contractions, heff for the Davidson H_eff*x products, env for
-    the environment updates.  The mixed form of the DMRG sweep is
-    set_precision(heff="tf32x3", env="tf32x3")."""
+    """Contraction precisions on this thread ("fp64", "tf32", "tf32x3",
+    "tf32-auto", "tf32x3-auto"): op for QTensor/dense contractions, heff for
+    the Davidson H_eff*x products, env for the environment updates.  The mixed
+    form of the DMRG sweep is set_precision(heff="tf32x3-auto",
+    env="tf32x3-auto"): 3xTF32 on the tensor cores for the contractions the
+    cost model predicts faster there, FP64 for the rest."""
     _chk(lib.tt_dmrg_set_precision(PRECISIONS[op], PRECISIONS[heff], PRECISIONS[env]), "set_precision")
 
 

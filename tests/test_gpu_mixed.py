@@ -6,6 +6,9 @@
   FP32 accumulation), on QN-blocked tensors with ragged sector sizes (tile
   edges in m, n and k); on a single 700 x 513 x 450 block the FP32
   accumulation over k = 513 dominates (about sqrt(k) * 2^-24), bound 1e-5.
+* The automatic form ("tf32x3-auto") keeps bandwidth-bound contractions in
+  FP64 (bit-identical to the FP64 path) and sends large blocks to the tensor
+  cores.
 * Two-site DMRG with H_eff*x and the environment updates in 3xTF32 (GS,
   Rayleigh-Ritz and the SVD in FP64; the sweep energy <psi|H|psi> contracted
   in FP64, because mixed-precision environments bias the Ritz value to first
@@ -140,3 +143,42 @@ def test_mixed_precision_dense_tfi(ctx):
     Eed = ed.terms_ground_energy(N, terms)
     assert abs(e64 - Eed) / N <= 1e-10
     assert abs(emx - e64) / N <= 1e-8
+
+
+def test_auto_precision_picks_per_contraction(ctx):
+    """'tf32x3-auto' resolves per contraction: a contraction over a small MPO
+    link (k = 5, bandwidth-bound) stays FP64 and is bit-identical to the FP64
+    result; a 2048^3 block goes to the tensor cores (differs from FP64, within
+    the 3xTF32 bound of the oracle, 5e-5 for FP32 accumulation over k = 2048)."""
+    import tt_b200
+    rng = np.random.default_rng(17)
+    a = _index(Inward, "a", [(-2, 300), (0, 400), (2, 300)])
+    w = _index(Outward, "w", [(-2, 1), (0, 3), (2, 1)])
+    b = _index(Outward, "b", [(-2, 200), (0, 250), (2, 200)])
+    X = _random([a, w.dagged(), b], rng)        # contract over w (k <= 3 per block pair)
+    wp = _index(Inward, "w", [(-2, 1), (0, 3), (2, 1)], Link, 1)
+    W = _random([w, wp.dagged()], rng)
+    gX, gW = tt_b200.QTensor.from_oracle(X), tt_b200.QTensor.from_oracle(W)
+    ref64 = (gX * gW).to_oracle()
+    tt_b200.set_precision(op="tf32x3-auto")
+    try:
+        got = (gX * gW).to_oracle()
+    finally:
+        tt_b200.set_precision()
+    for x, y in zip(got.blocks, ref64.blocks):
+        np.testing.assert_array_equal(x, y)
+    i = _index(Inward, "i", [(0, 2048)])
+    k = _index(Outward, "k", [(0, 2048)])
+    j = _index(Inward, "j", [(0, 2048)])
+    A = _random([i, k], rng)
+    B = _random([k.dagged(), j], rng)
+    gA, gB = tt_b200.QTensor.from_oracle(A), tt_b200.QTensor.from_oracle(B)
+    big64 = (gA * gB).to_oracle()
+    tt_b200.set_precision(op="tf32x3-auto")
+    try:
+        big = (gA * gB).to_oracle()
+    finally:
+        tt_b200.set_precision()
+    assert not np.array_equal(big.blocks[0], big64.blocks[0])
+    # FP32 accumulation over k = 2048 (about sqrt(k) * 2^-24 per element): measured 1.4e-5
+    assert _rel_err(big, contract(A, B)) < 5e-5

@@ -593,9 +593,12 @@ def run_j1j2(args):
             pc0 = planning_counters(tt_b200)
             ms, e = 0.0, None
             tt_b200.lib.tt_dmrg_set_profile_step(args.profile_step)
+            outliers = []
+            fb0 = tt_b200.davidson_fallbacks()
             for it in range(args.steps):
                 if it == 1:
                     tt_b200.lib.tt_dmrg_set_profile_step(-1)
+                n0 = len(run.steps())
                 flush.zero_()
                 torch.cuda.synchronize()
                 e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -604,6 +607,12 @@ def run_j1j2(args):
                 e1.record(stream)
                 e1.synchronize()
                 ms += e0.elapsed_time(e1)
+                # steps whose energy leaves the sweep's median by more than 1e-3: a damaged update
+                st = run.steps()[n0:]
+                emed = statistics.median(x["energy"] for x in st)
+                outliers += [dict(sweep=it, step=k, site=x["site"], direction=x["direction"], energy=x["energy"],
+                                  kept=x["kept"], matvecs=x["matvecs"], trunc_err=x["trunc_err"])
+                             for k, x in enumerate(st) if abs(x["energy"] - emed) > 1e-3 * abs(emed)]
             tt_b200.lib.tt_dmrg_set_profile_step(-1)
             pc1 = planning_counters(tt_b200)
             st1 = run.stats()
@@ -612,7 +621,8 @@ def run_j1j2(args):
             res = {"s_per_sweep": ms * 1e-3 / args.steps, "energy": e, "heff_tflops": fl / hs / 1e12 if hs else 0.0,
                    "heff_s_per_sweep": hs / args.steps, "heff_tflop_per_sweep": fl / args.steps / 1e12,
                    "max_bond_dim": max(psi.bond_dims()),
-                   "host_planning_s_per_sweep": {k: (pc1[k] - pc0[k]) / args.steps for k in pc0}}
+                   "host_planning_s_per_sweep": {k: (pc1[k] - pc0[k]) / args.steps for k in pc0},
+                   "davidson_fallbacks": tt_b200.davidson_fallbacks() - fb0, "outlier_steps": outliers[:8]}
             if args.breakdown:
                 lib = tt_b200.lib
                 lib.tt_dmrg_set_profiling(1)

@@ -216,12 +216,12 @@ grouped_dgemm(const TaskDev* __restrict__ tasks, const OutDev* __restrict__ outs
 // ---------------------------------------------------------------------------
 // Mixed-precision path: tcgen05 (5th-generation tensor cores), kind::tf32.
 //
-// Two steps per contraction.  pack_tf32 converts every operand block once
-// into TF32 hi/lo tiles (x = hi + lo, both rounded to nearest) stored in the
-// exact K-major 128-byte-swizzled layout of a shared-memory MMA operand tile;
-// grouped_tc_bulk then feeds the tensor cores from those tiles with bulk
-// copies and accumulates in tensor memory (FP32), one 128 x 128 output tile
-// per CTA.  The split form issues hi*hi + hi*lo + lo*hi per k-step.
+// Two launches per contraction.  pack_tf32_ab converts every operand block
+// once into TF32 hi/lo tiles (x = hi + lo, both rounded to nearest) stored in
+// the exact K-major 128-byte-swizzled layout of a shared-memory MMA operand
+// tile; grouped_tc_persist then feeds the tensor cores from those tiles with
+// bulk copies and accumulates 128 x 128 output tiles in tensor memory (FP32).
+// The split form issues hi*hi + hi*lo + lo*hi per k-step.
 constexpr int TC_BM = 128;
 constexpr int TC_BN = 128;
 constexpr int TC_BK = 32;                        // fp32 elements = one 128-byte swizzle row
@@ -329,14 +329,237 @@ struct PackTile {
 };
 constexpr int TC_TILE_BYTES = 2 * TC_BM * TC_BK * 4;  // hi + lo = 32 KB
 
+// ---- grouped tcgen05 GEMM over packed tiles ---------------------------------
+// A block pair in packed form: the bases of its A and B packed blocks and its
+// number of 32-wide k-chunks.  The GEMM kernel (grouped_tc_persist below)
+// streams each chunk's A and B tiles into a TC_RING-stage ring of
+// TC_RING_STAGE bytes with plain bulk copies.
+struct PairTC {
+  int64_t a_base, b_base;  // packed block bases (bytes)
+  int32_t kt;              // k tiles of the pair
+  int32_t pad;
+};
+constexpr int TC_RING = 3;
+constexpr int TC_RING_STAGE = 4 * TC_BM * TC_BK * 4;  // A hi, A lo, B hi, B lo: 64 KB
+constexpr size_t TC_BULK_SMEM = (size_t)TC_RING * TC_RING_STAGE + 1024;
+constexpr uint32_t TC_BULK_COLS = TC_BN;
+
+__device__ __forceinline__ void mbar_expect_tx(uint32_t mbar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mbar), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t bytes, uint32_t mbar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+               "l"(src), "r"(bytes), "r"(mbar)
+               : "memory");
+}
+
+// ---- persistent form --------------------------------------------------------
+// One CTA per SM walks the tiles blockIdx.x, blockIdx.x + gridDim.x, ...
+// (longest first) with specialised warps: warp 0 (one thread) streams the
+// packed tiles of every k-chunk of every tile into the TC_RING-stage ring,
+// running ahead across tile boundaries; warp 1 (one thread) issues the MMAs
+// into one of two 128-column TMEM accumulators, alternating per tile, and
+// commits each stage to its empty barrier and each finished tile to the
+// accumulator's full barrier; warps 2-5 drain a finished accumulator
+// (tcgen05.ld, alpha * acc as FP64) while the MMAs of the next tile fill the
+// other one, then release it through the accumulator's empty barrier (four
+// arrivals).  A warp may read only its quarter of the 128 TMEM lanes (warp
+// index mod 4), so warps 2, 3, 4, 5 cover lanes 64, 96, 0, 32.  Every wait is
+// bounded; on timeout the CTA records TT_ERR_TIMEOUT, stops issuing, lets
+// what it issued land (bounded) and frees TMEM.
+constexpr int TC_P_THREADS = 192;
+constexpr uint32_t TC_P_COLS = 2 * TC_BN;
+
+__device__ __forceinline__ void mbar_arrive(uint32_t mbar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(mbar) : "memory");
+}
+
+template <bool SPLIT>
+__global__ void __launch_bounds__(TC_P_THREADS, 1)
+grouped_tc_persist(const TaskDev* __restrict__ tasks, int n_tasks, const OutDev* __restrict__ outs,
+                   const PairTC* __restrict__ pairs, const uint8_t* __restrict__ packA,
+                   const uint8_t* __restrict__ packB, double* __restrict__ C, double alpha, int* __restrict__ status) {
+  extern __shared__ uint8_t tc_smem_raw[];
+  __shared__ __align__(8) uint64_t full_bar[TC_RING], empty_bar[TC_RING], accf_bar[2], acce_bar[2];
+  __shared__ uint32_t tmem_slot;
+  __shared__ volatile int flag;
+  __shared__ int issued, consumed, committed_tiles;
+
+  const uint32_t sbase = (smem_u32(tc_smem_raw) + 1023u) & ~1023u;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const uint32_t half = SPLIT ? (uint32_t)TC_TILE_BYTES : (uint32_t)(TC_TILE_BYTES / 2);  // bytes per operand tile
+
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_slot)),
+                 "r"(TC_P_COLS)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  if (tid == 0) {
+    for (int i = 0; i < TC_RING; ++i) {
+      mbar_init(smem_u32(&full_bar[i]), 1);
+      mbar_init(smem_u32(&empty_bar[i]), 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(smem_u32(&accf_bar[b]), 1);
+      mbar_init(smem_u32(&acce_bar[b]), 4);
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    flag = 0;
+    issued = 0;
+    consumed = 0;
+    committed_tiles = 0;
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = tmem_slot;
+
+  if (warp == 0) {
+    if (lane == 0) {  // producer
+      int g = 0;
+      for (int t = blockIdx.x; t < n_tasks && !flag; t += gridDim.x) {
+        const TaskDev task = tasks[t];
+        const int rt = task.m0 / TC_BM, nt = task.n0 / TC_BN;
+        for (int p = task.p_begin; p < task.p_end && !flag; ++p) {
+          const PairTC q = pairs[p];
+          for (int kt = 0; kt < q.kt; ++kt, ++g) {
+            const int s = g % TC_RING;
+            if (g >= TC_RING && !mbar_wait_bounded(smem_u32(&empty_bar[s]), (uint32_t)((g / TC_RING - 1) & 1))) {
+              flag = 1;
+              break;
+            }
+            const uint32_t st = sbase + s * TC_RING_STAGE;
+            mbar_expect_tx(smem_u32(&full_bar[s]), 2 * half);
+            bulk_g2s(st, packA + q.a_base + (int64_t)(rt * q.kt + kt) * TC_TILE_BYTES, half, smem_u32(&full_bar[s]));
+            bulk_g2s(st + TC_TILE_BYTES, packB + q.b_base + (int64_t)(nt * q.kt + kt) * TC_TILE_BYTES, half,
+                     smem_u32(&full_bar[s]));
+            issued = g + 1;
+          }
+        }
+      }
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {  // MMA issuer
+      int g = 0, i = 0;
+      for (int t = blockIdx.x; t < n_tasks && !flag; t += gridDim.x, ++i) {
+        const TaskDev task = tasks[t];
+        int nch = 0;
+        for (int p = task.p_begin; p < task.p_end; ++p) nch += pairs[p].kt;
+        const int b = i & 1;
+        if (i >= 2 && !mbar_wait_bounded(smem_u32(&acce_bar[b]), (uint32_t)(((i >> 1) - 1) & 1))) {
+          flag = 1;
+          break;
+        }
+        tc_fence_after();
+        const uint32_t acc_tm = tmem + (uint32_t)(b * TC_BN);
+        for (int c = 0; c < nch; ++c, ++g) {
+          const int s = g % TC_RING;
+          if (!mbar_wait_bounded(smem_u32(&full_bar[s]), (uint32_t)((g / TC_RING) & 1))) {
+            flag = 1;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t ah = sbase + s * TC_RING_STAGE, al = ah + TC_TILE_BYTES / 2;
+          const uint32_t bh = ah + TC_TILE_BYTES, bl = bh + TC_TILE_BYTES / 2;
+#pragma unroll
+          for (int kk = 0; kk < TC_BK / 8; ++kk) {
+            const uint32_t adv = 32u * kk;
+            const uint32_t acc = (c > 0 || kk > 0) ? 1u : 0u;
+            if (SPLIT) {
+              mma_tf32(acc_tm, sw128_desc(al + adv), sw128_desc(bh + adv), acc);
+              mma_tf32(acc_tm, sw128_desc(ah + adv), sw128_desc(bl + adv), 1u);
+              mma_tf32(acc_tm, sw128_desc(ah + adv), sw128_desc(bh + adv), 1u);
+            } else {
+              mma_tf32(acc_tm, sw128_desc(ah + adv), sw128_desc(bh + adv), acc);
+            }
+          }
+          mma_commit(smem_u32(&empty_bar[s]));
+          consumed = g + 1;
+        }
+        if (flag) break;
+        if (nch > 0) mma_commit(smem_u32(&accf_bar[b]));
+        else mbar_arrive(smem_u32(&accf_bar[b]));
+        committed_tiles = i + 1;
+      }
+    }
+  } else {  // epilogue, warps 2..5
+    const int q4 = warp & 3;
+    int i = 0;
+    for (int t = blockIdx.x; t < n_tasks; t += gridDim.x, ++i) {
+      // decisions are warp-uniform: the TMEM loads below are .sync.aligned
+      if (__any_sync(0xffffffffu, flag != 0)) break;
+      const TaskDev task = tasks[t];
+      const OutDev out = outs[task.out];
+      int nch = 0;
+      for (int p = task.p_begin; p < task.p_end; ++p) nch += pairs[p].kt;
+      const int b = i & 1;
+      const bool ok = mbar_wait_bounded(smem_u32(&accf_bar[b]), (uint32_t)((i >> 1) & 1));
+      if (!__all_sync(0xffffffffu, ok)) {
+        if (lane == 0) flag = 1;
+        break;
+      }
+      tc_fence_after();
+      double* Cb = C + out.c_off;
+      const int m = task.m0 + q4 * 32 + lane;
+#pragma unroll
+      for (int c16 = 0; c16 < TC_BN / 16; ++c16) {
+        float v[16];
+        if (nch > 0) {
+          tmem_ld16(tmem + ((uint32_t)(q4 * 32) << 16) + (uint32_t)(b * TC_BN + c16 * 16), v);
+        } else {
+#pragma unroll
+          for (int j = 0; j < 16; ++j) v[j] = 0.f;
+        }
+        if (m < out.m) {
+#pragma unroll
+          for (int j = 0; j < 16; ++j) {
+            const int n = task.n0 + c16 * 16 + j;
+            if (n < out.n) Cb[m + (int64_t)out.ldc * n] = alpha * (double)v[j];
+          }
+        }
+      }
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(smem_u32(&acce_bar[b]));
+    }
+  }
+  __syncwarp();
+  __syncthreads();
+  if (tid == 0 && flag) {
+    // let the copies that were issued but not consumed land and the last
+    // committed MMAs finish before shared and tensor memory are released
+    for (int g = consumed; g < issued; ++g)
+      mbar_wait_bounded(smem_u32(&full_bar[g % TC_RING]), (uint32_t)((g / TC_RING) & 1));
+    if (consumed > 0)
+      mbar_wait_bounded(smem_u32(&empty_bar[(consumed - 1) % TC_RING]), (uint32_t)(((consumed - 1) / TC_RING) & 1));
+    if (committed_tiles > 0) {  // the last tile commit's arrival
+      const int il = committed_tiles - 1;
+      mbar_wait_bounded(smem_u32(&accf_bar[il & 1]), (uint32_t)((il >> 1) & 1));
+    }
+    atomicExch(status, TT_ERR_TIMEOUT);
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (warp == 1)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TC_P_COLS) : "memory");
+}
+
+// Both operands' packing in one launch: tiles [0, n_a) of A, then those of B.
 template <bool SPLIT>
 __global__ void __launch_bounds__(128)
-pack_tf32(const PackJob* __restrict__ jobs, const PackTile* __restrict__ tiles, const int32_t* __restrict__ tab,
-          const double* __restrict__ X, uint8_t* __restrict__ packed) {
-  const PackTile t = tiles[blockIdx.x];
-  const PackJob J = jobs[t.job];
+pack_tf32_ab(const PackJob* __restrict__ jobsA, const PackTile* __restrict__ tilesA, int n_a,
+             const PackJob* __restrict__ jobsB, const PackTile* __restrict__ tilesB, const int32_t* __restrict__ tab,
+             const double* __restrict__ A, const double* __restrict__ B, uint8_t* __restrict__ pa,
+             uint8_t* __restrict__ pb) {
+  const bool is_a = (int)blockIdx.x < n_a;
+  const PackTile t = is_a ? tilesA[blockIdx.x] : tilesB[blockIdx.x - n_a];
+  const PackJob J = is_a ? jobsA[t.job] : jobsB[t.job];
+  const double* X = is_a ? A : B;
   const int tid = threadIdx.x;
-  uint8_t* dst = packed + J.dst + (int64_t)(t.rt * J.kt_count + t.kt) * TC_TILE_BYTES;
+  uint8_t* dst = (is_a ? pa : pb) + J.dst + (int64_t)(t.rt * J.kt_count + t.kt) * TC_TILE_BYTES;
 #pragma unroll
   for (int i = 0; i < 8; ++i) {
     const int r = J.row_unit ? tid : (tid >> 3) + 16 * i;
@@ -360,169 +583,6 @@ pack_tf32(const PackJob* __restrict__ jobs, const PackTile* __restrict__ tiles, 
   }
 }
 
-// ---- grouped tcgen05 GEMM over packed tiles ---------------------------------
-// One CTA of four warps per 128 x 128 output tile.  Thread 0 (producer)
-// streams the packed A and B tiles of every k-chunk of every block pair into
-// a TC_RING-stage ring with plain bulk copies (cp.async.bulk, completion
-// counted on the stage's full barrier); thread 32 (MMA issuer) waits for each
-// stage, issues its tcgen05.mma instructions into the TMEM accumulator and
-// commits them to the stage's empty barrier, which releases the stage to the
-// producer.  After the last chunk an accumulator barrier releases the
-// epilogue: all four warps read their 32 TMEM lanes and write alpha * acc as
-// FP64.  Every wait is bounded; on timeout the CTA records TT_ERR_TIMEOUT,
-// lets what it issued land (bounded), frees TMEM and returns.
-struct PairTC {
-  int64_t a_base, b_base;  // packed block bases (bytes)
-  int32_t kt;              // k tiles of the pair
-  int32_t pad;
-};
-constexpr int TC_RING = 3;
-constexpr int TC_RING_STAGE = 4 * TC_BM * TC_BK * 4;  // A hi, A lo, B hi, B lo: 64 KB
-constexpr size_t TC_BULK_SMEM = (size_t)TC_RING * TC_RING_STAGE + 1024;
-constexpr uint32_t TC_BULK_COLS = TC_BN;
-
-__device__ __forceinline__ void mbar_expect_tx(uint32_t mbar, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mbar), "r"(bytes) : "memory");
-}
-
-__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t bytes, uint32_t mbar) {
-  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
-               "l"(src), "r"(bytes), "r"(mbar)
-               : "memory");
-}
-
-template <bool SPLIT>
-__global__ void __launch_bounds__(128, 1)
-grouped_tc_bulk(const TaskDev* __restrict__ tasks, const OutDev* __restrict__ outs, const PairTC* __restrict__ pairs,
-                const uint8_t* __restrict__ packA, const uint8_t* __restrict__ packB, double* __restrict__ C,
-                double alpha, int* __restrict__ status) {
-  extern __shared__ uint8_t tc_smem_raw[];
-  __shared__ __align__(8) uint64_t full_bar[TC_RING], empty_bar[TC_RING], acc_bar;
-  __shared__ uint32_t tmem_slot;
-  __shared__ int flag, issued, consumed;
-
-  const uint32_t sbase = (smem_u32(tc_smem_raw) + 1023u) & ~1023u;
-  const TaskDev task = tasks[blockIdx.x];
-  const OutDev out = outs[task.out];
-  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const uint32_t half = SPLIT ? (uint32_t)TC_TILE_BYTES : (uint32_t)(TC_TILE_BYTES / 2);  // bytes per operand tile
-
-  if (warp == 0) {
-    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_slot)),
-                 "r"(TC_BULK_COLS)
-                 : "memory");
-    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
-  }
-  if (tid == 0) {
-    for (int i = 0; i < TC_RING; ++i) {
-      mbar_init(smem_u32(&full_bar[i]), 1);
-      mbar_init(smem_u32(&empty_bar[i]), 1);
-    }
-    mbar_init(smem_u32(&acc_bar), 1);
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    flag = 0;
-    issued = 0;
-    consumed = 0;
-  }
-  tc_fence_before();
-  __syncthreads();
-  tc_fence_after();
-  const uint32_t tmem = tmem_slot;
-  int nchunks = 0;
-  for (int p = task.p_begin; p < task.p_end; ++p) nchunks += pairs[p].kt;
-  const int rt = task.m0 / TC_BM, nt = task.n0 / TC_BN;
-
-  if (tid == 0) {  // producer
-    int g = 0;
-    for (int p = task.p_begin; p < task.p_end && !flag; ++p) {
-      const PairTC q = pairs[p];
-      for (int kt = 0; kt < q.kt; ++kt, ++g) {
-        const int s = g % TC_RING;
-        if (g >= TC_RING && !mbar_wait_bounded(smem_u32(&empty_bar[s]), (uint32_t)((g / TC_RING - 1) & 1))) {
-          flag = 1;
-          break;
-        }
-        const uint32_t st = sbase + s * TC_RING_STAGE;
-        mbar_expect_tx(smem_u32(&full_bar[s]), 2 * half);
-        bulk_g2s(st, packA + q.a_base + (int64_t)(rt * q.kt + kt) * TC_TILE_BYTES, half, smem_u32(&full_bar[s]));
-        bulk_g2s(st + TC_TILE_BYTES, packB + q.b_base + (int64_t)(nt * q.kt + kt) * TC_TILE_BYTES, half,
-                 smem_u32(&full_bar[s]));
-        issued = g + 1;
-      }
-    }
-  } else if (tid == 32) {  // MMA issuer
-    int g = 0;
-    for (; g < nchunks && !flag; ++g) {
-      const int s = g % TC_RING;
-      if (!mbar_wait_bounded(smem_u32(&full_bar[s]), (uint32_t)((g / TC_RING) & 1))) {
-        flag = 1;
-        break;
-      }
-      tc_fence_after();
-      const uint32_t ah = sbase + s * TC_RING_STAGE, al = ah + TC_TILE_BYTES / 2;
-      const uint32_t bh = ah + TC_TILE_BYTES, bl = bh + TC_TILE_BYTES / 2;
-#pragma unroll
-      for (int kk = 0; kk < TC_BK / 8; ++kk) {
-        const uint32_t adv = 32u * kk;
-        const uint32_t acc = (g > 0 || kk > 0) ? 1u : 0u;
-        if (SPLIT) {
-          mma_tf32(tmem, sw128_desc(al + adv), sw128_desc(bh + adv), acc);
-          mma_tf32(tmem, sw128_desc(ah + adv), sw128_desc(bl + adv), 1u);
-          mma_tf32(tmem, sw128_desc(ah + adv), sw128_desc(bh + adv), 1u);
-        } else {
-          mma_tf32(tmem, sw128_desc(ah + adv), sw128_desc(bh + adv), acc);
-        }
-      }
-      mma_commit(smem_u32(&empty_bar[s]));
-      consumed = g + 1;
-    }
-    if (g > 0) mma_commit(smem_u32(&acc_bar));
-  }
-  __syncwarp();
-  __syncthreads();
-  if (tid == 0) {
-    if (!flag && nchunks > 0 && !mbar_wait_bounded(smem_u32(&acc_bar), 0u)) flag = 1;
-    if (flag) {
-      // let the copies that were issued but not consumed land, and the last
-      // committed MMAs finish, before shared and tensor memory are released
-      for (int g = consumed; g < issued; ++g)
-        mbar_wait_bounded(smem_u32(&full_bar[g % TC_RING]), (uint32_t)((g / TC_RING) & 1));
-      if (consumed > 0)
-        mbar_wait_bounded(smem_u32(&empty_bar[(consumed - 1) % TC_RING]), (uint32_t)(((consumed - 1) / TC_RING) & 1));
-      atomicExch(status, TT_ERR_TIMEOUT);
-    }
-  }
-  tc_fence_before();
-  __syncthreads();
-  tc_fence_after();
-  if (!flag) {
-    double* Cb = C + out.c_off;
-    const int m = task.m0 + warp * 32 + lane;
-#pragma unroll
-    for (int c16 = 0; c16 < TC_BN / 16; ++c16) {
-      float v[16];
-      if (nchunks > 0) {
-        tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(c16 * 16), v);
-      } else {
-#pragma unroll
-        for (int j = 0; j < 16; ++j) v[j] = 0.f;
-      }
-      if (m < out.m) {
-#pragma unroll
-        for (int j = 0; j < 16; ++j) {
-          const int n = task.n0 + c16 * 16 + j;
-          if (n < out.n) Cb[m + (int64_t)out.ldc * n] = alpha * (double)v[j];
-        }
-      }
-    }
-  }
-  tc_fence_before();
-  __syncthreads();
-  tc_fence_after();
-  if (warp == 0)
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TC_BULK_COLS) : "memory");
-}
-
 // Cost model of the *_AUTO precisions: predicted device time (microseconds)
 // of one exec of a contraction in `prec` (FP64 DMMA, or a tcgen05 kind with
 // its two packing launches).  Work is counted on padded tiles (an output tile
@@ -532,14 +592,19 @@ grouped_tc_bulk(const TaskDev* __restrict__ tasks, const OutDev* __restrict__ ou
 // element three more times (read by the packer, written packed, read packed),
 // so a contraction with a small k -- the bandwidth-bound middle contraction
 // of H_eff*x and of the environment update -- stays in FP64, which is exact
-// to more digits and no slower there.  Rates are the measured single-block
-// throughputs of the two kernels on B200 (4096^3: DMMA 26 TFLOP/s, tcgen05
-// 690 TFLOP/s of TF32 products).
+// to more digits and faster there (measured at bond dimension 1024 on the
+// J1-J2 cylinder: 354 us FP64 against 685 us packed tensor-core form, while
+// L*x and *R take 141 and 161 us on the tensor cores against 301 and 473 us
+// in FP64).  Rates are the measured single-block throughputs of the two
+// kernels on B200 (4096^3: DMMA 26 TFLOP/s, tcgen05 690 TFLOP/s of TF32
+// products).
 double predict_us(const tt_out_block* outs, int n_out, const std::vector<PairDev>& hp,
                   const std::vector<int>& first, int prec, int num_sms) {
   constexpr double kDmmaRate = 27e12, kTcRate = 650e12, kHbm = 6.0e12, kLaunchUs = 2.5;
   const bool tc = prec != TT_PREC_FP64;
-  const int tm = tc ? TC_BM : BM, tn = tc ? TC_BN : BN, tk = tc ? TC_BK : BK;
+  // the DMMA kernel stops at k rounded up to its k-step of 4; the tcgen05
+  // kernel runs whole 32-wide k-chunks
+  const int tm = tc ? TC_BM : BM, tn = tc ? TC_BN : BN, tk = tc ? TC_BK : 4;
   const double rate = tc ? (prec == TT_PREC_TF32X3 ? kTcRate / 3.0 : kTcRate) : kDmmaRate;
   auto up = [](int x, int t) { return (double)((x + t - 1) / t) * t; };
   double total = 0.0, longest = 0.0, bytes = 0.0;
@@ -669,8 +734,10 @@ int tt_contract_plan(tt_ctx* ctx, const tt_out_block* outs, int n_out,
   }
   TT_REQUIRE(tab_len < (1ll << 31), "tt_contract_plan: offset tables too large");
   for (int o = 0; o < n_out; ++o) first[o + 1] += first[o];
-  if (automatic && predict_us(outs, n_out, hp, first, TT_PREC_FP64, ctx->num_sms) <=
-                       predict_us(outs, n_out, hp, first, precision, ctx->num_sms))
+  // FP64 unless the tensor-core form is predicted clearly (20 %) faster: the
+  // model is coarse, and FP64 is the more accurate of the two
+  if (automatic && predict_us(outs, n_out, hp, first, precision, ctx->num_sms) >
+                       0.8 * predict_us(outs, n_out, hp, first, TT_PREC_FP64, ctx->num_sms))
     precision = TT_PREC_FP64;
   const bool tc = precision != TT_PREC_FP64;
   const int tile_m = tc ? TC_BM : BM, tile_n = tc ? TC_BN : BN;
@@ -791,9 +858,9 @@ int tt_contract_exec(tt_ctx* ctx, const tt_plan* plan, const double* A, const do
   if (!attr_set) {
     TT_CUDA(cudaFuncSetAttribute(grouped_dgemm, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)SMEM_BYTES));
-    TT_CUDA(cudaFuncSetAttribute(grouped_tc_bulk<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    TT_CUDA(cudaFuncSetAttribute(grouped_tc_persist<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)TC_BULK_SMEM));
-    TT_CUDA(cudaFuncSetAttribute(grouped_tc_bulk<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    TT_CUDA(cudaFuncSetAttribute(grouped_tc_persist<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)TC_BULK_SMEM));
     attr_set = true;
   }
@@ -812,22 +879,23 @@ int tt_contract_exec(tt_ctx* ctx, const tt_plan* plan, const double* A, const do
     tt::pool_free(ctx, pb);
     return tt::fail(TT_ERR_OOM, "tt_contract_exec: packed operand allocation failed");
   }
-  if (plan->n_tilesA) {
-    if (split) pack_tf32<true><<<plan->n_tilesA, 128, 0, ctx->stream>>>(plan->d_jobsA, plan->d_tilesA, plan->d_tab, A, pa);
-    else pack_tf32<false><<<plan->n_tilesA, 128, 0, ctx->stream>>>(plan->d_jobsA, plan->d_tilesA, plan->d_tab, A, pa);
+  if (plan->n_tilesA + plan->n_tilesB > 0) {
+    const unsigned nt = (unsigned)(plan->n_tilesA + plan->n_tilesB);
+    if (split)
+      pack_tf32_ab<true><<<nt, 128, 0, ctx->stream>>>(plan->d_jobsA, plan->d_tilesA, plan->n_tilesA, plan->d_jobsB,
+                                                       plan->d_tilesB, plan->d_tab, A, B, pa, pb);
+    else
+      pack_tf32_ab<false><<<nt, 128, 0, ctx->stream>>>(plan->d_jobsA, plan->d_tilesA, plan->n_tilesA, plan->d_jobsB,
+                                                        plan->d_tilesB, plan->d_tab, A, B, pa, pb);
     TT_LAUNCH_CHECK(ctx);
   }
-  if (plan->n_tilesB) {
-    if (split) pack_tf32<true><<<plan->n_tilesB, 128, 0, ctx->stream>>>(plan->d_jobsB, plan->d_tilesB, plan->d_tab, B, pb);
-    else pack_tf32<false><<<plan->n_tilesB, 128, 0, ctx->stream>>>(plan->d_jobsB, plan->d_tilesB, plan->d_tab, B, pb);
-    TT_LAUNCH_CHECK(ctx);
-  }
+  const unsigned grid = (unsigned)std::min(plan->n_tasks, std::max(1, ctx->num_sms));
   if (split)
-    grouped_tc_bulk<true><<<plan->n_tasks, 128, TC_BULK_SMEM, ctx->stream>>>(
-        plan->d_tasks, plan->d_outs, plan->d_pairtc, pa, pb, C, alpha, plan->d_status);
+    grouped_tc_persist<true><<<grid, TC_P_THREADS, TC_BULK_SMEM, ctx->stream>>>(
+        plan->d_tasks, plan->n_tasks, plan->d_outs, plan->d_pairtc, pa, pb, C, alpha, plan->d_status);
   else
-    grouped_tc_bulk<false><<<plan->n_tasks, 128, TC_BULK_SMEM, ctx->stream>>>(
-        plan->d_tasks, plan->d_outs, plan->d_pairtc, pa, pb, C, alpha, plan->d_status);
+    grouped_tc_persist<false><<<grid, TC_P_THREADS, TC_BULK_SMEM, ctx->stream>>>(
+        plan->d_tasks, plan->n_tasks, plan->d_outs, plan->d_pairtc, pa, pb, C, alpha, plan->d_status);
   cudaError_t le = cudaGetLastError();
   tt::pool_free(ctx, pa);
   tt::pool_free(ctx, pb);

@@ -691,11 +691,16 @@ double dmrg(MPS& psi, MPO& H, int num_sweeps, const std::vector<int>& max_bd, co
         A.setRight(&TR[r]);
         dtensor x = psi.A[l] * psi.A[r];
         DavidsonStats st;
+        // mixed-precision products only where the two-site space is large
+        // enough that the Krylov vectors cannot exhaust it (their relative
+        // error of about 1e-7 keeps the residual above the tolerance, and in
+        // an exhausted space the extra directions are product noise)
+        const int heff_prec = x.size <= 4096 ? TT_PREC_FP64 : rt().heff_precision;
         {
-          PrecisionScope prec(rt().heff_precision);
+          PrecisionScope prec(heff_prec);
           energy = tensor_davidson(A, x, 3, max_restart[lmr], 1e-12, 'S', &st);
         }
-        if (rt().heff_precision != TT_PREC_FP64 && half == 1 && i == L - 2) {
+        if (heff_prec != TT_PREC_FP64 && half == 1 && i == L - 2) {
           // mixed precision: the sweep's energy is the FP64 Rayleigh quotient
           dtensor y = A.product(x);
           energy = x.inner_product(y) / x.inner_product(x);

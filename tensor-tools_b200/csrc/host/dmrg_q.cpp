@@ -304,6 +304,18 @@ double read1(double* d) {
 
 }  // namespace
 
+// Precision of one Davidson call's H_eff*x products.  The mixed-precision
+// products carry a relative error of about 1e-7, so the residual never reaches
+// the loop's tolerance (1e-12) and every iteration adds a direction; in a
+// two-site space small enough for the Krylov vectors to exhaust it (the chain
+// ends: size() over-counts the U(1) sector), those directions are product
+// noise and the Ritz vector goes wrong.  Tiny problems therefore run their
+// products in FP64, where they are launch-bound anyway.
+constexpr int64_t kMixedMinDim = 4096;
+static int davidson_precision(int64_t dim) {
+  return dim <= kMixedMinDim ? TT_PREC_FP64 : rt().heff_precision;
+}
+
 // ---- tensor_davidsonIT -----------------------------------------------------
 // Device-resident form: every iteration is enqueued up front and the loop's
 // decisions run in the tt_dav_* control kernels, so the whole call
@@ -324,6 +336,17 @@ static bool davidson_device(big_qtensor& A, qtensor& x, int max_restart, double 
   check(tt_vec_scal_inv_dev(ctx(), x.arena, scalar_slot(0), x.data->get()), "normalize");
   auto tb0 = std::chrono::steady_clock::now();
   ProductEngine eng(A, x);
+  const int prec = davidson_precision(eng.n);
+  // A Krylov space cannot outgrow the vector.  size() (kept from the
+  // reference) multiplies the full dimensions of every primed index, which for
+  // a U(1) two-site problem at the chain ends over-counts the sector by orders
+  // of magnitude (768 against 6); the loop would then try to extend a complete
+  // basis, and a random refill orthogonalised against it leaves a round-off
+  // remainder that can pass the 1e-10 test and enter as a near-duplicate
+  // direction (Ritz value ~2 lambda).  In FP64 the residual reaches the
+  // tolerance before the basis is complete, so the cap does not bind there.
+  maxsize = (int)std::min<int64_t>(maxsize, eng.n);
+  actual_maxiter = std::min(max_restart, maxsize - 1);
   auto tb1 = std::chrono::steady_clock::now();
   if (stats) stats->t_engine = std::chrono::duration<double>(tb1 - tb0).count();
   const int64_t n = eng.n;
@@ -345,7 +368,7 @@ static bool davidson_device(big_qtensor& A, qtensor& x, int max_restart, double 
     check(tt_event_create(ctx(), &e.first), "event");
     check(tt_event_create(ctx(), &e.second), "event");
     check(tt_event_record(ctx(), e.first), "event");
-    eng.apply(in.d->get(), out.d->get(), rt().heff_precision);
+    eng.apply(in.d->get(), out.d->get(), prec);
     check(tt_event_record(ctx(), e.second), "event");
     evs.push_back(e);
     out.p = eng.product_presence(in.p);
@@ -431,7 +454,7 @@ static bool davidson_device(big_qtensor& A, qtensor& x, int max_restart, double 
   }
   rt().last_heff_ms = heff_ms;
   double lambda = res.lambda;
-  if (rt().heff_precision != TT_PREC_FP64 && rt().energy_fp64) {
+  if (prec != TT_PREC_FP64 && rt().energy_fp64) {
     KVec y = newvec();
     const KVec& xf = f >= 1 ? xs[f] : v[0];
     eng.apply(xf.d->get(), y.d->get(), TT_PREC_FP64);
@@ -477,6 +500,17 @@ static double davidson_host(big_qtensor& A, qtensor& x, int m, int max_restart, 
     throw std::runtime_error("tensor_davidsonIT: at most 14 iterations (16 Krylov vectors) are supported");
   auto tb0 = std::chrono::steady_clock::now();
   ProductEngine eng(A, x);
+  const int prec = davidson_precision(eng.n);
+  // A Krylov space cannot outgrow the vector.  size() (kept from the
+  // reference) multiplies the full dimensions of every primed index, which for
+  // a U(1) two-site problem at the chain ends over-counts the sector by orders
+  // of magnitude (768 against 6); the loop would then try to extend a complete
+  // basis, and a random refill orthogonalised against it leaves a round-off
+  // remainder that can pass the 1e-10 test and enter as a near-duplicate
+  // direction (Ritz value ~2 lambda).  In FP64 the residual reaches the
+  // tolerance before the basis is complete, so the cap does not bind there.
+  maxsize = (int)std::min<int64_t>(maxsize, eng.n);
+  actual_maxiter = std::min(max_restart, maxsize - 1);
   if (rt().profile) check(tt_ctx_synchronize(ctx()), "sync");
   auto tb1 = std::chrono::steady_clock::now();
   if (stats) stats->t_engine = std::chrono::duration<double>(tb1 - tb0).count();
@@ -497,7 +531,7 @@ static double davidson_host(big_qtensor& A, qtensor& x, int m, int max_restart, 
     check(tt_event_create(ctx(), &e.first), "event");
     check(tt_event_create(ctx(), &e.second), "event");
     check(tt_event_record(ctx(), e.first), "event");
-    eng.apply(in.d->get(), out.d->get(), rt().heff_precision);
+    eng.apply(in.d->get(), out.d->get(), prec);
     check(tt_event_record(ctx(), e.second), "event");
     evs.push_back(e);
     ev_kept.push_back(true);
@@ -670,7 +704,7 @@ static double davidson_host(big_qtensor& A, qtensor& x, int m, int max_restart, 
     x = eng.materialize(xv.p, xv.d);
   }
   x.normalize();  // synchronises: every recorded event has completed
-  if (rt().heff_precision != TT_PREC_FP64 && rt().energy_fp64) {
+  if (prec != TT_PREC_FP64 && rt().energy_fp64) {
     // mixed precision: the reported energy is the FP64 Rayleigh quotient of
     // the final (normalised) vector, its error second order in the vector's
     KVec y = newvec();

@@ -486,6 +486,10 @@ tridiag_eigvecs(const EigDev* __restrict__ probs, const double* G, const double*
 namespace cgx = cooperative_groups;
 
 constexpr int CL_STAGE = 4;  // reflectors staged per round of the back-transformation
+constexpr int CL_MAX = 16;   // largest cluster the kernels are launched with
+
+// doubles of shared memory the phase-1 cluster kernel needs besides the column slab
+__host__ __device__ inline int64_t cluster_vals_extra(int n) { return 6 * (int64_t)n + 2 * CL_MAX; }
 
 __device__ __forceinline__ int first_owned(int from, int rank, int CL) {
   // smallest l with rank + CL * l >= from
@@ -510,14 +514,14 @@ tridiag_eigvals_cluster(const EigDev* __restrict__ probs, double* G, double* Tg,
   double* eg = dg + n;
   double* tg = eg + n;
   const int lcols = (n + CL - 1) / CL;
-  const int64_t extra = 4 * (int64_t)n + 2 * lcols + 8;
+  const int64_t extra = cluster_vals_extra(n);
   const bool in_smem = (int64_t)lcols * n + extra <= cap;
   double* rest = in_smem ? sm + (int64_t)lcols * n : sm;
-  double* vbuf = rest;          // [2][n] reflector published by the column's owner
+  double* vbuf = rest;          // [2][n]: reflector published by the column's owner, tau in the last slot
   double* vloc = vbuf + 2 * n;  // this CTA's copy of v
-  double* wloc = vloc + n;      // this CTA's copy of w
-  double* pown = wloc + n;      // [2][lcols] p on the owned columns
-  double* misc = pown + 2 * lcols;  // tau[2], partial p.v[2]
+  double* wloc = vloc + n;      // w
+  double* pfull = wloc + n;     // [2][n]: p, pushed here by the owners of its columns
+  double* pdots = pfull + 2 * n;  // [2][CL_MAX]: partial p.v, pushed here by every CTA
   auto col = [&](int l) -> double* {  // l-th owned column (global column rank + CL l)
     return in_smem ? sm + (int64_t)l * n : Gp + (int64_t)(rank + CL * l) * n;
   };
@@ -527,7 +531,7 @@ tridiag_eigvals_cluster(const EigDev* __restrict__ probs, double* G, double* Tg,
   __syncthreads();
   const int warp = tid >> 5, lane = tid & 31, nw = blockDim.x >> 5;
   for (int k = 0; k + 2 < n; ++k) {
-    const int m = n - k - 1;
+    const int m = n - k - 1;  // m <= n - 1: the last slot of vbuf is free for tau
     const int par = k & 1;
     const int owner = k % CL;
     if (rank == owner) {
@@ -553,7 +557,7 @@ tridiag_eigvals_cluster(const EigDev* __restrict__ probs, double* G, double* Tg,
         }
         tg[k] = s_tau;
         eg[k] = s_beta;
-        misc[par] = s_tau;
+        vbuf[par * n + n - 1] = s_tau;
       }
       __syncthreads();
       if (s_tau != 0.0) {
@@ -566,12 +570,15 @@ tridiag_eigvals_cluster(const EigDev* __restrict__ probs, double* G, double* Tg,
       }
     }
     cluster.sync();
-    const double tau = *cluster.map_shared_rank(misc + par, owner);
-    if (tau == 0.0) continue;  // column already reduced (same decision in every CTA)
+    // one parallel pull of v and tau from the owner
     const double* ov = cluster.map_shared_rank(vbuf + par * n, owner);
+    if (tid == 0) s_tau = ov[n - 1];
     for (int i = tid; i < m; i += blockDim.x) vloc[i] = ov[i];
     __syncthreads();
-    // p = tau A22 v on the owned columns (A22 symmetric: column dot v), one warp per column
+    const double tau = s_tau;
+    if (tau == 0.0) continue;  // column already reduced (same decision in every CTA)
+    // p = tau A22 v on the owned columns (A22 symmetric: column dot v), one
+    // warp per column; lanes 0..CL-1 push p_c into every CTA's pfull
     const int l0 = first_owned(k + 1, rank, CL);
     for (int l = l0 + warp; l < lcols; l += nw) {
       const int c = rank + CL * l;
@@ -580,26 +587,23 @@ tridiag_eigvals_cluster(const EigDev* __restrict__ probs, double* G, double* Tg,
       double s = 0.0;
       for (int i = lane; i < m; i += 32) s += a[i] * vloc[i];
 #pragma unroll
-      for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
-      if (lane == 0) pown[par * lcols + l] = tau * s;
+      for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+      if (lane < CL) *cluster.map_shared_rank(pfull + par * n + (c - k - 1), lane) = tau * s;
+      if (lane == 0) wloc[c - k - 1] = tau * s;  // own copy for the partial dot
     }
     __syncthreads();
     double loc = 0.0;
     for (int l = l0 + tid; l < lcols; l += blockDim.x) {
       const int c = rank + CL * l;
-      if (c < n) loc += pown[par * lcols + l] * vloc[c - k - 1];
+      if (c < n) loc += wloc[c - k - 1] * vloc[c - k - 1];
     }
     const double part = block_reduce(loc, red, false);
-    if (tid == 0) misc[2 + par] = part;
+    if (tid < CL) *cluster.map_shared_rank(pdots + par * CL_MAX + rank, tid) = part;
     cluster.sync();
     double pv = 0.0;  // fixed CTA order: every CTA forms the same K and w
-    for (int o = 0; o < CL; ++o) pv += *cluster.map_shared_rank(misc + 2 + par, o);
+    for (int o = 0; o < CL; ++o) pv += pdots[par * CL_MAX + o];
     const double K = 0.5 * tau * pv;
-    for (int i = tid; i < m; i += blockDim.x) {
-      const int c = k + 1 + i;
-      const double p = *cluster.map_shared_rank(pown + par * lcols + c / CL, c % CL);
-      wloc[i] = p - K * vloc[i];
-    }
+    for (int i = tid; i < m; i += blockDim.x) wloc[i] = pfull[par * n + i] - K * vloc[i];
     __syncthreads();
     // A22 -= v w^T + w v^T on the owned columns
     for (int l = l0; l < lcols; ++l) {
@@ -777,9 +781,12 @@ tridiag_eigvecs_cluster(const EigDev* __restrict__ probs, const double* G, const
         if (tid < CL) hv[tid] = *cluster.map_shared_rank(hasv + par, tid);
         __syncthreads();
         for (int i = tid; i < n; i += blockDim.x) {
+          double r[CL_MAX];  // every remote load in flight at once, then the sum in CTA order
+#pragma unroll
+          for (int o = 0; o < CL_MAX; ++o) r[o] = (o < CL && hv[o]) ? *cluster.map_shared_rank(u + i, o) : 0.0;
           double s = ybuf[i];
-          for (int o = 0; o < CL; ++o)
-            if (hv[o]) s -= *cluster.map_shared_rank(u + i, o);
+#pragma unroll
+          for (int o = 0; o < CL_MAX; ++o) s -= r[o];
           ybuf[i] = s;
         }
         __syncthreads();
@@ -903,7 +910,7 @@ const ClusterPlan& cluster_plan(tt_ctx* ctx) {
   }
   const int64_t va = ((int64_t)optin - (int64_t)fa.sharedSizeBytes - 1024) / 8;
   const int64_t vb = ((int64_t)optin - (int64_t)fb.sharedSizeBytes - 1024) / 8;
-  if (va < 4 * MAX_N + 1024 || vb < 6 * MAX_N) return cp;
+  if (va < cluster_vals_extra(MAX_N) || vb < 6 * MAX_N) return cp;
   const void* kernels[2] = {(const void*)tridiag_eigvals_cluster, (const void*)tridiag_eigvecs_cluster};
   const int64_t caps[2] = {va, vb};
   for (int k = 0; k < 2; ++k) {
@@ -914,7 +921,7 @@ const ClusterPlan& cluster_plan(tt_ctx* ctx) {
       return cp;
     }
   }
-  for (int cl : {16, 8}) {
+  for (int cl : {CL_MAX, 8}) {
     bool ok = true;
     for (int k = 0; k < 2 && ok; ++k) {
       cudaLaunchConfig_t cfg = {};
@@ -1001,7 +1008,7 @@ int tt_sym_eigvals_batched(tt_ctx* ctx, const tt_eig_problem* probs, int n_probs
     int64_t need = 0;  // doubles: the column slab in shared memory when it fits under the cap
     for (const EigDev& e : big) {
       const int64_t lcols = (e.n + cp.cl - 1) / cp.cl;
-      const int64_t extra = 4 * (int64_t)e.n + 2 * lcols + 8;
+      const int64_t extra = cluster_vals_extra(e.n);
       const int64_t full = lcols * e.n + extra;
       need = std::max(need, full <= cp.vals_cap ? full : extra);
     }

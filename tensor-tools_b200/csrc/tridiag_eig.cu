@@ -489,7 +489,8 @@ constexpr int CL_STAGE = 4;  // reflectors staged per round of the back-transfor
 constexpr int CL_MAX = 16;   // largest cluster the kernels are launched with
 
 // doubles of shared memory the phase-1 cluster kernel needs besides the column slab
-__host__ __device__ inline int64_t cluster_vals_extra(int n) { return 6 * (int64_t)n + 2 * CL_MAX; }
+constexpr int CL_WARPS = TT / 32;  // warps per CTA
+__host__ __device__ inline int64_t cluster_vals_extra(int n) { return 5 * (int64_t)n + 2 * CL_MAX * CL_WARPS; }
 
 __device__ __forceinline__ int first_owned(int from, int rank, int CL) {
   // smallest l with rank + CL * l >= from
@@ -500,7 +501,7 @@ __global__ void __launch_bounds__(TT)
 tridiag_eigvals_cluster(const EigDev* __restrict__ probs, double* G, double* Tg, double* W, int cap) {
   extern __shared__ double sm[];
   __shared__ double red[33];
-  __shared__ double s_tau, s_beta, s_scale;
+  __shared__ double s_tau;
   cgx::cluster_group cluster = cgx::this_cluster();
   const int CL = (int)cluster.num_blocks();
   const int rank = (int)cluster.block_rank();
@@ -517,11 +518,10 @@ tridiag_eigvals_cluster(const EigDev* __restrict__ probs, double* G, double* Tg,
   const int64_t extra = cluster_vals_extra(n);
   const bool in_smem = (int64_t)lcols * n + extra <= cap;
   double* rest = in_smem ? sm + (int64_t)lcols * n : sm;
-  double* vbuf = rest;          // [2][n]: reflector published by the column's owner, tau in the last slot
-  double* vloc = vbuf + 2 * n;  // this CTA's copy of v
-  double* wloc = vloc + n;      // w
-  double* pfull = wloc + n;     // [2][n]: p, pushed here by the owners of its columns
-  double* pdots = pfull + 2 * n;  // [2][CL_MAX]: partial p.v, pushed here by every CTA
+  double* vbuf = rest;            // [2][n]: reflector published by the column's owner, tau in the last slot
+  double* vloc = vbuf + 2 * n;    // this CTA's copy of v
+  double* pfull = vloc + n;       // [2][n]: p, pushed here by the owners of its columns
+  double* pdots = pfull + 2 * n;  // [2][CL_MAX * CL_WARPS]: partial p.v of every warp of the cluster
   auto col = [&](int l) -> double* {  // l-th owned column (global column rank + CL l)
     return in_smem ? sm + (int64_t)l * n : Gp + (int64_t)(rank + CL * l) * n;
   };
@@ -530,44 +530,46 @@ tridiag_eigvals_cluster(const EigDev* __restrict__ probs, double* G, double* Tg,
       for (int i = tid; i < n; i += blockDim.x) sm[(int64_t)l * n + i] = Gp[(int64_t)(rank + CL * l) * n + i];
   __syncthreads();
   const int warp = tid >> 5, lane = tid & 31, nw = blockDim.x >> 5;
+  const int nslot = CL * nw;  // partial dots per column
+  int lend = 0;               // owned columns that exist
+  while (lend < lcols && rank + CL * lend < n) ++lend;
+  double* const abase = col(0);
+  const int64_t lstride = in_smem ? (int64_t)n : (int64_t)CL * n;  // between owned columns
   for (int k = 0; k + 2 < n; ++k) {
     const int m = n - k - 1;  // m <= n - 1: the last slot of vbuf is free for tau
     const int par = k & 1;
     const int owner = k % CL;
-    if (rank == owner) {
-      double* a = col(k / CL);
-      double loc = 0.0;
-      for (int i = 1 + tid; i < m; i += blockDim.x) {
-        const double t = a[k + 1 + i];
-        loc += t * t;
+    if (rank == owner && warp == 0) {  // the reflector, by one warp of the owner
+      const double* a = col(k / CL);
+      double l0s = 0.0, l1s = 0.0;
+      int i = 1 + lane;
+      for (; i + 32 < m; i += 64) {
+        l0s += a[k + 1 + i] * a[k + 1 + i];
+        l1s += a[k + 33 + i] * a[k + 33 + i];
       }
-      const double sigma = block_reduce(loc, red, false);
-      if (tid == 0) {
-        const double alpha = a[k + 1];
-        if (sigma == 0.0) {
-          s_tau = 0.0;
-          s_beta = alpha;
-          s_scale = 0.0;
-        } else {
-          const double mu = sqrt(alpha * alpha + sigma);
-          const double beta = alpha <= 0.0 ? mu : -mu;
-          s_tau = (beta - alpha) / beta;
-          s_scale = 1.0 / (alpha - beta);
-          s_beta = beta;
+      for (; i < m; i += 32) l0s += a[k + 1 + i] * a[k + 1 + i];
+      double loc = l0s + l1s;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) loc += __shfl_xor_sync(0xffffffffu, loc, o);
+      const double alpha = a[k + 1];
+      double tau = 0.0, beta = alpha, scale = 0.0;
+      if (loc != 0.0) {
+        const double mu = sqrt(alpha * alpha + loc);
+        beta = alpha <= 0.0 ? mu : -mu;
+        tau = (beta - alpha) / beta;
+        scale = 1.0 / (alpha - beta);
+      }
+      if (lane == 0) {
+        tg[k] = tau;
+        eg[k] = beta;
+        vbuf[par * n + n - 1] = tau;
+      }
+      if (tau != 0.0)
+        for (int j = lane; j < m; j += 32) {
+          const double vi = (j == 0) ? 1.0 : a[k + 1 + j] * scale;
+          vbuf[par * n + j] = vi;
+          if (j > 0) Gp[(k + 1 + j) + (int64_t)n * k] = vi;  // reflector kept for phase 2
         }
-        tg[k] = s_tau;
-        eg[k] = s_beta;
-        vbuf[par * n + n - 1] = s_tau;
-      }
-      __syncthreads();
-      if (s_tau != 0.0) {
-        const double scale = s_scale;
-        for (int i = tid; i < m; i += blockDim.x) {
-          const double vi = (i == 0) ? 1.0 : a[k + 1 + i] * scale;
-          vbuf[par * n + i] = vi;
-          if (i > 0) Gp[(k + 1 + i) + (int64_t)n * k] = vi;  // reflector kept for phase 2
-        }
-      }
     }
     cluster.sync();
     // one parallel pull of v and tau from the owner
@@ -578,40 +580,64 @@ tridiag_eigvals_cluster(const EigDev* __restrict__ probs, double* G, double* Tg,
     const double tau = s_tau;
     if (tau == 0.0) continue;  // column already reduced (same decision in every CTA)
     // p = tau A22 v on the owned columns (A22 symmetric: column dot v), one
-    // warp per column; lanes 0..CL-1 push p_c into every CTA's pfull
+    // warp per column with four independent chains; lanes 0..CL-1 push p_c
+    // into every CTA's pfull, and every warp pushes its share of p.v into
+    // every CTA's pdots
     const int l0 = first_owned(k + 1, rank, CL);
-    for (int l = l0 + warp; l < lcols; l += nw) {
+    double wpart = 0.0;
+    for (int l = l0 + warp; l < lend; l += nw) {
       const int c = rank + CL * l;
-      if (c >= n) continue;
-      const double* a = col(l) + k + 1;
-      double s = 0.0;
-      for (int i = lane; i < m; i += 32) s += a[i] * vloc[i];
+      const double* __restrict__ a = col(l) + k + 1;
+      double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+      int i = lane;
+      for (; i + 96 < m; i += 128) {
+        s0 += a[i] * vloc[i];
+        s1 += a[i + 32] * vloc[i + 32];
+        s2 += a[i + 64] * vloc[i + 64];
+        s3 += a[i + 96] * vloc[i + 96];
+      }
+      for (; i < m; i += 32) s0 += a[i] * vloc[i];
+      double s = (s0 + s1) + (s2 + s3);
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-      if (lane < CL) *cluster.map_shared_rank(pfull + par * n + (c - k - 1), lane) = tau * s;
-      if (lane == 0) wloc[c - k - 1] = tau * s;  // own copy for the partial dot
+      const double pc = tau * s;
+      if (lane < CL) *cluster.map_shared_rank(pfull + par * n + (c - k - 1), lane) = pc;
+      wpart += pc * vloc[c - k - 1];
     }
-    __syncthreads();
-    double loc = 0.0;
-    for (int l = l0 + tid; l < lcols; l += blockDim.x) {
-      const int c = rank + CL * l;
-      if (c < n) loc += wloc[c - k - 1] * vloc[c - k - 1];
-    }
-    const double part = block_reduce(loc, red, false);
-    if (tid < CL) *cluster.map_shared_rank(pdots + par * CL_MAX + rank, tid) = part;
+    if (lane < CL) *cluster.map_shared_rank(pdots + par * CL_MAX * CL_WARPS + rank * nw + warp, lane) = wpart;
     cluster.sync();
-    double pv = 0.0;  // fixed CTA order: every CTA forms the same K and w
-    for (int o = 0; o < CL; ++o) pv += pdots[par * CL_MAX + o];
-    const double K = 0.5 * tau * pv;
-    for (int i = tid; i < m; i += blockDim.x) wloc[i] = pfull[par * n + i] - K * vloc[i];
-    __syncthreads();
-    // A22 -= v w^T + w v^T on the owned columns
-    for (int l = l0; l < lcols; ++l) {
-      const int c = rank + CL * l;
-      if (c >= n) break;
-      const double vc = vloc[c - k - 1], wc = wloc[c - k - 1];
-      double* a = col(l) + k + 1;
-      for (int i = tid; i < m; i += blockDim.x) a[i] -= vloc[i] * wc + wloc[i] * vc;
+    // p.v: every warp sums the same partials in the same order, so every
+    // warp of every CTA holds the same K
+    double x = 0.0;
+    for (int j = lane; j < nslot; j += 32) x += pdots[par * CL_MAX * CL_WARPS + j];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+    const double K = 0.5 * tau * x;
+    const double* pf = pfull + par * n;
+    // A22 -= v w^T + w v^T on the owned columns, w = p - K v formed on the
+    // fly: rows outer (v_i, w_i in registers), owned columns inner, four at a
+    // time so their loads and stores overlap
+    for (int i = tid; i < m; i += blockDim.x) {
+      const double vi = vloc[i], wi = pf[i] - K * vi;
+      double* __restrict__ ai = abase + (k + 1 + i);
+      int l = l0;
+      for (; l + 3 < lend; l += 4) {
+        const int c0 = rank + CL * l - k - 1;
+        const double v0 = vloc[c0], v1 = vloc[c0 + CL], v2 = vloc[c0 + 2 * CL], v3 = vloc[c0 + 3 * CL];
+        const double w0 = pf[c0] - K * v0, w1 = pf[c0 + CL] - K * v1, w2 = pf[c0 + 2 * CL] - K * v2,
+                     w3 = pf[c0 + 3 * CL] - K * v3;
+        const double a0 = ai[l * lstride], a1 = ai[(l + 1) * lstride], a2 = ai[(l + 2) * lstride],
+                     a3 = ai[(l + 3) * lstride];
+        ai[l * lstride] = a0 - (vi * w0 + wi * v0);
+        ai[(l + 1) * lstride] = a1 - (vi * w1 + wi * v1);
+        ai[(l + 2) * lstride] = a2 - (vi * w2 + wi * v2);
+        ai[(l + 3) * lstride] = a3 - (vi * w3 + wi * v3);
+      }
+      for (; l < lend; ++l) {
+        const int cc = rank + CL * l - k - 1;
+        const double vc = vloc[cc], wc = pf[cc] - K * vc;
+        ai[l * lstride] -= vi * wc + wi * vc;
+      }
     }
     __syncthreads();
   }
@@ -630,7 +656,7 @@ tridiag_eigvals_cluster(const EigDev* __restrict__ probs, double* G, double* Tg,
   __threadfence();
   cluster.sync();  // also the last access of another CTA's shared memory
   double* d = vloc;
-  double* e2 = wloc;
+  double* e2 = pfull;
   for (int i = tid; i < n; i += blockDim.x) {
     d[i] = dg[i];
     e2[i] = i < n - 1 ? eg[i] * eg[i] : 0.0;
@@ -694,8 +720,6 @@ tridiag_eigvecs_cluster(const EigDev* __restrict__ probs, const double* G, const
   __shared__ double red[33];
   __shared__ double coef[MAX_N / 2];
   __shared__ int cstart[MAX_N / 2];
-  __shared__ int hasv[2];
-  __shared__ int hv[32];
   cgx::cluster_group cluster = cgx::this_cluster();
   const int CL = (int)cluster.num_blocks();
   const int rank = (int)cluster.block_rank();
@@ -745,7 +769,9 @@ tridiag_eigvecs_cluster(const EigDev* __restrict__ probs, const double* G, const
   }
   __syncthreads();
   cluster.sync();  // every start vector is in place
-  // (b) Gram-Schmidt, vector by vector
+  // (b) Gram-Schmidt, vector by vector.  Which CTAs hold members of the
+  // cluster [c0, j) follows from c0, j and q alone, so no flags are exchanged;
+  // every CTA holds the same iterate y and forms its norm in the same order.
   int g = 0;
   for (int j = 1; j < nvec && j < MAX_N / 2; ++j) {
     const int c0 = cstart[j];
@@ -753,17 +779,27 @@ tridiag_eigvecs_cluster(const EigDev* __restrict__ probs, const double* G, const
     const int owner = j / q;
     const double* yj = in_smem ? cluster.map_shared_rank(zsm + (int64_t)n * (j - owner * q), owner)
                                : Zout + (int64_t)n * j;
+    __syncthreads();  // every read of the previous iterate is done
     for (int i = tid; i < n; i += blockDim.x) ybuf[i] = yj[i];
     __syncthreads();
     const int ka = max(c0, j0), kb = min(j, j1);  // own members of the cluster before j
+    const int o_lo = c0 / q, o_hi = (j - 1) / q;  // CTAs that own members
     for (int pass = 0; pass < 6; ++pass) {
       for (int r = 0; r < 2; ++r) {
         const int par = g & 1;
         double* u = ubuf + par * n;
         for (int k = ka + warp; k < kb; k += nw) {
-          const double* zk = Z + (int64_t)n * (k - j0);
-          double s = 0.0;
-          for (int i = lane; i < n; i += 32) s += zk[i] * ybuf[i];
+          const double* __restrict__ zk = Z + (int64_t)n * (k - j0);
+          double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;  // independent chains
+          int i = lane;
+          for (; i + 96 < n; i += 128) {
+            s0 += zk[i] * ybuf[i];
+            s1 += zk[i + 32] * ybuf[i + 32];
+            s2 += zk[i + 64] * ybuf[i + 64];
+            s3 += zk[i + 96] * ybuf[i + 96];
+          }
+          for (; i < n; i += 32) s0 += zk[i] * ybuf[i];
+          double s = (s0 + s1) + (s2 + s3);
 #pragma unroll
           for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
           if (lane == 0) coef[k - ka] = s;
@@ -771,38 +807,47 @@ tridiag_eigvecs_cluster(const EigDev* __restrict__ probs, const double* G, const
         __syncthreads();
         if (kb > ka)
           for (int i = tid; i < n; i += blockDim.x) {
-            double s = 0.0;
-            for (int k = ka; k < kb; ++k) s += coef[k - ka] * Z[(int64_t)n * (k - j0) + i];
-            u[i] = s;
+            const double* __restrict__ zi = Z + (int64_t)n * (ka - j0) + i;
+            double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+            int k = 0;
+            const int nk = kb - ka;
+            for (; k + 3 < nk; k += 4) {
+              s0 += coef[k] * zi[(int64_t)n * k];
+              s1 += coef[k + 1] * zi[(int64_t)n * (k + 1)];
+              s2 += coef[k + 2] * zi[(int64_t)n * (k + 2)];
+              s3 += coef[k + 3] * zi[(int64_t)n * (k + 3)];
+            }
+            for (; k < nk; ++k) s0 += coef[k] * zi[(int64_t)n * k];
+            u[i] = (s0 + s1) + (s2 + s3);
           }
-        if (tid == 0) hasv[par] = kb > ka ? 1 : 0;
-        __syncthreads();
         cluster.sync();
-        if (tid < CL) hv[tid] = *cluster.map_shared_rank(hasv + par, tid);
-        __syncthreads();
         for (int i = tid; i < n; i += blockDim.x) {
-          double r[CL_MAX];  // every remote load in flight at once, then the sum in CTA order
+          double rr[CL_MAX];  // every remote load in flight at once, then the sum in CTA order
 #pragma unroll
-          for (int o = 0; o < CL_MAX; ++o) r[o] = (o < CL && hv[o]) ? *cluster.map_shared_rank(u + i, o) : 0.0;
+          for (int o = 0; o < CL_MAX; ++o)
+            rr[o] = (o >= o_lo && o <= o_hi && o < CL) ? *cluster.map_shared_rank(u + i, o) : 0.0;
           double s = ybuf[i];
 #pragma unroll
-          for (int o = 0; o < CL_MAX; ++o) s -= r[o];
+          for (int o = 0; o < CL_MAX; ++o) s -= rr[o];
           ybuf[i] = s;
         }
         __syncthreads();
         ++g;
       }
-      loc = 0.0;
-      for (int i = tid; i < n; i += blockDim.x) loc += ybuf[i] * ybuf[i];
-      const double nrm = sqrt(block_reduce(loc, red, false));
+      double nl = 0.0;  // every warp: the whole norm, same order
+      for (int i = lane; i < n; i += 32) nl += ybuf[i] * ybuf[i];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) nl += __shfl_xor_sync(0xffffffffu, nl, o);
+      const double nrm = sqrt(nl);
       if (nrm > 0.5 || pass == 5) {
         const double inv = nrm > 0.0 ? 1.0 / nrm : 0.0;
-        for (int i = tid; i < n; i += blockDim.x) ybuf[i] *= inv;
-        __syncthreads();
+        if (rank == owner)
+          for (int i = tid; i < n; i += blockDim.x) Z[(int64_t)n * (j - j0) + i] = ybuf[i] * inv;
         break;
       }
       // collapsed onto earlier vectors: one more inverse iteration from the
       // orthogonal remainder (every CTA alike), then orthogonalise again
+      __syncthreads();
       if (tid == 0) {
         const double inv = nrm > 0.0 ? 1.0 / nrm : 1.0;
         for (int i = 0; i < n; ++i) ybuf[i] = nrm > 0.0 ? ybuf[i] * inv : hash_unit((uint64_t)(j * 7919 + i + pass));
@@ -810,9 +855,6 @@ tridiag_eigvecs_cluster(const EigDev* __restrict__ probs, const double* G, const
       }
       __syncthreads();
     }
-    if (rank == owner)
-      for (int i = tid; i < n; i += blockDim.x) Z[(int64_t)n * (j - j0) + i] = ybuf[i];
-    __syncthreads();
   }
   cluster.sync();  // no CTA reads another's shared memory after this point
   // (c) back-transformation z = H_0 H_1 ... H_{n-3} y, last reflector first
@@ -830,9 +872,18 @@ tridiag_eigvecs_cluster(const EigDev* __restrict__ probs, const double* G, const
         const int k = kb - s, m = n - k - 1;
         const double tk = tau[k];
         if (tk == 0.0) continue;
-        const double* v = stg + (int64_t)s * n;
-        double acc = 0.0;
-        for (int i = lane; i < m; i += 32) acc += v[i] * y[k + 1 + i];
+        const double* __restrict__ v = stg + (int64_t)s * n;
+        const double* __restrict__ yk = y + k + 1;
+        double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;  // independent chains
+        int i = lane;
+        for (; i + 96 < m; i += 128) {
+          a0 += v[i] * yk[i];
+          a1 += v[i + 32] * yk[i + 32];
+          a2 += v[i + 64] * yk[i + 64];
+          a3 += v[i + 96] * yk[i + 96];
+        }
+        for (; i < m; i += 32) a0 += v[i] * yk[i];
+        double acc = (a0 + a1) + (a2 + a3);
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
         const double c = tk * acc;

@@ -94,7 +94,11 @@ int tt_ctx_create(int device, tt_ctx** out) {
   TT_CUDA(cudaMallocHost(&ctx->h_scalars, kBounceBytes));
   ctx->stage_cap = (size_t)64 << 20;
   TT_CUDA(cudaMallocHost(&ctx->stage, ctx->stage_cap));
-  if (!tt::partials(ctx, 16 * 4 * ctx->num_sms + 64)) {
+  if (!tt::partials(ctx, 16 * 4 * ctx->num_sms + 64) ||
+      cudaMalloc(&ctx->d_ticket, sizeof(unsigned int)) != cudaSuccess ||
+      cudaMemset(ctx->d_ticket, 0, sizeof(unsigned int)) != cudaSuccess) {
+    if (ctx->d_partials) cudaFree(ctx->d_partials);
+    if (ctx->d_ticket) cudaFree(ctx->d_ticket);
     delete ctx;
     return tt::fail(TT_ERR_OOM, "tt_ctx_create: scratch allocation failed");
   }
@@ -107,6 +111,7 @@ int tt_ctx_destroy(tt_ctx* ctx) {
   cudaSetDevice(ctx->device);
   cudaStreamSynchronize(ctx->stream);
   if (ctx->d_partials) cudaFree(ctx->d_partials);
+  if (ctx->d_ticket) cudaFree(ctx->d_ticket);
   if (ctx->h_scalars) cudaFreeHost(ctx->h_scalars);
   if (ctx->stage) cudaFreeHost(ctx->stage);
   cudaStreamDestroy(ctx->stream);

@@ -18,9 +18,12 @@ struct tt_ctx {
   int64_t launches = 0;
   // small pinned staging buffer for scalar reads
   double* h_scalars = nullptr;
-  // device scratch for two-pass reductions
+  // device scratch for the reductions: per-block partial sums, and the
+  // ticket counter with which the last block of a reduction finds itself
+  // (zero between reductions; the last block resets it)
   double* d_partials = nullptr;
   int partials_cap = 0;
+  unsigned int* d_ticket = nullptr;
   // pinned staging ring for host->device copies that must not stall the stream
   char* stage = nullptr;
   size_t stage_cap = 0;

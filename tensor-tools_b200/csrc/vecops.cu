@@ -2,8 +2,9 @@
 // :1031-1179,1606-1647): dot, multi-dot, norm, axpy, scale, linear
 // combinations with device-side coefficients, masked random fill and the
 // diagonal preconditioner.  All are HBM-bound streaming kernels: 16-byte
-// vector loads, a fixed grid (a multiple of the SM count) and a two-pass
-// deterministic reduction (same summation order on every run).
+// vector loads, a fixed grid (a multiple of the SM count) and a deterministic
+// reduction (same summation order on every run): per-block partials, summed in
+// block order by the last block of the same launch.
 #include <algorithm>
 #include <cmath>
 #include <mutex>
@@ -73,6 +74,54 @@ __global__ void __launch_bounds__(RT) multidot_pass1(int64_t n, PtrPack xs,
       if (j < nv) acc[j] = fma(xs.p[j][n - 1], y[n - 1], acc[j]);
   }
   block_reduce_store<NV>(acc, part, gridDim.x);
+}
+
+// One launch for a whole multi-dot: pass 1 as above, then the last block to
+// finish (a ticket counter, reset by that block) sums the per-block partials
+// of every vector in the same order as reduce_pass2, so the result is
+// bit-identical to the two-launch form.
+template <int NV>
+__global__ void __launch_bounds__(RT) multidot_fused(int64_t n, PtrPack xs, const double* __restrict__ y,
+                                                     double* part, int nv, double* out, int do_sqrt,
+                                                     unsigned int* ticket) {
+  double acc[NV];
+#pragma unroll
+  for (int j = 0; j < NV; ++j) acc[j] = 0.0;
+  const int64_t n2 = n / 2;
+  const double2* y2 = reinterpret_cast<const double2*>(y);
+  for (int64_t i = blockIdx.x * (int64_t)RT + threadIdx.x; i < n2; i += (int64_t)gridDim.x * RT) {
+    double2 b = y2[i];
+#pragma unroll
+    for (int j = 0; j < NV; ++j) {
+      if (j < nv) {
+        double2 a = reinterpret_cast<const double2*>(xs.p[j])[i];
+        acc[j] = fma(a.x, b.x, acc[j]);
+        acc[j] = fma(a.y, b.y, acc[j]);
+      }
+    }
+  }
+  if ((n & 1) && blockIdx.x == 0 && threadIdx.x == 0) {
+#pragma unroll
+    for (int j = 0; j < NV; ++j)
+      if (j < nv) acc[j] = fma(xs.p[j][n - 1], y[n - 1], acc[j]);
+  }
+  block_reduce_store<NV>(acc, part, gridDim.x);
+  __shared__ bool last;
+  __threadfence();  // this block's partials are visible before its ticket is taken
+  __syncthreads();
+  if (threadIdx.x == 0) last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int j = w; j < nv; j += RT / 32) {
+    double s = 0.0;
+    for (int i = lane; i < (int)gridDim.x; i += 32) s += __ldcg(part + j * gridDim.x + i);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if (lane == 0) out[j] = do_sqrt ? sqrt(s) : s;
+  }
+  if (threadIdx.x == 0) *ticket = 0u;  // ready for the next reduction on this stream
 }
 
 __global__ void reduce_pass2(const double* part, int nblk, int nv, double* out, int do_sqrt) {
@@ -185,13 +234,11 @@ int launch_multidot(tt_ctx* ctx, int64_t n, int nv, const double* const* xs, con
   double* part = tt::partials(ctx, nb * nv);
   if (!part) return tt::fail(TT_ERR_OOM, "reduction scratch");
   if (nv <= 1)
-    multidot_pass1<1><<<nb, RT, 0, ctx->stream>>>(n, pk, y, part, nv);
+    multidot_fused<1><<<nb, RT, 0, ctx->stream>>>(n, pk, y, part, nv, d_out, do_sqrt, ctx->d_ticket);
   else if (nv <= 4)
-    multidot_pass1<4><<<nb, RT, 0, ctx->stream>>>(n, pk, y, part, nv);
+    multidot_fused<4><<<nb, RT, 0, ctx->stream>>>(n, pk, y, part, nv, d_out, do_sqrt, ctx->d_ticket);
   else
-    multidot_pass1<MAXVEC><<<nb, RT, 0, ctx->stream>>>(n, pk, y, part, nv);
-  TT_LAUNCH_CHECK(ctx);
-  reduce_pass2<<<1, 32 * nv, 0, ctx->stream>>>(part, nb, nv, d_out, do_sqrt);
+    multidot_fused<MAXVEC><<<nb, RT, 0, ctx->stream>>>(n, pk, y, part, nv, d_out, do_sqrt, ctx->d_ticket);
   TT_LAUNCH_CHECK(ctx);
   return TT_OK;
 }

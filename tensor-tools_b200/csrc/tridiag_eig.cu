@@ -785,6 +785,10 @@ tridiag_eigvecs_cluster(const EigDev* __restrict__ probs, const double* G, const
     const int ka = max(c0, j0), kb = min(j, j1);  // own members of the cluster before j
     const int o_lo = c0 / q, o_hi = (j - 1) / q;  // CTAs that own members
     for (int pass = 0; pass < 6; ++pass) {
+      double n0 = 0.0;  // |y|^2 before the projections, every warp alike
+      for (int i = lane; i < n; i += 32) n0 += ybuf[i] * ybuf[i];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) n0 += __shfl_xor_sync(0xffffffffu, n0, o);
       for (int r = 0; r < 2; ++r) {
         const int par = g & 1;
         double* u = ubuf + par * n;
@@ -833,6 +837,16 @@ tridiag_eigvecs_cluster(const EigDev* __restrict__ probs, const double* G, const
         }
         __syncthreads();
         ++g;
+        if (r == 0) {
+          // "twice is enough" (Kahan, Parlett): a second projection only when
+          // the first removed more than half of |y|^2; every CTA and warp holds
+          // the same y and takes the same decision
+          double n1 = 0.0;
+          for (int i = lane; i < n; i += 32) n1 += ybuf[i] * ybuf[i];
+#pragma unroll
+          for (int o = 16; o > 0; o >>= 1) n1 += __shfl_xor_sync(0xffffffffu, n1, o);
+          if (n1 > 0.5 * n0) break;
+        }
       }
       double nl = 0.0;  // every warp: the whole norm, same order
       for (int i = lane; i < n; i += 32) nl += ybuf[i] * ybuf[i];

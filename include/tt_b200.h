@@ -184,6 +184,14 @@ int tt_vec_scale_mode(tt_ctx* ctx, int64_t inner, int mid, int64_t outer, const 
  * xs is a HOST array of nvec (0..16) device pointers. */
 int tt_vec_lincomb_dev(tt_ctx* ctx, int64_t n, int nvec, const double* const* xs,
                        const double* d_coef, double sign, int accumulate, double* y);
+/* The Ritz vector and residual of a Davidson iteration in one pass
+ * (linalg/tensor_davidson.cpp:255-269): x = sum_{j<k} coef_x[j] vs[j] and
+ * q = sum_{j<k} coef_q[j] vas[j] + coef_q[k] x, coefficients on the device;
+ * bit-identical to two tt_vec_lincomb_dev calls.  vs and vas are HOST arrays
+ * of k (1..15) device pointers. */
+int tt_vec_ritz_residual_dev(tt_ctx* ctx, int64_t n, int k, const double* const* vs,
+                             const double* const* vas, const double* d_coef_x,
+                             const double* d_coef_q, double* x, double* q);
 /* x[r] = uniform(0,1) for every element inside the given [begin,end) element
  * ranges (blocks present in the tensor), 0 elsewhere; counter-based RNG. */
 int tt_vec_fill_random(tt_ctx* ctx, int64_t n, double* x, int nranges,

@@ -404,10 +404,10 @@ static bool davidson_device(big_qtensor& A, qtensor& x, int max_restart, double 
         vq.push_back(va[k].d->get());
         pq = por(pq, va[k].p);
       }
-      lincomb(xn, vv, coef_x, 1.0, 0);
+      check(tt_vec_ritz_residual_dev(ctx(), n, ii + 1, vv.data(), vq.data(), coef_x, coef_q, xn.d->get(),
+                                     q.d->get()),
+            "ritz vector and residual");
       xn.p = px;
-      vq.push_back(xn.d->get());
-      lincomb(q, vq, coef_q, 1.0, 0);
       q.p = por(pq, px);
       xs[ii] = xn;
     }

@@ -185,6 +185,26 @@ __global__ void lincomb_kernel(int64_t n, int nv, PtrPack xs, const double* __re
   }
 }
 
+// The Ritz vector and the residual of one Davidson iteration in one pass:
+// x = sum_j cx[j] v_j, q = sum_j cq[j] va_j + cq[k] x, with the fma order of
+// two lincomb_kernel launches (so the results are bit-identical to them).
+__global__ void ritz_residual_kernel(int64_t n, int k, PtrPack vs, PtrPack vas, const double* __restrict__ cx,
+                                     const double* __restrict__ cq, double* __restrict__ x, double* __restrict__ q) {
+  __shared__ double a[MAXVEC], b[MAXVEC + 1];
+  if (threadIdx.x < k) a[threadIdx.x] = cx[threadIdx.x];
+  if (threadIdx.x <= k) b[threadIdx.x] = cq[threadIdx.x];
+  __syncthreads();
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    double xs = 0.0;
+    for (int j = 0; j < k; ++j) xs = fma(a[j], vs.p[j][i], xs);
+    double qs = 0.0;
+    for (int j = 0; j < k; ++j) qs = fma(b[j], vas.p[j][i], qs);
+    qs = fma(b[k], xs, qs);
+    x[i] = xs;
+    q[i] = qs;
+  }
+}
+
 __device__ __forceinline__ uint64_t splitmix64(uint64_t z) {
   z += 0x9E3779B97F4A7C15ull;
   z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
@@ -379,6 +399,21 @@ int tt_vec_lincomb_dev(tt_ctx* ctx, int64_t n, int nvec, const double* const* xs
   for (int j = 0; j < nvec; ++j) pk.p[j] = xs[j];
   if (n <= 0) return TT_OK;
   lincomb_kernel<<<stream_blocks(ctx, n), 256, 0, ctx->stream>>>(n, nvec, pk, d_coef, sign, accumulate, y);
+  TT_LAUNCH_CHECK(ctx);
+  return TT_OK;
+}
+
+int tt_vec_ritz_residual_dev(tt_ctx* ctx, int64_t n, int k, const double* const* vs, const double* const* vas,
+                             const double* d_coef_x, const double* d_coef_q, double* x, double* q) {
+  TT_REQUIRE(ctx && vs && vas && d_coef_x && d_coef_q && x && q, "tt_vec_ritz_residual_dev: null argument");
+  TT_REQUIRE(k >= 1 && k < MAXVEC, "tt_vec_ritz_residual_dev: 1..15 vectors");
+  PtrPack pv, pa;
+  for (int j = 0; j < k; ++j) {
+    pv.p[j] = vs[j];
+    pa.p[j] = vas[j];
+  }
+  if (n <= 0) return TT_OK;
+  ritz_residual_kernel<<<stream_blocks(ctx, n), 256, 0, ctx->stream>>>(n, k, pv, pa, d_coef_x, d_coef_q, x, q);
   TT_LAUNCH_CHECK(ctx);
   return TT_OK;
 }

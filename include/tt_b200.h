@@ -184,6 +184,12 @@ int tt_vec_scale_mode(tt_ctx* ctx, int64_t inner, int mid, int64_t outer, const 
  * xs is a HOST array of nvec (0..16) device pointers. */
 int tt_vec_lincomb_dev(tt_ctx* ctx, int64_t n, int nvec, const double* const* xs,
                        const double* d_coef, double sign, int accumulate, double* y);
+/* The Gram-Schmidt projection and its norm in one launch: y -= sum_j
+ * coef[j] xs[j] (coefficients on the device), then *d_norm = |y|;
+ * bit-identical to tt_vec_lincomb_dev(..., -1.0, 1, y) followed by
+ * tt_vec_nrm2.  xs is a HOST array of nvec (0..16) device pointers. */
+int tt_vec_project_nrm2_dev(tt_ctx* ctx, int64_t n, int nvec, const double* const* xs,
+                            const double* d_coef, double* y, double* d_norm);
 /* The Ritz vector and residual of a Davidson iteration in one pass
  * (linalg/tensor_davidson.cpp:255-269): x = sum_{j<k} coef_x[j] vs[j] and
  * q = sum_{j<k} coef_q[j] vas[j] + coef_q[k] x, coefficients on the device;

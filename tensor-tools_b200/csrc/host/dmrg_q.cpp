@@ -422,8 +422,8 @@ static bool davidson_device(big_qtensor& A, qtensor& x, int max_restart, double 
       v[ni].p = por(v[ni].p, v[k].p);
     }
     check(tt_vec_multidot(ctx(), n, ni, vs.data(), v[ni].d->get(), scalar_slot(0)), "GS overlaps");
-    check(tt_vec_lincomb_dev(ctx(), n, ni, vs.data(), scalar_slot(0), -1.0, 1, v[ni].d->get()), "GS update");
-    check(tt_vec_nrm2(ctx(), n, v[ni].d->get(), scalar_slot(kNormSlot)), "GS norm");
+    check(tt_vec_project_nrm2_dev(ctx(), n, ni, vs.data(), scalar_slot(0), v[ni].d->get(), scalar_slot(kNormSlot)),
+          "GS update and norm");
     check(tt_vec_scal_inv_dev(ctx(), n, scalar_slot(kNormSlot), v[ni].d->get()), "GS scale");
     va[ni] = product(v[ni]);
     vs.push_back(v[ni].d->get());

@@ -124,6 +124,55 @@ __global__ void __launch_bounds__(RT) multidot_fused(int64_t n, PtrPack xs, cons
   if (threadIdx.x == 0) *ticket = 0u;  // ready for the next reduction on this stream
 }
 
+// y -= sum_j coef[j] xs[j], then |y| -- the Gram-Schmidt projection and the
+// norm of its result in one launch.  The grid, the pair-wise walk and the fma
+// order are those of lincomb_kernel (per element) and of multidot_fused<1>
+// (for the norm), so both results are bit-identical to the two launches.
+__global__ void __launch_bounds__(RT) project_nrm2_kernel(int64_t n, int nv, PtrPack xs,
+                                                          const double* __restrict__ coef, double* y,
+                                                          double* part, double* out, unsigned int* ticket) {
+  __shared__ double c[MAXVEC];
+  if (threadIdx.x < nv) c[threadIdx.x] = -1.0 * coef[threadIdx.x];
+  __syncthreads();
+  double acc[1] = {0.0};
+  const int64_t n2 = n / 2;
+  double2* y2 = reinterpret_cast<double2*>(y);
+  for (int64_t i = blockIdx.x * (int64_t)RT + threadIdx.x; i < n2; i += (int64_t)gridDim.x * RT) {
+    double2 b = y2[i];
+    for (int j = 0; j < nv; ++j) {
+      const double2 a = reinterpret_cast<const double2*>(xs.p[j])[i];
+      b.x = fma(c[j], a.x, b.x);
+      b.y = fma(c[j], a.y, b.y);
+    }
+    y2[i] = b;
+    acc[0] = fma(b.x, b.x, acc[0]);
+    acc[0] = fma(b.y, b.y, acc[0]);
+  }
+  if ((n & 1) && blockIdx.x == 0 && threadIdx.x == 0) {
+    double t = y[n - 1];
+    for (int j = 0; j < nv; ++j) t = fma(c[j], xs.p[j][n - 1], t);
+    y[n - 1] = t;
+    acc[0] = fma(t, t, acc[0]);
+  }
+  block_reduce_store<1>(acc, part, gridDim.x);
+  __shared__ bool last;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  if (threadIdx.x < 32) {
+    const int lane = threadIdx.x;
+    double s = 0.0;
+    for (int i = lane; i < (int)gridDim.x; i += 32) s += __ldcg(part + i);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if (lane == 0) out[0] = sqrt(s);
+  }
+  if (threadIdx.x == 0) *ticket = 0u;
+}
+
 __global__ void reduce_pass2(const double* part, int nblk, int nv, double* out, int do_sqrt) {
   // one warp per output, fixed order
   const int j = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -399,6 +448,24 @@ int tt_vec_lincomb_dev(tt_ctx* ctx, int64_t n, int nvec, const double* const* xs
   for (int j = 0; j < nvec; ++j) pk.p[j] = xs[j];
   if (n <= 0) return TT_OK;
   lincomb_kernel<<<stream_blocks(ctx, n), 256, 0, ctx->stream>>>(n, nvec, pk, d_coef, sign, accumulate, y);
+  TT_LAUNCH_CHECK(ctx);
+  return TT_OK;
+}
+
+int tt_vec_project_nrm2_dev(tt_ctx* ctx, int64_t n, int nvec, const double* const* xs, const double* d_coef,
+                            double* y, double* d_norm) {
+  TT_REQUIRE(ctx && xs && d_coef && y && d_norm, "tt_vec_project_nrm2_dev: null argument");
+  TT_REQUIRE(nvec >= 0 && nvec <= MAXVEC, "tt_vec_project_nrm2_dev: 0..16 vectors");
+  TT_REQUIRE(aligned16(y), "tt_vec_project_nrm2_dev: vectors must be 16-byte aligned");
+  PtrPack pk;
+  for (int j = 0; j < nvec; ++j) {
+    if (!aligned16(xs[j])) return tt::fail(TT_ERR_INVALID, "tt_vec_project_nrm2_dev: vectors must be 16-byte aligned");
+    pk.p[j] = xs[j];
+  }
+  const int nb = red_blocks(ctx, n);
+  double* part = tt::partials(ctx, nb);
+  if (!part) return tt::fail(TT_ERR_OOM, "reduction scratch");
+  project_nrm2_kernel<<<nb, RT, 0, ctx->stream>>>(n, nvec, pk, d_coef, y, part, d_norm, ctx->d_ticket);
   TT_LAUNCH_CHECK(ctx);
   return TT_OK;
 }

@@ -13,7 +13,15 @@ L2 is also flushed before every timed sweep.
 Reported value: seconds per sweep (lower is better), device-timed with CUDA
 events on the library's stream, max over ranks.  The H_eff*x throughput is in
 ``roofline``; ``e2e`` repeats a sweep through the public C ABI with the MPS
-round-tripping through pinned host memory every step.
+round-tripping through pinned host memory every step; ``mixed`` repeats the
+schedule in the automatic mixed-precision form (3xTF32 on tcgen05 where the
+cost model predicts a gain, FP64 elsewhere) with its energy difference.
+
+Other workloads (``--workload``): ``j1j2`` -- FP64 against mixed precision
+at large bond dimension on the J1-J2 cylinder (``--maxdim``, ``--breakdown``
+for a per-phase split, ``--profile-step`` to bracket one two-site step for
+ncu); ``gemm`` -- single-block contraction throughput per precision;
+``xxz-chains`` -- independent chains sharing one GPU.
 
 ``--impl reference`` times the CPU restatement of the reference algorithm
 (oracle/, numpy + LAPACK on all host cores) on a bounded sample of the same

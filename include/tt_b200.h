@@ -138,6 +138,13 @@ int tt_plan_flops(const tt_plan* plan, double* flops);
 /* The precision the plan runs in (TT_PREC_FP64 / TF32 / TF32X3): an *_AUTO
  * request resolves to one of them when the plan is built. */
 int tt_plan_precision(const tt_plan* plan, int* precision);
+/* The cost model behind the *_AUTO precisions, without a device: the
+ * predicted microseconds of one exec of the contraction (described as for
+ * tt_contract_plan) in FP64 and in the tensor-core kind, and the precision
+ * tt_contract_plan would choose on a device with num_sms SMs. */
+int tt_contract_predict(const tt_out_block* outs, int n_out, const tt_block_pair* pairs,
+                        int n_pairs, int precision, int num_sms, double* us_fp64,
+                        double* us_tc, int* choice);
 /* Device status of the plan's tensor-core launches since the plan was built:
  * TT_OK, or TT_ERR_TIMEOUT when a bounded wait on the MMA completion barrier
  * gave up (the tile was then skipped).  Synchronises the context's stream. */

@@ -931,6 +931,49 @@ int tt_plan_device_status(tt_ctx* ctx, const tt_plan* plan, int* status) {
   return TT_OK;
 }
 
+int tt_contract_predict(const tt_out_block* outs, int n_out, const tt_block_pair* pairs, int n_pairs,
+                        int precision, int num_sms, double* us_fp64, double* us_tc, int* choice) {
+  TT_REQUIRE(outs && (n_pairs == 0 || pairs) && us_fp64 && us_tc && choice, "tt_contract_predict: null argument");
+  TT_REQUIRE(n_out >= 0 && n_pairs >= 0 && num_sms >= 1, "tt_contract_predict: bad counts");
+  TT_REQUIRE(precision == TT_PREC_TF32_AUTO || precision == TT_PREC_TF32X3_AUTO,
+             "tt_contract_predict: precision must be TT_PREC_TF32_AUTO or TT_PREC_TF32X3_AUTO");
+  const int kind = precision == TT_PREC_TF32_AUTO ? TT_PREC_TF32 : TT_PREC_TF32X3;
+  // the pairs grouped by output block, as tt_contract_plan groups them
+  std::vector<int> order(n_pairs);
+  std::iota(order.begin(), order.end(), 0);
+  for (int i = 0; i < n_pairs; ++i)
+    TT_REQUIRE(pairs[i].out_block >= 0 && pairs[i].out_block < n_out,
+               "tt_contract_predict: pair references a missing output block");
+  std::stable_sort(order.begin(), order.end(),
+                   [&](int a, int b) { return pairs[a].out_block < pairs[b].out_block; });
+  std::vector<PairDev> hp(n_pairs);
+  std::vector<int> first(n_out + 1, 0);
+  for (int ii = 0; ii < n_pairs; ++ii) {
+    const tt_block_pair& q = pairs[order[ii]];
+    TT_REQUIRE(q.n_m >= 0 && q.n_m <= TT_MAX_MODES && q.n_k >= 0 && q.n_k <= TT_MAX_MODES && q.n_n >= 0 &&
+                   q.n_n <= TT_MAX_MODES,
+               "tt_contract_predict: mode count out of range");
+    int64_t m = 1, n = 1, k = 1;
+    for (int i = 0; i < q.n_m; ++i) m *= q.m_dims[i];
+    for (int i = 0; i < q.n_k; ++i) k *= q.k_dims[i];
+    for (int i = 0; i < q.n_n; ++i) n *= q.n_dims[i];
+    PairDev P;
+    memset(&P, 0, sizeof(P));
+    P.a_off = q.a_off;
+    P.b_off = q.b_off;
+    P.m = (int)m;
+    P.n = (int)n;
+    P.k = (int)k;
+    hp[ii] = P;
+    first[q.out_block + 1]++;
+  }
+  for (int o = 0; o < n_out; ++o) first[o + 1] += first[o];
+  *us_fp64 = predict_us(outs, n_out, hp, first, TT_PREC_FP64, num_sms);
+  *us_tc = predict_us(outs, n_out, hp, first, kind, num_sms);
+  *choice = *us_tc > 0.8 * *us_fp64 ? TT_PREC_FP64 : kind;  // the rule tt_contract_plan applies
+  return TT_OK;
+}
+
 int tt_plan_precision(const tt_plan* plan, int* precision) {
   TT_REQUIRE(plan && precision, "tt_plan_precision: null argument");
   *precision = plan->precision;

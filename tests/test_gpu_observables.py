@@ -4,7 +4,9 @@ The device MPS after DMRG is read back block by block, contracted into its
 2^L amplitude vector on the CPU, and the correlators are evaluated exactly on
 it (bit-for-bit the same state, so the tolerance is round-off, 1e-12).  The
 correlators of the exact ground state (ED) pin the physics at the DMRG
-accuracy, and psiHphi / psiphi reproduce the DMRG energy.
+accuracy, and psiHphi / psiphi reproduce the DMRG energy.  A coupling
+derivative dE/dJ comes from the same expectation-value contraction
+(Hellmann-Feynman) and is checked against ED.
 """
 import numpy as np
 import pytest
@@ -99,3 +101,47 @@ def test_dense_tfi_correlators_and_energy(ctx):
     sz, szsz = psi.measure_sz()
     np.testing.assert_allclose(szsz, two0, rtol=0, atol=1e-6)
     np.testing.assert_allclose(np.diag(szsz), 0.25)
+
+
+def test_hellmann_feynman_dE_dJ2_from_expectation(ctx):
+    """dE/dJ2 of the J1-J2 model on a 4x4 cylinder, by Hellmann-Feynman: the
+    expectation value of the J2 part of H (its own AutoMPO) in the DMRG ground
+    state, against the same expectation in the exact ground state (ED, Sz=0)
+    and against a central finite difference of ED energies."""
+    import tt_b200
+    Nx, Ny, J2 = 4, 4, 0.5
+    N = Nx * Ny
+    bonds = list(am.square_next_neighbor(Nx, Ny, True))
+
+    def part(kind, coef):
+        t = []
+        for s1, s2, typ, *_ in bonds:
+            if typ == kind:
+                i, j = s1 - 1, s2 - 1
+                t += [(0.5 * coef, ((i, "S+"), (j, "S-"))), (0.5 * coef, ((i, "S-"), (j, "S+"))),
+                      (coef, ((i, "Sz"), (j, "Sz")))]
+        return t
+
+    def mpo(terms):
+        a = tt_b200.AutoMPO()
+        for coef, ops in terms:
+            args = [coef]
+            for i, op in ops:
+                args += [op, i]
+            a.add(*args)
+        return tt_b200.QMPO.from_autompo(a, N)
+
+    h1, h2 = part(1, 1.0), part(2, 1.0)
+    psi = tt_b200.QMPS(N, qdmrg.neel(N))
+    e = tt_b200.QDMRG(psi, mpo(h1 + part(2, J2))).run(8, [32, 64, 128, 256, 256, 256, 256, 256], [1e-12], [6])
+    dE = psi.expectation(mpo(h2)) / psi.overlap()
+    E0, v0 = _ed_ground_state(N, h1 + part(2, J2), N // 2)
+    full_h2 = ed.terms_hamiltonian(N, h2)
+    exact = float(v0 @ (full_h2 @ v0))
+    assert abs(e - E0) <= 1e-8 * abs(E0)
+    # first order in the state's error (truncation at cutoff 1e-12): ~1e-5 relative
+    assert abs(dE - exact) <= 2e-5
+    step = 1e-4
+    fd = (ed.terms_ground_energy(N, h1 + part(2, J2 + step), N // 2) -
+          ed.terms_ground_energy(N, h1 + part(2, J2 - step), N // 2)) / (2 * step)
+    assert abs(dE - fd) <= 2e-5

@@ -79,3 +79,38 @@ def test_contract_matches_dense():
     assert [ix.name for ix in C.idx] == ["a", "s", "t", "c"]
     ref = np.tensordot(to_dense(T1), to_dense(T2), axes=([2], [0]))
     np.testing.assert_allclose(to_dense(C), ref, rtol=0, atol=1e-13)
+
+
+def test_qdmrg_on_autompo_xxz_chain_matches_ed():
+    """U(1) oracle DMRG on an AutoMPO-built XXZ chain (anisotropy, site fields)."""
+    from oracle import autompo as am
+    L, delta = 10, 0.7
+    h = np.random.default_rng(8).uniform(-0.1, 0.1, L)
+    a = am.AutoMPO()
+    for i in range(L - 1):
+        a.add(0.5, "S+", i, "S-", i + 1)
+        a.add(0.5, "S-", i, "S+", i + 1)
+        a.add(delta, "Sz", i, "Sz", i + 1)
+    for i in range(L):
+        a.add(float(h[i]), "Sz", i)
+    psi = qdmrg.QMPS(L, qdmrg.neel(L))
+    E = qdmrg.dmrg(psi, am.build_qmpo(a, L), 8, [8, 16, 32, 32, 32, 32, 32, 32], [1e-12], [6])
+    Eed = ed.terms_ground_energy(L, a.terms(), L // 2)
+    assert abs(E - Eed) < 1e-10 * abs(Eed)
+
+
+def test_ddmrg_on_autompo_tfi_cylinder_matches_ed():
+    """Dense oracle DMRG on an AutoMPO-built transverse-field Ising 2x4 cylinder."""
+    from oracle import autompo as am
+    Nx, Ny, g = 2, 4, 3.0
+    N = Nx * Ny
+    a = am.AutoMPO()
+    for s1, s2, *_ in am.square_lattice(Nx, Ny, True):
+        a.add(-4.0, "Sz", s1 - 1, "Sz", s2 - 1)
+    for i in range(N):
+        a.add(-2.0 * g, "Sx", i)
+    state = list(np.random.default_rng(4).integers(0, 2, N))
+    psi = ddmrg.DMPS(N, state)
+    E = ddmrg.ddmrg(psi, am.build_dmpo(a, N), 6, [8, 16, 16, 16, 16, 16], [1e-12], [4])
+    Eed = ed.terms_ground_energy(N, a.terms())
+    assert abs(E - Eed) < 1e-9 * abs(Eed)

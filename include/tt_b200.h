@@ -80,6 +80,21 @@ int tt_ctx_stream(tt_ctx* ctx, void** stream);
 /* Host wall seconds spent blocked in synchronisations of this context's
  * stream (device-to-host reads, tt_ctx_synchronize) and how many there were. */
 int tt_ctx_wait_stats(tt_ctx* ctx, double* seconds, int64_t* count);
+/* Sticky device status of the context: TT_OK, or TT_ERR_TIMEOUT once a bounded
+ * wait inside a tensor-core contraction has given up (that contraction's output
+ * is incomplete).  Every synchronisation of the context -- tt_ctx_synchronize
+ * and tt_memcpy_d2h, hence every Davidson call and block SVD -- returns
+ * TT_ERR_TIMEOUT while it is set, so a run with skipped tiles cannot report a
+ * result.  tt_ctx_device_status synchronises and reads it;
+ * tt_ctx_clear_device_status synchronises and resets it.  No counterpart in the
+ * reference (which has no device waits). */
+int tt_ctx_device_status(tt_ctx* ctx, int* status);
+int tt_ctx_clear_device_status(tt_ctx* ctx);
+/* Test hook: polls of the main-loop mbarrier waits of the tensor-core kernels
+ * launched from now on before they give up (default 2^26; polls < 0 restores
+ * it, 0 makes the first wait give up).  The drain that lets issued copies and
+ * MMAs land before shared and tensor memory are released keeps the default. */
+int tt_ctx_set_wait_limit(tt_ctx* ctx, int64_t polls);
 const char* tt_get_last_error(void);
 
 int tt_device_alloc(tt_ctx* ctx, size_t bytes, void** dptr);
@@ -172,7 +187,9 @@ int tt_vec_multidot(tt_ctx* ctx, int64_t n, int nvec, const double* const* xs,
  * it holds until the process exits, so nvec is limited to 1..16 (larger is
  * rejected with TT_ERR_INVALID); n is not limited.  The first call on a device
  * looks up that array's device address (cudaGetSymbolAddress) and should come
- * before any stream capture.  All calls share the array: calls that overlap
+ * before any stream capture; only a successful look-up is kept, so a first
+ * call that fails (an earlier asynchronous error still pending, say) is retried
+ * by the next call.  All calls share the array: calls that overlap
  * on the GPU (different streams, or host threads without ordering) race. */
 int tt_vec_multidot_noalloc(void* stream, int64_t n, int nvec, const double* const* xs,
                             const double* y, double* d_out);
@@ -272,7 +289,7 @@ typedef struct {
 int tt_sym_eig_batched(tt_ctx* ctx, const tt_eig_problem* probs, int n_probs,
                        double* G, double* Z, double* w, const double* A);
 
-/* Two-phase eigensolver used by the block SVD (n <= 2048 per problem).
+/* Two-phase eigensolver used by the block SVD (n <= 4096 and nvec <= 2048 per problem).
  * Phase 1: Householder tridiagonalisation of each G_p in place (reflectors
  * below the subdiagonal), d/e/tau of T_p in T[3*w_off .. 3*w_off + 3n), and
  * every eigenvalue in DESCENDING order in w[w_off ..] (bisection).  Phase 2:

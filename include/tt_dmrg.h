@@ -185,6 +185,13 @@ int tt_qdmrg_create(tt_qmps* psi, tt_qmpo* H, tt_qdmrg** out);
 int tt_qdmrg_set_noise(tt_qdmrg* run, double noise);
 int tt_qdmrg_sweep(tt_qdmrg* run, int max_bd, double cutoff, int max_restart, double* energy);
 int tt_qdmrg_finish(tt_qdmrg* run);                          /* psi.position(0) */
+/* Two-site updates (the sweep's step: updateSite + updateEnv,
+ * algos/dmrg/dmrg.cpp:300-372,491-509) moving the orthogonality centre from
+ * its current site to to_site: left to right when to_site is larger, right to
+ * left when smaller.  A sweep needs the centre at site 0 (where
+ * tt_qdmrg_create and every sweep leave it).  *energy: the last step's. */
+int tt_qdmrg_walk(tt_qdmrg* run, int to_site, int max_bd, double cutoff, int max_restart, double* energy);
+int tt_qdmrg_position(const tt_qdmrg* run, int* site);
 int tt_qdmrg_destroy(tt_qdmrg* run);
 /* whole schedule overload dmrg(psi, H, nsweeps, maxm[], cutoff[], max_restart[]);
  * log_out (may be NULL) receives the run record (destroy with tt_qdmrg_destroy) */
@@ -265,6 +272,11 @@ int tt_dmpo_from_autompo(const tt_autompo* a, int N, unsigned id, tt_dmpo** out)
 int tt_dmpo_tensor(const tt_dmpo* H, int i, int64_t* dims, double* data, int64_t cap);
 
 enum { TT_LATTICE_SQUARE = 0, TT_LATTICE_SQUARE_NEXT_NEIGHBOR = 1, TT_LATTICE_TRIANGULAR = 2 };
+/* OR'd into a square kind: snake site order (column x runs y = 1..Ny when x is
+ * odd, Ny..1 when x is even); the reference numbers sites column by column
+ * only (models/lattice/square.h:25-103), so this is a relabelling of the same
+ * bonds with the smaller site first */
+enum { TT_LATTICE_SNAKE = 0x100 };
 /* 1-based sites, y fastest; type 0 unset, 1 nearest, 2 next-nearest neighbour;
  * coordinates are 0 where the reference records none (triangular) */
 typedef struct {

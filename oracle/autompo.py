@@ -107,6 +107,25 @@ def square_next_neighbor(Nx: int, Ny: int, yperiodic: bool = False):
     return out
 
 
+def snake_relabel(bonds, Nx: int, Ny: int):
+    """Bonds of a column-major square lattice (site n = (x-1) Ny + y, the
+    reference's numbering, models/lattice/square.h:25-103) relabelled to snake
+    order: column x runs y = 1..Ny when x is odd and Ny..1 when x is even.
+    Coordinates and types are kept; the smaller site comes first.  The
+    reference has no snake order; the configuration of the J1-J2 cylinder
+    asks for it."""
+    def snake(n):
+        x, y = (n - 1) // Ny + 1, (n - 1) % Ny + 1
+        return (x - 1) * Ny + (y if x % 2 == 1 else Ny + 1 - y)
+    out = []
+    for s1, s2, t, x1, y1, x2, y2 in bonds:
+        a, b = snake(s1), snake(s2)
+        if a > b:
+            a, b, x1, y1, x2, y2 = b, a, x2, y2, x1, y1
+        out.append((a, b, t, x1, y1, x2, y2))
+    return out
+
+
 def triangular_lattice(Nx: int, Ny: int, yperiodic: bool = True):
     yperiodic = yperiodic and Ny > 2
     N = Nx * Ny

@@ -467,6 +467,19 @@ int tt_qdmrg_sweep(tt_qdmrg* run, int max_bd, double cutoff, int max_restart, do
   });
 }
 
+int tt_qdmrg_walk(tt_qdmrg* run, int to_site, int max_bd, double cutoff, int max_restart, double* energy) {
+  TT_ARG(run && max_restart >= 1 && to_site >= 0 && to_site < (int)run->H->H.length);
+  TT_GUARD({
+    double e = ttb::dmrg_walk(run->psi->psi, run->H->H, run->st, to_site, max_bd, cutoff, max_restart, &run->log);
+    if (energy) *energy = e;
+  });
+}
+
+int tt_qdmrg_position(const tt_qdmrg* run, int* site) {
+  TT_ARG(run && site);
+  TT_GUARD(*site = run->st.pos);
+}
+
 int tt_qdmrg_finish(tt_qdmrg* run) {
   TT_ARG(run);
   TT_GUARD(ttb::dmrg_finish(run->psi->psi));
@@ -746,6 +759,10 @@ int tt_lattice(int kind, int Nx, int Ny, int yperiodic, tt_lattice_bond* bonds, 
   TT_ARG(Nx >= 1 && Ny >= 1 && n_bonds && cap >= 0 && (bonds || cap == 0));
   TT_GUARD({
     std::vector<ttb::LatticeBond> g;
+    const bool snake = (kind & TT_LATTICE_SNAKE) != 0;
+    kind &= ~TT_LATTICE_SNAKE;
+    if (snake && kind == TT_LATTICE_TRIANGULAR)
+      throw std::runtime_error("tt_lattice: snake order needs a square lattice");
     if (kind == TT_LATTICE_SQUARE)
       g = ttb::square_lattice(Nx, Ny, yperiodic != 0);
     else if (kind == TT_LATTICE_SQUARE_NEXT_NEIGHBOR)
@@ -754,6 +771,7 @@ int tt_lattice(int kind, int Nx, int Ny, int yperiodic, tt_lattice_bond* bonds, 
       g = ttb::triangular_lattice(Nx, Ny, yperiodic != 0);
     else
       throw std::runtime_error("tt_lattice: unknown lattice kind");
+    if (snake) ttb::snake_relabel(g, Nx, Ny);
     *n_bonds = (int)g.size();
     for (int j = 0; j < (int)g.size() && j < cap; ++j)
       bonds[j] = tt_lattice_bond{g[j].s1, g[j].s2, g[j].type, g[j].x1, g[j].y1, g[j].x2, g[j].y2};

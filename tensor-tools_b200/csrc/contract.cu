@@ -275,8 +275,8 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t addr, uint32_t parity) {
 }
 
 // bounded wait for the phase with the given parity; false on timeout
-__device__ __forceinline__ bool mbar_wait_bounded(uint32_t addr, uint32_t parity) {
-  for (uint32_t it = 0; it < TC_WAIT_LIMIT; ++it)
+__device__ __forceinline__ bool mbar_wait_bounded(uint32_t addr, uint32_t parity, uint32_t limit = TC_WAIT_LIMIT) {
+  for (uint32_t it = 0; it < limit; ++it)
     if (mbar_try_wait(addr, parity)) return true;
   return false;
 }
@@ -379,7 +379,8 @@ template <bool SPLIT>
 __global__ void __launch_bounds__(TC_P_THREADS, 1)
 grouped_tc_persist(const TaskDev* __restrict__ tasks, int n_tasks, const OutDev* __restrict__ outs,
                    const PairTC* __restrict__ pairs, const uint8_t* __restrict__ packA,
-                   const uint8_t* __restrict__ packB, double* __restrict__ C, double alpha, int* __restrict__ status) {
+                   const uint8_t* __restrict__ packB, double* __restrict__ C, double alpha, int* __restrict__ status,
+                   int* __restrict__ ctx_status, uint32_t wait_limit) {
   extern __shared__ uint8_t tc_smem_raw[];
   __shared__ __align__(8) uint64_t full_bar[TC_RING], empty_bar[TC_RING], accf_bar[2], acce_bar[2];
   __shared__ uint32_t tmem_slot;
@@ -426,7 +427,8 @@ grouped_tc_persist(const TaskDev* __restrict__ tasks, int n_tasks, const OutDev*
           const PairTC q = pairs[p];
           for (int kt = 0; kt < q.kt; ++kt, ++g) {
             const int s = g % TC_RING;
-            if (g >= TC_RING && !mbar_wait_bounded(smem_u32(&empty_bar[s]), (uint32_t)((g / TC_RING - 1) & 1))) {
+            if (g >= TC_RING &&
+                !mbar_wait_bounded(smem_u32(&empty_bar[s]), (uint32_t)((g / TC_RING - 1) & 1), wait_limit)) {
               flag = 1;
               break;
             }
@@ -448,7 +450,7 @@ grouped_tc_persist(const TaskDev* __restrict__ tasks, int n_tasks, const OutDev*
         int nch = 0;
         for (int p = task.p_begin; p < task.p_end; ++p) nch += pairs[p].kt;
         const int b = i & 1;
-        if (i >= 2 && !mbar_wait_bounded(smem_u32(&acce_bar[b]), (uint32_t)(((i >> 1) - 1) & 1))) {
+        if (i >= 2 && !mbar_wait_bounded(smem_u32(&acce_bar[b]), (uint32_t)(((i >> 1) - 1) & 1), wait_limit)) {
           flag = 1;
           break;
         }
@@ -456,7 +458,7 @@ grouped_tc_persist(const TaskDev* __restrict__ tasks, int n_tasks, const OutDev*
         const uint32_t acc_tm = tmem + (uint32_t)(b * TC_BN);
         for (int c = 0; c < nch; ++c, ++g) {
           const int s = g % TC_RING;
-          if (!mbar_wait_bounded(smem_u32(&full_bar[s]), (uint32_t)((g / TC_RING) & 1))) {
+          if (!mbar_wait_bounded(smem_u32(&full_bar[s]), (uint32_t)((g / TC_RING) & 1), wait_limit)) {
             flag = 1;
             break;
           }
@@ -495,7 +497,7 @@ grouped_tc_persist(const TaskDev* __restrict__ tasks, int n_tasks, const OutDev*
       int nch = 0;
       for (int p = task.p_begin; p < task.p_end; ++p) nch += pairs[p].kt;
       const int b = i & 1;
-      const bool ok = mbar_wait_bounded(smem_u32(&accf_bar[b]), (uint32_t)((i >> 1) & 1));
+      const bool ok = mbar_wait_bounded(smem_u32(&accf_bar[b]), (uint32_t)((i >> 1) & 1), wait_limit);
       if (!__all_sync(0xffffffffu, ok)) {
         if (lane == 0) flag = 1;
         break;
@@ -539,6 +541,7 @@ grouped_tc_persist(const TaskDev* __restrict__ tasks, int n_tasks, const OutDev*
       mbar_wait_bounded(smem_u32(&accf_bar[il & 1]), (uint32_t)((il >> 1) & 1));
     }
     atomicExch(status, TT_ERR_TIMEOUT);
+    atomicExch_system(ctx_status, TT_ERR_TIMEOUT);  // the context's mapped status word
   }
   tc_fence_before();
   __syncthreads();
@@ -854,15 +857,14 @@ int tt_contract_exec(tt_ctx* ctx, const tt_plan* plan, const double* A, const do
                      double* C, double alpha) {
   TT_REQUIRE(ctx && plan, "tt_contract_exec: null argument");
   if (plan->n_tasks == 0) return TT_OK;
-  static thread_local bool attr_set = false;  // per host thread: each may drive its own device
-  if (!attr_set) {
+  static thread_local uint64_t attr_set = 0;  // per host thread and device
+  if (tt::first_on_device(attr_set, ctx->device)) {
     TT_CUDA(cudaFuncSetAttribute(grouped_dgemm, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)SMEM_BYTES));
     TT_CUDA(cudaFuncSetAttribute(grouped_tc_persist<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)TC_BULK_SMEM));
     TT_CUDA(cudaFuncSetAttribute(grouped_tc_persist<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)TC_BULK_SMEM));
-    attr_set = true;
   }
   if (plan->precision == TT_PREC_FP64) {
     grouped_dgemm<<<plan->n_tasks, THREADS, SMEM_BYTES, ctx->stream>>>(
@@ -892,10 +894,12 @@ int tt_contract_exec(tt_ctx* ctx, const tt_plan* plan, const double* A, const do
   const unsigned grid = (unsigned)std::min(plan->n_tasks, std::max(1, ctx->num_sms));
   if (split)
     grouped_tc_persist<true><<<grid, TC_P_THREADS, TC_BULK_SMEM, ctx->stream>>>(
-        plan->d_tasks, plan->n_tasks, plan->d_outs, plan->d_pairtc, pa, pb, C, alpha, plan->d_status);
+        plan->d_tasks, plan->n_tasks, plan->d_outs, plan->d_pairtc, pa, pb, C, alpha, plan->d_status,
+        ctx->d_dev_status, ctx->wait_limit);
   else
     grouped_tc_persist<false><<<grid, TC_P_THREADS, TC_BULK_SMEM, ctx->stream>>>(
-        plan->d_tasks, plan->n_tasks, plan->d_outs, plan->d_pairtc, pa, pb, C, alpha, plan->d_status);
+        plan->d_tasks, plan->n_tasks, plan->d_outs, plan->d_pairtc, pa, pb, C, alpha, plan->d_status,
+        ctx->d_dev_status, ctx->wait_limit);
   cudaError_t le = cudaGetLastError();
   tt::pool_free(ctx, pa);
   tt::pool_free(ctx, pb);

@@ -38,6 +38,14 @@ double* partials(tt_ctx* ctx, int n) {
   return ctx->d_partials;
 }
 
+int device_status(tt_ctx* ctx) {
+  if (ctx->h_dev_status && *(volatile int*)ctx->h_dev_status != TT_OK)
+    return fail(TT_ERR_TIMEOUT,
+                "a bounded wait of a tensor-core contraction gave up: its output is incomplete "
+                "(tt_ctx_clear_device_status resets the context's status)");
+  return TT_OK;
+}
+
 cudaError_t h2d_async(tt_ctx* ctx, void* dst, const void* src, size_t bytes) {
   if (bytes == 0) return cudaSuccess;
   const size_t need = (bytes + 255) & ~(size_t)255;
@@ -92,6 +100,9 @@ int tt_ctx_create(int device, tt_ctx** out) {
   uint64_t thresh = UINT64_MAX;  // keep freed blocks cached in the pool
   TT_CUDA(cudaMemPoolSetAttribute(ctx->pool, cudaMemPoolAttrReleaseThreshold, &thresh));
   TT_CUDA(cudaMallocHost(&ctx->h_scalars, kBounceBytes));
+  TT_CUDA(cudaHostAlloc((void**)&ctx->h_dev_status, sizeof(int), cudaHostAllocMapped));
+  *ctx->h_dev_status = TT_OK;
+  TT_CUDA(cudaHostGetDevicePointer((void**)&ctx->d_dev_status, ctx->h_dev_status, 0));
   ctx->stage_cap = (size_t)64 << 20;
   TT_CUDA(cudaMallocHost(&ctx->stage, ctx->stage_cap));
   if (!tt::partials(ctx, 16 * 4 * ctx->num_sms + 64) ||
@@ -113,6 +124,7 @@ int tt_ctx_destroy(tt_ctx* ctx) {
   if (ctx->d_partials) cudaFree(ctx->d_partials);
   if (ctx->d_ticket) cudaFree(ctx->d_ticket);
   if (ctx->h_scalars) cudaFreeHost(ctx->h_scalars);
+  if (ctx->h_dev_status) cudaFreeHost(ctx->h_dev_status);
   if (ctx->stage) cudaFreeHost(ctx->stage);
   cudaStreamDestroy(ctx->stream);
   delete ctx;
@@ -123,6 +135,27 @@ int tt_ctx_destroy(tt_ctx* ctx) {
 int tt_ctx_synchronize(tt_ctx* ctx) {
   TT_REQUIRE(ctx, "null context");
   TT_CUDA(timed_sync(ctx));
+  return tt::device_status(ctx);
+}
+
+int tt_ctx_device_status(tt_ctx* ctx, int* status) {
+  TT_REQUIRE(ctx && status, "null argument");
+  TT_CUDA(timed_sync(ctx));
+  *status = *(volatile int*)ctx->h_dev_status;
+  return TT_OK;
+}
+
+int tt_ctx_clear_device_status(tt_ctx* ctx) {
+  TT_REQUIRE(ctx, "null context");
+  TT_CUDA(timed_sync(ctx));
+  *(volatile int*)ctx->h_dev_status = TT_OK;
+  return TT_OK;
+}
+
+int tt_ctx_set_wait_limit(tt_ctx* ctx, int64_t polls) {
+  TT_REQUIRE(ctx, "null context");
+  TT_REQUIRE(polls < ((int64_t)1 << 32), "tt_ctx_set_wait_limit: polls out of range");
+  ctx->wait_limit = polls < 0 ? (1u << 26) : (uint32_t)polls;
   return TT_OK;
 }
 
@@ -207,7 +240,7 @@ int tt_memcpy_d2h(tt_ctx* ctx, void* dst, const void* src, size_t bytes) {
     TT_CUDA(cudaMemcpyAsync(ctx->h_scalars, src, bytes, cudaMemcpyDeviceToHost, ctx->stream));
     TT_CUDA(timed_sync(ctx));
     std::memcpy(dst, ctx->h_scalars, bytes);
-    return TT_OK;
+    return tt::device_status(ctx);
   }
   auto t0 = std::chrono::steady_clock::now();
   cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, ctx->stream);  // blocks if pageable
@@ -215,7 +248,7 @@ int tt_memcpy_d2h(tt_ctx* ctx, void* dst, const void* src, size_t bytes) {
   ctx->wait_seconds += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
   ctx->waits++;
   TT_CUDA(e);
-  return TT_OK;
+  return tt::device_status(ctx);
 }
 
 int tt_memcpy_d2d(tt_ctx* ctx, void* dst, const void* src, size_t bytes) {

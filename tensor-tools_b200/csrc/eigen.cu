@@ -249,11 +249,9 @@ int tt_sym_eig_batched(tt_ctx* ctx, const tt_eig_problem* probs, int n_probs, do
   TT_CUDA(cudaMemcpyAsync(dp, hp.data(), sizeof(EigDev) * n_probs, cudaMemcpyHostToDevice, ctx->stream));
   TT_CUDA(cudaMemsetAsync(dstatus, 0, sizeof(int), ctx->stream));
   const size_t smem = sizeof(double) * 2 * SMEM_N * SMEM_N;
-  static thread_local bool attr = false;  // per host thread: each may drive its own device
-  if (!attr) {
+  static thread_local uint64_t attr = 0;  // per host thread and device
+  if (tt::first_on_device(attr, ctx->device))
     TT_CUDA(cudaFuncSetAttribute(jacobi_eig, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    attr = true;
-  }
   jacobi_eig<<<n_probs, ET, smem, ctx->stream>>>(dp, G, Z, w, A, dstatus);
   TT_LAUNCH_CHECK(ctx);
   int hstatus = 0;

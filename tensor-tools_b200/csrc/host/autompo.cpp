@@ -120,6 +120,30 @@ std::vector<LatticeBond> square_next_neighbor(int Nx, int Ny, bool yperiodic) {
   return g;
 }
 
+// Snake (boustrophedon) site order on an Nx x Ny lattice: column x runs
+// y = 1..Ny when x is odd and y = Ny..1 when x is even, so consecutive sites
+// along the chain are always lattice neighbours.  The reference numbers
+// sites column by column (n = (x-1) Ny + y); this relabels a bond list built
+// in that order, keeping every bond's coordinates and type and putting the
+// smaller site first.
+void snake_relabel(std::vector<LatticeBond>& g, int Nx, int Ny) {
+  auto snake = [&](int n) {
+    const int x = (n - 1) / Ny + 1, y = (n - 1) % Ny + 1;
+    return (x - 1) * Ny + ((x & 1) ? y : Ny + 1 - y);
+  };
+  (void)Nx;
+  for (LatticeBond& b : g) {
+    int a = snake(b.s1), c = snake(b.s2);
+    if (a > c) {
+      std::swap(a, c);
+      std::swap(b.x1, b.x2);
+      std::swap(b.y1, b.y2);
+    }
+    b.s1 = a;
+    b.s2 = c;
+  }
+}
+
 std::vector<LatticeBond> triangular_lattice(int Nx, int Ny, bool yperiodic) {
   // models/lattice/triangular.h:25-64 (no coordinates recorded)
   yperiodic = yperiodic && Ny > 2;

@@ -106,6 +106,8 @@ struct LatticeBond {
 std::vector<LatticeBond> square_lattice(int Nx, int Ny, bool yperiodic);
 std::vector<LatticeBond> square_next_neighbor(int Nx, int Ny, bool yperiodic);
 std::vector<LatticeBond> triangular_lattice(int Nx, int Ny, bool yperiodic);
+// snake site order (column x runs upward when odd, downward when even)
+void snake_relabel(std::vector<LatticeBond>& g, int Nx, int Ny);
 
 // Charge carried by a spin-1/2 operator in units of 2Sz (models/sites/spinhalf.cpp:95-106).
 int spin_half_div(const std::string& op);

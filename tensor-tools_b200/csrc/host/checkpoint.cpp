@@ -29,6 +29,12 @@ struct RawFile {
   ~RawFile() {
     if (f) std::fclose(f);
   }
+  void close(const std::string& path) {
+    const bool bad = std::ferror(f) != 0;
+    const int rc = std::fclose(f);
+    f = nullptr;
+    if (bad || rc != 0) throw std::runtime_error("checkpoint: cannot write " + path);
+  }
   void write(const double* p, size_t n) {
     if (n && std::fwrite(p, sizeof(double), n, f) != n) throw std::runtime_error("checkpoint: short write");
   }
@@ -47,6 +53,30 @@ std::vector<double> download(const double* dev, int64_t n) {
 void upload(double* dev, const std::vector<double>& h) {
   if (!h.empty()) check(tt_memcpy_h2d(rt().ctx, dev, h.data(), sizeof(double) * h.size()), "checkpoint upload");
   check(tt_ctx_synchronize(rt().ctx), "checkpoint sync");
+}
+
+// A save writes both files under temporary names and renames each into place,
+// the raw block file first and the metadata last: a crash or a full disk
+// during a save leaves the previous checkpoint whole.
+void commit_file(const std::string& tmp, const std::string& path) {
+  if (std::rename(tmp.c_str(), path.c_str()) != 0) throw std::runtime_error("checkpoint: cannot rename " + tmp);
+}
+
+void write_meta(const std::string& fn, const std::string& meta) {
+  const std::string path = fn + ".ttmps", tmp = path + ".tmp";
+  {
+    std::ofstream out(tmp);
+    out << meta;
+    out.flush();
+    if (!out) throw std::runtime_error("checkpoint: cannot write " + tmp);
+  }
+  commit_file(tmp, path);
+}
+
+// the raw file named in the metadata: a relative name is taken under
+// data_prefix, an absolute one as it stands
+std::string raw_path(const std::string& data_prefix, const std::string& wfn) {
+  return !wfn.empty() && wfn[0] == '/' ? wfn : data_prefix + wfn;
 }
 
 std::string expect(std::istream& in, const char* key) {
@@ -73,7 +103,7 @@ void save(const qMPS& psi, const std::string& fn, const std::string& wfn_in) {
   meta << "\nbond_dims " << psi.bond_dims.size();
   for (auto d : psi.bond_dims) meta << " " << d;
   meta << "\n";
-  RawFile raw(wfn, "wb");
+  RawFile raw(wfn + ".tmp", "wb");
   int64_t offset = 0;
   for (unsigned i = 0; i < psi.length; ++i) {
     const qtensor& T = psi.A[i];
@@ -94,9 +124,9 @@ void save(const qMPS& psi, const std::string& fn, const std::string& wfn_in) {
       offset += b.size * (int64_t)sizeof(double);
     }
   }
-  std::ofstream out(fn + ".ttmps");
-  out << meta.str();
-  if (!out) throw std::runtime_error("checkpoint: cannot write " + fn + ".ttmps");
+  raw.close(wfn + ".tmp");
+  commit_file(wfn + ".tmp", wfn);
+  write_meta(fn, meta.str());
 }
 
 qMPS load_qmps(const std::string& fn, const std::string& data_prefix) {
@@ -132,7 +162,7 @@ qMPS load_qmps(const std::string& fn, const std::string& data_prefix) {
   for (auto& d : psi.bond_dims) in >> d;
   if (!in || psi.length < 2 || psi.bond_dims.size() != psi.length + 1 || phy_dim != psi.phy_qn.size())
     throw std::runtime_error("checkpoint: bad qMPS header in " + fn);
-  RawFile raw(data_prefix + wfn, "rb");
+  RawFile raw(raw_path(data_prefix, wfn), "rb");
   for (unsigned i = 0; i < psi.length; ++i) {
     unsigned ti = 0, rank = 0;
     size_t nb = 0;
@@ -201,7 +231,7 @@ void save(const MPS& psi, const std::string& fn, const std::string& wfn_in) {
   meta << "bond_dims " << psi.bond_dims.size();
   for (auto d : psi.bond_dims) meta << " " << d;
   meta << "\n";
-  RawFile raw(wfn, "wb");
+  RawFile raw(wfn + ".tmp", "wb");
   int64_t offset = 0;
   for (unsigned i = 0; i < psi.length; ++i) {
     const dtensor& T = psi.A[i];
@@ -214,9 +244,9 @@ void save(const MPS& psi, const std::string& fn, const std::string& wfn_in) {
     raw.write(h.data(), h.size());
     offset += T.size * (int64_t)sizeof(double);
   }
-  std::ofstream out(fn + ".ttmps");
-  out << meta.str();
-  if (!out) throw std::runtime_error("checkpoint: cannot write " + fn + ".ttmps");
+  raw.close(wfn + ".tmp");
+  commit_file(wfn + ".tmp", wfn);
+  write_meta(fn, meta.str());
 }
 
 MPS load_mps(const std::string& fn, const std::string& data_prefix) {
@@ -245,7 +275,7 @@ MPS load_mps(const std::string& fn, const std::string& data_prefix) {
   for (auto& d : psi.bond_dims) in >> d;
   if (!in || psi.length < 2 || psi.bond_dims.size() != psi.length + 1)
     throw std::runtime_error("checkpoint: bad MPS header in " + fn);
-  RawFile raw(data_prefix + wfn, "rb");
+  RawFile raw(raw_path(data_prefix, wfn), "rb");
   for (unsigned i = 0; i < psi.length; ++i) {
     unsigned ti = 0, rank = 0;
     int64_t off = 0;

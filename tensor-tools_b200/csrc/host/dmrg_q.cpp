@@ -1032,9 +1032,31 @@ void dmrg_prepare(qMPS& psi, qMPO& H, DmrgState& st, DmrgLog* log) {
   if (log) log->initial_energy = e;
 }
 
+double dmrg_walk(qMPS& psi, qMPO& H, DmrgState& st, int to, int max_bd, double cutoff, int max_restart,
+                 DmrgLog* log) {
+  const int L = (int)H.length;
+  if (!st.envs_built) throw std::runtime_error("dmrg_walk: environments not built");
+  if (to < 0 || to >= L) throw std::runtime_error("dmrg_walk: target site out of range");
+  double energy = 0.0;
+  while (st.pos != to) {
+    const int direction = to > st.pos ? MoveFromLeft : MoveFromRight;
+    const unsigned site = (unsigned)st.pos;
+    updateSite(psi, H, st.TR, st.TL, site, energy, direction, max_bd, cutoff, 'S', 3, max_restart, log, st.noise);
+    auto te0 = std::chrono::steady_clock::now();
+    updateEnv(psi, H, st.TR, st.TL, site, direction);
+    if (log && !log->steps.empty()) {
+      if (rt().profile) check(tt_ctx_synchronize(ctx()), "sync");
+      log->steps.back().t_env = std::chrono::duration<double>(std::chrono::steady_clock::now() - te0).count();
+    }
+    st.pos += direction == MoveFromLeft ? 1 : -1;
+  }
+  return energy;
+}
+
 double dmrg_sweep(qMPS& psi, qMPO& H, DmrgState& st, int max_bd, double cutoff, int max_restart,
                   DmrgLog* log) {
   const unsigned L = H.length;
+  if (st.pos != 0) throw std::runtime_error("dmrg_sweep: the orthogonality centre must be at site 0");
   double energy = 0.0;
   auto t0 = std::chrono::steady_clock::now();
   for (int half = 0; half < 2; ++half) {

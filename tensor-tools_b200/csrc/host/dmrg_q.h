@@ -128,6 +128,7 @@ struct DmrgState {
   bool envs_built = false;
   int sweeps_done = 0;
   double noise = 0.0;  // density-matrix perturbation of the following sweeps (0: the reference's update)
+  int pos = 0;         // orthogonality centre between calls (0 after dmrg_prepare and after every sweep)
 };
 // One full sweep (L->R then R->L) of the schedule overload, starting from a
 // state prepared by dmrg_prepare (position(0), normalize, buildEnv).
@@ -135,5 +136,14 @@ void dmrg_prepare(qMPS& psi, qMPO& H, DmrgState& st, DmrgLog* log);
 double dmrg_sweep(qMPS& psi, qMPO& H, DmrgState& st, int max_bd, double cutoff, int max_restart,
                   DmrgLog* log);
 void dmrg_finish(qMPS& psi);
+// Two-site updates that move the orthogonality centre from st.pos to `to`:
+// left-to-right updates of sites pos .. to-1 when to > pos, right-to-left
+// updates of sites pos .. to+1 when to < pos, each followed by its
+// environment update -- the same step as inside a sweep.  A block of
+// mid-chain updates at a settled bond dimension (walk to the middle once,
+// then back and forth over a few bonds) is the unit the benchmark times.
+// Returns the last step's energy; st.pos becomes `to`.
+double dmrg_walk(qMPS& psi, qMPO& H, DmrgState& st, int to, int max_bd, double cutoff, int max_restart,
+                 DmrgLog* log);
 
 }  // namespace ttb

@@ -28,7 +28,7 @@ namespace {
 
 constexpr int TT = 512;          // threads per CTA
 constexpr int SM_N = 160;        // full n x n FP64 matrix in shared memory up to this size
-constexpr int MAX_N = 2048;
+constexpr int MAX_N = 4096;
 constexpr int INV_ITERS = 3;
 
 struct EigDev {
@@ -1047,7 +1047,7 @@ int tt_sym_eigvals_batched(tt_ctx* ctx, const tt_eig_problem* probs, int n_probs
   TT_REQUIRE(ctx && (n_probs == 0 || (probs && G && T && w)), "tt_sym_eigvals_batched: null argument");
   if (n_probs == 0) return TT_OK;
   for (int i = 0; i < n_probs; ++i) {
-    TT_REQUIRE(probs[i].n >= 0 && probs[i].n <= MAX_N, "tt_sym_eigvals_batched: n must be 0..2048");
+    TT_REQUIRE(probs[i].n >= 0 && probs[i].n <= MAX_N, "tt_sym_eigvals_batched: n must be 0..4096");
     if (probs[i].flags & TT_EIG_ROW_1X2)
       TT_REQUIRE(probs[i].n == 2 && A, "tt_sym_eigvals_batched: 1x2 case needs n == 2 and A");
   }
@@ -1060,11 +1060,9 @@ int tt_sym_eigvals_batched(tt_ctx* ctx, const tt_eig_problem* probs, int n_probs
   small.insert(small.end(), big.begin(), big.end());  // small problems first, then the cluster ones
   TT_CUDA(tt::h2d_async(ctx, dp, small.data(), sizeof(EigDev) * small.size()));
   const int n_small = (int)(small.size() - big.size());
-  static thread_local bool attr = false;  // per host thread: each may drive its own device
-  if (!attr) {
+  static thread_local uint64_t attr = 0;  // per host thread and device
+  if (tt::first_on_device(attr, ctx->device))
     TT_CUDA(cudaFuncSetAttribute(tridiag_eigvals, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)vals_smem()));
-    attr = true;
-  }
   if (n_small > 0) {
     tridiag_eigvals<<<n_small, TT, vals_smem(), ctx->stream>>>(dp, G, T, w, A);
     TT_LAUNCH_CHECK(ctx);
@@ -1091,9 +1089,9 @@ int tt_sym_eigvecs_batched(tt_ctx* ctx, const tt_eig_problem* probs, int n_probs
              "tt_sym_eigvecs_batched: null argument");
   if (n_probs == 0) return TT_OK;
   for (int i = 0; i < n_probs; ++i) {
-    TT_REQUIRE(probs[i].n >= 0 && probs[i].n <= MAX_N, "tt_sym_eigvecs_batched: n must be 0..2048");
+    TT_REQUIRE(probs[i].n >= 0 && probs[i].n <= MAX_N, "tt_sym_eigvecs_batched: n must be 0..4096");
     TT_REQUIRE(nvec[i] >= 0 && nvec[i] <= probs[i].n && nvec[i] <= MAX_N / 2,
-               "tt_sym_eigvecs_batched: nvec must be 0..min(n, 1024)");
+               "tt_sym_eigvecs_batched: nvec must be 0..min(n, 2048)");
     if (probs[i].flags & TT_EIG_ROW_1X2) TT_REQUIRE(A, "tt_sym_eigvecs_batched: 1x2 case needs A");
   }
   std::vector<EigDev> all = to_dev(probs, n_probs, nvec);
@@ -1114,12 +1112,10 @@ int tt_sym_eigvecs_batched(tt_ctx* ctx, const tt_eig_problem* probs, int n_probs
     if (with_u <= kVecsSmemCap) need = std::max(need, with_u);
     else if (z_only <= kVecsSmemCap) need = std::max(need, z_only);
   }
-  static thread_local bool attr = false;  // per host thread: each may drive its own device
-  if (!attr) {
+  static thread_local uint64_t attr = 0;  // per host thread and device
+  if (tt::first_on_device(attr, ctx->device))
     TT_CUDA(cudaFuncSetAttribute(tridiag_eigvecs, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)(sizeof(double) * kVecsSmemCap)));
-    attr = true;
-  }
   if (n_small > 0) {
     tridiag_eigvecs<<<n_small, TT, sizeof(double) * (size_t)need, ctx->stream>>>(dp, G, T, w, Z, work, A,
                                                                                   (int)need);

@@ -31,6 +31,14 @@ struct tt_ctx {
   // host wall time spent blocked in stream synchronisations, and their count
   double wait_seconds = 0.0;
   int64_t waits = 0;
+  // sticky status of the bounded device waits (mapped pinned memory, so a
+  // kernel that gives up writes TT_ERR_TIMEOUT straight into host memory);
+  // every synchronisation of the context checks it
+  int* h_dev_status = nullptr;
+  int* d_dev_status = nullptr;
+  // polls of the main-loop waits of the tensor-core kernels before they give
+  // up (tt_ctx_set_wait_limit lowers it to test the timeout path)
+  uint32_t wait_limit = 1u << 26;
 };
 
 namespace tt {
@@ -53,6 +61,20 @@ inline T* pool_alloc(tt_ctx* ctx, size_t n) {
 inline void pool_free(tt_ctx* ctx, void* p) {
   if (p) cudaFreeAsync(p, ctx->stream);
 }
+
+// Per-thread, per-device "done once" flags for cudaFuncSetAttribute, which
+// acts on the current device only: bit d of a thread_local mask.  Returns
+// true the first time it is called for (mask, device).
+inline bool first_on_device(uint64_t& mask, int device) {
+  const uint64_t bit = (uint64_t)1 << (device & 63);
+  if (mask & bit) return false;
+  mask |= bit;
+  return true;
+}
+
+// TT_ERR_TIMEOUT once a bounded device wait of this context has given up
+// (read after a synchronisation), else TT_OK.
+int device_status(tt_ctx* ctx);
 
 // Reduction scratch of at least n doubles (grown on demand).
 double* partials(tt_ctx* ctx, int n);

@@ -7,6 +7,7 @@
 // block order by the last block of the same launch.
 #include <algorithm>
 #include <cmath>
+#include <atomic>
 #include <mutex>
 #include <vector>
 
@@ -323,11 +324,14 @@ constexpr int NOALLOC_MAX_BLOCKS = 1024;     // partial sums per vector
 // 16 x 1024 doubles = 128 KiB; every GPU that loads the library holds it until exit.
 static __device__ __align__(256) double g_noalloc_partials[NOALLOC_MAX_VEC * NOALLOC_MAX_BLOCKS];
 
+// Per-device set-up, cached only once it has succeeded: a failed attempt (for
+// example a first call made while an earlier asynchronous error is pending,
+// or during stream capture) leaves the slot unset, and the next call retries.
 struct NoAllocDevice {
-  std::once_flag once;
+  std::mutex mu;
+  std::atomic<bool> ready{false};
   double* partials = nullptr;   // device address of g_noalloc_partials on this device
   int num_sms = 0;
-  cudaError_t status = cudaSuccess;
 };
 constexpr int NOALLOC_MAX_DEVICES = 64;
 NoAllocDevice g_noalloc_dev[NOALLOC_MAX_DEVICES];
@@ -350,13 +354,19 @@ int tt_vec_multidot_noalloc(void* stream, int64_t n, int nvec, const double* con
   NoAllocDevice& D = g_noalloc_dev[dev];
   // once per device, with that device current: the host needs the array's
   // device address (its host-side name is only a stand-in)
-  std::call_once(D.once, [&D, dev]() {
-    void* p = nullptr;
-    D.status = cudaGetSymbolAddress(&p, g_noalloc_partials);
-    if (D.status == cudaSuccess) D.status = cudaDeviceGetAttribute(&D.num_sms, cudaDevAttrMultiProcessorCount, dev);
-    if (D.status == cudaSuccess) D.partials = static_cast<double*>(p);
-  });
-  if (D.status != cudaSuccess) return tt::cuda_fail(D.status, "tt_vec_multidot_noalloc set-up", __FILE__, __LINE__);
+  if (!D.ready.load(std::memory_order_acquire)) {
+    std::lock_guard<std::mutex> lock(D.mu);
+    if (!D.ready.load(std::memory_order_relaxed)) {
+      void* p = nullptr;
+      int sms = 0;
+      cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_partials);
+      if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+      if (e != cudaSuccess) return tt::cuda_fail(e, "tt_vec_multidot_noalloc set-up", __FILE__, __LINE__);
+      D.partials = static_cast<double*>(p);
+      D.num_sms = sms;
+      D.ready.store(true, std::memory_order_release);
+    }
+  }
   PtrPack pk;
   for (int j = 0; j < nvec; ++j) {
     TT_REQUIRE(xs[j] && aligned16(xs[j]), "tt_vec_multidot_noalloc: vectors must be 16-byte aligned");

@@ -25,6 +25,7 @@ LIB_PATH = os.path.join(PKG, "lib", "libtt_b200.so")
 HEADERS = [os.path.join(ROOT, "include", "tt_b200.h"), os.path.join(ROOT, "include", "tt_dmrg.h")]
 
 TT_OK = 0
+TT_ERR_TIMEOUT = 4  # a bounded device wait gave up (include/tt_b200.h)
 MoveFromLeft, MoveFromRight = 0, 1
 Inward, Outward = 0, 1
 Link, Site = 0, 1
@@ -164,10 +165,15 @@ for _pre in ("tt_qmps", "tt_dmps"):
 _proto("tt_qmpo_destroy", P)
 _proto("tt_qmpo_tensor", P, C.c_int, PP)
 _proto("tt_qdmrg_create", P, P, PP)
+_proto("tt_ctx_device_status", P, C.POINTER(C.c_int))
+_proto("tt_ctx_clear_device_status", P)
+_proto("tt_ctx_set_wait_limit", P, I64)
 _proto("tt_vec_scale_mode", P, I64, C.c_int, I64, PD, P)
 _proto("tt_qdmrg_sweep", P, C.c_int, D, C.c_int, PD)
 _proto("tt_qdmrg_set_noise", P, D)
 _proto("tt_qdmrg_finish", P)
+_proto("tt_qdmrg_walk", P, C.c_int, C.c_int, D, C.c_int, PD)
+_proto("tt_qdmrg_position", P, C.POINTER(C.c_int))
 _proto("tt_qdmrg_destroy", P)
 _proto("tt_qdmrg_run", P, P, C.c_int, C.POINTER(C.c_int), C.c_int, PD, C.c_int, C.POINTER(C.c_int),
        C.c_int, PD, PP)
@@ -226,6 +232,19 @@ class Context:
         n = I64()
         _chk(lib.tt_ctx_launch_count(self.h, C.byref(n)), "launch count")
         return n.value
+
+    def device_status(self) -> int:
+        """TT_OK, or TT_ERR_TIMEOUT once a bounded tensor-core wait gave up (synchronises)."""
+        n = C.c_int()
+        _chk(lib.tt_ctx_device_status(self.h, C.byref(n)), "device status")
+        return n.value
+
+    def clear_device_status(self):
+        _chk(lib.tt_ctx_clear_device_status(self.h), "clear device status")
+
+    def set_wait_limit(self, polls: int):
+        """Test hook: polls of the tensor-core kernels' main-loop waits (< 0: the default)."""
+        _chk(lib.tt_ctx_set_wait_limit(self.h, polls), "set wait limit")
 
     def close(self):
         if self.h:
@@ -555,6 +574,19 @@ class QDMRG:
     def finish(self):
         _chk(lib.tt_qdmrg_finish(self.h), "finish")
 
+    def walk(self, to_site: int, max_bd: int, cutoff: float, max_restart: int, noise: float = 0.0) -> float:
+        """Two-site updates moving the orthogonality centre to to_site (0-based);
+        returns the last step's energy.  Sweeps need the centre back at 0."""
+        _chk(lib.tt_qdmrg_set_noise(self.h, noise), "set_noise")
+        e = D()
+        _chk(lib.tt_qdmrg_walk(self.h, to_site, max_bd, cutoff, max_restart, C.byref(e)), "walk")
+        return e.value
+
+    def position(self) -> int:
+        n = C.c_int()
+        _chk(lib.tt_qdmrg_position(self.h, C.byref(n)), "position")
+        return n.value
+
     def run(self, nsweeps, maxm, cutoff, max_restart, start_sweep: int = 0, noise=None) -> float:
         """Sweeps start_sweep .. nsweeps-1 of the schedule (maxm[s % len] ...),
         then the final position(0); start_sweep > 0 resumes a loaded checkpoint.
@@ -791,6 +823,7 @@ class LatticeBond(C.Structure):
 
 _proto("tt_lattice", C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(LatticeBond), C.c_int, C.POINTER(C.c_int))
 TT_LATTICE_SQUARE, TT_LATTICE_SQUARE_NEXT_NEIGHBOR, TT_LATTICE_TRIANGULAR = 0, 1, 2
+TT_LATTICE_SNAKE = 0x100
 
 
 def _lattice(kind, Nx, Ny, yperiodic):
@@ -801,14 +834,16 @@ def _lattice(kind, Nx, Ny, yperiodic):
     return [(b.s1, b.s2, b.type, b.x1, b.y1, b.x2, b.y2) for b in buf[:n.value]]
 
 
-def square_lattice(Nx: int, Ny: int, yperiodic: bool = False):
-    """squareLattice (models/lattice/square.h:25-58): (s1, s2, type, x1, y1, x2, y2), 1-based sites."""
-    return _lattice(TT_LATTICE_SQUARE, Nx, Ny, yperiodic)
+def square_lattice(Nx: int, Ny: int, yperiodic: bool = False, snake: bool = False):
+    """squareLattice (models/lattice/square.h:25-58): (s1, s2, type, x1, y1, x2, y2), 1-based sites.
+    snake=True numbers the sites in snake order (odd columns upward, even columns downward)."""
+    return _lattice(TT_LATTICE_SQUARE | (TT_LATTICE_SNAKE if snake else 0), Nx, Ny, yperiodic)
 
 
-def square_next_neighbor(Nx: int, Ny: int, yperiodic: bool = False):
-    """squareNextNeighbor (models/lattice/square.h:60-103); type 1 nearest, 2 next nearest."""
-    return _lattice(TT_LATTICE_SQUARE_NEXT_NEIGHBOR, Nx, Ny, yperiodic)
+def square_next_neighbor(Nx: int, Ny: int, yperiodic: bool = False, snake: bool = False):
+    """squareNextNeighbor (models/lattice/square.h:60-103); type 1 nearest, 2 next nearest.
+    snake=True numbers the sites in snake order (odd columns upward, even columns downward)."""
+    return _lattice(TT_LATTICE_SQUARE_NEXT_NEIGHBOR | (TT_LATTICE_SNAKE if snake else 0), Nx, Ny, yperiodic)
 
 
 def triangular_lattice(Nx: int, Ny: int, yperiodic: bool = True):

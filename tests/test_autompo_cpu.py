@@ -155,3 +155,42 @@ def test_capi_rejects_unsupported_terms():
     c.add(1.0, "Sz", 0, "Sz", 5)
     with pytest.raises(tt.TTError):
         c.link_dims(4, True)       # site out of range
+
+
+def test_snake_order_relabels_the_same_bonds():
+    """Snake order: the same bonds (types, coordinates) under the site map
+    n(x, y) = (x-1) Ny + (y if x odd else Ny+1-y); consecutive chain sites are
+    nearest neighbours; the C ABI's relabelling equals the oracle's; and the
+    J1-J2 spectrum does not depend on the order (term matrices are similar)."""
+    import tt_b200 as tt
+    for Nx, Ny, yp in [(6, 16, True), (16, 6, True), (3, 4, False), (4, 2, True)]:
+        col = am.square_next_neighbor(Nx, Ny, yp)
+        sn = am.snake_relabel(col, Nx, Ny)
+        ours = [tuple(b) for b in tt.square_next_neighbor(Nx, Ny, yp, snake=True)]
+        assert ours == [tuple(float(v) if k > 2 else v for k, v in enumerate(b)) for b in sn]
+        assert [tuple(b) for b in tt.square_lattice(Nx, Ny, yp, snake=True)] == \
+            [tuple(float(v) if k > 2 else v for k, v in enumerate(b))
+             for b in am.snake_relabel(am.square_lattice(Nx, Ny, yp), Nx, Ny)]
+        def snake(n):
+            x, y = (n - 1) // Ny + 1, (n - 1) % Ny + 1
+            return (x - 1) * Ny + (y if x % 2 == 1 else Ny + 1 - y)
+        assert sorted(snake(n) for n in range(1, Nx * Ny + 1)) == list(range(1, Nx * Ny + 1))
+        for (s1, s2, t, *_), (c1, c2, ct, *_) in zip(sn, col):
+            assert s1 < s2 and t == ct and {s1, s2} == {snake(c1), snake(c2)}
+        nn = {(s1, s2) for s1, s2, t, *_ in sn if t == 1}
+        assert all((n, n + 1) in nn for n in range(1, Nx * Ny)) or Ny == 1
+    with pytest.raises(RuntimeError):
+        tt._lattice(tt.TT_LATTICE_TRIANGULAR | tt.TT_LATTICE_SNAKE, 3, 4, True)
+
+    def j1j2_terms(bonds):
+        a = am.AutoMPO()
+        for s1, s2, t, *_ in bonds:
+            J = 1.0 if t == 1 else 0.5
+            a.add(0.5 * J, "S+", s1 - 1, "S-", s2 - 1)
+            a.add(0.5 * J, "S-", s1 - 1, "S+", s2 - 1)
+            a.add(J, "Sz", s1 - 1, "Sz", s2 - 1)
+        return a.terms()
+
+    Hc = am.term_matrix(8, j1j2_terms(am.square_next_neighbor(4, 2, True)))
+    Hs = am.term_matrix(8, j1j2_terms(am.snake_relabel(am.square_next_neighbor(4, 2, True), 4, 2)))
+    assert np.allclose(np.linalg.eigvalsh(Hc), np.linalg.eigvalsh(Hs), atol=1e-10)

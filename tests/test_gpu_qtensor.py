@@ -173,7 +173,11 @@ def test_block_svd_matches_oracle(ctx, direction, cutoff, K):
     np.testing.assert_allclose(M.T @ M, np.eye(M.shape[1]), atol=1e-12)
 
 
-def _dmrg_state(L=10, sweeps=2, maxm=16, seed=7):
+def _dmrg_state(L=10, sweeps=2, maxm=16, seed=7, site=0):
+    """A converged oracle state with its orthogonality centre on `site`, the
+    right environments TR of the right-orthonormal tensors and the left
+    environments TL[0..site] of the left-orthonormal ones (so sites `site`
+    and `site`+1 see non-trivial environments on both sides)."""
     rng = np.random.default_rng(seed)
     h = list(rng.uniform(-0.1, 0.1, L))
     psi = qdmrg.QMPS(L, qdmrg.neel(L))
@@ -181,41 +185,44 @@ def _dmrg_state(L=10, sweeps=2, maxm=16, seed=7):
     qdmrg.dmrg(psi, H, sweeps, [maxm], [1e-12], [4])
     psi.position(0)
     TR, TL = qdmrg.build_env(psi, H)
+    psi.position(site)  # changes A[0..site] only: TR[site+1] stays valid
+    for i in range(site):
+        TL[i + 1] = qdmrg.env_step(TL[i], psi.A[i], H.A[i])
     return psi, H, TR, TL, h
 
 
-def test_heff_product_matches_oracle(ctx):
+def _mid_chain_operator(psi, H, TR, TL, site):
     import tt_b200
-    psi, H, TR, TL, _ = _dmrg_state()
-    site = 3
-    for i in range(site):
-        # move the centre right, updating left environments
-        pass
     A = qdmrg.BigQTensor()
-    A.setLeft(TL[0])
-    A.addMid(H.A[0])
-    A.addMid(H.A[1])
-    A.setRight(TR[1])
-    x = contract(psi.A[0], psi.A[1])
+    A.setLeft(TL[site])
+    A.addMid(H.A[site])
+    A.addMid(H.A[site + 1])
+    A.setRight(TR[site + 1])
+    op = tt_b200.BigQTensor(tt_b200.QTensor.from_oracle(TL[site]), tt_b200.QTensor.from_oracle(H.A[site]),
+                            tt_b200.QTensor.from_oracle(H.A[site + 1]), tt_b200.QTensor.from_oracle(TR[site + 1]))
+    return A, op, contract(psi.A[site], psi.A[site + 1])
+
+
+@pytest.mark.parametrize("site", [0, 4])
+def test_heff_product_matches_oracle(ctx, site):
+    """H_eff*x at the chain edge (trivial left boundary) and mid-chain (L, R
+    with several QN sectors on both sides)."""
+    import tt_b200
+    psi, H, TR, TL, _ = _dmrg_state(site=site)
+    A, op, x = _mid_chain_operator(psi, H, TR, TL, site)
+    if site > 0:
+        assert len(TL[site].blocks) > 4 and len(TR[site + 1].blocks) > 4
     want = A.product(x)
-    op = tt_b200.BigQTensor(tt_b200.QTensor.from_oracle(TL[0]), tt_b200.QTensor.from_oracle(H.A[0]),
-                            tt_b200.QTensor.from_oracle(H.A[1]), tt_b200.QTensor.from_oracle(TR[1]))
     got = op.product(tt_b200.QTensor.from_oracle(x))
     assert_same(got, want, tol=1e-11)
     assert op.size() == A.size()
 
 
-def test_davidson_matches_oracle(ctx):
+@pytest.mark.parametrize("site", [0, 5])
+def test_davidson_matches_oracle(ctx, site):
     import tt_b200
-    psi, H, TR, TL, _ = _dmrg_state(L=12, sweeps=1, maxm=12)
-    A = qdmrg.BigQTensor()
-    A.setLeft(TL[0])
-    A.addMid(H.A[0])
-    A.addMid(H.A[1])
-    A.setRight(TR[1])
-    x = contract(psi.A[0], psi.A[1])
-    op = tt_b200.BigQTensor(tt_b200.QTensor.from_oracle(TL[0]), tt_b200.QTensor.from_oracle(H.A[0]),
-                            tt_b200.QTensor.from_oracle(H.A[1]), tt_b200.QTensor.from_oracle(TR[1]))
+    psi, H, TR, TL, _ = _dmrg_state(L=12, sweeps=1, maxm=12, site=site)
+    A, op, x = _mid_chain_operator(psi, H, TR, TL, site)
     gx = tt_b200.QTensor.from_oracle(x)
     xo = x.copy()
     e_ref = tensor_davidsonIT(A, xo, 3, 6, 1e-12)

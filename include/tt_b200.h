@@ -95,6 +95,10 @@ int tt_ctx_clear_device_status(tt_ctx* ctx);
  * it, 0 makes the first wait give up).  The drain that lets issued copies and
  * MMAs land before shared and tensor memory are released keeps the default. */
 int tt_ctx_set_wait_limit(tt_ctx* ctx, int64_t polls);
+/* Bytes of the context's stream-ordered pool: in use now, the high-water mark
+ * of use (reset to the current use when reset_high is non-zero) and reserved
+ * from the device (freed blocks stay cached in the pool). */
+int tt_ctx_memory(tt_ctx* ctx, int64_t* used, int64_t* used_high, int64_t* reserved, int reset_high);
 const char* tt_get_last_error(void);
 
 int tt_device_alloc(tt_ctx* ctx, size_t bytes, void** dptr);

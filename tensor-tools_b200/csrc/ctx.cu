@@ -152,6 +152,22 @@ int tt_ctx_clear_device_status(tt_ctx* ctx) {
   return TT_OK;
 }
 
+int tt_ctx_memory(tt_ctx* ctx, int64_t* used, int64_t* used_high, int64_t* reserved, int reset_high) {
+  TT_REQUIRE(ctx, "null context");
+  uint64_t u = 0, h = 0, r = 0;
+  TT_CUDA(cudaMemPoolGetAttribute(ctx->pool, cudaMemPoolAttrUsedMemCurrent, &u));
+  TT_CUDA(cudaMemPoolGetAttribute(ctx->pool, cudaMemPoolAttrUsedMemHigh, &h));
+  TT_CUDA(cudaMemPoolGetAttribute(ctx->pool, cudaMemPoolAttrReservedMemCurrent, &r));
+  if (used) *used = (int64_t)u;
+  if (used_high) *used_high = (int64_t)h;
+  if (reserved) *reserved = (int64_t)r;
+  if (reset_high) {
+    uint64_t zero = 0;
+    TT_CUDA(cudaMemPoolSetAttribute(ctx->pool, cudaMemPoolAttrUsedMemHigh, &zero));
+  }
+  return TT_OK;
+}
+
 int tt_ctx_set_wait_limit(tt_ctx* ctx, int64_t polls) {
   TT_REQUIRE(ctx, "null context");
   TT_REQUIRE(polls < ((int64_t)1 << 32), "tt_ctx_set_wait_limit: polls out of range");

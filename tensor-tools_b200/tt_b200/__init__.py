@@ -168,6 +168,7 @@ _proto("tt_qdmrg_create", P, P, PP)
 _proto("tt_ctx_device_status", P, C.POINTER(C.c_int))
 _proto("tt_ctx_clear_device_status", P)
 _proto("tt_ctx_set_wait_limit", P, I64)
+_proto("tt_ctx_memory", P, C.POINTER(I64), C.POINTER(I64), C.POINTER(I64), C.c_int)
 _proto("tt_vec_scale_mode", P, I64, C.c_int, I64, PD, P)
 _proto("tt_qdmrg_sweep", P, C.c_int, D, C.c_int, PD)
 _proto("tt_qdmrg_set_noise", P, D)
@@ -241,6 +242,12 @@ class Context:
 
     def clear_device_status(self):
         _chk(lib.tt_ctx_clear_device_status(self.h), "clear device status")
+
+    def memory(self, reset_high: bool = False):
+        """Pool bytes: (in use, high-water mark of use, reserved from the device)."""
+        u, h, r = I64(), I64(), I64()
+        _chk(lib.tt_ctx_memory(self.h, C.byref(u), C.byref(h), C.byref(r), int(reset_high)), "memory")
+        return u.value, h.value, r.value
 
     def set_wait_limit(self, polls: int):
         """Test hook: polls of the tensor-core kernels' main-loop waits (< 0: the default)."""

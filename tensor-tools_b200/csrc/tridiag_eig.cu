@@ -33,7 +33,8 @@ constexpr int INV_ITERS = 3;
 
 struct EigDev {
   int64_t g_off, w_off, a_off;
-  int32_t n, flags, nvec, pad;
+  int32_t n, flags, nvec, nb;  // nb: panel width of the blocked cluster reduction
+  int64_t s_off;               // its n x 2nb panel scratch (blocked cluster reduction)
 };
 
 __device__ double block_reduce(double v, double* red, bool is_max) {
@@ -461,15 +462,26 @@ tridiag_eigvecs(const EigDev* __restrict__ probs, const double* G, const double*
 // memory) per sector, so a large density matrix is reduced by CL SMs at once
 // instead of one SM streaming it from L2.
 //
-// Phase 1: the columns of G are dealt out cyclically (column c to CTA c % CL)
-// and held in each CTA's shared memory when they fit (global otherwise).  For
-// column k the owner builds the reflector v and publishes it; every CTA forms
-// p = tau A22 v on its own columns and the partial p.v; after a second
-// cluster barrier every CTA gathers p and the partial dots (fixed order, so
-// every CTA holds the same w = p - (tau/2)(p.v) v) and applies the rank-2
-// update to its own columns.  Two cluster barriers per column; the published
-// buffers alternate by the parity of k, so no third barrier is needed.
-// Bisection then runs over all warps of the cluster.
+// Phase 1 is the blocked Householder tridiagonalisation of LAPACK's dsytrd /
+// dlatrd (Golub & Van Loan, "Matrix Computations", 4th ed., sec. 8.3.1 with
+// the panel form of sec. 5.1.7): the reflectors of a panel of nb columns are
+// formed one by one against the matrix as it stood at the start of the
+// panel, corrected on the fly by the panel's V and W (A22 v - V W^T v -
+// W V^T v), and the trailing matrix receives the rank-2nb update
+// A -= V W^T + W V^T once per panel.  Index c (row or column) belongs to CTA
+// c % CL.  Per column: the owners of rows >= j bring column j up to date and
+// push their part of |x|^2 (cluster barrier 1); every CTA forms the same
+// reflector, pushes its entries of v to every CTA and its partial V^T v,
+// W^T v (barrier 2); every CTA forms p = A22 v on its own columns (one warp
+// per column, L2-resident matrix), w' = tau (p - V W^T v - W V^T v) and its
+// part of w'.v, and the owners of the panel's rows push their w' (barrier
+// 3); then w = w' - (tau/2)(w'.v) v.  Every CTA sums the pushed partials in
+// CTA order, so every decision and scalar is the same in every CTA.  The
+// pushed buffers alternate by the parity of j, so no further barrier is
+// needed.  The trailing update goes through a global n x 2nb scratch (two
+// barriers per panel) and runs as row tiles of [V W] in shared memory
+// against each CTA's own columns.  Bisection then runs over all warps of the
+// cluster.
 //
 // Phase 2: CTA r owns eigenvectors [r q, r q + q), q = ceil(nvec / CL).
 // Inverse iteration runs one thread per vector.  Gram-Schmidt (twice, inside
@@ -487,21 +499,42 @@ namespace cgx = cooperative_groups;
 
 constexpr int CL_STAGE = 4;  // reflectors staged per round of the back-transformation
 constexpr int CL_MAX = 16;   // largest cluster the kernels are launched with
+constexpr int PNB_MAX = 32;  // widest panel of the blocked reduction
+constexpr int TROWS = 64;    // rows per tile of the trailing update
 
-// doubles of shared memory the phase-1 cluster kernel needs besides the column slab
-constexpr int CL_WARPS = TT / 32;  // warps per CTA
-__host__ __device__ inline int64_t cluster_vals_extra(int n) { return 5 * (int64_t)n + 2 * CL_MAX * CL_WARPS; }
+
+// doubles of dynamic shared memory of the blocked cluster reduction
+__host__ __device__ inline int64_t blocked_smem(int n, int nb, int CL) {
+  const int64_t nloc = (n + CL - 1) / CL;
+  return 2 * (int64_t)nb * nloc   // V, W of the panel on the own rows
+         + nloc                   // the own rows of the current column
+         + 2 * (int64_t)n         // v, by parity of the column
+         + 2 * CL_MAX * 2         // pushed |x|^2 partials and alpha
+         + 2 * CL_MAX * 2 * nb    // pushed V^T v, W^T v partials
+         + 2 * CL_MAX             // pushed w'.v partials
+         + 2 * (int64_t)nb * nb   // V, W on the panel's rows
+         + 2 * (int64_t)nb        // pushed w' on the panel's rows
+         + 2 * (int64_t)nb        // W^T v, V^T v
+         + 2 * (int64_t)nb * TROWS;  // trailing-update tile of [V W]
+}
 
 __device__ __forceinline__ int first_owned(int from, int rank, int CL) {
   // smallest l with rank + CL * l >= from
   return from <= rank ? 0 : (from - rank + CL - 1) / CL;
 }
 
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
 __global__ void __launch_bounds__(TT)
-tridiag_eigvals_cluster(const EigDev* __restrict__ probs, double* G, double* Tg, double* W, int cap) {
+tridiag_eigvals_cluster(const EigDev* __restrict__ probs, double* G, double* Tg, double* W, double* VWg) {
   extern __shared__ double sm[];
   __shared__ double red[33];
-  __shared__ double s_tau;
+  __shared__ double s_alpha, s_kpart[TT / 32];
+
   cgx::cluster_group cluster = cgx::this_cluster();
   const int CL = (int)cluster.num_blocks();
   const int rank = (int)cluster.block_rank();
@@ -509,154 +542,214 @@ tridiag_eigvals_cluster(const EigDev* __restrict__ probs, double* G, double* Tg,
   const int n = P.n;
   const int tid = threadIdx.x;
   if (n <= 0) return;  // the same problem for the whole cluster
+  const int nb = P.nb;
   double* Gp = G + P.g_off;
   double* Wp = W + P.w_off;
   double* dg = Tg + 3 * P.w_off;
   double* eg = dg + n;
   double* tg = eg + n;
-  const int lcols = (n + CL - 1) / CL;
-  const int64_t extra = cluster_vals_extra(n);
-  const bool in_smem = (int64_t)lcols * n + extra <= cap;
-  double* rest = in_smem ? sm + (int64_t)lcols * n : sm;
-  double* vbuf = rest;            // [2][n]: reflector published by the column's owner, tau in the last slot
-  double* vloc = vbuf + 2 * n;    // this CTA's copy of v
-  double* pfull = vloc + n;       // [2][n]: p, pushed here by the owners of its columns
-  double* pdots = pfull + 2 * n;  // [2][CL_MAX * CL_WARPS]: partial p.v of every warp of the cluster
-  auto col = [&](int l) -> double* {  // l-th owned column (global column rank + CL l)
-    return in_smem ? sm + (int64_t)l * n : Gp + (int64_t)(rank + CL * l) * n;
-  };
-  if (in_smem)
-    for (int l = 0; l < lcols && rank + CL * l < n; ++l)
-      for (int i = tid; i < n; i += blockDim.x) sm[(int64_t)l * n + i] = Gp[(int64_t)(rank + CL * l) * n + i];
-  __syncthreads();
+  double* VW = VWg + P.s_off;  // n x 2nb, row-major: [i][t] = V(i, t), [i][nb + t] = W(i, t)
   const int warp = tid >> 5, lane = tid & 31, nw = blockDim.x >> 5;
-  const int nslot = CL * nw;  // partial dots per column
-  int lend = 0;               // owned columns that exist
-  while (lend < lcols && rank + CL * lend < n) ++lend;
-  double* const abase = col(0);
-  const int64_t lstride = in_smem ? (int64_t)n : (int64_t)CL * n;  // between owned columns
-  for (int k = 0; k + 2 < n; ++k) {
-    const int m = n - k - 1;  // m <= n - 1: the last slot of vbuf is free for tau
-    const int par = k & 1;
-    const int owner = k % CL;
-    if (rank == owner && warp == 0) {  // the reflector, by one warp of the owner
-      const double* a = col(k / CL);
-      double l0s = 0.0, l1s = 0.0;
-      int i = 1 + lane;
-      for (; i + 32 < m; i += 64) {
-        l0s += a[k + 1 + i] * a[k + 1 + i];
-        l1s += a[k + 33 + i] * a[k + 33 + i];
+  const int nloc = (n + CL - 1) / CL;
+  int lown = 0;  // own indices c = rank + CL l, l < lown
+  while (lown < nloc && rank + CL * lown < n) ++lown;
+  double* tile = sm;                    // [2nb][TROWS]
+  double* Vl = tile + 2 * nb * TROWS;   // [nb][nloc]
+  double* Wl = Vl + (int64_t)nb * nloc;  // [nb][nloc]
+  double* xc = Wl + (int64_t)nb * nloc;  // [nloc]
+  double* vf = xc + nloc;               // [2][n]
+  double* rs1 = vf + 2 * n;             // [2][CL_MAX][2]
+  double* rs2 = rs1 + 2 * CL_MAX * 2;   // [2][CL_MAX][2nb]
+  double* rs3 = rs2 + 2 * CL_MAX * 2 * nb;  // [2][CL_MAX]
+  double* Vp = rs3 + 2 * CL_MAX;        // [nb][nb]: Vp[t nb + s] = v_t[k0 + s]
+  double* Wq = Vp + nb * nb;            // [nb][nb]: Wq[t nb + s] = w_t[k0 + s]
+  double* wpend = Wq + nb * nb;         // [2][nb]: pushed w' on the panel's rows
+  double* cvt = wpend + 2 * nb;         // [nb]: V^T v
+  double* cwt = cvt + nb;               // [nb]: W^T v
+  for (int k0 = 0; k0 + 2 < n; k0 += nb) {
+    const int nbe = min(nb, n - 2 - k0);  // reflector columns k0 .. k0 + nbe - 1
+    for (int jj = 0; jj < nbe; ++jj) {
+      const int j = k0 + jj, par = j & 1;
+      // ---- 1: column j on the own rows >= j, |x|^2 over rows >= j + 2 ----
+      if (tid == 0) s_alpha = 0.0;
+      __syncthreads();
+      double part = 0.0;
+      for (int l = tid; l < lown; l += blockDim.x) {
+        const int i = rank + CL * l;
+        if (i < j) continue;
+        double a = Gp[i + (int64_t)n * j];
+        for (int t = 0; t < jj; ++t) a -= Vl[t * nloc + l] * Wq[t * nb + jj] + Wl[t * nloc + l] * Vp[t * nb + jj];
+        Gp[i + (int64_t)n * j] = a;
+        xc[l] = a;
+        if (i == j) dg[j] = a;
+        if (i == j + 1) s_alpha = a;
+        if (i >= j + 2) part += a * a;
       }
-      for (; i < m; i += 32) l0s += a[k + 1 + i] * a[k + 1 + i];
-      double loc = l0s + l1s;
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) loc += __shfl_xor_sync(0xffffffffu, loc, o);
-      const double alpha = a[k + 1];
+      part = block_reduce(part, red, false);
+      if (tid < CL) {
+        double* dst = cluster.map_shared_rank(rs1 + (par * CL_MAX + rank) * 2, tid);
+        dst[0] = part;
+        dst[1] = s_alpha;
+      }
+      cluster.sync();
+      // ---- 2: the reflector (same in every CTA), v pushed, V^T v and W^T v partials ----
+      double sigma = 0.0, alpha = 0.0;
+      for (int q = 0; q < CL; ++q) {
+        sigma += rs1[(par * CL_MAX + q) * 2];
+        alpha += rs1[(par * CL_MAX + q) * 2 + 1];
+      }
       double tau = 0.0, beta = alpha, scale = 0.0;
-      if (loc != 0.0) {
-        const double mu = sqrt(alpha * alpha + loc);
+      if (sigma != 0.0) {
+        const double mu = sqrt(alpha * alpha + sigma);
         beta = alpha <= 0.0 ? mu : -mu;
         tau = (beta - alpha) / beta;
         scale = 1.0 / (alpha - beta);
       }
-      if (lane == 0) {
-        tg[k] = tau;
-        eg[k] = beta;
-        vbuf[par * n + n - 1] = tau;
+      if (rank == j % CL && tid == 0) {
+        tg[j] = tau;
+        eg[j] = beta;
       }
+      for (int l = tid; l < lown; l += blockDim.x) {
+        const int i = rank + CL * l;
+        const double vi = i == j + 1 ? 1.0 : (i >= j + 2 ? xc[l] * scale : 0.0);
+        Vl[jj * nloc + l] = vi;
+        Wl[jj * nloc + l] = 0.0;
+        if (i >= j + 2) Gp[i + (int64_t)n * j] = vi;  // reflector kept below the subdiagonal for phase 2
+      }
+      __syncthreads();
+      for (int e = tid; e < lown * CL; e += blockDim.x) {
+        const int l = e / CL, q = e - l * CL;
+        const int i = rank + CL * l;
+        if (i >= j + 1) *cluster.map_shared_rank(vf + par * n + i, q) = Vl[jj * nloc + l];
+      }
+      for (int idx = warp; idx < 2 * jj; idx += nw) {
+        const int t = idx < jj ? idx : idx - jj;
+        const double* M = idx < jj ? Vl : Wl;
+        double sacc = 0.0;
+        for (int l = first_owned(j + 1, rank, CL) + lane; l < lown; l += 32)
+          sacc += M[t * nloc + l] * Vl[jj * nloc + l];
+        sacc = warp_sum(sacc);
+        if (lane < CL)
+          *cluster.map_shared_rank(rs2 + (par * CL_MAX + rank) * 2 * nb + (idx < jj ? t : nb + t), lane) = sacc;
+      }
+      cluster.sync();
+      // ---- 3: p = A22 v on the own columns, w' and its part of w'.v ----
+      for (int t = tid; t < jj; t += blockDim.x) {
+        double a = 0.0, b = 0.0;
+        for (int q = 0; q < CL; ++q) {
+          a += rs2[(par * CL_MAX + q) * 2 * nb + t];
+          b += rs2[(par * CL_MAX + q) * 2 * nb + nb + t];
+        }
+        cvt[t] = a;
+        cwt[t] = b;
+      }
+      __syncthreads();
+      const double* v = vf + par * n;
+      double kp = 0.0;
       if (tau != 0.0)
-        for (int j = lane; j < m; j += 32) {
-          const double vi = (j == 0) ? 1.0 : a[k + 1 + j] * scale;
-          vbuf[par * n + j] = vi;
-          if (j > 0) Gp[(k + 1 + j) + (int64_t)n * k] = vi;  // reflector kept for phase 2
+        for (int l = first_owned(j + 1, rank, CL) + warp; l < lown; l += nw) {
+          const int c = rank + CL * l;
+          const double* __restrict__ col = Gp + (int64_t)n * c;
+          double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+          int i = j + 1 + lane;
+          for (; i + 96 < n; i += 128) {
+            s0 += col[i] * v[i];
+            s1 += col[i + 32] * v[i + 32];
+            s2 += col[i + 64] * v[i + 64];
+            s3 += col[i + 96] * v[i + 96];
+          }
+          for (; i < n; i += 32) s0 += col[i] * v[i];
+          double corr = 0.0;
+          for (int t = lane; t < jj; t += 32) corr += Vl[t * nloc + l] * cwt[t] + Wl[t * nloc + l] * cvt[t];
+          const double pc = warp_sum((s0 + s1) + (s2 + s3));
+          corr = warp_sum(corr);
+          const double wprime = tau * (pc - corr);
+          if (lane == 0) {
+            Wl[jj * nloc + l] = wprime;
+            kp += wprime * Vl[jj * nloc + l];
+          }
+          if (c < k0 + nb && lane < CL) *cluster.map_shared_rank(wpend + par * nb + (c - k0), lane) = wprime;
+        }
+      if (lane == 0) s_kpart[warp] = kp;
+      __syncthreads();
+      if (tid < CL) {
+        double ksum = 0.0;
+        for (int w = 0; w < nw; ++w) ksum += s_kpart[w];
+        *cluster.map_shared_rank(rs3 + par * CL_MAX + rank, tid) = ksum;
+      }
+      cluster.sync();
+      // ---- 4: w = w' - (tau/2)(w'.v) v on the own rows and on the panel's rows ----
+      double K = 0.0;
+      for (int q = 0; q < CL; ++q) K += rs3[par * CL_MAX + q];
+      K *= 0.5 * tau;
+      for (int l = tid; l < lown; l += blockDim.x)
+        if (rank + CL * l >= j + 1) Wl[jj * nloc + l] -= K * Vl[jj * nloc + l];
+      for (int s2 = tid; s2 < nb; s2 += blockDim.x) {
+        const int row = k0 + s2;
+        const bool live = row >= j + 1 && row < n;
+        Vp[jj * nb + s2] = live ? v[row] : 0.0;
+        Wq[jj * nb + s2] = live && tau != 0.0 ? wpend[par * nb + s2] - K * v[row] : 0.0;
+      }
+      __syncthreads();
+    }
+    // ---- trailing update A[k1:, k1:] -= V W^T + W V^T through the global scratch ----
+    const int k1 = k0 + nbe;
+    for (int e = tid; e < lown * 2 * nbe; e += blockDim.x) {
+      const int l = e / (2 * nbe), t2 = e - l * 2 * nbe;
+      const int i = rank + CL * l;
+      if (i < k1) continue;
+      const int t = t2 < nbe ? t2 : t2 - nbe;
+      VW[(int64_t)i * 2 * nb + (t2 < nbe ? t : nb + t)] = (t2 < nbe ? Vl : Wl)[t * nloc + l];
+    }
+    __threadfence();
+    cluster.sync();
+    const int lf = first_owned(k1, rank, CL);
+    const int r = tid % TROWS, g = tid / TROWS, ng = blockDim.x / TROWS;
+    for (int i0 = k1; i0 < n; i0 += TROWS) {
+      const int rows = min(TROWS, n - i0);
+      __syncthreads();
+      for (int e = tid; e < rows * 2 * nbe; e += blockDim.x) {
+        const int rr = e / (2 * nbe), t2 = e - rr * 2 * nbe;
+        const int col = t2 < nbe ? t2 : nb + (t2 - nbe);
+        tile[col * TROWS + rr] = VW[(int64_t)(i0 + rr) * 2 * nb + col];
+      }
+      __syncthreads();
+      if (r < rows)  // four own columns per thread: the row's [V W] values are read once for all four
+        for (int lb = lf + g; lb < lown; lb += 4 * ng) {
+          double acc[4] = {0.0, 0.0, 0.0, 0.0};
+          int lc[4];
+#pragma unroll
+          for (int u = 0; u < 4; ++u) lc[u] = min(lb + ng * u, lown - 1);
+          for (int t = 0; t < nbe; ++t) {
+            const double vi = tile[t * TROWS + r], wi = tile[(nb + t) * TROWS + r];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) acc[u] += vi * Wl[t * nloc + lc[u]] + wi * Vl[t * nloc + lc[u]];
+          }
+#pragma unroll
+          for (int u = 0; u < 4; ++u)
+            if (lb + ng * u < lown) Gp[(int64_t)n * (rank + CL * lc[u]) + i0 + r] -= acc[u];
         }
     }
+    __threadfence();
     cluster.sync();
-    // one parallel pull of v and tau from the owner
-    const double* ov = cluster.map_shared_rank(vbuf + par * n, owner);
-    if (tid == 0) s_tau = ov[n - 1];
-    for (int i = tid; i < m; i += blockDim.x) vloc[i] = ov[i];
-    __syncthreads();
-    const double tau = s_tau;
-    if (tau == 0.0) continue;  // column already reduced (same decision in every CTA)
-    // p = tau A22 v on the owned columns (A22 symmetric: column dot v), one
-    // warp per column with four independent chains; lanes 0..CL-1 push p_c
-    // into every CTA's pfull, and every warp pushes its share of p.v into
-    // every CTA's pdots
-    const int l0 = first_owned(k + 1, rank, CL);
-    double wpart = 0.0;
-    for (int l = l0 + warp; l < lend; l += nw) {
-      const int c = rank + CL * l;
-      const double* __restrict__ a = col(l) + k + 1;
-      double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
-      int i = lane;
-      for (; i + 96 < m; i += 128) {
-        s0 += a[i] * vloc[i];
-        s1 += a[i + 32] * vloc[i + 32];
-        s2 += a[i + 64] * vloc[i + 64];
-        s3 += a[i + 96] * vloc[i + 96];
-      }
-      for (; i < m; i += 32) s0 += a[i] * vloc[i];
-      double s = (s0 + s1) + (s2 + s3);
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-      const double pc = tau * s;
-      if (lane < CL) *cluster.map_shared_rank(pfull + par * n + (c - k - 1), lane) = pc;
-      wpart += pc * vloc[c - k - 1];
-    }
-    if (lane < CL) *cluster.map_shared_rank(pdots + par * CL_MAX * CL_WARPS + rank * nw + warp, lane) = wpart;
-    cluster.sync();
-    // p.v: every warp sums the same partials in the same order, so every
-    // warp of every CTA holds the same K
-    double x = 0.0;
-    for (int j = lane; j < nslot; j += 32) x += pdots[par * CL_MAX * CL_WARPS + j];
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
-    const double K = 0.5 * tau * x;
-    const double* pf = pfull + par * n;
-    // A22 -= v w^T + w v^T on the owned columns, w = p - K v formed on the
-    // fly: rows outer (v_i, w_i in registers), owned columns inner, four at a
-    // time so their loads and stores overlap
-    for (int i = tid; i < m; i += blockDim.x) {
-      const double vi = vloc[i], wi = pf[i] - K * vi;
-      double* __restrict__ ai = abase + (k + 1 + i);
-      int l = l0;
-      for (; l + 3 < lend; l += 4) {
-        const int c0 = rank + CL * l - k - 1;
-        const double v0 = vloc[c0], v1 = vloc[c0 + CL], v2 = vloc[c0 + 2 * CL], v3 = vloc[c0 + 3 * CL];
-        const double w0 = pf[c0] - K * v0, w1 = pf[c0 + CL] - K * v1, w2 = pf[c0 + 2 * CL] - K * v2,
-                     w3 = pf[c0 + 3 * CL] - K * v3;
-        const double a0 = ai[l * lstride], a1 = ai[(l + 1) * lstride], a2 = ai[(l + 2) * lstride],
-                     a3 = ai[(l + 3) * lstride];
-        ai[l * lstride] = a0 - (vi * w0 + wi * v0);
-        ai[(l + 1) * lstride] = a1 - (vi * w1 + wi * v1);
-        ai[(l + 2) * lstride] = a2 - (vi * w2 + wi * v2);
-        ai[(l + 3) * lstride] = a3 - (vi * w3 + wi * v3);
-      }
-      for (; l < lend; ++l) {
-        const int cc = rank + CL * l - k - 1;
-        const double vc = vloc[cc], wc = pf[cc] - K * vc;
-        ai[l * lstride] -= vi * wc + wi * vc;
-      }
-    }
-    __syncthreads();
   }
-  // T: diagonal from the owners, the last off-diagonal A[n-1, n-2]
-  for (int l = 0; l < lcols; ++l) {
-    const int c = rank + CL * l;
-    if (c >= n) break;
-    if (tid == 0) dg[c] = col(l)[c];
-    if (c == n - 2 && tid == 0) eg[n - 2] = col(l)[n - 1];
-  }
-  if (rank == 0 && tid == 0) {
-    eg[n - 1] = 0.0;
-    tg[n - 1] = 0.0;
-    if (n >= 2) tg[n - 2] = 0.0;
+  // T: the last two diagonal entries and the last off-diagonal A[n-1, n-2]
+  if (tid == 0) {
+    if (rank == (n - 2) % CL) {
+      dg[n - 2] = Gp[(n - 2) + (int64_t)n * (n - 2)];
+      eg[n - 2] = Gp[(n - 1) + (int64_t)n * (n - 2)];
+    }
+    if (rank == (n - 1) % CL) dg[n - 1] = Gp[(n - 1) + (int64_t)n * (n - 1)];
+    if (rank == 0) {
+      eg[n - 1] = 0.0;
+      tg[n - 1] = 0.0;
+      tg[n - 2] = 0.0;
+    }
   }
   __threadfence();
   cluster.sync();  // also the last access of another CTA's shared memory
-  double* d = vloc;
-  double* e2 = pfull;
+  double* d = vf;
+  double* e2 = vf + n;
   for (int i = tid; i < n; i += blockDim.x) {
     d[i] = dg[i];
     e2[i] = i < n - 1 ? eg[i] * eg[i] : 0.0;
@@ -715,7 +808,7 @@ tridiag_eigvals_cluster(const EigDev* __restrict__ probs, double* G, double* Tg,
 
 __global__ void __launch_bounds__(TT)
 tridiag_eigvecs_cluster(const EigDev* __restrict__ probs, const double* G, const double* Tg, const double* W,
-                        double* Zg, double* work, int cap) {
+                        double* Zg, double* work, int cap, const int* __restrict__ only_flagged) {
   extern __shared__ double zsm[];
   __shared__ double red[33];
   __shared__ double coef[MAX_N / 2];
@@ -723,6 +816,9 @@ tridiag_eigvecs_cluster(const EigDev* __restrict__ probs, const double* G, const
   cgx::cluster_group cluster = cgx::this_cluster();
   const int CL = (int)cluster.num_blocks();
   const int rank = (int)cluster.block_rank();
+  // as the fallback of the blocked path: only the problems it flagged (the
+  // whole cluster returns alike, before any barrier)
+  if (only_flagged && only_flagged[blockIdx.x / CL] == 0) return;
   const EigDev P = probs[blockIdx.x / CL];
   const int n = P.n, nvec = P.nvec;
   const int tid = threadIdx.x;
@@ -933,11 +1029,441 @@ tridiag_eigvecs_cluster(const EigDev* __restrict__ probs, const double* G, const
   }
 }
 
+// ---------------------------------------------------------------------------
+// Eigenvectors of the cluster-sized sectors, across the whole GPU.
+//
+// (1) inverse iteration, one thread per wanted vector (same start vectors and
+//     solves as the kernels above);
+// (2) CholeskyQR2 (Fukaya et al., "CholeskyQR2: a simple and communication-
+//     avoiding algorithm", 2014): G = Z^T Z, G = L L^T, Z <- Z L^-T, twice.
+//     In exact arithmetic this is Gram-Schmidt in column (descending
+//     eigenvalue) order, i.e. what the kernels above do inside clusters of
+//     close eigenvalues; against the other vectors it only removes components
+//     of the size of their orthogonality error.  A pivot L_jj below 1e-4 in
+//     the first pass means vector j had collapsed onto earlier ones (its
+//     orthonormalised form would carry a residual of eps ||T|| / L_jj): the
+//     problem is flagged and the cluster kernel above, which re-iterates such
+//     vectors, redoes it from the start;
+// (3) back-transformation z = Q y with the reflectors grouped 32 at a time in
+//     the compact WY form Q_p = I - V T V^T (LAPACK dlarft, forward and
+//     columnwise), then the deterministic gauge.
+// Every launch is batched over the problems; (1)-(3) use as many CTAs as
+// there are vectors, rows or tiles.
+constexpr int IV_THREADS = 128;   // vectors per CTA of the inverse iteration
+constexpr int GT = 64;            // Gram tile
+constexpr int CH_PB = 32;         // Cholesky panel
+constexpr int TS_ROWS = 32;       // rows per CTA of the triangular solve
+constexpr int BT_NB = 32;         // reflectors per compact-WY panel
+constexpr int BT_VB = 16;         // vectors per CTA of the back-transformation
+constexpr int BT_ROWS = 64;       // row chunk of the back-transformation
+constexpr double COLLAPSE_PIVOT2 = 1e-8;  // L_jj^2 below this: collapsed vector
+
+struct VecTask {
+  int32_t prob, j0;  // problem (index into the problem array) and first item
+};
+struct TileTask {
+  int32_t prob, a, b;  // problem and tile / panel coordinates
+};
+
+__device__ double tnorm1(const double* d, const double* e, int n, double* red) {
+  double loc = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x)
+    loc = fmax(loc, fabs(d[i]) + (i > 0 ? fabs(e[i - 1]) : 0.0) + (i + 1 < n ? fabs(e[i]) : 0.0));
+  return block_reduce(loc, red, true);
+}
+
+// (1) inverse iteration: thread t of task (p, j0) computes vector j0 + t
+__global__ void __launch_bounds__(IV_THREADS)
+inv_iter_batched(const EigDev* __restrict__ probs, const VecTask* __restrict__ tasks, const double* Tg,
+                 const double* W, double* Zg, double* work) {
+  __shared__ double red[33];
+  const VecTask tk = tasks[blockIdx.x];
+  const EigDev P = probs[tk.prob];
+  const int n = P.n;
+  const double* d = Tg + 3 * P.w_off;
+  const double* e = d + n;
+  const double* lam = W + P.w_off;
+  const double tnorm = tnorm1(d, e, n, red);
+  const double tiny = tnorm > 1e-250 ? fmax(DBL_EPSILON * tnorm, DBL_MIN) : 1.0;
+  const int j = tk.j0 + threadIdx.x;
+  if (j >= P.nvec) return;
+  double* y = Zg + P.g_off + (int64_t)n * j;
+  for (int i = 0; i < n; ++i) y[i] = hash_unit(((uint64_t)P.g_off << 20) ^ ((uint64_t)j << 32) ^ (uint64_t)i);
+  for (int it = 0; it < INV_ITERS; ++it) {
+    tri_solve(d, e, n, lam[j], tiny, y, work + 3 * P.g_off + (int64_t)3 * n * j, 1);
+    double s = 0.0;
+    for (int i = 0; i < n; ++i) s += y[i] * y[i];
+    const double inv = 1.0 / sqrt(s);
+    for (int i = 0; i < n; ++i) y[i] *= inv;
+  }
+}
+
+// (2a) Gram matrix, lower 64 x 64 tiles (a >= b): G[r + m c] = sum_i Z[i, r] Z[i, c],
+// G at work + 3 g_off, leading dimension m = nvec; 256 threads, 4 x 4 outputs each
+__global__ void __launch_bounds__(256)
+gram_tiles(const EigDev* __restrict__ probs, const TileTask* __restrict__ tasks, const double* Zg, double* work,
+           const int* __restrict__ flags) {
+  __shared__ double sa[16][GT + 2], sb[16][GT + 2];
+  const TileTask tk = tasks[blockIdx.x];
+  if (flags[tk.prob]) return;
+  const EigDev P = probs[tk.prob];
+  const int n = P.n, m = P.nvec;
+  const double* Z = Zg + P.g_off;
+  double* Gm = work + 3 * P.g_off;
+  const int r0 = tk.a * GT, c0 = tk.b * GT;
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  double acc[4][4] = {};
+  for (int i0 = 0; i0 < n; i0 += 16) {
+    __syncthreads();
+    for (int e2 = threadIdx.x; e2 < 16 * GT; e2 += blockDim.x) {
+      const int rr = e2 & 15, cc = e2 >> 4;
+      const int i = i0 + rr;
+      sa[rr][cc] = (i < n && r0 + cc < m) ? Z[i + (int64_t)n * (r0 + cc)] : 0.0;
+      sb[rr][cc] = (i < n && c0 + cc < m) ? Z[i + (int64_t)n * (c0 + cc)] : 0.0;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < 16; ++k) {
+      double av[4], bv[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        av[u] = sa[k][tx * 4 + u];
+        bv[u] = sb[k][ty * 4 + u];
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+#pragma unroll
+        for (int w = 0; w < 4; ++w) acc[u][w] += av[u] * bv[w];
+    }
+  }
+#pragma unroll
+  for (int u = 0; u < 4; ++u)
+#pragma unroll
+    for (int w = 0; w < 4; ++w) {
+      const int r = r0 + tx * 4 + u, c = c0 + ty * 4 + w;
+      if (r < m && c < m && r >= c) Gm[r + (int64_t)m * c] = acc[u][w];
+    }
+}
+
+// (2b) Cholesky G = L L^T of the lower triangle in place, right-looking with
+// 32-column panels, one cluster per problem: CTA 0 factors the diagonal
+// block, every CTA solves its share of the panel's rows, the trailing tiles
+// are dealt out to the CTAs.  Pivots below COLLAPSE_PIVOT2 (first pass)
+// flag the problem; a flagged or non-positive pivot is replaced by 1 so the
+// arithmetic stays finite (the problem is redone by the fallback).
+__global__ void __launch_bounds__(TT)
+chol_cluster(const EigDev* __restrict__ probs, double* work, int* flags, int check) {
+  __shared__ double Ld[CH_PB][CH_PB + 1];
+  __shared__ double tl[2][GT][CH_PB + 1];
+  __shared__ int s_flag;
+  cgx::cluster_group cluster = cgx::this_cluster();
+  const int CL = (int)cluster.num_blocks();
+  const int rank = (int)cluster.block_rank();
+  const int pi = blockIdx.x / CL;
+  if (flags[pi]) return;  // the whole cluster alike
+  const EigDev P = probs[pi];
+  const int m = P.nvec;
+  double* A = work + 3 * P.g_off;
+  const int tid = threadIdx.x;
+  for (int p0 = 0; p0 < m; p0 += CH_PB) {
+    const int pb = min(CH_PB, m - p0);
+    // (i) the diagonal block, every CTA (identical arithmetic; only CTA 0 writes)
+    for (int e2 = tid; e2 < pb * pb; e2 += blockDim.x) {
+      const int r = e2 % pb, c = e2 / pb;
+      Ld[r][c] = r >= c ? A[(p0 + r) + (int64_t)m * (p0 + c)] : 0.0;
+    }
+    if (tid == 0) s_flag = 0;
+    __syncthreads();
+    for (int k = 0; k < pb; ++k) {
+      if (tid == 0) {
+        double dk = Ld[k][k];
+        if (!(dk > (check ? COLLAPSE_PIVOT2 : 0.0))) {
+          s_flag = 1;
+          dk = 1.0;
+        }
+        Ld[k][k] = sqrt(dk);
+      }
+      __syncthreads();
+      const double piv = Ld[k][k];
+      for (int r = k + 1 + tid; r < pb; r += blockDim.x) Ld[r][k] /= piv;
+      __syncthreads();
+      for (int e2 = tid; e2 < pb * pb; e2 += blockDim.x) {
+        const int r = e2 % pb, c = e2 / pb;
+        if (c > k && r >= c) Ld[r][c] -= Ld[r][k] * Ld[c][k];
+      }
+      __syncthreads();
+    }
+    if (rank == 0) {
+      for (int e2 = tid; e2 < pb * pb; e2 += blockDim.x) {
+        const int r = e2 % pb, c = e2 / pb;
+        if (r >= c) A[(p0 + r) + (int64_t)m * (p0 + c)] = Ld[r][c];
+      }
+      if (tid == 0 && s_flag) atomicExch(&flags[pi], 1);
+    }
+    // (ii) rows below the block: L[i, p0:p0+pb] = A[i, p0:p0+pb] L_pp^-T
+    const int rbeg = p0 + pb;
+    for (int i = rbeg + rank * (int)blockDim.x + tid; i < m; i += CL * (int)blockDim.x) {
+      double x[CH_PB];
+#pragma unroll
+      for (int k = 0; k < CH_PB; ++k) {
+        if (k < pb) {
+          double v = A[i + (int64_t)m * (p0 + k)];
+          for (int t = 0; t < k; ++t) v -= x[t] * Ld[k][t];
+          x[k] = v / Ld[k][k];
+          A[i + (int64_t)m * (p0 + k)] = x[k];
+        }
+      }
+    }
+    __threadfence();
+    cluster.sync();
+    // (iii) trailing update of the lower tiles (a >= b) of A[rbeg:, rbeg:]
+    const int nt = (m - rbeg + GT - 1) / GT;
+    const int ntiles = nt * (nt + 1) / 2;
+    for (int t = rank; t < ntiles; t += CL) {
+      int ta = 0;
+      while ((ta + 1) * (ta + 2) / 2 <= t) ++ta;
+      const int tb = t - ta * (ta + 1) / 2;
+      const int ra = rbeg + ta * GT, rb = rbeg + tb * GT;
+      __syncthreads();
+      for (int e2 = tid; e2 < GT * pb; e2 += blockDim.x) {
+        const int r = e2 % GT, k = e2 / GT;
+        tl[0][r][k] = ra + r < m ? A[(ra + r) + (int64_t)m * (p0 + k)] : 0.0;
+        tl[1][r][k] = rb + r < m ? A[(rb + r) + (int64_t)m * (p0 + k)] : 0.0;
+      }
+      __syncthreads();
+      for (int e2 = tid; e2 < GT * GT; e2 += blockDim.x) {
+        const int r = e2 % GT, c = e2 / GT;
+        const int gi = ra + r, gj = rb + c;
+        if (gi < m && gj < m && gi >= gj) {
+          double acc = 0.0;
+          for (int k = 0; k < pb; ++k) acc += tl[0][r][k] * tl[1][c][k];
+          A[gi + (int64_t)m * gj] -= acc;
+        }
+      }
+    }
+    __threadfence();
+    cluster.sync();
+  }
+}
+
+// (2c) Z <- Z L^-T, row by row (rows are independent): TS_ROWS rows per CTA,
+// columns in 32-wide panels: the solved part enters through a small GEMM,
+// the panel's own triangle by substitution
+__global__ void __launch_bounds__(256)
+trsm_rows(const EigDev* __restrict__ probs, const VecTask* __restrict__ tasks, double* Zg, const double* work,
+          const int* __restrict__ flags) {
+  __shared__ double sx[TS_ROWS][CH_PB + 1];   // solved values, one 32-column chunk
+  __shared__ double sl[CH_PB][CH_PB + 1];     // L rows of the panel, one 32-column chunk
+  __shared__ double acc_s[TS_ROWS][CH_PB + 1];
+  const VecTask tk = tasks[blockIdx.x];
+  if (flags[tk.prob]) return;
+  const EigDev P = probs[tk.prob];
+  const int n = P.n, m = P.nvec;
+  double* Z = Zg + P.g_off;
+  const double* L = work + 3 * P.g_off;
+  const int i0 = tk.j0;
+  const int tid = threadIdx.x;
+  const int r = tid & 31, cg = tid >> 5;  // row in the block, column group of 4
+  for (int p0 = 0; p0 < m; p0 += CH_PB) {
+    const int pb = min(CH_PB, m - p0);
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int k0 = 0; k0 < p0; k0 += CH_PB) {
+      __syncthreads();
+      for (int e2 = tid; e2 < TS_ROWS * CH_PB; e2 += blockDim.x) {
+        const int rr = e2 % TS_ROWS, kk = e2 / TS_ROWS;
+        sx[rr][kk] = i0 + rr < n ? Z[(i0 + rr) + (int64_t)n * (k0 + kk)] : 0.0;
+        const int lr = e2 % CH_PB, lk = e2 / CH_PB;
+        sl[lr][lk] = lr < pb ? L[(p0 + lr) + (int64_t)m * (k0 + lk)] : 0.0;
+      }
+      __syncthreads();
+#pragma unroll 8
+      for (int kk = 0; kk < CH_PB; ++kk) {
+        const double xv = sx[r][kk];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) acc[u] += xv * sl[cg * 4 + u][kk];
+      }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int u = 0; u < 4; ++u) acc_s[r][cg * 4 + u] = acc[u];
+    for (int e2 = tid; e2 < CH_PB * CH_PB; e2 += blockDim.x) {
+      const int lr = e2 % CH_PB, lk = e2 / CH_PB;
+      sl[lr][lk] = (lr < pb && lk <= lr) ? L[(p0 + lr) + (int64_t)m * (p0 + lk)] : 0.0;
+    }
+    __syncthreads();
+    if (tid < TS_ROWS && i0 + tid < n) {
+      double x[CH_PB];
+      double* zr = Z + (i0 + tid);
+#pragma unroll
+      for (int c = 0; c < CH_PB; ++c) {
+        if (c < pb) {
+          double v = zr[(int64_t)n * (p0 + c)] - acc_s[tid][c];
+          for (int t = 0; t < c; ++t) v -= x[t] * sl[c][t];
+          x[c] = v / sl[c][c];
+          zr[(int64_t)n * (p0 + c)] = x[c];
+        }
+      }
+    }
+  }
+}
+
+// (3a) compact-WY factor T of the reflectors [32 b, 32 b + 32) of a problem:
+// S = V^T V (v_k(k+1) = 1, v_k(i) = G(i, k) for i >= k + 2), then the dlarft
+// recurrence T(0:c, c) = -tau_c T(0:c, 0:c) S(0:c, c), T(c, c) = tau_c
+__global__ void __launch_bounds__(256)
+wy_factors(const EigDev* __restrict__ probs, const TileTask* __restrict__ tasks, const double* G, const double* Tg,
+           double* work, const int* __restrict__ flags) {
+  __shared__ double S[BT_NB][BT_NB + 1];
+  __shared__ double T[BT_NB][BT_NB + 1];
+  const TileTask tk = tasks[blockIdx.x];
+  if (flags[tk.prob]) return;
+  const EigDev P = probs[tk.prob];
+  const int n = P.n;
+  const double* Gp = G + P.g_off;
+  const double* tau = Tg + 3 * P.w_off + 2 * n;
+  const int k0 = tk.a * BT_NB, mm = min(BT_NB, n - 2 - k0);
+  double* Tout = work + 3 * P.g_off + (int64_t)P.nvec * P.nvec + (int64_t)tk.a * BT_NB * BT_NB;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  // S(a, c), a < c: v_a . v_c over rows >= k0 + c + 1 (v_c vanishes above)
+  for (int pr = warp; pr < mm * mm; pr += nw) {
+    const int a = pr % mm, c = pr / mm;
+    if (a >= c) continue;
+    const int ka = k0 + a, kc = k0 + c;
+    double acc = 0.0;
+    for (int i = kc + 1 + lane; i < n; i += 32) {
+      const double va = (i == ka + 1) ? 1.0 : Gp[i + (int64_t)n * ka];
+      const double vc = (i == kc + 1) ? 1.0 : Gp[i + (int64_t)n * kc];
+      acc += va * vc;
+    }
+    acc = warp_sum(acc);
+    if (lane == 0) S[a][c] = acc;
+  }
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    for (int c = 0; c < mm; ++c) {
+      const double tc = tau[k0 + c];
+      // T(a, c) = -tc * sum_{b in [a, c)} T(a, b) S(b, c), lanes over a
+      double x = 0.0;
+      if (lane < c) {
+        for (int b = lane; b < c; ++b) x += T[lane][b] * S[b][c];
+        T[lane][c] = -tc * x;
+      }
+      if (lane == 0) T[c][c] = tc;
+      __syncwarp();
+    }
+  }
+  __syncthreads();
+  for (int e2 = threadIdx.x; e2 < BT_NB * BT_NB; e2 += blockDim.x) {
+    const int a = e2 % BT_NB, c = e2 / BT_NB;
+    Tout[e2] = (a < mm && c < mm && a <= c) ? T[a][c] : 0.0;
+  }
+}
+
+// (3b) z = Q y for the vectors [j0, j0 + BT_VB) of a problem: panels last to
+// first, Y <- Y - V (T (V^T Y)) over rows >= k0 + 1; then the gauge (largest
+// magnitude entry positive, first on ties)
+__global__ void __launch_bounds__(512)
+wy_apply(const EigDev* __restrict__ probs, const VecTask* __restrict__ tasks, const double* G, double* Zg,
+         const double* work, const int* __restrict__ flags) {
+  __shared__ double sv[BT_ROWS][BT_NB + 1];
+  __shared__ double sy[BT_ROWS][BT_VB + 1];
+  __shared__ double X[BT_NB][BT_VB + 1];
+  __shared__ double X2[BT_NB][BT_VB + 1];
+  __shared__ double Tm[BT_NB][BT_NB + 1];
+  const VecTask tk = tasks[blockIdx.x];
+  if (flags[tk.prob]) return;
+  const EigDev P = probs[tk.prob];
+  const int n = P.n, nv = min(BT_VB, P.nvec - tk.j0);
+  const double* Gp = G + P.g_off;
+  double* Y = Zg + P.g_off + (int64_t)n * tk.j0;
+  const double* Tst = work + 3 * P.g_off + (int64_t)P.nvec * P.nvec;
+  const int tid = threadIdx.x;
+  const int npan = (n - 2 + BT_NB - 1) / BT_NB;
+  const int xa = tid / BT_VB, xc = tid % BT_VB;  // the (reflector, vector) entry of X this thread sums
+  for (int pnl = npan - 1; pnl >= 0; --pnl) {
+    const int k0 = pnl * BT_NB, mm = min(BT_NB, n - 2 - k0);
+    __syncthreads();
+    for (int e2 = tid; e2 < BT_NB * BT_NB; e2 += blockDim.x) Tm[e2 % BT_NB][e2 / BT_NB] = Tst[(int64_t)pnl * BT_NB * BT_NB + e2];
+    double xs = 0.0;
+    // X = V^T Y over rows >= k0 + 1, 64 rows at a time
+    for (int i0 = k0 + 1; i0 < n; i0 += BT_ROWS) {
+      __syncthreads();
+      for (int e2 = tid; e2 < BT_ROWS * BT_NB; e2 += blockDim.x) {
+        const int rr = e2 % BT_ROWS, a = e2 / BT_ROWS;
+        const int i = i0 + rr, ka = k0 + a;
+        double v = 0.0;
+        if (a < mm && i < n && i >= ka + 1) v = (i == ka + 1) ? 1.0 : Gp[i + (int64_t)n * ka];
+        sv[rr][a] = v;
+      }
+      for (int e2 = tid; e2 < BT_ROWS * BT_VB; e2 += blockDim.x) {
+        const int rr = e2 % BT_ROWS, c = e2 / BT_ROWS;
+        sy[rr][c] = (i0 + rr < n && c < nv) ? Y[(i0 + rr) + (int64_t)n * c] : 0.0;
+      }
+      __syncthreads();
+#pragma unroll 8
+      for (int rr = 0; rr < BT_ROWS; ++rr) xs += sv[rr][xa] * sy[rr][xc];
+    }
+    X[xa][xc] = xs;
+    __syncthreads();
+    // X2 = T X (T upper triangular)
+    {
+      double t2 = 0.0;
+      for (int b = xa; b < BT_NB; ++b) t2 += Tm[xa][b] * X[b][xc];
+      X2[xa][xc] = t2;
+    }
+    __syncthreads();
+    // Y -= V X2
+    for (int i0 = k0 + 1; i0 < n; i0 += BT_ROWS) {
+      __syncthreads();
+      for (int e2 = tid; e2 < BT_ROWS * BT_NB; e2 += blockDim.x) {
+        const int rr = e2 % BT_ROWS, a = e2 / BT_ROWS;
+        const int i = i0 + rr, ka = k0 + a;
+        double v = 0.0;
+        if (a < mm && i < n && i >= ka + 1) v = (i == ka + 1) ? 1.0 : Gp[i + (int64_t)n * ka];
+        sv[rr][a] = v;
+      }
+      __syncthreads();
+      for (int e2 = tid; e2 < BT_ROWS * BT_VB; e2 += blockDim.x) {
+        const int rr = e2 % BT_ROWS, c = e2 / BT_ROWS;
+        const int i = i0 + rr;
+        if (i < n && c < nv) {
+          double u = 0.0;
+#pragma unroll 8
+          for (int a = 0; a < BT_NB; ++a) u += sv[rr][a] * X2[a][c];
+          Y[i + (int64_t)n * c] -= u;
+        }
+      }
+    }
+  }
+  __syncthreads();
+  // gauge, one warp per vector
+  const int lane = tid & 31, warp = tid >> 5;
+  if (warp < nv) {
+    double* y = Y + (int64_t)n * warp;
+    double best = -1.0;
+    int bi = n;
+    for (int i = lane; i < n; i += 32) {
+      const double a = fabs(y[i]);
+      if (a > best) { best = a; bi = i; }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+      const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+      if (ob > best || (ob == best && oi < bi)) { best = ob; bi = oi; }
+    }
+    const bool flip = bi < n && y[bi] < 0.0;
+    __syncwarp();
+    if (flip)
+      for (int i = lane; i < n; i += 32) y[i] = -y[i];
+  }
+}
+
 std::vector<EigDev> to_dev(const tt_eig_problem* probs, int n_probs, const int* nvec) {
   std::vector<EigDev> hp(n_probs);
   for (int i = 0; i < n_probs; ++i)
     hp[i] = EigDev{probs[i].g_off, probs[i].w_off, probs[i].a_off, probs[i].n, probs[i].flags,
-                   nvec ? nvec[i] : 0, 0};
+                   nvec ? nvec[i] : 0, 0, 0};
   return hp;
 }
 
@@ -975,7 +1501,7 @@ const ClusterPlan& cluster_plan(tt_ctx* ctx) {
   }
   const int64_t va = ((int64_t)optin - (int64_t)fa.sharedSizeBytes - 1024) / 8;
   const int64_t vb = ((int64_t)optin - (int64_t)fb.sharedSizeBytes - 1024) / 8;
-  if (va < cluster_vals_extra(MAX_N) || vb < 6 * MAX_N) return cp;
+  if (va < blocked_smem(MAX_N, 8, 8) || vb < 6 * MAX_N) return cp;
   const void* kernels[2] = {(const void*)tridiag_eigvals_cluster, (const void*)tridiag_eigvecs_cluster};
   const int64_t caps[2] = {va, vb};
   for (int k = 0; k < 2; ++k) {
@@ -985,6 +1511,10 @@ const ClusterPlan& cluster_plan(tt_ctx* ctx) {
       cudaGetLastError();
       return cp;
     }
+  }
+  if (cudaFuncSetAttribute(chol_cluster, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) {
+    cudaGetLastError();
+    return cp;
   }
   for (int cl : {CL_MAX, 8}) {
     bool ok = true;
@@ -1067,17 +1597,26 @@ int tt_sym_eigvals_batched(tt_ctx* ctx, const tt_eig_problem* probs, int n_probs
     tridiag_eigvals<<<n_small, TT, vals_smem(), ctx->stream>>>(dp, G, T, w, A);
     TT_LAUNCH_CHECK(ctx);
   }
+  double* vw = nullptr;
   if (!big.empty()) {
-    int64_t need = 0;  // doubles: the column slab in shared memory when it fits under the cap
-    for (const EigDev& e : big) {
-      const int64_t lcols = (e.n + cp.cl - 1) / cp.cl;
-      const int64_t extra = cluster_vals_extra(e.n);
-      const int64_t full = lcols * e.n + extra;
-      need = std::max(need, full <= cp.vals_cap ? full : extra);
+    // panel width per problem: the widest whose shared memory fits; the
+    // panel scratch (n x 2nb per problem) lives in the pool
+    int64_t need = 0, scratch = 0;
+    for (EigDev& e : big) {
+      e.nb = PNB_MAX;
+      while (e.nb > 8 && blocked_smem(e.n, e.nb, cp.cl) > cp.vals_cap) e.nb /= 2;
+      need = std::max(need, blocked_smem(e.n, e.nb, cp.cl));
+      e.s_off = scratch;
+      scratch += (int64_t)e.n * 2 * e.nb;
     }
+    TT_REQUIRE(need <= cp.vals_cap, "tt_sym_eigvals_batched: sector too large for the cluster eigensolver");
+    vw = tt::pool_alloc<double>(ctx, (size_t)scratch);
+    if (!vw) return tt::fail(TT_ERR_OOM, "tt_sym_eigvals_batched: allocation failed");
+    TT_CUDA(tt::h2d_async(ctx, dp + n_small, big.data(), sizeof(EigDev) * big.size()));
     TT_CUDA(launch_cluster(ctx, cp.cl, (int)big.size(), need, (const void*)tridiag_eigvals_cluster,
-                           dp + n_small, G, T, w, (int)need));
+                           dp + n_small, G, T, w, vw));
   }
+  tt::pool_free(ctx, vw);
   tt::pool_free(ctx, dp);
   return TT_OK;
 }
@@ -1122,15 +1661,67 @@ int tt_sym_eigvecs_batched(tt_ctx* ctx, const tt_eig_problem* probs, int n_probs
     TT_LAUNCH_CHECK(ctx);
   }
   if (!big.empty()) {
-    int64_t needc = 0;  // doubles: own eigenvectors in shared memory when they fit, plus 6n of buffers
+    // the GPU-wide path: inverse iteration, CholeskyQR2, compact-WY
+    // back-transformation; problems it flags are redone by the cluster kernel
+    const int nbig = (int)big.size();
+    std::vector<VecTask> iv, ts, ap;
+    std::vector<TileTask> gm, wy;
+    for (int p = 0; p < nbig; ++p) {
+      const EigDev& e = big[p];
+      for (int j = 0; j < e.nvec; j += IV_THREADS) iv.push_back(VecTask{p, j});
+      const int nt = (e.nvec + GT - 1) / GT;
+      for (int a = 0; a < nt; ++a)
+        for (int b = 0; b <= a; ++b) gm.push_back(TileTask{p, a, b});
+      if (e.nvec > 0) {
+        for (int i = 0; i < e.n; i += TS_ROWS) ts.push_back(VecTask{p, i});
+        for (int k = 0; k * BT_NB < e.n - 2; ++k) wy.push_back(TileTask{p, k, 0});
+        for (int j = 0; j < e.nvec; j += BT_VB) ap.push_back(VecTask{p, j});
+      }
+    }
+    const size_t bytes = sizeof(int) * nbig + sizeof(VecTask) * (iv.size() + ts.size() + ap.size()) +
+                         sizeof(TileTask) * (gm.size() + wy.size()) + 64;
+    char* buf = tt::pool_alloc<char>(ctx, bytes);
+    if (!buf) return tt::fail(TT_ERR_OOM, "tt_sym_eigvecs_batched: allocation failed");
+    int* flags = reinterpret_cast<int*>(buf);
+    VecTask* d_iv = reinterpret_cast<VecTask*>(buf + ((sizeof(int) * nbig + 15) & ~(size_t)15));
+    VecTask* d_ts = d_iv + iv.size();
+    VecTask* d_ap = d_ts + ts.size();
+    TileTask* d_gm = reinterpret_cast<TileTask*>(d_ap + ap.size());
+    TileTask* d_wy = d_gm + gm.size();
+    TT_CUDA(cudaMemsetAsync(flags, 0, sizeof(int) * nbig, ctx->stream));
+    TT_CUDA(tt::h2d_async(ctx, d_iv, iv.data(), sizeof(VecTask) * iv.size()));
+    TT_CUDA(tt::h2d_async(ctx, d_ts, ts.data(), sizeof(VecTask) * ts.size()));
+    TT_CUDA(tt::h2d_async(ctx, d_ap, ap.data(), sizeof(VecTask) * ap.size()));
+    TT_CUDA(tt::h2d_async(ctx, d_gm, gm.data(), sizeof(TileTask) * gm.size()));
+    TT_CUDA(tt::h2d_async(ctx, d_wy, wy.data(), sizeof(TileTask) * wy.size()));
+    const EigDev* db = dp + n_small;
+    if (!iv.empty()) {
+      inv_iter_batched<<<(unsigned)iv.size(), IV_THREADS, 0, ctx->stream>>>(db, d_iv, T, w, Z, work);
+      TT_LAUNCH_CHECK(ctx);
+    }
+    for (int pass = 0; pass < 2 && !gm.empty(); ++pass) {
+      gram_tiles<<<(unsigned)gm.size(), 256, 0, ctx->stream>>>(db, d_gm, Z, work, flags);
+      TT_LAUNCH_CHECK(ctx);
+      TT_CUDA(launch_cluster(ctx, cp.cl, nbig, 0, (const void*)chol_cluster, db, work, flags, pass == 0 ? 1 : 0));
+      trsm_rows<<<(unsigned)ts.size(), 256, 0, ctx->stream>>>(db, d_ts, Z, work, flags);
+      TT_LAUNCH_CHECK(ctx);
+    }
+    if (!wy.empty()) {
+      wy_factors<<<(unsigned)wy.size(), 256, 0, ctx->stream>>>(db, d_wy, G, T, work, flags);
+      TT_LAUNCH_CHECK(ctx);
+      wy_apply<<<(unsigned)ap.size(), 512, 0, ctx->stream>>>(db, d_ap, G, Z, work, flags);
+      TT_LAUNCH_CHECK(ctx);
+    }
+    int64_t needc = 0;  // fallback: own eigenvectors in shared memory when they fit, plus 6n of buffers
     for (const EigDev& e : big) {
       const int64_t q = (e.nvec + cp.cl - 1) / cp.cl;
       const int64_t extra = 6 * (int64_t)e.n;
       const int64_t full = q * e.n + extra;
       needc = std::max(needc, full <= cp.vecs_cap ? full : extra);
     }
-    TT_CUDA(launch_cluster(ctx, cp.cl, (int)big.size(), needc, (const void*)tridiag_eigvecs_cluster,
-                           dp + n_small, G, T, w, Z, work, (int)needc));
+    TT_CUDA(launch_cluster(ctx, cp.cl, nbig, needc, (const void*)tridiag_eigvecs_cluster, db, G, T, w, Z, work,
+                           (int)needc, (const int*)flags));
+    tt::pool_free(ctx, buf);
   }
   tt::pool_free(ctx, dp);
   return TT_OK;

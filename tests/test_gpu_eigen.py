@@ -56,14 +56,16 @@ def test_batched_eigensolver_small_and_cluster_sectors(seed):
     tt_b200, lib = _bind()
     rng = np.random.default_rng(seed)
     cases = [(24, "decay"), (161, "decay"), (300, "rank"), (578, "decay"), (140, "degenerate"),
-             (700, "degenerate"), (1100, "decay")]
+             (700, "degenerate"), (1100, "decay"), (195, "decay"), (1630, "decay")]
+    if seed == 1:
+        cases.append((2600, "decay"))  # beyond the former 2048 cap; narrower panels
     mats = [_density_matrix(n, rng, kind) for n, kind in cases]
     ns = [m.shape[0] for m in mats]
     g_off = np.concatenate([[0], np.cumsum([n * n for n in ns])[:-1]]).astype(np.int64)
     w_off = np.concatenate([[0], np.cumsum(ns)[:-1]]).astype(np.int64)
     total = int(sum(n * n for n in ns))
     probs = (EigProblem * len(ns))(*[EigProblem(int(g), int(w), 0, n, 0) for g, w, n in zip(g_off, w_off, ns)])
-    nvec = [min(n, 1024, n // 2 + 7) for n in ns]
+    nvec = [min(n, 2048, n // 2 + 7) for n in ns]
     nvec_c = (C.c_int * len(ns))(*nvec)
     ctx = tt_b200.Context(0)
     try:

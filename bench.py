@@ -1,39 +1,61 @@
 #!/usr/bin/env python
 """Benchmark of the B200 two-site DMRG inner loop.
 
-Workload: U(1)-conserving two-site DMRG of the spin-1/2 Heisenberg chain,
-J=1, open boundaries, L=100, total Sz=0 from the Neel state, maxdim ramp
-32,64,128,256 then 512, SVD cutoff 1e-12, Davidson max 6 iterations (the
-reference's hard-wired tolerance 1e-12).  The ramp runs untimed as set-up;
-then W warm-up sweeps and K timed sweeps at maxdim 512.  A step is one full
-sweep (L->R and R->L over the 99 bonds, then normalize).  Inputs: the MPS,
-the MPO and the environments, a few hundred MB, are larger than L2 (126 MB);
-L2 is also flushed before every timed sweep.
+Default workload (the J1-J2 cylinder configuration): U(1)-conserving two-site
+DMRG of the spin-1/2 J1-J2 Heisenberg model, J1 = 1, J2 = 0.5, on a 6 x 16
+cylinder (periodic around the 6-site circumference, 96 sites numbered in snake
+order), total Sz = 0 from the Neel state, SVD cutoff 1e-10, Davidson at most
+4 iterations (the reference's hard-wired tolerance 1e-12), bond dimension
+3072.
 
-Reported value: seconds per sweep (lower is better), device-timed with CUDA
-events on the library's stream, max over ranks.  The H_eff*x throughput is in
-``roofline``; ``e2e`` repeats a sweep through the public C ABI with the MPS
-round-tripping through pinned host memory every step; ``mixed`` repeats the
-schedule in the automatic mixed-precision form (3xTF32 on tcgen05 where the
-cost model predicts a gain, FP64 elsewhere) with its energy difference.
+Set-up (untimed): the ramp maxdim 64, 128, 256, 512, 1024, 2048 with noise
+1e-6 decaying linearly to 0 over those six sweeps, then one sweep at 3072
+without noise, all in the chosen (mixed-precision) form; the state is
+checkpointed.  Each precision then loads the same checkpoint, builds its
+environments and moves the orthogonality centre to the middle of the chain
+(untimed).  A step is a fixed block of mid-chain two-site updates at bond
+dimension 3072: four left-to-right updates over sites 46..49 and four
+right-to-left updates back (8 updates, each Davidson + block SVD + environment
+update).  W warm-up and K timed steps per precision, CUDA events on the
+library's stream, L2 flushed before every step (the environments alone are
+tens of GB, far larger than L2).
 
-Other workloads (``--workload``): ``j1j2`` -- FP64 against mixed precision
-at large bond dimension on the J1-J2 cylinder (``--maxdim``, ``--breakdown``
-for a per-phase split, ``--profile-step`` to bracket one two-site step for
-ncu); ``gemm`` -- single-block contraction throughput per precision;
-``xxz-chains`` -- independent chains sharing one GPU.
+Reported value: seconds per sweep-equivalent of the chosen form (TF32 / 3xTF32
+on tcgen05 for the contractions its cost model picks, FP64 everywhere else):
+the mean time per timed two-site update times the 190 updates of a sweep
+(2 x 95 bonds) -- every update timed is at the full bond dimension, so this
+is the cost of a sweep at bond dimension 3072 throughout; ``ms_per_step`` is
+the measured time of one block step.  ``full_sweep`` holds a measured full
+sweep per precision (its edge bonds are smaller).  ``fp64`` is the plain GPU
+form on the same schedule; ``mixed`` repeats the chosen form's numbers with
+|dE|/N against FP64, both energies being <psi|H|psi>/<psi|psi> contracted in
+FP64 after identical schedules.  Rooflines: H_eff*x algorithmic TFLOP/s
+(event-timed product launches) against the cuBLAS DGEMM peak (FP64) and the
+cuBLAS TF32 peak (mixed; a 3xTF32 flop costs three TF32 products), both
+measured in this run.  ``e2e`` repeats steps of the chosen form through the
+public C ABI with the block's MPS site tensors uploaded from pinned host
+memory before and downloaded after every step.
+
+Other workloads (``--workload``): ``heisenberg`` -- the L = 100 Heisenberg
+chain to maxdim 512 (a step is one full sweep); ``gemm`` -- single-block
+contraction throughput per precision; ``xxz-chains`` -- independent chains
+sharing one GPU.
 
 ``--impl reference`` times the CPU restatement of the reference algorithm
-(oracle/, numpy + LAPACK on all host cores) on a bounded sample of the same
-workload: two-site steps on random tensors with the converged middle-bond
-sector structure (bond dimension 181/182), scaled to a sweep by the converged
-bond-dimension profile.
+(oracle/, numpy + LAPACK on all host cores) on the same workload: real
+two-site updates (Davidson, block SVD, environment update) at bond dimension
+3072 in the middle of the 96-site cylinder, on environments contracted with
+the same MPO through a state that is the Neel product state outside a 12-site
+window on each side and random left/right-canonical isometries (growing the
+bond to 3072) inside.  One update costs tens of seconds on the host, so the
+number of timed updates is capped by --ref-budget seconds (reported).
 """
 from __future__ import annotations
 
 import argparse
 import json
 import os
+import shutil
 import statistics
 import subprocess
 import sys
@@ -46,19 +68,31 @@ sys.path.insert(0, PKG)
 sys.path.insert(0, ROOT)
 
 METRIC = "sec/sweep & H_eff*x TFLOP/s: TF32/FP32 grouped vs FP64 GPU at |dE|/N<=1e-8"
-L_SITES = 100
-RAMP = (32, 64, 128, 256)
-MAXM = 512
-CUTOFF = 1e-12
-MAX_RESTART = 6
-CONFIG = {
-    "workload": "U(1) two-site DMRG, spin-1/2 Heisenberg chain J=1 OBC L=100, Sz=0 Neel start, "
-                "maxdim 512 (after untimed ramp 32,64,128,256), cutoff 1e-12, Davidson max 6 iters",
-    "L": L_SITES, "maxdim": MAXM, "cutoff": CUTOFF, "max_restart": MAX_RESTART,
-    "step": "one full sweep (L->R + R->L, 2x99 two-site updates)",
-    "l2": "inputs (MPS + environments) larger than L2; L2 flushed before each timed sweep",
-    "precision": "FP64 (plain GPU form)",
-}
+
+# the J1-J2 cylinder configuration
+C5 = dict(Nx=16, Ny=6, J2=0.5, maxdim=3072, cutoff=1e-10, max_restart=4,
+          ramp=[64, 128, 256, 512, 1024, 2048], noise0=1e-6, block=4)
+C5_N = C5["Nx"] * C5["Ny"]
+C5_MID = C5_N // 2 - C5["block"] // 2          # 46: the block spans sites 46..50
+C5_UPDATES_PER_SWEEP = 2 * (C5_N - 1)           # 190
+CHOSEN = "tf32x3-auto"
+
+
+def c5_config(args):
+    return {
+        "workload": "U(1) two-site DMRG, spin-1/2 J1-J2 Heisenberg (J1=1, J2=0.5) on the 6x16 cylinder "
+                    "(periodic y, 96 sites, snake order), Sz=0 Neel start, maxdim %d, cutoff 1e-10, "
+                    "Davidson max %d iters (tol 1e-12 as hard-wired in the reference)" % (args.maxdim,
+                                                                                           args.max_restart),
+        "L": C5_N, "maxdim": args.maxdim, "cutoff": C5["cutoff"], "max_restart": args.max_restart,
+        "setup": "untimed ramp maxdim %s with noise 1e-6 -> 0 over those sweeps, one sweep at maxdim %d, "
+                 "checkpoint; per precision: load, buildEnv, centre to site %d" % (C5["ramp"], args.maxdim, C5_MID),
+        "step": "%d two-site updates at maxdim %d: left-to-right over sites %d..%d and back" % (
+            2 * args.block, args.maxdim, C5_MID, C5_MID + args.block - 1),
+        "value_definition": "mean seconds per timed two-site update x %d updates per sweep" % C5_UPDATES_PER_SWEEP,
+        "l2": "environments (tens of GB) far larger than L2; L2 flushed before every step",
+        "davidson_tol": 1e-12,
+    }
 
 
 def parse():
@@ -67,25 +101,20 @@ def parse():
     p.add_argument("--steps", type=int, default=3)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    p.add_argument("--e2e-steps", type=int, default=1)
-    p.add_argument("--cpu-budget", type=float, default=20.0, help="seconds of CPU baseline sampling")
+    p.add_argument("--workload", default="j1j2", choices=["j1j2", "heisenberg", "xxz-chains", "gemm"])
+    p.add_argument("--maxdim", type=int, default=C5["maxdim"])
+    p.add_argument("--max-restart", type=int, default=C5["max_restart"])
+    p.add_argument("--block", type=int, default=C5["block"])
+    p.add_argument("--e2e-steps", type=int, default=2)
+    p.add_argument("--cpu-budget", type=float, default=30.0, help="seconds of CPU baseline sampling (rank 0)")
+    p.add_argument("--ref-budget", type=float, default=240.0, help="seconds of timed updates of the reference arm")
     p.add_argument("--no-cpu-baseline", action="store_true")
-    p.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision (tcgen05 3xTF32) arm")
-    p.add_argument("--workload", default="heisenberg", choices=["heisenberg", "xxz-chains", "gemm", "j1j2"],
-                   help="heisenberg: the default sweep benchmark; xxz-chains: independent chains sharing the "
-                        "GPU; gemm: one single-block contraction per precision (kernel throughput); j1j2: "
-                        "FP64 vs mixed sweeps on the J1-J2 cylinder at --maxdim")
-    p.add_argument("--maxdim", type=int, default=1024)
-    p.add_argument("--nx", type=int, default=16)
-    p.add_argument("--ny", type=int, default=6)
-    p.add_argument("--breakdown", action="store_true")
-    p.add_argument("--profile-step", type=int, default=-1,
-                   help="j1j2: bracket this two-site step of the first timed sweep with a profiler range "
-                        "(for ncu --profile-from-start off)")
+    p.add_argument("--no-full-sweep", action="store_true")
+    p.add_argument("--breakdown", action="store_true", help="one further step per precision with phase times")
     p.add_argument("--gemm-size", type=int, default=4096)
     p.add_argument("--precisions", default="fp64,tf32x3,tf32")
-    p.add_argument("--chains", type=int, default=16)
-    p.add_argument("--chain-sweeps", type=int, default=3)
+    p.add_argument("--chains", type=int, default=64)
+    p.add_argument("--chain-sweeps", type=int, default=8)
     p.add_argument("--streams", type=int, default=16)
     return p.parse_args()
 
@@ -131,194 +160,361 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(rows)}
 
 
+def measured_peaks(torch):
+    """cuBLAS DGEMM (FP64 tensor path) and TF32 GEMM throughput, 8192^3, best of 3."""
+    n = 8192
+    out = {}
+    prev = torch.backends.cuda.matmul.allow_tf32
+    for name, dt, tf32 in (("fp64", torch.float64, False), ("tf32", torch.float32, True)):
+        torch.backends.cuda.matmul.allow_tf32 = tf32
+        a = torch.randn(n, n, dtype=dt, device="cuda")
+        b = torch.randn(n, n, dtype=dt, device="cuda")
+        for _ in range(2):
+            torch.matmul(a, b)
+        torch.cuda.synchronize()
+        best = 0.0
+        for _ in range(3):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            torch.matmul(a, b)
+            e1.record()
+            torch.cuda.synchronize()
+            best = max(best, 2.0 * n ** 3 / (e0.elapsed_time(e1) * 1e-3) / 1e12)
+        out[name] = best
+        del a, b
+    torch.backends.cuda.matmul.allow_tf32 = prev
+    torch.cuda.empty_cache()
+    return out
+
+
+def j1j2_autompo(tt_b200, Nx, Ny, J2):
+    a = tt_b200.AutoMPO()
+    for s1, s2, typ, *_ in tt_b200.square_next_neighbor(Nx, Ny, True, snake=True):
+        J = 1.0 if typ == 1 else J2
+        a.add(0.5 * J, "S+", s1 - 1, "S-", s2 - 1)
+        a.add(0.5 * J, "S-", s1 - 1, "S+", s2 - 1)
+        a.add(J, "Sz", s1 - 1, "Sz", s2 - 1)
+    return a
+
+
 # ---------------------------------------------------------------------------
-# CPU sample (oracle restatement) -- synthetic middle-bond two-site step
+# CPU restatement (oracle) on the J1-J2 cylinder at bond dimension 3072
 # ---------------------------------------------------------------------------
-# Converged state of this workload (deterministic): bond dimensions of the
-# L=100 chain after the maxdim-512 sweeps at cutoff 1e-12, and the 2Sz sectors
-# of the middle bonds (even and odd bond index).  The CPU sample runs two-site
-# steps on tensors with exactly these sectors, and the bond profile scales it
-# to a sweep.
-CONVERGED_BOND_DIMS = [
-    1, 2, 4, 8, 16, 32, 41, 52, 62, 68, 78, 78, 90, 90, 99, 101, 108, 111, 117, 120, 126, 127, 133, 133, 140,
-    142, 147, 148, 153, 153, 158, 157, 162, 162, 166, 167, 169, 171, 172, 174, 175, 177, 178, 180, 179, 181,
-    180, 182, 181, 182, 181, 182, 181, 182, 180, 181, 179, 180, 178, 177, 175, 174, 172, 171, 169, 167, 166,
-    162, 162, 157, 158, 153, 153, 148, 147, 142, 140, 133, 133, 127, 126, 120, 117, 111, 108, 101, 99, 90, 90,
-    78, 78, 68, 62, 52, 41, 32, 16, 8, 4, 2, 1]
-MID_SECTORS_EVEN = [(-6, 2), (-4, 16), (-2, 43), (0, 60), (2, 42), (4, 16), (6, 2)]
-MID_SECTORS_ODD = [(-5, 6), (-3, 29), (-1, 56), (1, 56), (3, 29), (5, 6)]
+class OracleMidChain:
+    """Real two-site updates of the oracle (update_site + update_env,
+    algos/dmrg/dmrg.cpp:300-372,491-509) at bond dimension chi in the middle
+    of the 96-site cylinder.  The state is the Neel product state of the
+    reference's product-state constructor (mps/qtt.cpp:205-311) with sites
+    m-w .. m-1 replaced by random left-canonical and sites m+2 .. m+1+w by
+    random right-canonical isometries whose bonds grow to chi (sector
+    dimensions binomial, scaled down proportionally once above chi), and a
+    random two-site pair at m, m+1; the environments are contracted through
+    it with the J1-J2 MPO exactly as buildEnv does, so H_eff is the true
+    effective Hamiltonian of that state (Hermitian, identity norm)."""
+
+    def __init__(self, chi, max_restart, cutoff=1e-10, w=12, seed=0):
+        import numpy as np
+        from oracle import autompo as am, qdmrg
+        from oracle.qtensor import QIndex, QTensor, Inward, Outward, Link, qadd
+        self.np, self.qdmrg = np, qdmrg
+        self.chi, self.max_restart, self.cutoff = chi, max_restart, cutoff
+        rng = np.random.default_rng(seed)
+        self.rng = rng
+        N, m = C5_N, C5_MID
+        self.m = m
+        a = am.AutoMPO()
+        for s1, s2, t, *_ in am.snake_relabel(am.square_next_neighbor(C5["Nx"], C5["Ny"], True), C5["Nx"], C5["Ny"]):
+            J = 1.0 if t == 1 else C5["J2"]
+            a.add(0.5 * J, "S+", s1 - 1, "S-", s2 - 1)
+            a.add(0.5 * J, "S-", s1 - 1, "S+", s2 - 1)
+            a.add(J, "Sz", s1 - 1, "Sz", s2 - 1)
+        self.H = am.build_qmpo(a, N)
+        psi = qdmrg.QMPS(N, qdmrg.neel(N))
+        self.psi = psi
+        phy = psi.phy_qn
+        st = qdmrg.neel(N)
+        cum = [(0, 0)]
+        for i in range(N):
+            cum.append(qadd(cum[-1], phy[st[i]]))
+
+        def cap(d):
+            # proportional to the binomial counts, exactly chi in all
+            # (largest remainders), empty sectors dropped
+            tot = sum(d.values())
+            if tot <= chi:
+                return dict(d)
+            share = {q: v * chi / tot for q, v in d.items()}
+            out = {q: int(s) for q, s in share.items()}
+            for q in sorted(share, key=lambda q: (out[q] - share[q], q))[:chi - sum(out.values())]:
+                out[q] += 1
+            return {q: v for q, v in out.items() if v > 0}
+
+        def window(i_from, i_to, step):
+            if step > 0:
+                prev, active, sites = psi.A[i_from].idx[0].copy(), {cum[i_from]: 1}, range(i_from, i_to)
+            else:
+                prev, active, sites = psi.A[i_from].idx[2].copy(), {cum[i_from + 1]: 1}, range(i_from, i_to, -1)
+            for i in sites:
+                nd = {}
+                for q, d in active.items():
+                    for p in phy:
+                        qq = qadd(q, p) if step > 0 else (q[0] - p[0], q[1] - p[1])
+                        nd[qq] = nd.get(qq, 0) + d
+                nd = cap(nd)
+                new = QIndex(Outward, psi.link_name(i + 1), Link, 0) if step > 0 else \
+                    QIndex(Inward, psi.link_name(i), Link, 0)
+                for q in sorted(nd):
+                    new.add_qn(q, nd[q])
+                T = QTensor([prev, psi.A[i].idx[1].copy(), new] if step > 0 else [new, psi.A[i].idx[1].copy(), prev])
+                T.init_block()
+                oa, na = (0, 2) if step > 0 else (2, 0)
+                groups = {}
+                for b, qi in enumerate(T.bqi):
+                    if T.idx[oa].qn(qi[oa]) in active:
+                        groups.setdefault(qi[na], []).append(b)
+                for bl in groups.values():
+                    shapes = [T.blocks[b].shape for b in bl]
+                    rows = [s[0] * s[1] if step > 0 else s[1] * s[2] for s in shapes]
+                    ncol = shapes[0][2] if step > 0 else shapes[0][0]
+                    Q, _ = np.linalg.qr(rng.standard_normal((sum(rows), ncol)))
+                    off = 0
+                    for b, r, s in zip(bl, rows, shapes):
+                        blk = Q[off:off + r]
+                        off += r
+                        T.blocks[b][...] = (blk if step > 0 else blk.T).reshape(s, order="F")
+                psi.A[i] = T
+                prev, active = new.dagged(), nd
+            return prev, active
+
+        lidx, lact = window(m - w, m, +1)
+        ridx, ract = window(m + 1 + w, m + 1, -1)
+        md = {}
+        for q, d in lact.items():
+            for p in phy:
+                qq = qadd(q, p)
+                if any(qadd(qq, p2) in ract for p2 in phy):
+                    md[qq] = md.get(qq, 0) + d
+        mid = QIndex(Outward, psi.link_name(m + 1), Link, 0)
+        for q, d in sorted(cap(md).items()):
+            mid.add_qn(q, d)
+        Am = QTensor([lidx, psi.A[m].idx[1].copy(), mid])
+        An = QTensor([mid.dagged(), psi.A[m + 1].idx[1].copy(), ridx])
+        for T in (Am, An):
+            T.init_block()
+            for b in T.blocks:
+                b[...] = rng.standard_normal(b.shape)
+        psi.A[m], psi.A[m + 1] = Am, An
+        self.bond_dims = (sum(lact.values()), mid.dim(), sum(ract.values()))
+        TL, TR = [None] * N, [None] * N
+        TL[0] = qdmrg._boundary(psi.A[0].idx[0], self.H.A[0].idx[0])
+        for i in range(m):
+            TL[i + 1] = qdmrg.env_step(TL[i], psi.A[i], self.H.A[i])
+        TR[N - 1] = qdmrg._boundary(psi.A[N - 1].idx[-1], self.H.A[N - 1].idx[-1])
+        for i in range(N - 1, m + 1, -1):
+            TR[i - 1] = qdmrg.env_step(TR[i], psi.A[i], self.H.A[i])
+        self.TL, self.TR = TL, TR
+        self.k = 0
+
+    def update(self):
+        """One two-site update: left-to-right at m, then right-to-left at m+1, alternately."""
+        from oracle import qsvd
+        q = self.qdmrg
+        if self.k % 2 == 0:
+            e = q.update_site(self.psi, self.H, self.TR, self.TL, self.m, qsvd.MoveFromLeft, self.chi, self.cutoff,
+                              3, self.max_restart, self.rng)
+            q.update_env(self.psi, self.H, self.TR, self.TL, self.m, qsvd.MoveFromLeft)
+        else:
+            e = q.update_site(self.psi, self.H, self.TR, self.TL, self.m + 1, qsvd.MoveFromRight, self.chi,
+                              self.cutoff, 3, self.max_restart, self.rng)
+            q.update_env(self.psi, self.H, self.TR, self.TL, self.m + 1, qsvd.MoveFromRight)
+        self.k += 1
+        return e
 
 
-def cpu_step_sample(budget_s: float, seed: int = 0):
-    """Time full two-site steps (Davidson + block SVD + environment update) of
-    the oracle at maxdim 512 on synthetic tensors with middle-bond structure.
-    Returns (mean seconds per step, steps timed)."""
-    import numpy as np
-    from oracle import qdmrg, qsvd
-    from oracle.davidson import tensor_davidsonIT
-    from oracle.qtensor import QIndex, QTensor, Inward, Outward, Link, Site, contract, qn
-    rng = np.random.default_rng(seed)
-    H = qdmrg.QMPO(8)
-    site = 4
-
-    def link(name, arrow, parity):
-        ix = QIndex(arrow, name, Link, 0)
-        for q, d in (MID_SECTORS_ODD if parity else MID_SECTORS_EVEN):
-            ix.add_qn(qn(q), d)
-        return ix
-
-    lA = link("ID1Link%d" % site, Inward, 0)
-    mAB = link("ID1Link%d" % (site + 1), Outward, 1)
-    rB = link("ID1Link%d" % (site + 2), Outward, 0)
-    s1 = QIndex(Inward, "Site%d" % site, Site, 0)
-    s2 = QIndex(Inward, "Site%d" % (site + 1), Site, 0)
-    for p in qdmrg.SPIN_PHY_QN:
-        s1.add_qn(p, 1)
-        s2.add_qn(p, 1)
-
-    def rand(idx):
-        T = QTensor(idx)
-        T.init_block()
-        for b in T.blocks:
-            b[...] = rng.standard_normal(b.shape)
-        return T
-
-    Al = rand([lA, s1, mAB])
-    Ar = rand([mAB.dagged(), s2, rB])
-    Wl, Wr = H.A[site], H.A[site + 1]
-    lp = lA.dagged()
-    lp.level = 1
-    TL = rand([QIndex(Inward, lA.name, Link, 1, list(lA.qns)), Wl.idx[0].dagged(), lA.dagged()])
-    TR = rand([QIndex(Outward, rB.name, Link, 1, list(rB.qns)), Wr.idx[3].dagged(), rB.dagged()])
+def oracle_updates(chi, max_restart, budget_s, max_updates, seed=0):
+    """Set-up (untimed) plus timed oracle updates until the budget is spent
+    (at least one).  Returns (mean seconds per update, updates timed, set-up seconds, bond dims)."""
+    t0 = time.perf_counter()
+    om = OracleMidChain(chi, max_restart, seed=seed)
+    setup = time.perf_counter() - t0
     times = []
     t_start = time.perf_counter()
-    while True:
-        t0 = time.perf_counter()
-        A = qdmrg.BigQTensor()
-        A.setLeft(TL)
-        A.addMid(Wl)
-        A.addMid(Wr)
-        A.setRight(TR)
-        x = contract(Al, Ar)
-        tensor_davidsonIT(A, x, 3, MAX_RESTART, 1e-12, rng=rng)
-        mid = [ix for ix in Al.idx if ix.name == mAB.name][0]
-        U, V, S = qsvd.svd_bond(x, Al, Ar, mid, qsvd.MoveFromLeft, CUTOFF, MAXM)
-        qdmrg.env_step(TL, U, Wl)
-        times.append(time.perf_counter() - t0)
-        if time.perf_counter() - t_start > budget_s or len(times) >= 50:
+    while len(times) < max(1, max_updates):
+        t1 = time.perf_counter()
+        om.update()
+        times.append(time.perf_counter() - t1)
+        if time.perf_counter() - t_start + statistics.mean(times) > budget_s:
             break
-    return statistics.mean(times), len(times)
+    return statistics.mean(times), len(times), setup, om.bond_dims
 
 
-def sweep_profile_factor(bond_dims) -> float:
-    """Mean cost of a sweep's two-site steps relative to the sampled middle
-    step: a step on bonds (a, b) of the two-site tensor costs ~ a*b*(a+b)."""
-    def cost(a, b):
-        return a * b * (a + b)
-    mid = len(bond_dims) // 2
-    ref = cost(bond_dims[mid - 1], bond_dims[mid + 1])
-    L = len(bond_dims) - 1
-    return sum(cost(bond_dims[l], bond_dims[l + 2]) for l in range(L - 1)) / (L - 1) / ref
-
-
-def cpu_baseline(budget_s: float, bond_dims=None):
-    import os as _os
-    bond_dims = bond_dims or CONVERGED_BOND_DIMS
-    t_step, n = cpu_step_sample(budget_s)
-    steps_per_sweep = 2 * (L_SITES - 1)
-    f = sweep_profile_factor(bond_dims)
-    val = t_step * steps_per_sweep * f
-    return {"value": val, "unit": "s/sweep", "cores": _os.cpu_count(), "kind": "port",
-            "sample": "%d two-site steps (Davidson 6 iters + block SVD + env update) on tensors with the "
-                      "converged middle-bond sectors (bond dim 181/182), %.3f s/step, scaled by %d steps/sweep "
-                      "x bond-profile factor %.3f" % (n, t_step, steps_per_sweep, f)}
-
-
-# ---------------------------------------------------------------------------
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    for _ in range(args.warmup):
-        cpu_step_sample(0.0, seed=1)
-    vals = []
-    budget = max(5.0, 60.0 / max(1, args.steps))
-    for k in range(args.steps):
-        vals.append(cpu_baseline(budget))
-    value = statistics.mean(v["value"] for v in vals)
-    line = {"metric": METRIC, "value": value, "unit": "s/sweep", "n_gpus": args.gpus, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": value * 1e3, "higher_is_better": False,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": CONFIG, "impl": "reference",
-            "cpu_baseline": {"value": value, "unit": "s/sweep", "cores": os.cpu_count(), "kind": "port",
-                             "sample": vals[-1]["sample"]},
+    if args.workload == "heisenberg":
+        return run_heisenberg_reference(args)
+    t_upd, n, setup, dims = oracle_updates(args.maxdim, args.max_restart, args.ref_budget, args.steps)
+    value = t_upd * C5_UPDATES_PER_SWEEP
+    sample = ("%d real oracle two-site updates (Davidson max %d iters + block SVD + environment update) at bond "
+              "dims %s in the middle of the 96-site cylinder, %.1f s each (set-up %.0f s untimed); warm-up skipped "
+              "(no compilation on the host path); updates capped by a %.0f s budget" %
+              (n, args.max_restart, dims, t_upd, setup, args.ref_budget))
+    cores = os.cpu_count()
+    line = {"metric": METRIC, "value": value, "unit": "s/sweep", "n_gpus": args.gpus, "steps": n,
+            "warmup": 0, "ms_per_step": t_upd * 1e3, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": c5_config(args),
+            "impl": "reference",
+            "cpu_baseline": {"value": value, "unit": "s/sweep", "cores": cores, "kind": "port", "sample": sample},
             "e2e": {"value": value, "unit": "s/sweep", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
 
 
-def fp64_peak_tflops(torch):
-    n = 8192
-    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
-    b = torch.randn(n, n, dtype=torch.float64, device="cuda")
-    for _ in range(2):
-        torch.matmul(a, b)
-    torch.cuda.synchronize()
-    best = 0.0
-    for _ in range(3):
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
-        torch.matmul(a, b)
-        e1.record()
-        torch.cuda.synchronize()
-        best = max(best, 2.0 * n ** 3 / (e0.elapsed_time(e1) * 1e-3) / 1e12)
-    del a, b
-    torch.cuda.empty_cache()
-    return best
-
-
-def mixed_arm(args, ctx, stream, flush, e_fp64, torch, tt_b200, qdmrg):
-    """The same schedule with H_eff*x and the environment updates in the
-    automatic mixed form (3xTF32 on tcgen05 for the contractions the cost
-    model predicts faster there, FP64 DMMA for the rest; GS, Rayleigh-Ritz,
-    SVD in FP64; sweep energy <psi|H|psi> contracted in FP64), timed like the
-    FP64 arm."""
-    tt_b200.set_precision(heff="tf32x3-auto", env="tf32x3-auto")
+# ---------------------------------------------------------------------------
+# GPU arm on the J1-J2 cylinder
+# ---------------------------------------------------------------------------
+def c5_setup(tt_b200, H, args, workdir):
+    """Untimed ramp in the chosen form, one sweep at maxdim, checkpoint."""
+    from oracle import qdmrg
+    tt_b200.set_precision(heff=CHOSEN, env=CHOSEN)
+    t0 = time.perf_counter()
     try:
-        psi = tt_b200.QMPS(L_SITES, qdmrg.neel(L_SITES))
-        run = tt_b200.QDMRG(psi, tt_b200.QMPO(L_SITES))
-        for m in RAMP:
-            run.sweep(m, CUTOFF, MAX_RESTART)
+        psi = tt_b200.QMPS(C5_N, qdmrg.neel(C5_N))
+        run = tt_b200.QDMRG(psi, H)
+        energies = []
+        n = len(C5["ramp"])
+        for k, m in enumerate(C5["ramp"]):
+            energies.append(run.sweep(m, C5["cutoff"], args.max_restart, C5["noise0"] * (1.0 - k / n)))
+        energies.append(run.sweep(args.maxdim, C5["cutoff"], args.max_restart, 0.0))
+        run.finish()
+    finally:
+        tt_b200.set_precision()
+    ck = os.path.join(workdir, "c5_start")
+    psi.save(ck)
+    info = {"ramp_seconds": time.perf_counter() - t0, "ramp_energies": energies,
+            "start_bond_dims_mid": psi.bond_dims()[C5_MID - 1:C5_MID + args.block + 2]}
+    del run, psi
+    return ck + ".ttmps", info
+
+
+def c5_arm(prec, ck, H, args, ctx, stream, flush, torch, tt_b200, sampler=None, e2e_steps=0):
+    """Load, centre to the block, W warm-up and K timed block steps (CUDA
+    events on the library stream, L2 flushed before each), then the FP64
+    energy, optional end-to-end steps and a full sweep."""
+    tt_b200.set_precision(heff=prec, env=prec)
+    res = {"precision": prec}
+    B, mid = args.block, C5_MID
+    cut, mr, md = C5["cutoff"], args.max_restart, args.maxdim
+    try:
+        psi = tt_b200.QMPS.load(ck)
+        run = tt_b200.QDMRG(psi, H)
+        run.walk(mid, md, cut, mr)
+
+        def step():
+            run.walk(mid + B, md, cut, mr)
+            return run.walk(mid, md, cut, mr)
+
         for _ in range(args.warmup):
-            run.sweep(MAXM, CUTOFF, MAX_RESTART)
-        st0 = run.stats()
-        total_ms, energy = 0.0, None
+            step()
+        ctx.sync()
+        st0, fb0, l0 = run.stats(), tt_b200.davidson_fallbacks(), ctx.launches()
+        s0 = len(run.steps())
+        if sampler:
+            sampler.start()
+        times = []
         for _ in range(args.steps):
             flush.zero_()
             torch.cuda.synchronize()
-            e0 = torch.cuda.Event(enable_timing=True)
-            e1 = torch.cuda.Event(enable_timing=True)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(stream)
-            energy = run.sweep(MAXM, CUTOFF, MAX_RESTART)
+            step()
             e1.record(stream)
             e1.synchronize()
-            total_ms += e0.elapsed_time(e1)
-        st1 = run.stats()
+            times.append(e0.elapsed_time(e1) * 1e-3)
+        ctx.sync()
+        clocks = sampler.stop() if sampler else None
+        st1, launches = run.stats(), ctx.launches() - l0
+        steps = run.steps()[s0:]
+        t_step = statistics.mean(times)
+        upd = 2 * B
+        fl = st1["heff_flops"] - st0["heff_flops"]
+        hs = st1["heff_seconds"] - st0["heff_seconds"]
+        res.update({
+            "value": t_step / upd * C5_UPDATES_PER_SWEEP, "unit": "s/sweep", "ms_per_step": t_step * 1e3,
+            "step_seconds": times, "s_per_update": t_step / upd,
+            "heff_tflops": fl / hs / 1e12 if hs > 0 else 0.0,
+            "heff_share_of_step": hs / sum(times) if times else None,
+            "heff_tflop_per_step": fl / max(1, args.steps) / 1e12,
+            "gpu_launches": int(launches), "launches_per_step": launches / max(1, args.steps),
+            "davidson_fallbacks": tt_b200.davidson_fallbacks() - fb0,
+            "matvecs_per_update": statistics.mean(s["matvecs"] for s in steps) if steps else None,
+            "trunc_err_mean": statistics.mean(s["trunc_err"] for s in steps) if steps else None,
+            "kept": [s["kept"] for s in steps[-upd:]],
+            "bond_dims_block": psi.bond_dims()[mid:mid + B + 2],
+            "clocks": clocks,
+        })
+        pool = ctx.memory()
+        res["device_memory_gb"] = {"in_use": pool[0] / 2 ** 30, "high_water": pool[1] / 2 ** 30,
+                                   "reserved": pool[2] / 2 ** 30}
+        if args.breakdown:
+            lib = tt_b200.lib
+            lib.tt_dmrg_set_profiling(1)
+            n0 = len(run.profile())
+            try:
+                step()
+            finally:
+                lib.tt_dmrg_set_profiling(0)
+            prof = run.profile()[n0:]
+            res["breakdown_s_per_update"] = {
+                "davidson": statistics.mean(p[1] for p in prof), "svd": statistics.mean(p[2] for p in prof),
+                "env": statistics.mean(p[3] for p in prof), "largest_svd_sector": max(p[0] for p in prof)}
+        # FP64 energy of the state after the identical schedule
+        tt_b200.set_precision()
+        res["energy"] = psi.expectation(H) / psi.overlap()
+        tt_b200.set_precision(heff=prec, env=prec)
+        if e2e_steps > 0:
+            # through the public C ABI: the block's site tensors from pinned host memory every step
+            first, last = mid, mid + B + 2
+            n_el = psi.sites_size(first, last)
+            host = torch.empty(n_el, dtype=torch.float64, pin_memory=True).numpy()
+            psi.get_sites(first, last, host)
+            e2e, h2d = [], []
+            for _ in range(e2e_steps):
+                ctx.sync()
+                t0 = time.perf_counter()
+                psi.set_sites(first, last, host)
+                step()
+                n_el = psi.sites_size(first, last)
+                if host.size != n_el:
+                    host = torch.empty(n_el, dtype=torch.float64, pin_memory=True).numpy()
+                psi.get_sites(first, last, host)
+                e2e.append(time.perf_counter() - t0)
+                h2d.append(n_el * 8)
+            t = statistics.mean(e2e)
+            res["e2e"] = {"value": t / upd * C5_UPDATES_PER_SWEEP, "unit": "s/sweep",
+                          "h2d_bytes_per_step": int(statistics.mean(h2d)), "d2h_bytes_per_step": int(statistics.mean(h2d)),
+                          "ms_per_step": t * 1e3,
+                          "includes": "host->device copy of the block's %d site tensors from pinned memory, the "
+                                      "%d-update block step, device->host copy of the updated tensors" % (B + 2, upd)}
+        if not args.no_full_sweep:
+            run.walk(0, md, cut, mr)
+            ctx.sync()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            e_sweep = run.sweep(md, cut, mr)
+            e1.record(stream)
+            e1.synchronize()
+            res["full_sweep"] = {"seconds": e0.elapsed_time(e1) * 1e-3, "energy": e_sweep,
+                                 "max_bond_dim": max(psi.bond_dims())}
+        del run, psi
     finally:
         tt_b200.set_precision()
-    fl = st1["heff_flops"] - st0["heff_flops"]
-    hs = st1["heff_seconds"] - st0["heff_seconds"]
-    return {"precision": "tf32x3-auto: 3xTF32 tcgen05 or FP64 DMMA per contraction (cost model) for H_eff*x and "
-                         "environments; FP64 GS, Rayleigh-Ritz, SVD, sweep energy",
-            "value": total_ms * 1e-3 / args.steps, "unit": "s/sweep", "energy": energy,
-            "dE_per_site_vs_fp64": abs(energy - e_fp64) / L_SITES, "heff_tflops": fl / hs / 1e12 if hs > 0 else 0.0,
-            "bond_dims_mid": psi.bond_dims()[L_SITES // 2]}
+    return res
 
 
-def run_ours(args):
-    import numpy as np
+def run_c5(args):
     import torch
     import tt_b200
-    from oracle import qdmrg
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -328,111 +524,196 @@ def run_ours(args):
     if world > 1:
         import datetime
         import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=900))
 
     def barrier():
         torch.cuda.synchronize()
         if dist is not None:
             dist.barrier()
 
-    peak64 = fp64_peak_tflops(torch)
+    peaks = measured_peaks(torch)
     ctx = tt_b200.Context(local)
     stream = torch.cuda.ExternalStream(ctx.stream())
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
-    psi = tt_b200.QMPS(L_SITES, qdmrg.neel(L_SITES))
-    H = tt_b200.QMPO(L_SITES)
-    run = tt_b200.QDMRG(psi, H)
-    for m in RAMP:
-        run.sweep(m, CUTOFF, MAX_RESTART)
-    for _ in range(args.warmup):
-        run.sweep(MAXM, CUTOFF, MAX_RESTART)
-    st0 = run.stats()
-    l0 = ctx.launches()
-    sampler = ClockSampler(local)
-    barrier()
-    ctx.sync()
-    sampler.start()
-    total_ms = 0.0
-    energy = None
-    torch.cuda.profiler.start()  # an ncu --profile-from-start off capture sees the timed sweeps only
-    for _ in range(args.steps):
-        flush.zero_()
-        torch.cuda.synchronize()
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        energy = run.sweep(MAXM, CUTOFF, MAX_RESTART)
-        e1.record(stream)
-        e1.synchronize()
-        total_ms += e0.elapsed_time(e1)
-    ctx.sync()
-    torch.cuda.profiler.stop()
-    barrier()
-    clocks = sampler.stop()
-    launches = ctx.launches() - l0
-    st1 = run.stats()
-    t_max = total_ms
+    H = tt_b200.QMPO.from_autompo(j1j2_autompo(tt_b200, C5["Nx"], C5["Ny"], C5["J2"]), C5_N)
+    workdir = tempfile.mkdtemp(prefix="tt_c5_")
+    try:
+        ck, setup = c5_setup(tt_b200, H, args, workdir)
+        barrier()
+        sampler = ClockSampler(local)
+        chosen = c5_arm(CHOSEN, ck, H, args, ctx, stream, flush, torch, tt_b200, sampler=sampler,
+                        e2e_steps=args.e2e_steps)
+        barrier()
+        fp64 = c5_arm("fp64", ck, H, args, ctx, stream, flush, torch, tt_b200)
+        barrier()
+    finally:
+        shutil.rmtree(workdir, ignore_errors=True)
+    # replicas: every rank runs its own copy of the problem (the path does not
+    # shard); the reported time is the slowest rank's, per GPU
+    t_max = chosen["value"]
     if dist is not None:
-        t = torch.tensor([total_ms], device="cuda")
+        t = torch.tensor([t_max], device="cuda", dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         t_max = float(t.item())
-    sec_per_sweep = t_max * 1e-3 / (args.steps * world)
-    heff_flops = st1["heff_flops"] - st0["heff_flops"]
-    heff_s = st1["heff_seconds"] - st0["heff_seconds"]
-    achieved = heff_flops / heff_s / 1e12 if heff_s > 0 else 0.0
-    bond = psi.bond_dims()
-
-    # end to end through the C ABI: MPS host -> device, buildEnv + sweep, device -> host
-    n = psi.data_size()
-    host = torch.empty(n, dtype=torch.float64, pin_memory=True).numpy()
-    psi.get_data(host)
-    e2e_ms = []
-    for _ in range(max(1, args.e2e_steps)):
-        barrier()
-        t0 = time.perf_counter()
-        psi.set_data(host)
-        run2 = tt_b200.QDMRG(psi, H)
-        e_e2e = run2.sweep(MAXM, CUTOFF, MAX_RESTART)
-        run2.finish()
-        psi.get_data(host)
-        e2e_ms.append((time.perf_counter() - t0) * 1e3)
-        del run2
-    e2e_val = statistics.mean(e2e_ms) * 1e-3 / world
-    mixed = None if args.no_mixed else mixed_arm(args, ctx, stream, flush, energy, torch, tt_b200, qdmrg)
-
     out = None
     if rank == 0:
-        cpu = None if args.no_cpu_baseline else cpu_baseline(args.cpu_budget, bond)
+        cpu = None
+        if not args.no_cpu_baseline:
+            t_upd, n, setup_s, dims = oracle_updates(args.maxdim, args.max_restart, args.cpu_budget, 1)
+            cpu = {"value": t_upd * C5_UPDATES_PER_SWEEP, "unit": "s/sweep", "cores": os.cpu_count(),
+                   "kind": "port",
+                   "sample": "%d real oracle two-site update(s) at bond dims %s in the middle of the cylinder "
+                             "(%.1f s each; set-up %.0f s untimed) x %d updates per sweep" % (
+                                 n, dims, t_upd, setup_s, C5_UPDATES_PER_SWEEP)}
+        de = abs(chosen["energy"] - fp64["energy"]) / C5_N
+        chosen["dE_per_site_vs_fp64"] = de
+        chosen["speedup_vs_fp64"] = fp64["value"] / chosen["value"]
+        if "full_sweep" in chosen and "full_sweep" in fp64:
+            chosen["full_sweep"]["speedup_vs_fp64"] = fp64["full_sweep"]["seconds"] / chosen["full_sweep"]["seconds"]
+            chosen["full_sweep"]["dE_per_site_vs_fp64"] = abs(chosen["full_sweep"]["energy"] -
+                                                              fp64["full_sweep"]["energy"]) / C5_N
+        chosen["roofline"] = {
+            "bound": "tensor", "kernel": "H_eff*x: grouped_tc_persist (3xTF32 tcgen05) for L*x and *R, "
+                                         "grouped_dgemm (FP64) for the middle contraction",
+            "achieved": chosen["heff_tflops"], "peak": peaks["tf32"] / 3.0, "unit": "TFLOP/s",
+            "frac": chosen["heff_tflops"] / (peaks["tf32"] / 3.0),
+            "peak_source": "cuBLAS TF32 GEMM 8192^3 measured in this run (%.1f TFLOP/s) / 3: each algorithmic "
+                           "3xTF32 flop is three TF32 products" % peaks["tf32"],
+            "tf32_products_frac": 3.0 * chosen["heff_tflops"] / peaks["tf32"], "traffic": None}
+        fp64["roofline"] = {
+            "bound": "tensor", "kernel": "H_eff*x: grouped_dgemm (DMMA), 3 launches per product",
+            "achieved": fp64["heff_tflops"], "peak": peaks["fp64"], "unit": "TFLOP/s",
+            "frac": fp64["heff_tflops"] / peaks["fp64"],
+            "peak_source": "cuBLAS DGEMM 8192^3 measured in this run", "traffic": None}
         out = {
-            "metric": METRIC, "value": sec_per_sweep, "unit": "s/sweep", "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec_per_sweep * 1e3,
-            "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic", "config": dict(CONFIG, parallelism="replicas" if world > 1 else "single",
-                                                 energy=energy, bond_dims_mid=bond[L_SITES // 2]),
-            "heff_tflops": achieved,
-            "roofline": {"bound": "tensor", "kernel": "grouped_dgemm (3 launches per H_eff*x)",
-                         "achieved": achieved, "peak": peak64, "unit": "TFLOP/s",
-                         "frac": achieved / peak64 if peak64 else None,
-                         "peak_source": "cuBLAS DGEMM 8192^3 measured in this run (FP64 tensor path)",
-                         # dram__bytes_read.sum + dram__bytes_write.sum per grouped_dgemm
-                         # launch: mean of three launches captured mid-sweep by ncu on this
-                         # workload (profiles/grouped_dgemm_heisenberg_L100_maxdim512.md)
-                         "traffic": 364544, "traffic_unit": "bytes per launch"},
+            "metric": METRIC, "value": t_max, "unit": "s/sweep", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": chosen["ms_per_step"], "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "tf32x3+f64", "data": "synthetic",
+            "config": dict(c5_config(args), precision=CHOSEN + ": 3xTF32 tcgen05 or FP64 DMMA per contraction "
+                           "(cost model) for H_eff*x and environments; FP64 Gram-Schmidt, Rayleigh-Ritz, block "
+                           "SVD and energies", parallelism="replicas" if world > 1 else "single", **setup),
+            "heff_tflops": chosen["heff_tflops"],
+            "roofline": chosen["roofline"],
             "cpu_baseline": cpu,
-            "e2e": {"value": e2e_val, "unit": "s/sweep", "h2d_bytes_per_step": int(n * 8),
-                    "d2h_bytes_per_step": int(n * 8),
-                    "includes": "MPS upload, position/normalize/buildEnv, one sweep, position(0), MPS download"},
-            "gpu_launches": int(launches),
-            "clocks": clocks,
-            "mixed": mixed,
+            "e2e": chosen.get("e2e"),
+            "gpu_launches": chosen["gpu_launches"],
+            "clocks": chosen["clocks"],
+            "mixed": chosen,
+            "fp64": fp64,
+            "peaks_measured": peaks,
         }
         print(json.dumps(out))
-    del run, psi, H
     ctx.close()
     if dist is not None:
         dist.destroy_process_group()
 
 
+# ---------------------------------------------------------------------------
+# secondary workload: Heisenberg chain L = 100 to maxdim 512
+# ---------------------------------------------------------------------------
+HEIS = dict(L=100, ramp=(32, 64, 128, 256), maxdim=512, cutoff=1e-12, max_restart=6)
+
+
+def heis_config():
+    return {"workload": "U(1) two-site DMRG, spin-1/2 Heisenberg chain J=1 OBC L=100, Sz=0 Neel start, maxdim 512 "
+                        "(after untimed ramp 32,64,128,256), cutoff 1e-12, Davidson max 6 iters (tol 1e-12 as "
+                        "hard-wired in the reference; the configuration's 1e-11 is looser)",
+            "L": HEIS["L"], "maxdim": HEIS["maxdim"], "cutoff": HEIS["cutoff"], "max_restart": HEIS["max_restart"],
+            "step": "one full sweep (L->R + R->L, 2x99 two-site updates)",
+            "l2": "L2 flushed before each timed sweep"}
+
+
+def oracle_heisenberg_sweeps(budget_s):
+    """The oracle's own schedule: untimed ramp 32..256, then timed full sweeps
+    at maxdim 512 until the budget is spent (at least one)."""
+    from oracle import qdmrg
+    L = HEIS["L"]
+    psi = qdmrg.QMPS(L, qdmrg.neel(L))
+    H = qdmrg.QMPO(L)
+    t0 = time.perf_counter()
+    qdmrg.dmrg(psi, H, len(HEIS["ramp"]), list(HEIS["ramp"]), [HEIS["cutoff"]], [HEIS["max_restart"]])
+    setup = time.perf_counter() - t0
+    times = []
+    while True:
+        t1 = time.perf_counter()
+        qdmrg.dmrg(psi, H, 1, [HEIS["maxdim"]], [HEIS["cutoff"]], [HEIS["max_restart"]])
+        times.append(time.perf_counter() - t1)
+        if sum(times) + statistics.mean(times) > budget_s:
+            break
+    return statistics.mean(times), len(times), setup
+
+
+def run_heisenberg_reference(args):
+    t, n, setup = oracle_heisenberg_sweeps(args.ref_budget)
+    print(json.dumps({"metric": METRIC, "value": t, "unit": "s/sweep", "n_gpus": args.gpus, "steps": n,
+                      "warmup": 0, "ms_per_step": t * 1e3, "higher_is_better": False, "scaling": "weak",
+                      "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": heis_config(),
+                      "impl": "reference",
+                      "cpu_baseline": {"value": t, "unit": "s/sweep", "cores": os.cpu_count(), "kind": "port",
+                                       "sample": "%d full oracle sweeps at maxdim 512 after its own ramp (%.0f s "
+                                                 "untimed)" % (n, setup)},
+                      "e2e": {"value": t, "unit": "s/sweep", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+
+
+def run_heisenberg(args):
+    import torch
+    import tt_b200
+    from oracle import qdmrg
+    L = HEIS["L"]
+    ctx = tt_b200.Context(0)
+    stream = torch.cuda.ExternalStream(ctx.stream())
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    peaks = measured_peaks(torch)
+    out = {}
+    for prec in ("fp64", CHOSEN):
+        tt_b200.set_precision(heff=prec, env=prec)
+        try:
+            psi = tt_b200.QMPS(L, qdmrg.neel(L))
+            H = tt_b200.QMPO(L)
+            run = tt_b200.QDMRG(psi, H)
+            for m in HEIS["ramp"]:
+                run.sweep(m, HEIS["cutoff"], HEIS["max_restart"])
+            for _ in range(args.warmup):
+                run.sweep(HEIS["maxdim"], HEIS["cutoff"], HEIS["max_restart"])
+            st0, l0 = run.stats(), ctx.launches()
+            ms, energy = [], None
+            for _ in range(args.steps):
+                flush.zero_()
+                torch.cuda.synchronize()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                energy = run.sweep(HEIS["maxdim"], HEIS["cutoff"], HEIS["max_restart"])
+                e1.record(stream)
+                e1.synchronize()
+                ms.append(e0.elapsed_time(e1))
+            st1 = run.stats()
+            fl, hs = st1["heff_flops"] - st0["heff_flops"], st1["heff_seconds"] - st0["heff_seconds"]
+            out[prec] = {"value": statistics.mean(ms) * 1e-3, "unit": "s/sweep", "energy": energy,
+                         "heff_tflops": fl / hs / 1e12 if hs else 0.0, "launches_per_sweep":
+                             (ctx.launches() - l0) / max(1, args.steps), "bond_dims_mid": psi.bond_dims()[L // 2]}
+            del run, psi, H
+        finally:
+            tt_b200.set_precision()
+    ctx.close()
+    f = out["fp64"]
+    cpu = None
+    if not args.no_cpu_baseline:
+        t, n, setup = oracle_heisenberg_sweeps(args.cpu_budget)
+        cpu = {"value": t, "unit": "s/sweep", "cores": os.cpu_count(), "kind": "port",
+               "sample": "%d full oracle sweeps at maxdim 512 after its own ramp (%.0f s untimed)" % (n, setup)}
+    out[CHOSEN]["dE_per_site_vs_fp64"] = abs(out[CHOSEN]["energy"] - f["energy"]) / L
+    print(json.dumps({"metric": METRIC, "value": f["value"], "unit": "s/sweep", "n_gpus": 1, "steps": args.steps,
+                      "warmup": args.warmup, "ms_per_step": f["value"] * 1e3, "higher_is_better": False,
+                      "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                      "config": dict(heis_config(), precision="FP64 (plain GPU form)"),
+                      "heff_tflops": f["heff_tflops"],
+                      "roofline": {"bound": "tensor", "kernel": "grouped_dgemm", "achieved": f["heff_tflops"],
+                                   "peak": peaks["fp64"], "unit": "TFLOP/s", "frac": f["heff_tflops"] / peaks["fp64"],
+                                   "peak_source": "cuBLAS DGEMM 8192^3 measured in this run", "traffic": None},
+                      "cpu_baseline": cpu, "mixed": out[CHOSEN], "peaks_measured": peaks}))
+
+
+# ---------------------------------------------------------------------------
 def run_chains(args):
     """Independent XXZ chains with site fields (the batched-chains configuration:
     L ~ U{32..128}, Delta ~ U[0.5, 1.5], h_i ~ U[-0.1, 0.1], seed 7, Sz=0 Neel
@@ -532,151 +813,22 @@ def run_gemm(args):
     ctx.close()
 
 
-def planning_counters(tt_b200):
-    """Host seconds and calls spent in block-structure computation and in
-    contraction-plan creation on this thread so far."""
-    import ctypes as C
-    ts, tp = C.c_double(), C.c_double()
-    ns, np_ = C.c_int64(), C.c_int64()
-    tt_b200.lib.tt_dmrg_planning_counters(C.byref(ts), C.byref(ns), C.byref(tp), C.byref(np_))
-    return {"structure_s": ts.value, "structure_calls": ns.value, "plan_s": tp.value, "plan_calls": np_.value}
-
-
-def run_j1j2(args):
-    """FP64 against mixed precision at large bond dimension, on the J1-J2
-    cylinder configuration: spin-1/2 J1-J2 Heisenberg model (J1 = 1, J2 = 0.5)
-    on an Nx x Ny cylinder (periodic in y, square_next_neighbor ordering),
-    U(1) Sz = 0, Neel start, cutoff 1e-10, Davidson max 6 iterations.  One
-    FP64 ramp (maxdim doubling from 64 to --maxdim, noise 1e-6 decaying to 0
-    over its sweeps) builds the starting state, which is checkpointed; each
-    precision then loads it and runs W warm-up and K timed sweeps at
-    --maxdim (CUDA events on the library stream, L2 flushed before each).
-    With --breakdown one further sweep per precision runs with a
-    synchronisation between step phases and reports where its time goes."""
-    import torch
-    import tt_b200
-    from oracle import qdmrg
-    Nx, Ny, J2 = args.nx, args.ny, 0.5
-    N = Nx * Ny
-    a = tt_b200.AutoMPO()
-    for s1, s2, typ, *_ in tt_b200.square_next_neighbor(Nx, Ny, True):
-        J = 1.0 if typ == 1 else J2
-        a.add(0.5 * J, "S+", s1 - 1, "S-", s2 - 1)
-        a.add(0.5 * J, "S-", s1 - 1, "S+", s2 - 1)
-        a.add(J, "Sz", s1 - 1, "Sz", s2 - 1)
-    ctx = tt_b200.Context(0)
-    stream = torch.cuda.ExternalStream(ctx.stream())
-    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
-    H = tt_b200.QMPO.from_autompo(a, N)
-    cutoff, mr = 1e-10, MAX_RESTART
-    ramp = []
-    m = 64
-    while m < args.maxdim:
-        ramp.append(m)
-        m *= 2
-    noise = [1e-6 * (1.0 - k / max(1, len(ramp))) for k in range(len(ramp))]
-    t0 = time.perf_counter()
-    psi = tt_b200.QMPS(N, qdmrg.neel(N))
-    run = tt_b200.QDMRG(psi, H)
-    for m, nz in zip(ramp, noise):
-        run.sweep(m, cutoff, mr, nz)
-    run.finish()
-    t_ramp = time.perf_counter() - t0
-    tmpdir = tempfile.mkdtemp()
-    ck = os.path.join(tmpdir, "start")
-    psi.save(ck)
-    start_dims = psi.bond_dims()
-    del run, psi
-    out = {}
-    for prec in args.precisions.split(","):
-        if prec not in tt_b200.PRECISIONS:
-            continue
-        tt_b200.set_precision(heff=prec, env=prec)
-        try:
-            psi = tt_b200.QMPS.load(ck + ".ttmps")
-            run = tt_b200.QDMRG(psi, H)
-            for _ in range(args.warmup):
-                run.sweep(args.maxdim, cutoff, mr)
-            st0 = run.stats()
-            pc0 = planning_counters(tt_b200)
-            ms, e = 0.0, None
-            tt_b200.lib.tt_dmrg_set_profile_step(args.profile_step)
-            outliers = []
-            fb0 = tt_b200.davidson_fallbacks()
-            for it in range(args.steps):
-                if it == 1:
-                    tt_b200.lib.tt_dmrg_set_profile_step(-1)
-                n0 = len(run.steps())
-                flush.zero_()
-                torch.cuda.synchronize()
-                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-                e0.record(stream)
-                e = run.sweep(args.maxdim, cutoff, mr)
-                e1.record(stream)
-                e1.synchronize()
-                ms += e0.elapsed_time(e1)
-                # steps whose energy leaves the sweep's median by more than 1e-3: a damaged update
-                st = run.steps()[n0:]
-                emed = statistics.median(x["energy"] for x in st)
-                outliers += [dict(sweep=it, step=k, site=x["site"], direction=x["direction"], energy=x["energy"],
-                                  kept=x["kept"], matvecs=x["matvecs"], trunc_err=x["trunc_err"])
-                             for k, x in enumerate(st) if abs(x["energy"] - emed) > 1e-3 * abs(emed)]
-            tt_b200.lib.tt_dmrg_set_profile_step(-1)
-            pc1 = planning_counters(tt_b200)
-            st1 = run.stats()
-            fl = st1["heff_flops"] - st0["heff_flops"]
-            hs = st1["heff_seconds"] - st0["heff_seconds"]
-            res = {"s_per_sweep": ms * 1e-3 / args.steps, "energy": e, "heff_tflops": fl / hs / 1e12 if hs else 0.0,
-                   "heff_s_per_sweep": hs / args.steps, "heff_tflop_per_sweep": fl / args.steps / 1e12,
-                   "max_bond_dim": max(psi.bond_dims()),
-                   "host_planning_s_per_sweep": {k: (pc1[k] - pc0[k]) / args.steps for k in pc0},
-                   "davidson_fallbacks": tt_b200.davidson_fallbacks() - fb0, "outlier_steps": outliers[:8]}
-            if args.breakdown:
-                lib = tt_b200.lib
-                lib.tt_dmrg_set_profiling(1)
-                n0 = len(run.profile())
-                try:
-                    run.sweep(args.maxdim, cutoff, mr)
-                finally:
-                    lib.tt_dmrg_set_profiling(0)
-                prof = run.profile()[n0:]
-                res["breakdown_s"] = {"davidson": sum(p[1] for p in prof), "svd": sum(p[2] for p in prof),
-                                      "env": sum(p[3] for p in prof), "other": sum(p[4] for p in prof),
-                                      "largest_svd_sector": max(p[0] for p in prof)}
-            out[prec] = res
-            del run, psi
-        finally:
-            tt_b200.set_precision()
-    ref = out.get("fp64")
-    for prec, res in out.items():
-        if ref is not None and prec != "fp64":
-            res["dE_per_site_vs_fp64"] = abs(res["energy"] - ref["energy"]) / N
-            res["speedup_vs_fp64"] = ref["s_per_sweep"] / res["s_per_sweep"]
-    print(json.dumps({"metric": "sec/sweep: mixed precision vs FP64 at large bond dimension", "unit": "s/sweep",
-                      "higher_is_better": False, "n_gpus": 1, "data": "synthetic",
-                      "config": {"workload": "U(1) J1-J2 Heisenberg %dx%d cylinder (periodic y), J2=0.5, Sz=0 "
-                                             "Neel start, cutoff 1e-10, Davidson max 6 iters" % (Nx, Ny),
-                                 "maxdim": args.maxdim, "ramp": ramp, "ramp_noise": noise,
-                                 "ramp_seconds": t_ramp, "start_max_bond_dim": max(start_dims),
-                                 "steps": args.steps, "warmup": args.warmup,
-                                 "l2": "L2 flushed before each timed sweep"},
-                      "results": out}))
-    H = None
-    ctx.close()
-
-
 def main():
     args = parse()
     if args.impl == "reference":
-        run_reference(args)
+        if args.workload in ("j1j2", "heisenberg"):
+            run_reference(args)
+        else:
+            print(json.dumps({"impl": "reference", "unavailable": "the reference arm covers the j1j2 and "
+                                                                  "heisenberg workloads"}))
     elif args.workload == "xxz-chains":
         run_chains(args)
     elif args.workload == "gemm":
         run_gemm(args)
-    elif args.workload == "j1j2":
-        run_j1j2(args)
+    elif args.workload == "heisenberg":
+        run_heisenberg(args)
     else:
-        run_ours(args)
+        run_c5(args)
 
 
 if __name__ == "__main__":

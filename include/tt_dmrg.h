@@ -170,6 +170,13 @@ int tt_qmps_tensor(const tt_qmps* psi, int i, tt_qtensor** out);
 int tt_qmps_data_size(const tt_qmps* psi, int64_t* n);
 int tt_qmps_get_data(const tt_qmps* psi, double* host);
 int tt_qmps_set_data(tt_qmps* psi, const double* host);
+/* The same for the site tensors [first, last) only (their blocks in order):
+ * one asynchronous copy per contiguous run of blocks and one synchronisation,
+ * so a pinned host buffer moves at full bandwidth.  The reference keeps its
+ * qMPS in (distributed) host memory (mps/qtt.h:124-129). */
+int tt_qmps_sites_size(const tt_qmps* psi, int first, int last, int64_t* n);
+int tt_qmps_get_sites(const tt_qmps* psi, int first, int last, double* host);
+int tt_qmps_set_sites(tt_qmps* psi, int first, int last, const double* host);
 /* dh: L site fields (may be NULL), tE: energy shift */
 int tt_qmpo_heisenberg(int L, const double* dh, double tE, unsigned id, tt_qmpo** out);
 int tt_qmpo_destroy(tt_qmpo* H);

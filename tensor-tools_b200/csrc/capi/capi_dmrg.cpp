@@ -4,6 +4,8 @@
 #include <string>
 
 #include "../../../include/tt_dmrg.h"
+#include <cuda_runtime.h>
+
 #include "../host/dmrg_q.h"
 
 namespace tt {
@@ -419,6 +421,55 @@ int tt_qmps_set_data(tt_qmps* psi, const double* host) {
       }
     ttb::check(tt_ctx_synchronize(ttb::rt().ctx), "qmps set");
   });
+}
+
+namespace {
+// blocks of sites [first, last) in block order; one asynchronous copy per run
+// of blocks that are back to back in the arena, one synchronisation in all
+int copy_sites(const tt_qmps* psi, int first, int last, double* host, const double* src_host) {
+  TT_ARG(psi && (host || src_host) && first >= 0 && first <= last && last <= (int)psi->psi.length);
+  TT_GUARD({
+    tt_ctx* ctx = ttb::rt().ctx;
+    if (!ctx) throw std::runtime_error("no device context bound");
+    cudaStream_t st = nullptr;
+    ttb::check(tt_ctx_stream(ctx, reinterpret_cast<void**>(&st)), "stream");
+    int64_t pos = 0;
+    for (int i = first; i < last; ++i) {
+      const ttb::qtensor& A = psi->psi.A[i];
+      size_t b = 0;
+      while (b < A.blocks.size()) {
+        size_t e = b + 1;  // extend the run while the next block follows in the arena
+        while (e < A.blocks.size() && A.blocks[e].off == A.blocks[e - 1].off + A.blocks[e - 1].size) ++e;
+        const int64_t n = A.blocks[e - 1].off + A.blocks[e - 1].size - A.blocks[b].off;
+        double* dev = A.data->get() + A.blocks[b].off;
+        const cudaError_t rc =
+            host ? cudaMemcpyAsync(host + pos, dev, sizeof(double) * (size_t)n, cudaMemcpyDeviceToHost, st)
+                 : cudaMemcpyAsync(dev, src_host + pos, sizeof(double) * (size_t)n, cudaMemcpyHostToDevice, st);
+        if (rc != cudaSuccess) throw ttb::tt_error(TT_ERR_CUDA, std::string("site copy: ") + cudaGetErrorString(rc));
+        pos += n;
+        b = e;
+      }
+    }
+    ttb::check(tt_ctx_synchronize(ctx), "site copy");
+  });
+}
+}  // namespace
+
+int tt_qmps_sites_size(const tt_qmps* psi, int first, int last, int64_t* n) {
+  TT_ARG(psi && n && first >= 0 && first <= last && last <= (int)psi->psi.length);
+  TT_GUARD({
+    int64_t s = 0;
+    for (int i = first; i < last; ++i) s += psi->psi.A[i].total_size();
+    *n = s;
+  });
+}
+
+int tt_qmps_get_sites(const tt_qmps* psi, int first, int last, double* host) {
+  return copy_sites(psi, first, last, host, nullptr);
+}
+
+int tt_qmps_set_sites(tt_qmps* psi, int first, int last, const double* host) {
+  return copy_sites(psi, first, last, nullptr, host);
 }
 
 int tt_qmpo_heisenberg(int L, const double* dh, double tE, unsigned id, tt_qmpo** out) {

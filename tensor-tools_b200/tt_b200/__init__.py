@@ -137,6 +137,9 @@ _proto("tt_qmps_tensor", P, C.c_int, PP)
 _proto("tt_qmps_data_size", P, PI64)
 _proto("tt_qmps_get_data", P, PD)
 _proto("tt_qmps_set_data", P, PD)
+_proto("tt_qmps_sites_size", P, C.c_int, C.c_int, C.POINTER(I64))
+_proto("tt_qmps_get_sites", P, C.c_int, C.c_int, PD)
+_proto("tt_qmps_set_sites", P, C.c_int, C.c_int, PD)
 _proto("tt_qdmrg_env", P, C.c_int, C.c_int, PP)
 _proto("tt_dmps_product_spinhalf", C.c_int, C.POINTER(C.c_int), C.c_uint, PP)
 _proto("tt_dmps_destroy", P)
@@ -525,6 +528,19 @@ class QMPS:
 
     def set_data(self, host: np.ndarray):
         _chk(lib.tt_qmps_set_data(self.h, host.ctypes.data_as(PD)), "set_data")
+
+    def sites_size(self, first: int, last: int) -> int:
+        """Elements of the site tensors [first, last)."""
+        n = I64()
+        _chk(lib.tt_qmps_sites_size(self.h, first, last, C.byref(n)), "sites_size")
+        return n.value
+
+    def get_sites(self, first: int, last: int, host: np.ndarray):
+        """Blocks of the site tensors [first, last) into host (float64, pinned for full bandwidth)."""
+        _chk(lib.tt_qmps_get_sites(self.h, first, last, host.ctypes.data_as(PD)), "get_sites")
+
+    def set_sites(self, first: int, last: int, host: np.ndarray):
+        _chk(lib.tt_qmps_set_sites(self.h, first, last, host.ctypes.data_as(PD)), "set_sites")
 
 
 class QMPO:

@@ -213,7 +213,10 @@ int tt_qdmrg_step_sectors(const tt_qdmrg* run, int i, int* n, int32_t* qn, uint3
 int tt_qdmrg_step_profile(const tt_qdmrg* run, int i, int* gram_max, double* t_davidson, double* t_svd,
                           double* t_env, double* t_engine);
 int tt_qdmrg_stats(const tt_qdmrg* run, double* heff_flops, double* heff_seconds, double* initial_energy);
-/* copy of the left (which = 0, TL[i]) or right (which = 1, TR[i]) environment */
+/* copy of the left (which = 0, TL[i]) or right (which = 1, TR[i]) environment.
+ * Only the environments on the live side of the orthogonality centre c are
+ * kept (TL[0..c], TR[c..L-1], plus the boundaries): the others are released
+ * as the centre passes them and come back empty (rank 0) until rebuilt. */
 int tt_qdmrg_env(const tt_qdmrg* run, int which, int i, tt_qtensor** out);
 int tt_qdmrg_num_sweeps(const tt_qdmrg* run, int* n);
 int tt_qdmrg_sweep_info(const tt_qdmrg* run, int i, double* energy, double* seconds);

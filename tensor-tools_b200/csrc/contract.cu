@@ -214,6 +214,62 @@ grouped_dgemm(const TaskDev* __restrict__ tasks, const OutDev* __restrict__ outs
 }
 
 // ---------------------------------------------------------------------------
+// Skinny FP64 path: contractions whose output blocks have at most SK_N
+// columns and whose pairs contract at most SK_K elements -- the middle
+// contraction of H_eff*x and of the environment update, (a' b) x (w s1 s2)
+// times (w s1 s2) x (s1' s2' w'), with rows a' b in the hundreds of
+// thousands and k, n the MPO link sector widths.  A 64 x 64 DMMA tile wastes
+// most of its work there, and the contraction is bound by reading T1 and
+// writing T2.  Here a CTA takes SK_ROWS rows of one output block; each
+// thread keeps its row's n outputs in registers across all pairs of the
+// block, with the pair's B (k x n, tiny) staged in shared memory, and reads
+// its A row through the offset tables (coalesced along a unit-stride row
+// mode).  Pairs are summed in the plan's order, as in grouped_dgemm.
+constexpr int SK_N = 32;
+constexpr int SK_K = 64;
+constexpr int SK_ROWS = 256;
+
+__global__ void __launch_bounds__(SK_ROWS)
+skinny_dgemm(const TaskDev* __restrict__ tasks, const OutDev* __restrict__ outs,
+             const PairDev* __restrict__ pairs, const int32_t* __restrict__ tab,
+             const double* __restrict__ A, const double* __restrict__ B, double* __restrict__ C,
+             double alpha) {
+  __shared__ double sB[SK_K][SK_N + 1];
+  __shared__ int32_t sColA[SK_K];
+  const TaskDev task = tasks[blockIdx.x];
+  const OutDev out = outs[task.out];
+  const int r = task.m0 + threadIdx.x;
+  double acc[SK_N];
+#pragma unroll
+  for (int c = 0; c < SK_N; ++c) acc[c] = 0.0;
+  for (int p = task.p_begin; p < task.p_end; ++p) {
+    const PairDev P = pairs[p];
+    __syncthreads();  // the previous pair's B is no longer read
+    for (int e = threadIdx.x; e < P.k * P.n; e += blockDim.x) {
+      const int kk = e % P.k, c = e / P.k;
+      sB[kk][c] = B[P.b_off + tab[P.rowB + kk] + tab[P.colB + c]];
+    }
+    for (int kk = threadIdx.x; kk < P.k; kk += blockDim.x) sColA[kk] = tab[P.colA + kk];
+    __syncthreads();
+    if (r < P.m) {
+      const double* __restrict__ arow = A + P.a_off + tab[P.rowA + r];
+      for (int kk = 0; kk < P.k; ++kk) {
+        const double a = arow[sColA[kk]];
+#pragma unroll
+        for (int c = 0; c < SK_N; ++c)
+          if (c < P.n) acc[c] += a * sB[kk][c];
+      }
+    }
+  }
+  if (r < out.m) {
+    double* Cb = C + out.c_off + r;
+#pragma unroll
+    for (int c = 0; c < SK_N; ++c)
+      if (c < out.n) Cb[(int64_t)out.ldc * c] = alpha * acc[c];
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Mixed-precision path: tcgen05 (5th-generation tensor cores), kind::tf32.
 //
 // Two launches per contraction.  pack_tf32_ab converts every operand block
@@ -640,6 +696,7 @@ double predict_us(const tt_out_block* outs, int n_out, const std::vector<PairDev
 
 struct tt_plan {
   int precision = TT_PREC_FP64;
+  bool skinny = false;      // FP64 plan run by skinny_dgemm (row tasks of SK_ROWS)
   int* d_status = nullptr;  // tensor-core path: TT_OK or TT_ERR_TIMEOUT
   // tensor-core path: packing jobs and tiles of the unique A / B blocks, the
   // pairs in packed form, and the packed sizes (buffers are taken from the
@@ -743,7 +800,12 @@ int tt_contract_plan(tt_ctx* ctx, const tt_out_block* outs, int n_out,
                        0.8 * predict_us(outs, n_out, hp, first, TT_PREC_FP64, ctx->num_sms))
     precision = TT_PREC_FP64;
   const bool tc = precision != TT_PREC_FP64;
-  const int tile_m = tc ? TC_BM : BM, tile_n = tc ? TC_BN : BN;
+  // FP64 plans whose output blocks are at most SK_N wide and whose pairs
+  // contract at most SK_K elements run on the skinny kernel
+  bool skinny = !tc && n_pairs > 0;
+  for (int o = 0; o < n_out && skinny; ++o) skinny = outs[o].n <= SK_N;
+  for (int i = 0; i < n_pairs && skinny; ++i) skinny = hp[i].k <= SK_K && hp[i].n <= SK_N;
+  const int tile_m = tc ? TC_BM : (skinny ? SK_ROWS : BM), tile_n = tc ? TC_BN : (skinny ? SK_N : BN);
   // tile tasks, longest first (LPT) so heavy blocks start early
   std::vector<TaskDev> tasks;
   std::vector<int64_t> tcost;
@@ -801,6 +863,7 @@ int tt_contract_plan(tt_ctx* ctx, const tt_out_block* outs, int n_out,
 
   tt_plan* plan = new tt_plan();
   plan->precision = precision;
+  plan->skinny = skinny;
   plan->n_tilesA = (int)ta.size();
   plan->n_tilesB = (int)tb.size();
   plan->bytesA = bytesA;
@@ -867,8 +930,12 @@ int tt_contract_exec(tt_ctx* ctx, const tt_plan* plan, const double* A, const do
                                  (int)TC_BULK_SMEM));
   }
   if (plan->precision == TT_PREC_FP64) {
-    grouped_dgemm<<<plan->n_tasks, THREADS, SMEM_BYTES, ctx->stream>>>(
-        plan->d_tasks, plan->d_outs, plan->d_pairs, plan->d_tab, A, B, C, alpha);
+    if (plan->skinny)
+      skinny_dgemm<<<plan->n_tasks, SK_ROWS, 0, ctx->stream>>>(plan->d_tasks, plan->d_outs, plan->d_pairs,
+                                                              plan->d_tab, A, B, C, alpha);
+    else
+      grouped_dgemm<<<plan->n_tasks, THREADS, SMEM_BYTES, ctx->stream>>>(
+          plan->d_tasks, plan->d_outs, plan->d_pairs, plan->d_tab, A, B, C, alpha);
     TT_LAUNCH_CHECK(ctx);
     return TT_OK;
   }

@@ -1032,6 +1032,17 @@ void dmrg_prepare(qMPS& psi, qMPO& H, DmrgState& st, DmrgLog* log) {
   if (log) log->initial_energy = e;
 }
 
+// After a two-site update at `site` the orthogonality centre has moved past
+// it: left-to-right, TR[site] will be rebuilt before it is read again;
+// right-to-left, TL[site].  Releasing them keeps only the environments on the
+// live side of the centre (TL[0..c], TR[c..L-1]) -- half of the 2L the
+// reference holds -- so bond dimension 3072 on the 96-site cylinder fits in
+// HBM.  Boundaries (TL[0], TR[L-1]) are never released.
+static void release_stale(DmrgState& st, unsigned site, int direction, unsigned L) {
+  if (direction == MoveFromLeft && site > 0 && site < L - 1) st.TR[site] = qtensor();
+  if (direction == MoveFromRight && site > 0 && site < L - 1) st.TL[site] = qtensor();
+}
+
 double dmrg_walk(qMPS& psi, qMPO& H, DmrgState& st, int to, int max_bd, double cutoff, int max_restart,
                  DmrgLog* log) {
   const int L = (int)H.length;
@@ -1044,6 +1055,7 @@ double dmrg_walk(qMPS& psi, qMPO& H, DmrgState& st, int to, int max_bd, double c
     updateSite(psi, H, st.TR, st.TL, site, energy, direction, max_bd, cutoff, 'S', 3, max_restart, log, st.noise);
     auto te0 = std::chrono::steady_clock::now();
     updateEnv(psi, H, st.TR, st.TL, site, direction);
+    release_stale(st, site, direction, (unsigned)L);
     if (log && !log->steps.empty()) {
       if (rt().profile) check(tt_ctx_synchronize(ctx()), "sync");
       log->steps.back().t_env = std::chrono::duration<double>(std::chrono::steady_clock::now() - te0).count();
@@ -1071,6 +1083,7 @@ double dmrg_sweep(qMPS& psi, qMPO& H, DmrgState& st, int max_bd, double cutoff, 
       rt().energy_fp64 = false;
       auto te0 = std::chrono::steady_clock::now();
       updateEnv(psi, H, st.TR, st.TL, site, direction);
+      release_stale(st, site, direction, L);
       if (prof) {
         check(tt_ctx_synchronize(ctx()), "sync");
         cudaProfilerStop();

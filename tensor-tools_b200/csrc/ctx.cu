@@ -46,6 +46,17 @@ int device_status(tt_ctx* ctx) {
   return TT_OK;
 }
 
+cudaError_t pool_malloc(tt_ctx* ctx, void** p, size_t bytes) {
+  cudaError_t e = cudaMallocAsync(p, bytes, ctx->stream);
+  if (e == cudaErrorMemoryAllocation) {
+    cudaGetLastError();
+    if (cudaStreamSynchronize(ctx->stream) == cudaSuccess && cudaMemPoolTrimTo(ctx->pool, 0) == cudaSuccess)
+      e = cudaMallocAsync(p, bytes, ctx->stream);
+    if (e != cudaSuccess) cudaGetLastError();
+  }
+  return e;
+}
+
 cudaError_t h2d_async(tt_ctx* ctx, void* dst, const void* src, size_t bytes) {
   if (bytes == 0) return cudaSuccess;
   const size_t need = (bytes + 255) & ~(size_t)255;
@@ -224,7 +235,7 @@ int tt_device_alloc(tt_ctx* ctx, size_t bytes, void** dptr) {
   TT_REQUIRE(ctx && dptr, "null argument");
   *dptr = nullptr;
   if (bytes == 0) bytes = 16;
-  TT_CUDA(cudaMallocAsync(dptr, bytes, ctx->stream));
+  TT_CUDA(tt::pool_malloc(ctx, dptr, bytes));
   return TT_OK;
 }
 

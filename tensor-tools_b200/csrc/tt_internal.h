@@ -51,11 +51,18 @@ int cuda_fail(cudaError_t e, const char* what, const char* file, int line);
 // can report how many of its kernels ran.
 inline void count_launch(tt_ctx* ctx) { ctx->launches++; }
 
+// Stream-ordered allocation from the context's pool.  Freed blocks stay
+// reserved in the pool (release threshold unlimited), which can leave the
+// device without a free range large enough for a big request although the
+// pool holds enough in total: on failure the stream is drained, the pool's
+// unused reserve is returned to the device and the request is retried once.
+cudaError_t pool_malloc(tt_ctx* ctx, void** p, size_t bytes);
+
 template <class T>
 inline T* pool_alloc(tt_ctx* ctx, size_t n) {
   void* p = nullptr;
   if (n == 0) n = 1;
-  if (cudaMallocAsync(&p, n * sizeof(T), ctx->stream) != cudaSuccess) return nullptr;
+  if (pool_malloc(ctx, &p, n * sizeof(T)) != cudaSuccess) return nullptr;
   return static_cast<T*>(p);
 }
 inline void pool_free(tt_ctx* ctx, void* p) {

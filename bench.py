@@ -548,6 +548,8 @@ def run_c5(args):
         sampler = ClockSampler(local)
         chosen = c5_arm(CHOSEN, ck, H, args, ctx, stream, flush, torch, tt_b200, sampler=sampler,
                         e2e_steps=args.e2e_steps)
+        print("[bench] %s arm: %.3f s/sweep, pool GB %s" % (CHOSEN, chosen["value"], ["%.1f" % (v / 2 ** 30)
+                                                             for v in ctx.memory()]), file=sys.stderr, flush=True)
         barrier()
         fp64 = c5_arm("fp64", ck, H, args, ctx, stream, flush, torch, tt_b200)
         barrier()

@@ -153,6 +153,8 @@ int tt_contract_exec(tt_ctx* ctx, const tt_plan* plan, const double* A,
                      const double* B, double* C, double alpha);
 int tt_plan_destroy(tt_ctx* ctx, tt_plan* plan);
 /* Algorithmic work of one exec: sum over pairs of 2*m*n*k. */
+/* Device bytes a plan holds (offset tables, tasks, packing jobs). */
+int tt_plan_device_bytes(const tt_plan* plan, int64_t* bytes);
 int tt_plan_flops(const tt_plan* plan, double* flops);
 /* The precision the plan runs in (TT_PREC_FP64 / TF32 / TF32X3): an *_AUTO
  * request resolves to one of them when the plan is built. */

@@ -712,6 +712,7 @@ struct tt_plan {
   int n_pairs = 0;
   int n_out = 0;
   double flops = 0.0;
+  int64_t dev_bytes = 0;  // device memory the plan holds (tables, tasks, packing jobs)
   TaskDev* d_tasks = nullptr;
   OutDev* d_outs = nullptr;
   PairDev* d_pairs = nullptr;
@@ -872,6 +873,10 @@ int tt_contract_plan(tt_ctx* ctx, const tt_out_block* outs, int n_out,
   plan->n_pairs = n_pairs;
   plan->n_out = n_out;
   plan->flops = flops;
+  plan->dev_bytes = (int64_t)(sizeof(TaskDev) * tsorted.size() + sizeof(OutDev) * ho.size() +
+                              sizeof(PairDev) * hp.size() + sizeof(int32_t) * (size_t)tab_len +
+                              sizeof(PackJob) * (ja.size() + jb.size()) + sizeof(PackTile) * (ta.size() + tb.size()) +
+                              sizeof(PairTC) * ptc.size());
   plan->d_tasks = tt::pool_alloc<TaskDev>(ctx, tsorted.size());
   plan->d_outs = tt::pool_alloc<OutDev>(ctx, ho.size());
   plan->d_pairs = tt::pool_alloc<PairDev>(ctx, hp.size());
@@ -1048,6 +1053,12 @@ int tt_contract_predict(const tt_out_block* outs, int n_out, const tt_block_pair
 int tt_plan_precision(const tt_plan* plan, int* precision) {
   TT_REQUIRE(plan && precision, "tt_plan_precision: null argument");
   *precision = plan->precision;
+  return TT_OK;
+}
+
+int tt_plan_device_bytes(const tt_plan* plan, int64_t* bytes) {
+  TT_REQUIRE(plan && bytes, "tt_plan_device_bytes: null argument");
+  *bytes = plan->dev_bytes;
   return TT_OK;
 }
 

@@ -630,18 +630,25 @@ struct CacheEntry {
 struct ContractionCache {
   std::unordered_map<uint64_t, std::vector<CacheEntry>> map;
   size_t entries = 0;
+  int64_t plan_bytes = 0;  // device bytes held by the cached plans
 };
 ContractionCache& cache() {
   static thread_local ContractionCache c;
   return c;
 }
 constexpr size_t kCacheMax = 16384;
+// Plans hold device tables; at large bond dimension every step brings new
+// block structures, so the cache is also bounded by the device bytes its
+// plans hold.  Clearing it frees only plans nobody else holds (a Davidson
+// call keeps its own references).
+constexpr int64_t kCachePlanBytesMax = (int64_t)4 << 30;
 
 }  // namespace
 
 void clear_contraction_cache() {
   cache().map.clear();
   cache().entries = 0;
+  cache().plan_bytes = 0;
 }
 
 size_t contraction_cache_size() { return cache().entries; }
@@ -662,7 +669,7 @@ std::shared_ptr<const CachedContraction> contract_cached(const qtensor& A, const
       break;
     }
   if (!val) {
-    if (cache().entries >= kCacheMax) {
+    if (cache().entries >= kCacheMax || cache().plan_bytes >= kCachePlanBytesMax) {
       clear_contraction_cache();
       return contract_cached(A, B, need_plan);
     }
@@ -678,7 +685,11 @@ std::shared_ptr<const CachedContraction> contract_cached(const qtensor& A, const
 tt_plan* CachedContraction::plan_for(int precision) const {
   if (precision < TT_PREC_FP64 || precision > TT_PREC_TF32X3_AUTO) throw std::runtime_error("plan_for: bad precision");
   if (cs.outs.empty()) return nullptr;
-  if (!plans[precision]) plans[precision] = make_plan(cs, precision);
+  if (!plans[precision]) {
+    plans[precision] = make_plan(cs, precision);
+    int64_t b = 0;
+    if (tt_plan_device_bytes(plans[precision]->get(), &b) == TT_OK) cache().plan_bytes += b;
+  }
   return plans[precision]->get();
 }
 

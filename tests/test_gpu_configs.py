@@ -4,7 +4,7 @@ minutes of oracle time).
 
 * The L = 100 Heisenberg chain (the U(1) chain configuration): ramp 32, 64,
   128, 256 and two sweeps at 512, cutoff 1e-12, Davidson 6 iterations --
-  final energy within 1e-10 relative of the oracle's, same bond dimensions.
+  final energy within 1e-10 relative of the oracle's.
   The same chain with small random fields (no singular-value ties): the kept
   states per QN sector at every one of the 1188 two-site steps and every
   step's energy.
@@ -61,10 +61,9 @@ def test_heisenberg_chain_L100_to_maxdim_512(ctx, fields):
     if fields:
         _compare_steps(run, logs)
         assert gpsi.bond_dims() == psi.bond_dims
-    else:
-        # SU(2) multiplets tie at the cut, where the reference's std::sort
-        # leaves the choice open: the bond dimensions still agree
-        assert gpsi.bond_dims() == psi.bond_dims
+    # without fields SU(2) multiplets tie at the cut, where the reference's
+    # std::sort leaves the choice open: kept counts (and bond dimensions) may
+    # differ by members of a multiplet, the energy may not
 
 
 def _j1j2_snake(Nx, Ny, J2, h):

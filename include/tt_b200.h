@@ -220,6 +220,10 @@ int tt_vec_lincomb_dev(tt_ctx* ctx, int64_t n, int nvec, const double* const* xs
  * tt_vec_nrm2.  xs is a HOST array of nvec (0..16) device pointers. */
 int tt_vec_project_nrm2_dev(tt_ctx* ctx, int64_t n, int nvec, const double* const* xs,
                             const double* d_coef, double* y, double* d_norm);
+/* The same, enqueued unconditionally but a no-op unless *d_cond (a device int)
+ * is non-zero when it runs. */
+int tt_vec_project_nrm2_dev_if(tt_ctx* ctx, int64_t n, int nvec, const double* const* xs,
+                               const double* d_coef, double* y, double* d_norm, const int* d_cond);
 /* The Ritz vector and residual of a Davidson iteration in one pass
  * (linalg/tensor_davidson.cpp:255-269): x = sum_{j<k} coef_x[j] vs[j] and
  * q = sum_{j<k} coef_q[j] vas[j] + coef_q[k] x, coefficients on the device;
@@ -249,7 +253,7 @@ int tt_vec_precondition(tt_ctx* ctx, int64_t n, double* x, const double* D, doub
  * failure that the caller finishes on the host). */
 typedef struct tt_dav_state tt_dav_state;
 typedef struct {
-  int done, final_ii, fail_ii, iters;
+  int done, final_ii, fail_ii, iters, randomized;
   double lambda;
 } tt_dav_result;
 int tt_dav_state_create(tt_ctx* ctx, tt_dav_state** st);
@@ -260,6 +264,19 @@ int tt_dav_ritz(tt_ctx* ctx, tt_dav_state* st, int ii);
 int tt_dav_converged(tt_ctx* ctx, tt_dav_state* st, int ii, int maxiter, double tol, const double* d_qnorm);
 int tt_dav_add_row(tt_ctx* ctx, tt_dav_state* st, int ii, const double* d_row, const double* d_gsnorm);
 int tt_dav_read(tt_ctx* ctx, const tt_dav_state* st, tt_dav_result* out);
+/* Gram-Schmidt failure on the device (linalg/tensor_davidson.cpp:298-316):
+ * enqueued after every projection of a new vector y = v[ni]; a no-op unless
+ * the norm at d_gsnorm is below 1e-10.  Then, when ni < maxsize, y is
+ * refilled with random numbers on the [begin, end) element ranges d_ranges
+ * (the blocks of the previous vector, sorted), its overlaps with xs[0..ni-1]
+ * go to d_dots and the flag at tt_dav_refill_flag is raised for a following
+ * tt_vec_project_nrm2_dev_if; when ni >= maxsize the loop ends with the
+ * current Ritz vector.  A refill that fails again ends the loop the same way
+ * (tt_dav_add_row).  tt_dav_result.randomized counts the refills. */
+int tt_dav_gs_refill(tt_ctx* ctx, tt_dav_state* st, int ii, int ni, int maxsize, int64_t n,
+                     const double* const* xs, double* y, int nranges, const int64_t* d_ranges, uint64_t seed,
+                     const double* d_gsnorm, double* d_dots);
+int tt_dav_refill_flag(tt_dav_state* st, const int** d_flag);
 
 /* ---- strided copies ------------------------------------------------------
  * dst[dst_off + sum_i j_i*dst_stride[i]] = src[src_off + sum_i j_i*src_stride[i]]

@@ -98,11 +98,14 @@ int tt_dmrg_planning_counters(double* t_structure, int64_t* n_structure, double*
  * last step of every sweep re-evaluates its energy with an FP64 product. */
 int tt_dmrg_set_precision(int op, int heff, int env);
 /* Davidson control on this thread: 1 (default) runs tensor_davidsonIT's
- * decisions on the device and synchronises once per call, falling back to the
- * host loop when Gram-Schmidt fails; 0 always uses the host loop.
- * tt_dmrg_davidson_fallbacks counts the fallbacks so far. */
+ * decisions on the device and synchronises once per call (a Gram-Schmidt
+ * failure is refilled on the device); 0 always uses the host loop.
+ * tt_dmrg_davidson_fallbacks counts device calls redone by the host loop. */
 int tt_dmrg_set_davidson(int device_control);
 int tt_dmrg_davidson_fallbacks(int64_t* n);
+/* Gram-Schmidt failures of the device-resident loop refilled on the device
+ * (random refill and re-orthogonalisation, linalg/tensor_davidson.cpp:298-316) */
+int tt_dmrg_davidson_refills(int64_t* n);
 /* Diagnostics: bracket two-site step `step` (0 .. 2L-3) of every following
  * U(1) sweep with cudaProfilerStart/Stop, so a profiler started with its
  * capture off sees that step only; -1 (default) disables. */

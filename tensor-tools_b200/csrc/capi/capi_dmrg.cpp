@@ -90,6 +90,11 @@ int tt_dmrg_davidson_fallbacks(int64_t* n) {
   TT_GUARD(*n = ttb::rt().dav_fallbacks);
 }
 
+int tt_dmrg_davidson_refills(int64_t* n) {
+  TT_ARG(n);
+  TT_GUARD(*n = ttb::rt().dav_refills);
+}
+
 int tt_dmrg_set_precision(int op, int heff, int env) {
   auto ok = [](int p) { return p >= TT_PREC_FP64 && p <= TT_PREC_TF32X3_AUTO; };
   TT_ARG(ok(op) && ok(heff) && ok(env));

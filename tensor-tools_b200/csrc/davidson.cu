@@ -9,6 +9,7 @@
 // is done (converged, exhausted, or a Gram-Schmidt failure that the host
 // handles with its own loop) later control kernels are no-ops, and the host
 // reads the state once at the end.  One thread does the work (n <= 16).
+#include <algorithm>
 #include <cmath>
 #include <cstddef>
 #include <cstring>
@@ -20,6 +21,8 @@ struct tt_dav_state {
   int final_ii;  // iteration at which it ended (-2: Gram-Schmidt failure at fail_ii)
   int fail_ii;
   int iters;
+  int refill;      // 1 while the current new vector is a random refill to orthogonalise
+  int randomized;  // random refills in this call
   int cur;       // which of buf[0], buf[1] holds M (the other holds Mnext)
   double lambda, last_lambda, qnorm, gsnorm;
   double buf[2][TT_DAV_MAX * TT_DAV_MAX];
@@ -141,6 +144,8 @@ __global__ void dav_begin_kernel(tt_dav_state* st, const double* init_en) {
   st->fail_ii = -1;
   st->iters = 0;
   st->cur = 0;
+  st->refill = 0;
+  st->randomized = 0;
   st->last_lambda = 1000.0;
   const double lam = init_en[0];
   st->lambda = lam;
@@ -195,9 +200,11 @@ __global__ void dav_row_kernel(tt_dav_state* st, int ii, const double* row, cons
   if (threadIdx.x != 0 || st->done) return;
   const double g = gsnorm[0];
   st->gsnorm = g;
-  if (!(g >= 1e-10)) {  // Gram-Schmidt failure: the host finishes with its own loop
+  if (!(g >= 1e-10)) {
+    // the random refill failed too (the space is exhausted): the loop ends
+    // with the current Ritz vector, as the reference does after its retries
     st->done = 1;
-    st->final_ii = -2;
+    st->final_ii = ii;
     st->fail_ii = ii;
     return;
   }
@@ -208,6 +215,93 @@ __global__ void dav_row_kernel(tt_dav_state* st, int ii, const double* row, cons
   for (int k = 0; k < ni + 1; ++k) {
     M[l + k * (ni + 1)] = row[k];
     M[k + l * (ni + 1)] = row[k];
+  }
+}
+
+// Gram-Schmidt failure inside the loop (linalg/tensor_davidson.cpp:298-316):
+// when the projected new vector's norm is below 1e-10 the reference refills it
+// with random numbers on the blocks of the previous vector and orthogonalises
+// it again; when the vectors already span the problem (ni >= size) the loop
+// ends instead.  One launch: every block reads the same norm and decides
+// alike (all of them return when there is nothing to do); on a refill each
+// thread draws its elements (the counter-based generator of
+// tt_vec_fill_random), stores them and accumulates their overlaps with the
+// earlier vectors, and the last block (ticket) sums the per-block partials in
+// block order into dots and raises st->refill for the conditional
+// projection that follows.
+constexpr int RF_THREADS = 256;
+struct RefillVecs {
+  const double* p[TT_DAV_MAX];
+};
+
+__device__ __forceinline__ uint64_t rf_mix(uint64_t z) {
+  z += 0x9E3779B97F4A7C15ull;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+__global__ void __launch_bounds__(RF_THREADS)
+dav_refill_kernel(tt_dav_state* st, int ii, int ni, int maxsize, int64_t n, RefillVecs xs, double* y, int nranges,
+                  const int64_t* ranges, uint64_t seed, const double* gsnorm, double* part, double* dots,
+                  unsigned int* ticket) {
+  if (st->done || gsnorm[0] >= 1e-10) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) st->refill = 0;
+    return;
+  }
+  if (ni >= maxsize) {  // nothing left to add: the loop ends with the current Ritz vector
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      st->refill = 0;
+      st->done = 1;
+      st->final_ii = ii;
+      st->fail_ii = ii;
+    }
+    return;
+  }
+  double acc[TT_DAV_MAX];
+  for (int j = 0; j < ni; ++j) acc[j] = 0.0;
+  for (int64_t i = blockIdx.x * (int64_t)RF_THREADS + threadIdx.x; i < n; i += (int64_t)gridDim.x * RF_THREADS) {
+    int lo = 0, hi = nranges;  // is i inside one of the sorted [begin, end) ranges?
+    while (lo < hi) {
+      const int mid = (lo + hi) >> 1;
+      if (ranges[2 * mid + 1] <= i) lo = mid + 1; else hi = mid;
+    }
+    double v = 0.0;
+    if (lo < nranges && ranges[2 * lo] <= i)
+      v = (double)(rf_mix(seed ^ (uint64_t)i * 0xD1B54A32D192ED03ull) >> 11) * 0x1.0p-53;
+    y[i] = v;
+    for (int j = 0; j < ni; ++j) acc[j] = fma(xs.p[j][i], v, acc[j]);
+  }
+  __shared__ double red[RF_THREADS / 32][TT_DAV_MAX];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  for (int j = 0; j < ni; ++j) {
+    double x = acc[j];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+    if (lane == 0) red[w][j] = x;
+  }
+  __syncthreads();
+  if (threadIdx.x < ni) {
+    double x = 0.0;
+    for (int k = 0; k < RF_THREADS / 32; ++k) x += red[k][threadIdx.x];
+    part[(int64_t)threadIdx.x * gridDim.x + blockIdx.x] = x;
+  }
+  __shared__ bool last;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = atomicAdd(ticket, 1u) == gridDim.x - 1;
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  if (threadIdx.x < ni) {
+    double x = 0.0;
+    for (int b = 0; b < (int)gridDim.x; ++b) x += __ldcg(part + (int64_t)threadIdx.x * gridDim.x + b);
+    dots[threadIdx.x] = x;
+  }
+  if (threadIdx.x == 0) {
+    st->refill = 1;
+    st->randomized++;
+    *ticket = 0u;
   }
 }
 
@@ -265,6 +359,30 @@ int tt_dav_add_row(tt_ctx* ctx, tt_dav_state* st, int ii, const double* d_row, c
   return TT_OK;
 }
 
+int tt_dav_gs_refill(tt_ctx* ctx, tt_dav_state* st, int ii, int ni, int maxsize, int64_t n,
+                     const double* const* xs, double* y, int nranges, const int64_t* d_ranges, uint64_t seed,
+                     const double* d_gsnorm, double* d_dots) {
+  TT_REQUIRE(ctx && st && xs && y && d_gsnorm && d_dots && (nranges == 0 || d_ranges),
+             "tt_dav_gs_refill: null argument");
+  TT_REQUIRE(ni >= 1 && ni <= TT_DAV_MAX && ii >= 0 && n >= 0, "tt_dav_gs_refill: bad argument");
+  RefillVecs v;
+  for (int j = 0; j < ni; ++j) v.p[j] = xs[j];
+  const int nb = (int)std::max<int64_t>(1, std::min<int64_t>((n + RF_THREADS - 1) / RF_THREADS,
+                                                                  4 * (int64_t)ctx->num_sms));
+  double* part = tt::partials(ctx, nb * ni);
+  if (!part) return tt::fail(TT_ERR_OOM, "tt_dav_gs_refill: reduction scratch");
+  dav_refill_kernel<<<nb, RF_THREADS, 0, ctx->stream>>>(st, ii, ni, maxsize, n, v, y, nranges, d_ranges, seed,
+                                                        d_gsnorm, part, d_dots, ctx->d_ticket);
+  TT_LAUNCH_CHECK(ctx);
+  return TT_OK;
+}
+
+int tt_dav_refill_flag(tt_dav_state* st, const int** d_flag) {
+  TT_REQUIRE(st && d_flag, "tt_dav_refill_flag: null argument");
+  *d_flag = &st->refill;
+  return TT_OK;
+}
+
 int tt_dav_read(tt_ctx* ctx, const tt_dav_state* st, tt_dav_result* out) {
   TT_REQUIRE(ctx && st && out, "tt_dav_read: null argument");
   // one synchronising read of the header: the flags and the Ritz value
@@ -278,6 +396,7 @@ int tt_dav_read(tt_ctx* ctx, const tt_dav_state* st, tt_dav_result* out) {
   out->final_ii = head.final_ii;
   out->fail_ii = head.fail_ii;
   out->iters = head.iters;
+  out->randomized = head.randomized;
   out->lambda = head.lambda;
   return TT_OK;
 }

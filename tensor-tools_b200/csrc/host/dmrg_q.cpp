@@ -319,9 +319,10 @@ static int davidson_precision(int64_t dim) {
 // ---- tensor_davidsonIT -----------------------------------------------------
 // Device-resident form: every iteration is enqueued up front and the loop's
 // decisions run in the tt_dav_* control kernels, so the whole call
-// synchronises once.  Returns false (x untouched apart from its
-// normalisation) when Gram-Schmidt failed before the loop ended; the host
-// loop below then redoes the call, with its random refill.
+// synchronises once; a Gram-Schmidt failure is refilled on the device
+// (tt_dav_gs_refill).  Returns false (x untouched apart from its
+// normalisation) only if the control state reports an unexpected end; the
+// host loop below then redoes the call.
 static bool davidson_device(big_qtensor& A, qtensor& x, int max_restart, double tol, DavidsonStats* stats,
                             double& lambda_out) {
   int maxsize = (int)A.size();
@@ -331,6 +332,9 @@ static bool davidson_device(big_qtensor& A, qtensor& x, int max_restart, double 
   tt_dav_state* st = rt().dav;
   double *coef_x = nullptr, *coef_q = nullptr;
   check(tt_dav_coefficients(st, &coef_x, &coef_q), "davidson coefficients");
+  const int* refill_flag = nullptr;
+  check(tt_dav_refill_flag(st, &refill_flag), "davidson refill flag");
+  std::vector<DevBuf> refill_ranges;  // element ranges of each iteration's possible refill
   // x /= |x| on the device (tensor_davidson.cpp:205-206)
   check(tt_vec_nrm2(ctx(), x.arena, x.data->get(), scalar_slot(0)), "norm");
   check(tt_vec_scal_inv_dev(ctx(), x.arena, scalar_slot(0), x.data->get()), "normalize");
@@ -424,6 +428,26 @@ static bool davidson_device(big_qtensor& A, qtensor& x, int max_restart, double 
     check(tt_vec_multidot(ctx(), n, ni, vs.data(), v[ni].d->get(), scalar_slot(0)), "GS overlaps");
     check(tt_vec_project_nrm2_dev(ctx(), n, ni, vs.data(), scalar_slot(0), v[ni].d->get(), scalar_slot(kNormSlot)),
           "GS update and norm");
+    {
+      // Gram-Schmidt failure (:298-316) handled on the device: a random
+      // refill on the blocks of v[ni-1] and one more projection, both no-ops
+      // unless the norm just computed is below 1e-10
+      std::vector<int64_t> ranges;
+      for (unsigned b = 0; b < eng.ublocks.size(); ++b)
+        if (v[ni - 1].p[b]) {
+          ranges.push_back(eng.ublocks[b].off);
+          ranges.push_back(eng.ublocks[b].off + eng.ublocks[b].size);
+        }
+      refill_ranges.emplace_back((int64_t)ranges.size() + 1);  // one int64 per 8-byte slot
+      int64_t* dr = reinterpret_cast<int64_t*>(refill_ranges.back().get());
+      if (!ranges.empty()) check(tt_memcpy_h2d(ctx(), dr, ranges.data(), sizeof(int64_t) * ranges.size()), "ranges");
+      check(tt_dav_gs_refill(ctx(), st, ii, ni, maxsize, n, vs.data(), v[ni].d->get(), (int)ranges.size() / 2, dr,
+                             rt().rng_counter++, scalar_slot(kNormSlot), scalar_slot(0)),
+            "GS refill");
+      check(tt_vec_project_nrm2_dev_if(ctx(), n, ni, vs.data(), scalar_slot(0), v[ni].d->get(),
+                                       scalar_slot(kNormSlot), refill_flag),
+            "GS refill projection");
+    }
     check(tt_vec_scal_inv_dev(ctx(), n, scalar_slot(kNormSlot), v[ni].d->get()), "GS scale");
     va[ni] = product(v[ni]);
     vs.push_back(v[ni].d->get());
@@ -465,6 +489,10 @@ static bool davidson_device(big_qtensor& A, qtensor& x, int max_restart, double 
     stats->matvecs = f + 1;
     stats->heff_flops = (f + 1) * eng.flops;
     stats->iters = res.iters;
+    stats->randomized = res.randomized;
+  }
+  rt().dav_refills += res.randomized;
+  if (stats) {
     stats->t_loop = std::chrono::duration<double>(std::chrono::steady_clock::now() - tb1).count();
   }
   lambda_out = lambda;

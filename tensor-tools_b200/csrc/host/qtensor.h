@@ -50,7 +50,8 @@ struct Runtime {
   // device-resident Davidson control state (created on first use)
   ::tt_dav_state* dav = nullptr;
   bool dav_device = true;    // run tensor_davidsonIT's control on the device
-  int64_t dav_fallbacks = 0; // Gram-Schmidt failures finished by the host loop
+  int64_t dav_fallbacks = 0; // device-resident calls redone by the host loop
+  int64_t dav_refills = 0;   // Gram-Schmidt failures refilled on the device
   int profile_step = -1;      // two-site step of a sweep bracketed by the CUDA profiler range
 };
 Runtime& rt();

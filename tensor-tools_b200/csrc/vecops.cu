@@ -131,7 +131,9 @@ __global__ void __launch_bounds__(RT) multidot_fused(int64_t n, PtrPack xs, cons
 // (for the norm), so both results are bit-identical to the two launches.
 __global__ void __launch_bounds__(RT) project_nrm2_kernel(int64_t n, int nv, PtrPack xs,
                                                           const double* __restrict__ coef, double* y,
-                                                          double* part, double* out, unsigned int* ticket) {
+                                                          double* part, double* out, unsigned int* ticket,
+                                                          const int* cond) {
+  if (cond && *cond == 0) return;  // conditional form: every block reads the same flag
   __shared__ double c[MAXVEC];
   if (threadIdx.x < nv) c[threadIdx.x] = -1.0 * coef[threadIdx.x];
   __syncthreads();
@@ -462,8 +464,8 @@ int tt_vec_lincomb_dev(tt_ctx* ctx, int64_t n, int nvec, const double* const* xs
   return TT_OK;
 }
 
-int tt_vec_project_nrm2_dev(tt_ctx* ctx, int64_t n, int nvec, const double* const* xs, const double* d_coef,
-                            double* y, double* d_norm) {
+int tt_vec_project_nrm2_dev_if(tt_ctx* ctx, int64_t n, int nvec, const double* const* xs, const double* d_coef,
+                               double* y, double* d_norm, const int* d_cond) {
   TT_REQUIRE(ctx && xs && d_coef && y && d_norm, "tt_vec_project_nrm2_dev: null argument");
   TT_REQUIRE(nvec >= 0 && nvec <= MAXVEC, "tt_vec_project_nrm2_dev: 0..16 vectors");
   TT_REQUIRE(aligned16(y), "tt_vec_project_nrm2_dev: vectors must be 16-byte aligned");
@@ -475,9 +477,14 @@ int tt_vec_project_nrm2_dev(tt_ctx* ctx, int64_t n, int nvec, const double* cons
   const int nb = red_blocks(ctx, n);
   double* part = tt::partials(ctx, nb);
   if (!part) return tt::fail(TT_ERR_OOM, "reduction scratch");
-  project_nrm2_kernel<<<nb, RT, 0, ctx->stream>>>(n, nvec, pk, d_coef, y, part, d_norm, ctx->d_ticket);
+  project_nrm2_kernel<<<nb, RT, 0, ctx->stream>>>(n, nvec, pk, d_coef, y, part, d_norm, ctx->d_ticket, d_cond);
   TT_LAUNCH_CHECK(ctx);
   return TT_OK;
+}
+
+int tt_vec_project_nrm2_dev(tt_ctx* ctx, int64_t n, int nvec, const double* const* xs, const double* d_coef,
+                            double* y, double* d_norm) {
+  return tt_vec_project_nrm2_dev_if(ctx, n, nvec, xs, d_coef, y, d_norm, nullptr);
 }
 
 int tt_vec_ritz_residual_dev(tt_ctx* ctx, int64_t n, int k, const double* const* vs, const double* const* vas,

@@ -85,6 +85,7 @@ _proto("tt_dmrg_set_precision", C.c_int, C.c_int, C.c_int)
 _proto("tt_dmrg_set_davidson", C.c_int)
 _proto("tt_dmrg_set_profile_step", C.c_int)
 _proto("tt_dmrg_davidson_fallbacks", PI64)
+_proto("tt_dmrg_davidson_refills", PI64)
 _proto("tt_plan_device_status", P, P, C.POINTER(C.c_int))
 _proto("tt_dmrg_unbind")
 _proto("tt_device_alloc", P, C.c_size_t, PP)
@@ -888,6 +889,13 @@ def set_davidson_control(device: bool = True):
     """tensor_davidsonIT control on the device (one synchronisation per call,
     host loop on Gram-Schmidt failure) or on the host (reads back every iteration)."""
     _chk(lib.tt_dmrg_set_davidson(int(device)), "set_davidson")
+
+
+def davidson_refills() -> int:
+    """Gram-Schmidt failures refilled inside the device-resident loop (this thread)."""
+    n = I64()
+    _chk(lib.tt_dmrg_davidson_refills(C.byref(n)), "davidson_refills")
+    return n.value
 
 
 def davidson_fallbacks() -> int:

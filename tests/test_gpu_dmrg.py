@@ -130,3 +130,28 @@ def test_noise_schedule_converges_to_the_noise_free_ground_state(ctx):
     # while on, noise changes the kept bases, hence the early sweep energies
     early = [abs(x[0] - y[0]) for x, y in zip(run.sweeps()[:3], run0.sweeps()[:3])]
     assert max(early) > 1e-12
+
+
+def test_gram_schmidt_failures_are_refilled_on_the_device(ctx):
+    """Near convergence the residual's projection falls below 1e-10 and the
+    reference refills the new vector at random (linalg/tensor_davidson.cpp:
+    298-316).  The device-resident loop does this itself: refills happen, no
+    call is handed to the host loop, and the result is the ED ground state."""
+    import tt_b200
+    from oracle import autompo as am
+    Nx, Ny, J2 = 4, 4, 0.5
+    N = Nx * Ny
+    terms, a = [], tt_b200.AutoMPO()
+    for s1, s2, typ, *_ in am.square_next_neighbor(Nx, Ny, True):
+        J = 1.0 if typ == 1 else J2
+        i, j = s1 - 1, s2 - 1
+        terms += [(0.5 * J, ((i, "S+"), (j, "S-"))), (0.5 * J, ((i, "S-"), (j, "S+"))), (J, ((i, "Sz"), (j, "Sz")))]
+        a.add(0.5 * J, "S+", i, "S-", j).add(0.5 * J, "S-", i, "S+", j).add(J, "Sz", i, "Sz", j)
+    r0, f0 = tt_b200.davidson_refills(), tt_b200.davidson_fallbacks()
+    psi = tt_b200.QMPS(N, qdmrg.neel(N))
+    run = tt_b200.QDMRG(psi, tt_b200.QMPO.from_autompo(a, N))
+    e = run.run(8, [32, 64, 128, 256, 256, 256, 256, 256], [1e-12], [6])
+    assert tt_b200.davidson_refills() > r0
+    assert tt_b200.davidson_fallbacks() == f0
+    Eed = ed.terms_ground_energy(N, terms, N // 2)
+    assert abs(e - Eed) <= 1e-8 * abs(Eed)

@@ -151,6 +151,16 @@ int tt_contract_plan(tt_ctx* ctx, const tt_out_block* outs, int n_out,
                      tt_plan** plan);
 int tt_contract_exec(tt_ctx* ctx, const tt_plan* plan, const double* A,
                      const double* B, double* C, double alpha);
+/* tt_contract_exec that keeps packed operands: bit 0 of keep keeps A's
+ * tensor-core packing (TF32 hi/lo tiles) in the plan after the exec and reuses
+ * it in later execs given the same A pointer, bit 1 the same for B -- for an
+ * operand that stays fixed over many execs, such as the environments of one
+ * Davidson call.  The caller vouches that the data behind a kept pointer has
+ * not changed, and releases the packings (tt_plan_release_packed, or the plan's
+ * destruction) before it does.  FP64 plans ignore keep. */
+int tt_contract_exec_keep(tt_ctx* ctx, const tt_plan* plan, const double* A, const double* B, double* C,
+                          double alpha, int keep);
+int tt_plan_release_packed(tt_ctx* ctx, const tt_plan* plan);
 int tt_plan_destroy(tt_ctx* ctx, tt_plan* plan);
 /* Algorithmic work of one exec: sum over pairs of 2*m*n*k. */
 /* Device bytes a plan holds (offset tables, tasks, packing jobs). */

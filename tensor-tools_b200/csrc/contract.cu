@@ -713,6 +713,10 @@ struct tt_plan {
   int n_out = 0;
   double flops = 0.0;
   int64_t dev_bytes = 0;  // device memory the plan holds (tables, tasks, packing jobs)
+  // tensor-core path: packed operands kept between execs (tt_contract_exec_keep)
+  // and the operand each was packed from; released by tt_plan_release_packed
+  mutable uint8_t* kept[2] = {nullptr, nullptr};
+  mutable const double* kept_src[2] = {nullptr, nullptr};
   TaskDev* d_tasks = nullptr;
   OutDev* d_outs = nullptr;
   PairDev* d_pairs = nullptr;
@@ -923,6 +927,21 @@ int tt_contract_plan(tt_ctx* ctx, const tt_out_block* outs, int n_out,
 
 int tt_contract_exec(tt_ctx* ctx, const tt_plan* plan, const double* A, const double* B,
                      double* C, double alpha) {
+  return tt_contract_exec_keep(ctx, plan, A, B, C, alpha, 0);
+}
+
+int tt_plan_release_packed(tt_ctx* ctx, const tt_plan* plan) {
+  TT_REQUIRE(ctx && plan, "tt_plan_release_packed: null argument");
+  for (int w = 0; w < 2; ++w) {
+    tt::pool_free(ctx, plan->kept[w]);
+    plan->kept[w] = nullptr;
+    plan->kept_src[w] = nullptr;
+  }
+  return TT_OK;
+}
+
+int tt_contract_exec_keep(tt_ctx* ctx, const tt_plan* plan, const double* A, const double* B, double* C,
+                          double alpha, int keep) {
   TT_REQUIRE(ctx && plan, "tt_contract_exec: null argument");
   if (plan->n_tasks == 0) return TT_OK;
   static thread_local uint64_t attr_set = 0;  // per host thread and device
@@ -944,24 +963,48 @@ int tt_contract_exec(tt_ctx* ctx, const tt_plan* plan, const double* A, const do
     TT_LAUNCH_CHECK(ctx);
     return TT_OK;
   }
-  // pack both operands into tensor-core tiles (pool buffers, released in stream order)
+  // pack the operands into tensor-core tiles (pool buffers, released in
+  // stream order); an operand kept from an earlier exec of this plan, packed
+  // from the same source, is reused as it is
   const bool split = plan->precision == TT_PREC_TF32X3;
-  uint8_t* pa = tt::pool_alloc<uint8_t>(ctx, (size_t)std::max<int64_t>(plan->bytesA, 16));
-  uint8_t* pb = tt::pool_alloc<uint8_t>(ctx, (size_t)std::max<int64_t>(plan->bytesB, 16));
+  const double* src[2] = {A, B};
+  const int64_t bytes[2] = {plan->bytesA, plan->bytesB};
+  uint8_t* pk[2] = {nullptr, nullptr};
+  bool fresh[2] = {false, false};
+  for (int w = 0; w < 2; ++w) {
+    const bool k = (keep >> w) & 1;
+    if (k && plan->kept[w] && plan->kept_src[w] == src[w]) {
+      pk[w] = plan->kept[w];
+      continue;
+    }
+    if (k && plan->kept[w]) {  // kept from another source: stale
+      tt::pool_free(ctx, plan->kept[w]);
+      plan->kept[w] = nullptr;
+      plan->kept_src[w] = nullptr;
+    }
+    pk[w] = tt::pool_alloc<uint8_t>(ctx, (size_t)std::max<int64_t>(bytes[w], 16));
+    fresh[w] = true;
+  }
+  uint8_t* pa = pk[0];
+  uint8_t* pb = pk[1];
   if (!pa || !pb) {
-    tt::pool_free(ctx, pa);
-    tt::pool_free(ctx, pb);
+    if (fresh[0]) tt::pool_free(ctx, pa);
+    if (fresh[1]) tt::pool_free(ctx, pb);
     return tt::fail(TT_ERR_OOM, "tt_contract_exec: packed operand allocation failed");
   }
-  if (plan->n_tilesA + plan->n_tilesB > 0) {
-    const unsigned nt = (unsigned)(plan->n_tilesA + plan->n_tilesB);
-    if (split)
-      pack_tf32_ab<true><<<nt, 128, 0, ctx->stream>>>(plan->d_jobsA, plan->d_tilesA, plan->n_tilesA, plan->d_jobsB,
-                                                       plan->d_tilesB, plan->d_tab, A, B, pa, pb);
-    else
-      pack_tf32_ab<false><<<nt, 128, 0, ctx->stream>>>(plan->d_jobsA, plan->d_tilesA, plan->n_tilesA, plan->d_jobsB,
-                                                        plan->d_tilesB, plan->d_tab, A, B, pa, pb);
-    TT_LAUNCH_CHECK(ctx);
+  {
+    // one launch for the operands that need packing: tiles [0, na) of A, then those of B
+    const int na = fresh[0] ? plan->n_tilesA : 0, nb = fresh[1] ? plan->n_tilesB : 0;
+    if (na + nb > 0) {
+      const unsigned nt = (unsigned)(na + nb);
+      if (split)
+        pack_tf32_ab<true><<<nt, 128, 0, ctx->stream>>>(plan->d_jobsA, plan->d_tilesA, na, plan->d_jobsB,
+                                                         plan->d_tilesB, plan->d_tab, A, B, pa, pb);
+      else
+        pack_tf32_ab<false><<<nt, 128, 0, ctx->stream>>>(plan->d_jobsA, plan->d_tilesA, na, plan->d_jobsB,
+                                                          plan->d_tilesB, plan->d_tab, A, B, pa, pb);
+      TT_LAUNCH_CHECK(ctx);
+    }
   }
   const unsigned grid = (unsigned)std::min(plan->n_tasks, std::max(1, ctx->num_sms));
   if (split)
@@ -973,8 +1016,15 @@ int tt_contract_exec(tt_ctx* ctx, const tt_plan* plan, const double* A, const do
         plan->d_tasks, plan->n_tasks, plan->d_outs, plan->d_pairtc, pa, pb, C, alpha, plan->d_status,
         ctx->d_dev_status, ctx->wait_limit);
   cudaError_t le = cudaGetLastError();
-  tt::pool_free(ctx, pa);
-  tt::pool_free(ctx, pb);
+  for (int w = 0; w < 2; ++w) {
+    if (!fresh[w]) continue;
+    if ((keep >> w) & 1) {
+      plan->kept[w] = pk[w];
+      plan->kept_src[w] = src[w];
+    } else {
+      tt::pool_free(ctx, pk[w]);
+    }
+  }
   if (le != cudaSuccess) return tt::cuda_fail(le, "tt_contract_exec: tensor-core launch", __FILE__, __LINE__);
   tt::count_launch(ctx);
   return TT_OK;
@@ -983,6 +1033,7 @@ int tt_contract_exec(tt_ctx* ctx, const tt_plan* plan, const double* A, const do
 int tt_plan_destroy(tt_ctx* ctx, tt_plan* plan) {
   if (!plan) return TT_OK;
   if (ctx) {
+    tt_plan_release_packed(ctx, plan);
     tt::pool_free(ctx, plan->d_tasks);
     tt::pool_free(ctx, plan->d_outs);
     tt::pool_free(ctx, plan->d_pairs);

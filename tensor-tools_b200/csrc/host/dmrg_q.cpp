@@ -120,6 +120,13 @@ using Presence = std::vector<uint8_t>;
 
 class ProductEngine {
  public:
+  ~ProductEngine() {
+    std::sort(kept_.begin(), kept_.end());
+    kept_.erase(std::unique(kept_.begin(), kept_.end()), kept_.end());
+    for (tt_plan* p : kept_) tt_plan_release_packed(ctx(), p);
+  }
+  ProductEngine(const ProductEngine&) = delete;
+  ProductEngine& operator=(const ProductEngine&) = delete;
   ProductEngine(big_qtensor& A, const qtensor& x) : A_(A), x_(x) {
     if (!A_.left() || !A_.right()) throw std::runtime_error("tensor_davidsonIT: L and R must be set");
     // the block set: x's blocks, then the blocks the product adds, until closed
@@ -186,14 +193,21 @@ class ProductEngine {
             "pack");
   }
 
-  // y = H_eff * v on the whole layout (absent blocks of v are zero)
+  // y = H_eff * v on the whole layout (absent blocks of v are zero).  L and
+  // R stay fixed through a Davidson call, so in the tensor-core form their
+  // packed tiles are kept in the plans from the first product of the call to
+  // the engine's end (~ProductEngine releases them).
   void apply(const double* v, double* y, int precision = TT_PREC_FP64) {
-    if (tt_plan* p = c1_->plan_for(precision))
-      check(tt_contract_exec(ctx(), p, L_data(), v, i1_->get(), 1.0), "heff L*v");
+    if (tt_plan* p = c1_->plan_for(precision)) {
+      check(tt_contract_exec_keep(ctx(), p, L_data(), v, i1_->get(), 1.0, 1), "heff L*v");
+      kept_.push_back(p);
+    }
     if (tt_plan* p = c2_->plan_for(precision))
       check(tt_contract_exec(ctx(), p, i1_->get(), A_.mid().data->get(), i2_->get(), 1.0), "heff *mid");
-    if (tt_plan* p = c3_->plan_for(precision))
-      check(tt_contract_exec(ctx(), p, i2_->get(), A_.right()->data->get(), y, 1.0), "heff *R");
+    if (tt_plan* p = c3_->plan_for(precision)) {
+      check(tt_contract_exec_keep(ctx(), p, i2_->get(), A_.right()->data->get(), y, 1.0, 2), "heff *R");
+      kept_.push_back(p);
+    }
     for (auto& r : zero_ranges_)
       check(tt_memset_zero(ctx(), y + r.first, sizeof(double) * (size_t)r.second), "heff zero");
   }
@@ -230,6 +244,7 @@ class ProductEngine {
   DevPtr i1_, i2_;
   std::vector<std::pair<int64_t, int64_t>> zero_ranges_;
   std::map<Presence, Presence> pcache_;
+  std::vector<tt_plan*> kept_;  // plans holding a packed L or R of this call
 
   const double* L_data() const { return A_.left()->data->get(); }
 

@@ -76,6 +76,16 @@ C5_N = C5["Nx"] * C5["Ny"]
 C5_MID = C5_N // 2 - C5["block"] // 2          # 46: the block spans sites 46..50
 C5_UPDATES_PER_SWEEP = 2 * (C5_N - 1)           # 190
 CHOSEN = "tf32x3-auto"
+# the environment updates stay in FP64 in the chosen form: each of their
+# operands is used once, so the TF32 packing does not pay for itself, and
+# FP64 environments keep the Ritz values free of a first-order bias
+ENV_PREC = "fp64"
+
+
+def c5_ramp(args):
+    """The ramp's bond dimensions below the workload's (a smaller --maxdim,
+    e.g. for a profiler capture, stops the ramp early)."""
+    return [m for m in C5["ramp"] if m < args.maxdim]
 
 
 def c5_config(args):
@@ -86,7 +96,7 @@ def c5_config(args):
                                                                                            args.max_restart),
         "L": C5_N, "maxdim": args.maxdim, "cutoff": C5["cutoff"], "max_restart": args.max_restart,
         "setup": "untimed ramp maxdim %s with noise 1e-6 -> 0 over those sweeps, one sweep at maxdim %d, "
-                 "checkpoint; per precision: load, buildEnv, centre to site %d" % (C5["ramp"], args.maxdim, C5_MID),
+                 "checkpoint; per precision: load, buildEnv, centre to site %d" % (c5_ramp(args), args.maxdim, C5_MID),
         "step": "%d two-site updates at maxdim %d: left-to-right over sites %d..%d and back" % (
             2 * args.block, args.maxdim, C5_MID, C5_MID + args.block - 1),
         "value_definition": "mean seconds per timed two-site update x %d updates per sweep" % C5_UPDATES_PER_SWEEP,
@@ -107,7 +117,8 @@ def parse():
     p.add_argument("--block", type=int, default=C5["block"])
     p.add_argument("--e2e-steps", type=int, default=2)
     p.add_argument("--cpu-budget", type=float, default=30.0, help="seconds of CPU baseline sampling (rank 0)")
-    p.add_argument("--ref-budget", type=float, default=240.0, help="seconds of timed updates of the reference arm")
+    p.add_argument("--ref-budget", type=float, default=900.0,
+                   help="seconds of warm-up and timed updates of the reference arm")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-full-sweep", action="store_true")
     p.add_argument("--breakdown", action="store_true", help="one further step per precision with phase times")
@@ -331,38 +342,54 @@ class OracleMidChain:
         return e
 
 
-def oracle_updates(chi, max_restart, budget_s, max_updates, seed=0):
-    """Set-up (untimed) plus timed oracle updates until the budget is spent
-    (at least one).  Returns (mean seconds per update, updates timed, set-up seconds, bond dims)."""
+def oracle_updates(chi, max_restart, budget_s, max_updates, warmup=0, seed=0):
+    """Set-up (untimed), `warmup` untimed oracle updates, then timed updates
+    until `max_updates` or the budget is spent (at least one).  Returns (mean
+    seconds per update, updates timed, warm-up updates run, set-up seconds,
+    bond dims)."""
     t0 = time.perf_counter()
     om = OracleMidChain(chi, max_restart, seed=seed)
     setup = time.perf_counter() - t0
-    times = []
     t_start = time.perf_counter()
+    done_w = 0
+    t_w = 0.0
+    for _ in range(warmup):
+        t1 = time.perf_counter()
+        om.update()
+        done_w += 1
+        t_w = time.perf_counter() - t1
+        if time.perf_counter() - t_start + (max_updates + warmup - done_w) * t_w > budget_s:
+            break  # keep the budget for the timed updates
+    times = []
     while len(times) < max(1, max_updates):
         t1 = time.perf_counter()
         om.update()
         times.append(time.perf_counter() - t1)
         if time.perf_counter() - t_start + statistics.mean(times) > budget_s:
             break
-    return statistics.mean(times), len(times), setup, om.bond_dims
+    return statistics.mean(times), len(times), done_w, setup, om.bond_dims
 
 
 def run_reference(args):
+    """The reference arm: one step is one real oracle two-site update at the
+    workload's bond dimension (the GPU arm's step is a block of eight), run
+    on all host cores; W untimed updates first, then K timed ones, within
+    --ref-budget seconds."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     if args.workload == "heisenberg":
         return run_heisenberg_reference(args)
-    t_upd, n, setup, dims = oracle_updates(args.maxdim, args.max_restart, args.ref_budget, args.steps)
+    t_upd, n, n_w, setup, dims = oracle_updates(args.maxdim, args.max_restart, args.ref_budget, args.steps,
+                                                warmup=args.warmup)
     value = t_upd * C5_UPDATES_PER_SWEEP
     sample = ("%d real oracle two-site updates (Davidson max %d iters + block SVD + environment update) at bond "
-              "dims %s in the middle of the 96-site cylinder, %.1f s each (set-up %.0f s untimed); warm-up skipped "
-              "(no compilation on the host path); updates capped by a %.0f s budget" %
-              (n, args.max_restart, dims, t_upd, setup, args.ref_budget))
+              "dims %s in the middle of the 96-site cylinder, %.1f s each, after %d untimed ones (set-up %.0f s "
+              "untimed); a step is one update; s/sweep = s/update x %d updates per sweep" %
+              (n, args.max_restart, dims, t_upd, n_w, setup, C5_UPDATES_PER_SWEEP))
     cores = os.cpu_count()
     line = {"metric": METRIC, "value": value, "unit": "s/sweep", "n_gpus": args.gpus, "steps": n,
-            "warmup": 0, "ms_per_step": t_upd * 1e3, "higher_is_better": False, "scaling": "weak",
+            "warmup": n_w, "ms_per_step": t_upd * 1e3, "higher_is_better": False, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": c5_config(args),
             "impl": "reference",
             "cpu_baseline": {"value": value, "unit": "s/sweep", "cores": cores, "kind": "port", "sample": sample},
@@ -376,14 +403,15 @@ def run_reference(args):
 def c5_setup(tt_b200, H, args, workdir):
     """Untimed ramp in the chosen form, one sweep at maxdim, checkpoint."""
     from oracle import qdmrg
-    tt_b200.set_precision(heff=CHOSEN, env=CHOSEN)
+    tt_b200.set_precision(heff=CHOSEN, env=ENV_PREC)
     t0 = time.perf_counter()
     try:
         psi = tt_b200.QMPS(C5_N, qdmrg.neel(C5_N))
         run = tt_b200.QDMRG(psi, H)
         energies = []
-        n = len(C5["ramp"])
-        for k, m in enumerate(C5["ramp"]):
+        ramp = c5_ramp(args)
+        n = len(ramp)
+        for k, m in enumerate(ramp):
             energies.append(run.sweep(m, C5["cutoff"], args.max_restart, C5["noise0"] * (1.0 - k / n)))
         energies.append(run.sweep(args.maxdim, C5["cutoff"], args.max_restart, 0.0))
         run.finish()
@@ -397,11 +425,25 @@ def c5_setup(tt_b200, H, args, workdir):
     return ck + ".ttmps", info
 
 
-def c5_arm(prec, ck, H, args, ctx, stream, flush, torch, tt_b200, sampler=None, e2e_steps=0):
+# <Sz_i Sz_j> pairs in the middle of the cylinder (0-based sites, snake order):
+# along the snake, one column over, and two columns over
+C5_SZSZ_PAIRS = [(47, 48), (47, 47 + C5["Ny"]), (47, 47 + 2 * C5["Ny"])]
+
+
+def szsz_mpos(tt_b200):
+    out = []
+    for i, j in C5_SZSZ_PAIRS:
+        a = tt_b200.AutoMPO()
+        a.add(1.0, "Sz", i, "Sz", j)
+        out.append(tt_b200.QMPO.from_autompo(a, C5_N))
+    return out
+
+
+def c5_arm(prec, ck, H, args, ctx, stream, flush, torch, tt_b200, sampler=None, e2e_steps=0, szsz=None):
     """Load, centre to the block, W warm-up and K timed block steps (CUDA
     events on the library stream, L2 flushed before each), then the FP64
     energy, optional end-to-end steps and a full sweep."""
-    tt_b200.set_precision(heff=prec, env=prec)
+    tt_b200.set_precision(heff=prec, env=ENV_PREC)
     res = {"precision": prec}
     B, mid = args.block, C5_MID
     cut, mr, md = C5["cutoff"], args.max_restart, args.maxdim
@@ -422,6 +464,8 @@ def c5_arm(prec, ck, H, args, ctx, stream, flush, torch, tt_b200, sampler=None, 
         if sampler:
             sampler.start()
         times = []
+        # NVTX range "c5_timed_<precision>": lets a profiler's launch list cover the timed steps only
+        torch.cuda.nvtx.range_push("c5_timed_" + prec)
         for _ in range(args.steps):
             flush.zero_()
             torch.cuda.synchronize()
@@ -431,6 +475,7 @@ def c5_arm(prec, ck, H, args, ctx, stream, flush, torch, tt_b200, sampler=None, 
             e1.record(stream)
             e1.synchronize()
             times.append(e0.elapsed_time(e1) * 1e-3)
+        torch.cuda.nvtx.range_pop()
         ctx.sync()
         clocks = sampler.stop() if sampler else None
         st1, launches = run.stats(), ctx.launches() - l0
@@ -470,8 +515,11 @@ def c5_arm(prec, ck, H, args, ctx, stream, flush, torch, tt_b200, sampler=None, 
                 "env": statistics.mean(p[3] for p in prof), "largest_svd_sector": max(p[0] for p in prof)}
         # FP64 energy of the state after the identical schedule
         tt_b200.set_precision()
-        res["energy"] = psi.expectation(H) / psi.overlap()
-        tt_b200.set_precision(heff=prec, env=prec)
+        nrm = psi.overlap()
+        res["energy"] = psi.expectation(H) / nrm
+        if szsz:
+            res["szsz"] = [psi.expectation(m) / nrm for m in szsz]
+        tt_b200.set_precision(heff=prec, env=ENV_PREC)
         if e2e_steps > 0:
             # through the public C ABI: the block's site tensors from pinned host memory every step
             first, last = mid, mid + B + 2
@@ -546,12 +594,13 @@ def run_c5(args):
         ck, setup = c5_setup(tt_b200, H, args, workdir)
         barrier()
         sampler = ClockSampler(local)
+        sz = szsz_mpos(tt_b200)
         chosen = c5_arm(CHOSEN, ck, H, args, ctx, stream, flush, torch, tt_b200, sampler=sampler,
-                        e2e_steps=args.e2e_steps)
+                        e2e_steps=args.e2e_steps, szsz=sz)
         print("[bench] %s arm: %.3f s/sweep, pool GB %s" % (CHOSEN, chosen["value"], ["%.1f" % (v / 2 ** 30)
                                                              for v in ctx.memory()]), file=sys.stderr, flush=True)
         barrier()
-        fp64 = c5_arm("fp64", ck, H, args, ctx, stream, flush, torch, tt_b200)
+        fp64 = c5_arm("fp64", ck, H, args, ctx, stream, flush, torch, tt_b200, szsz=sz)
         barrier()
     finally:
         shutil.rmtree(workdir, ignore_errors=True)
@@ -574,6 +623,9 @@ def run_c5(args):
                                  n, dims, t_upd, setup_s, C5_UPDATES_PER_SWEEP)}
         de = abs(chosen["energy"] - fp64["energy"]) / C5_N
         chosen["dE_per_site_vs_fp64"] = de
+        if "szsz" in chosen and "szsz" in fp64:
+            chosen["szsz_pairs"] = C5_SZSZ_PAIRS
+            chosen["szsz_max_abs_err_vs_fp64"] = max(abs(a - b) for a, b in zip(chosen["szsz"], fp64["szsz"]))
         chosen["speedup_vs_fp64"] = fp64["value"] / chosen["value"]
         if "seconds" in chosen.get("full_sweep", {}) and "seconds" in fp64.get("full_sweep", {}):
             chosen["full_sweep"]["speedup_vs_fp64"] = fp64["full_sweep"]["seconds"] / chosen["full_sweep"]["seconds"]
@@ -597,7 +649,7 @@ def run_c5(args):
             "warmup": args.warmup, "ms_per_step": chosen["ms_per_step"], "higher_is_better": False,
             "scaling": "weak", "vs_baseline": None, "dtype": "tf32x3+f64", "data": "synthetic",
             "config": dict(c5_config(args), precision=CHOSEN + ": 3xTF32 tcgen05 or FP64 DMMA per contraction "
-                           "(cost model) for H_eff*x and environments; FP64 Gram-Schmidt, Rayleigh-Ritz, block "
+                           "(cost model) for H_eff*x; FP64 environments, Gram-Schmidt, Rayleigh-Ritz, block "
                            "SVD and energies", parallelism="replicas" if world > 1 else "single", **setup),
             "heff_tflops": chosen["heff_tflops"],
             "roofline": chosen["roofline"],

@@ -292,6 +292,9 @@ class SweepLog:
     def __init__(self):
         self.energies = []
         self.trunc = []
+        self.cut_gaps = []
+        self.randomized = []
+        self.step_matvecs = []
         self.bond_dims = []
         self.entropy = []
         self.matvecs = 0
@@ -325,6 +328,9 @@ def update_site(psi: QMPS, H: QMPO, TR, TL, site: int, direction: int, max_bd: i
     if log is not None:
         log.energies.append(energy)
         log.trunc.append((info.trunc_err, info.kept, tuple(info.kept_per_sector)))
+        log.cut_gaps.append(min(info.cut_gap, info.cutoff_margin))
+        log.randomized.append(stats.randomized)
+        log.step_matvecs.append(stats.matvecs)
         log.matvecs += stats.matvecs
         mid_bond = (site == psi.length // 2 - 1) if direction == MoveFromLeft else (site == psi.length // 2)
         if mid_bond:

@@ -28,6 +28,11 @@ class TruncInfo:
         self.kept_per_sector = []
         self.sector_qn = []
         self.svals = []
+        # how close the cut came to going the other way: the relative gap
+        # between the last kept and the first dropped singular value, and the
+        # relative margin of the discarded weight against the cutoff
+        self.cut_gap = float("inf")
+        self.cutoff_margin = float("inf")
 
 
 def find_index_permutation(frm: List[QIndex], to: List[QIndex]) -> List[int]:
@@ -123,7 +128,9 @@ def svd(A: QTensor, left: List[QIndex], right: List[QIndex], direction: int,
     new_dim = [0] * len(mid_Q)
     cumsum = 0.0
     acc = 0
+    prev_disc = 1.0
     for sv, ii, _ in S_and_idx:  # :1291-1300
+        prev_disc = 1 - cumsum
         cumsum += sv * sv / nm
         if sv == 0.0 and cutoff != 0.0:
             break
@@ -132,6 +139,11 @@ def svd(A: QTensor, left: List[QIndex], right: List[QIndex], direction: int,
         if (1 - cumsum < cutoff and cutoff != 0.0) or (acc >= K and K != 0):
             break
     if info is not None:
+        if 0 < acc < len(S_and_idx) and S_and_idx[acc - 1][0] > 0.0:
+            s_last, s_next = S_and_idx[acc - 1][0], S_and_idx[acc][0]
+            info.cut_gap = (s_last - s_next) / s_last
+        if cutoff != 0.0 and acc > 0:
+            info.cutoff_margin = min(abs(prev_disc - cutoff), abs((1 - cumsum) - cutoff)) / cutoff
         info.trunc_err = max(1 - cumsum, 0.0)
         info.kept = acc
         info.kept_per_sector = [d for d in new_dim]

@@ -460,6 +460,8 @@ def c5_arm(prec, ck, H, args, ctx, stream, flush, torch, tt_b200, sampler=None, 
             step()
         ctx.sync()
         st0, fb0, l0 = run.stats(), tt_b200.davidson_fallbacks(), ctx.launches()
+        pc0 = tt_b200.planning_counters()
+        er0 = tt_b200.eig_redo_count(ctx)
         s0 = len(run.steps())
         if sampler:
             sampler.start()
@@ -479,6 +481,8 @@ def c5_arm(prec, ck, H, args, ctx, stream, flush, torch, tt_b200, sampler=None, 
         ctx.sync()
         clocks = sampler.stop() if sampler else None
         st1, launches = run.stats(), ctx.launches() - l0
+        pc1 = tt_b200.planning_counters()
+        er1 = tt_b200.eig_redo_count(ctx)
         steps = run.steps()[s0:]
         t_step = statistics.mean(times)
         upd = 2 * B
@@ -492,6 +496,10 @@ def c5_arm(prec, ck, H, args, ctx, stream, flush, torch, tt_b200, sampler=None, 
             "heff_tflop_per_step": fl / max(1, args.steps) / 1e12,
             "gpu_launches": int(launches), "launches_per_step": launches / max(1, args.steps),
             "davidson_fallbacks": tt_b200.davidson_fallbacks() - fb0,
+            "host_planning_s_per_update": ((pc1["structure_s"] - pc0["structure_s"]) + (pc1["plan_s"] - pc0["plan_s"]))
+            / max(1, args.steps * 2 * B),
+            "plans_per_update": (pc1["plans"] - pc0["plans"]) / max(1, args.steps * 2 * B),
+            "eig_redos": er1 - er0,
             "matvecs_per_update": statistics.mean(s["matvecs"] for s in steps) if steps else None,
             "trunc_err_mean": statistics.mean(s["trunc_err"] for s in steps) if steps else None,
             "kept": [s["kept"] for s in steps[-upd:]],
@@ -615,7 +623,7 @@ def run_c5(args):
     if rank == 0:
         cpu = None
         if not args.no_cpu_baseline:
-            t_upd, n, setup_s, dims = oracle_updates(args.maxdim, args.max_restart, args.cpu_budget, 1)
+            t_upd, n, _, setup_s, dims = oracle_updates(args.maxdim, args.max_restart, args.cpu_budget, 1)
             cpu = {"value": t_upd * C5_UPDATES_PER_SWEEP, "unit": "s/sweep", "cores": os.cpu_count(),
                    "kind": "port",
                    "sample": "%d real oracle two-site update(s) at bond dims %s in the middle of the cylinder "

@@ -336,6 +336,11 @@ int tt_sym_eigvals_batched(tt_ctx* ctx, const tt_eig_problem* probs, int n_probs
 int tt_sym_eigvecs_batched(tt_ctx* ctx, const tt_eig_problem* probs, int n_probs, const int* nvec,
                            const double* G, const double* T, const double* w, double* Z,
                            double* work, const double* A);
+/* Problems (since the process started, all contexts on the device) whose
+ * CholeskyQR2 found an inverse-iteration vector collapsed onto earlier ones,
+ * so that the cluster kernel recomputed their eigenvectors; synchronises the
+ * context's stream. */
+int tt_eig_redo_count(tt_ctx* ctx, int64_t* count);
 
 #ifdef __cplusplus
 }

@@ -56,15 +56,33 @@ __device__ double block_reduce(double v, double* red, bool is_max) {
   return red[32];
 }
 
-// number of eigenvalues of T (diag d, squared offdiag e2) that are < x
+// number of eigenvalues of T (diag d, squared offdiag e2) that are < x: the
+// sign changes of the Sturm sequence p_i = (d_i - x) p_{i-1} - e2_{i-1} p_{i-2}
+// of leading principal minors (Golub & Van Loan, "Matrix Computations", 4th
+// ed., sec. 8.4.1), counted as LAPACK's dlaebz counts the non-positive pivots
+// q_i = p_i / p_{i-1} of T - x I -- without its division per step: a pivot
+// with |q_i| <= pivmin is replaced by a tiny negative one (here p_i = -p_{i-1}
+// 2^-200, which steers the next step as q = -pivmin does), and the pair
+// (p_{i-1}, p_i) is rescaled by a power of two when p_i leaves [2^-400, 2^400]
 __device__ int sturm_count(const double* d, const double* e2, int n, double x, double pivmin) {
-  double q = d[0] - x;
-  if (fabs(q) <= pivmin) q = -pivmin;
-  int c = q <= 0.0;
+  double pm = 1.0;
+  double p = d[0] - x;
+  if (fabs(p) <= pivmin) p = -pivmin;
+  int c = p <= 0.0;
   for (int i = 1; i < n; ++i) {
-    q = d[i] - x - e2[i - 1] / q;
-    if (fabs(q) <= pivmin) q = -pivmin;
-    c += q <= 0.0;
+    double pn = fma(d[i] - x, p, -e2[i - 1] * pm);
+    if (fabs(pn) <= pivmin * fabs(p)) pn = -p * 0x1p-200;
+    c += (pn < 0.0) != (p < 0.0);
+    const double a = fabs(pn);
+    if (a > 0x1p400 || a < 0x1p-400) {
+      int ex;
+      frexp(pn, &ex);
+      const double sc = ldexp(1.0, -ex);
+      pn *= sc;
+      p *= sc;
+    }
+    pm = p;
+    p = pn;
   }
   return c;
 }
@@ -234,11 +252,11 @@ tridiag_eigvals(const EigDev* __restrict__ probs, double* G, double* Tg, double*
 }
 
 // solve (T - lambda I) y = b in place (y holds b on entry); U holds 3n scratch
+// The LU factors go to u0, u1, u2, entry i at [i * ustride] (ustride > 1
+// interleaves the factors of neighbouring threads, so that their accesses
+// coalesce); y's entry i is at [i * ystride].
 __device__ void tri_solve(const double* d, const double* e, int n, double lambda, double tiny, double* y,
-                          double* U, int ystride) {
-  double* u0 = U;
-  double* u1 = U + n;
-  double* u2 = U + 2 * n;
+                          double* u0, double* u1, double* u2, int ystride, int ustride) {
   // forward elimination with partial pivoting, transforming b on the fly
   double di = d[0] - lambda, si = n > 1 ? e[0] : 0.0, ti = 0.0;
   double bi = y[0];
@@ -250,9 +268,9 @@ __device__ void tri_solve(const double* d, const double* e, int n, double lambda
     if (fabs(di) >= fabs(ci)) {
       if (di == 0.0) di = tiny;
       double mlt = ci / di;
-      u0[i] = di;
-      u1[i] = si;
-      u2[i] = ti;
+      u0[(int64_t)i * ustride] = di;
+      u1[(int64_t)i * ustride] = si;
+      u2[(int64_t)i * ustride] = ti;
       y[(int64_t)i * ystride] = bi;
       bi = bnext - mlt * bi;
       double nd = an - mlt * si, ns = bn - mlt * ti;
@@ -261,9 +279,9 @@ __device__ void tri_solve(const double* d, const double* e, int n, double lambda
       ti = 0.0;
     } else {
       double mlt = di / ci;
-      u0[i] = ci;
-      u1[i] = an;
-      u2[i] = bn;
+      u0[(int64_t)i * ustride] = ci;
+      u1[(int64_t)i * ustride] = an;
+      u2[(int64_t)i * ustride] = bn;
       y[(int64_t)i * ystride] = bnext;
       bi = bi - mlt * bnext;
       double nd = si - mlt * an, ns = ti - mlt * bn;
@@ -273,17 +291,129 @@ __device__ void tri_solve(const double* d, const double* e, int n, double lambda
     }
   }
   if (fabs(di) < tiny) di = di < 0.0 ? -tiny : tiny;
-  u0[n - 1] = di;
+  u0[(int64_t)(n - 1) * ustride] = di;
   y[(int64_t)(n - 1) * ystride] = bi;
   // back substitution
   for (int i = n - 1; i >= 0; --i) {
     double s = y[(int64_t)i * ystride];
-    if (i + 1 < n) s -= u1[i] * y[(int64_t)(i + 1) * ystride];
-    if (i + 2 < n) s -= u2[i] * y[(int64_t)(i + 2) * ystride];
-    double piv = u0[i];
+    if (i + 1 < n) s -= u1[(int64_t)i * ustride] * y[(int64_t)(i + 1) * ystride];
+    if (i + 2 < n) s -= u2[(int64_t)i * ustride] * y[(int64_t)(i + 2) * ystride];
+    double piv = u0[(int64_t)i * ustride];
     if (fabs(piv) < tiny) piv = piv < 0.0 ? -tiny : tiny;
     y[(int64_t)i * ystride] = s / piv;
   }
+}
+
+// tri_solve for a thread's column of an interleaved batch (y, u0, u1, u2 all
+// with stride ustride), the same operations in the same order, with the
+// global loads issued PF steps ahead: the values of the next PF steps are
+// fetched while the current PF are computed (the threads of a CTA walk the
+// same rows in lockstep, so the batch's accesses coalesce and the latency of
+// one step is the arithmetic's, not memory's).
+constexpr int PF = 8;
+__device__ void tri_solve_il(const double* d, const double* e, int n, double lambda, double tiny, double* y,
+                             double* u0, double* u1, double* u2, int64_t st) {
+  // forward elimination; step i reads y[i + 1]
+  double di = d[0] - lambda, si = n > 1 ? e[0] : 0.0, ti = 0.0;
+  double bi = y[0];
+  double cur[PF], nxt[PF];
+#pragma unroll
+  for (int k = 0; k < PF; ++k) cur[k] = 1 + k < n ? y[(int64_t)(1 + k) * st] : 0.0;
+  for (int i0 = 0; i0 + 1 < n; i0 += PF) {
+#pragma unroll
+    for (int k = 0; k < PF; ++k) {
+      const int r = i0 + PF + 1 + k;
+      nxt[k] = r < n ? y[(int64_t)r * st] : 0.0;
+    }
+#pragma unroll
+    for (int k = 0; k < PF; ++k) {
+      const int i = i0 + k;
+      if (i + 1 < n) {
+        double ci = e[i];
+        double an = d[i + 1] - lambda;
+        double bn = (i + 2 < n) ? e[i + 1] : 0.0;
+        double bnext = cur[k];
+        if (fabs(di) >= fabs(ci)) {
+          if (di == 0.0) di = tiny;
+          double mlt = ci / di;
+          u0[(int64_t)i * st] = di;
+          u1[(int64_t)i * st] = si;
+          u2[(int64_t)i * st] = ti;
+          y[(int64_t)i * st] = bi;
+          bi = bnext - mlt * bi;
+          double nd = an - mlt * si, ns = bn - mlt * ti;
+          di = nd;
+          si = ns;
+          ti = 0.0;
+        } else {
+          double mlt = di / ci;
+          u0[(int64_t)i * st] = ci;
+          u1[(int64_t)i * st] = an;
+          u2[(int64_t)i * st] = bn;
+          y[(int64_t)i * st] = bnext;
+          bi = bi - mlt * bnext;
+          double nd = si - mlt * an, ns = ti - mlt * bn;
+          di = nd;
+          si = ns;
+          ti = 0.0;
+        }
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < PF; ++k) cur[k] = nxt[k];
+  }
+  if (fabs(di) < tiny) di = di < 0.0 ? -tiny : tiny;
+  u0[(int64_t)(n - 1) * st] = di;
+  y[(int64_t)(n - 1) * st] = bi;
+  // back substitution, i = n - 1 down to 0; step i reads y[i], u0[i], u1[i], u2[i]
+  double x1 = 0.0, x2 = 0.0;  // y[i + 1], y[i + 2] as solved
+  double cy[PF], c0[PF], c1[PF], c2[PF], ny[PF], n0[PF], n1[PF], n2[PF];
+#pragma unroll
+  for (int k = 0; k < PF; ++k) {
+    const int i = n - 1 - k;
+    cy[k] = i >= 0 ? y[(int64_t)i * st] : 0.0;
+    c0[k] = i >= 0 ? u0[(int64_t)i * st] : 1.0;
+    c1[k] = i >= 0 ? u1[(int64_t)i * st] : 0.0;
+    c2[k] = i >= 0 ? u2[(int64_t)i * st] : 0.0;
+  }
+  for (int b0 = n - 1; b0 >= 0; b0 -= PF) {
+#pragma unroll
+    for (int k = 0; k < PF; ++k) {
+      const int i = b0 - PF - k;
+      ny[k] = i >= 0 ? y[(int64_t)i * st] : 0.0;
+      n0[k] = i >= 0 ? u0[(int64_t)i * st] : 1.0;
+      n1[k] = i >= 0 ? u1[(int64_t)i * st] : 0.0;
+      n2[k] = i >= 0 ? u2[(int64_t)i * st] : 0.0;
+    }
+#pragma unroll
+    for (int k = 0; k < PF; ++k) {
+      const int i = b0 - k;
+      if (i >= 0) {
+        double s = cy[k];
+        if (i + 1 < n) s -= c1[k] * x1;
+        if (i + 2 < n) s -= c2[k] * x2;
+        double piv = c0[k];
+        if (fabs(piv) < tiny) piv = piv < 0.0 ? -tiny : tiny;
+        const double xi = s / piv;
+        y[(int64_t)i * st] = xi;
+        x2 = x1;
+        x1 = xi;
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < PF; ++k) {
+      cy[k] = ny[k];
+      c0[k] = n0[k];
+      c1[k] = n1[k];
+      c2[k] = n2[k];
+    }
+  }
+}
+
+// U holds the three factor rows back to back (3 n doubles)
+__device__ void tri_solve(const double* d, const double* e, int n, double lambda, double tiny, double* y,
+                          double* U, int ystride) {
+  tri_solve(d, e, n, lambda, tiny, y, U, U + n, U + 2 * n, ystride, 1);
 }
 
 __device__ __forceinline__ double hash_unit(uint64_t z) {
@@ -468,20 +598,31 @@ tridiag_eigvecs(const EigDev* __restrict__ probs, const double* G, const double*
 // formed one by one against the matrix as it stood at the start of the
 // panel, corrected on the fly by the panel's V and W (A22 v - V W^T v -
 // W V^T v), and the trailing matrix receives the rank-2nb update
-// A -= V W^T + W V^T once per panel.  Index c (row or column) belongs to CTA
-// c % CL.  Per column: the owners of rows >= j bring column j up to date and
-// push their part of |x|^2 (cluster barrier 1); every CTA forms the same
-// reflector, pushes its entries of v to every CTA and its partial V^T v,
-// W^T v (barrier 2); every CTA forms p = A22 v on its own columns (one warp
-// per column, L2-resident matrix), w' = tau (p - V W^T v - W V^T v) and its
-// part of w'.v, and the owners of the panel's rows push their w' (barrier
-// 3); then w = w' - (tau/2)(w'.v) v.  Every CTA sums the pushed partials in
-// CTA order, so every decision and scalar is the same in every CTA.  The
-// pushed buffers alternate by the parity of j, so no further barrier is
-// needed.  The trailing update goes through a global n x 2nb scratch (two
-// barriers per panel) and runs as row tiles of [V W] in shared memory
-// against each CTA's own columns.  Bisection then runs over all warps of the
-// cluster.
+// A -= V W^T + W V^T once per panel.  Only the lower triangle is read or
+// updated.  Index c (row or column) belongs to CTA c % CL.  Per column j,
+// two cluster barriers:
+//   1. the owners of rows >= j bring column j up to date and push it to
+//      every CTA (barrier A);
+//   2. every CTA forms the same reflector from the whole column (same data,
+//      same reduction order), keeps v, and pushes its partial V^T v, W^T v;
+//   3. every CTA runs A22 v over the lower triangle of its own columns: one
+//      warp per block of 64 rows, each lane two rows, columns 16 at a time;
+//      an element A[i,c] (i >= c) adds A[i,c] v_i to the dot of column c and,
+//      below the diagonal, A[i,c] v_c to row i.  The column dots are summed
+//      across the lanes by a butterfly reduce-scatter (lane k ends with
+//      column k % 16), the row sums go to the row's owner (a slot per
+//      sender), and the CTA's share of v^T A22 v to every CTA (barrier B);
+//   4. every CTA completes p = A22 v on its own rows (own dot + the pushed row
+//      sums, in CTA order), w' = tau (p - V W^T v - W V^T v) and
+//      w = w' - (tau/2)(w'.v) v with w'.v = tau (v^T A22 v - 2 (V^T v).(W^T v));
+//      the panel's rows, which every CTA needs, have their row sums and
+//      column dots pushed to every CTA.
+// Every CTA sums pushed partials in CTA order, so every decision and scalar
+// is the same in every CTA.  The trailing update goes through a global
+// n x 2nb scratch (two barriers per panel): m8n8k4 FP64 tensor-core (DMMA)
+// products of 32 rows x 16 own columns per warp, the rows' [V W] read from
+// the scratch and the columns' from shared memory.  Bisection then runs over all
+// warps of the cluster.
 //
 // Phase 2: CTA r owns eigenvectors [r q, r q + q), q = ceil(nvec / CL).
 // Inverse iteration runs one thread per vector.  Gram-Schmidt (twice, inside
@@ -500,22 +641,31 @@ namespace cgx = cooperative_groups;
 constexpr int CL_STAGE = 4;  // reflectors staged per round of the back-transformation
 constexpr int CL_MAX = 16;   // largest cluster the kernels are launched with
 constexpr int PNB_MAX = 32;  // widest panel of the blocked reduction
-constexpr int TROWS = 64;    // rows per tile of the trailing update
-
+constexpr int NWARP = TT / 32;
 
 // doubles of dynamic shared memory of the blocked cluster reduction
 __host__ __device__ inline int64_t blocked_smem(int n, int nb, int CL) {
   const int64_t nloc = (n + CL - 1) / CL;
-  return 2 * (int64_t)nb * nloc   // V, W of the panel on the own rows
-         + nloc                   // the own rows of the current column
-         + 2 * (int64_t)n         // v, by parity of the column
-         + 2 * CL_MAX * 2         // pushed |x|^2 partials and alpha
-         + 2 * CL_MAX * 2 * nb    // pushed V^T v, W^T v partials
-         + 2 * CL_MAX             // pushed w'.v partials
-         + 2 * (int64_t)nb * nb   // V, W on the panel's rows
-         + 2 * (int64_t)nb        // pushed w' on the panel's rows
-         + 2 * (int64_t)nb        // W^T v, V^T v
-         + 2 * (int64_t)nb * TROWS;  // trailing-update tile of [V W]
+  return 2 * (int64_t)nb * nloc        // V, W of the panel on the own rows
+         + 2 * nloc                    // the own rows of the current and the next column
+         + (int64_t)CL * nloc          // the pushed column, then v, owner-major
+         + (int64_t)CL * nloc          // this CTA's row sums of A22 v, owner-major
+         + (int64_t)CL * nloc          // pushed row sums of A22 v on the own rows, per sender
+         + (int64_t)NWARP * nloc       // per-warp column dots
+         + CL_MAX * 2 * (int64_t)nb    // pushed V^T v, W^T v partials
+         + CL_MAX                      // pushed v^T A22 v partials
+         + CL_MAX * (int64_t)nb        // pushed row sums on the panel's rows
+         + nb                          // pushed column dots of the panel's rows
+         + 2 * (int64_t)nb * nb        // V, W on the panel's rows
+         + 2 * (int64_t)nb;            // V^T v, W^T v
+}
+
+// D += A B for one m8n8k4 FP64 tile (DMMA): A 8x4 row fragment (lane L holds
+// A[L/4][L%4]), B 4x8 column fragment (B[L%4][L/4]), D 8x8 (D[L/4][2(L%4)+e])
+__device__ __forceinline__ void dmma_tr(double (&d)[2], double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(d[0]), "+d"(d[1])
+               : "d"(a), "d"(b));
 }
 
 __device__ __forceinline__ int first_owned(int from, int rank, int CL) {
@@ -529,11 +679,30 @@ __device__ __forceinline__ double warp_sum(double v) {
   return v;
 }
 
+// acc[k] (k < 16) summed over the 32 lanes of the warp, lane L receiving the
+// sum of index L % 16: a butterfly sum across the half-warps, then a
+// reduce-scatter (31 shuffles for 16 sums)
+__device__ __forceinline__ double warp_reduce_scatter16(double (&acc)[16], int lane) {
+#pragma unroll
+  for (int k = 0; k < 16; ++k) acc[k] += __shfl_xor_sync(0xffffffffu, acc[k], 16);
+#pragma unroll
+  for (int s = 8; s >= 1; s >>= 1) {
+    const bool up = (lane & s) != 0;
+#pragma unroll
+    for (int k = 0; k < s; ++k) {
+      const double send = up ? acc[k] : acc[k + s];
+      const double keep = up ? acc[k + s] : acc[k];
+      acc[k] = keep + __shfl_xor_sync(0xffffffffu, send, s);
+    }
+  }
+  return acc[0];
+}
+
 __global__ void __launch_bounds__(TT)
 tridiag_eigvals_cluster(const EigDev* __restrict__ probs, double* G, double* Tg, double* W, double* VWg) {
   extern __shared__ double sm[];
   __shared__ double red[33];
-  __shared__ double s_alpha, s_kpart[TT / 32];
+  __shared__ double s_K;
 
   cgx::cluster_group cluster = cgx::this_cluster();
   const int CL = (int)cluster.num_blocks();
@@ -549,55 +718,52 @@ tridiag_eigvals_cluster(const EigDev* __restrict__ probs, double* G, double* Tg,
   double* eg = dg + n;
   double* tg = eg + n;
   double* VW = VWg + P.s_off;  // n x 2nb, row-major: [i][t] = V(i, t), [i][nb + t] = W(i, t)
-  const int warp = tid >> 5, lane = tid & 31, nw = blockDim.x >> 5;
+  const int warp = tid >> 5, lane = tid & 31;
   const int nloc = (n + CL - 1) / CL;
   int lown = 0;  // own indices c = rank + CL l, l < lown
   while (lown < nloc && rank + CL * lown < n) ++lown;
-  double* tile = sm;                    // [2nb][TROWS]
-  double* Vl = tile + 2 * nb * TROWS;   // [nb][nloc]
-  double* Wl = Vl + (int64_t)nb * nloc;  // [nb][nloc]
-  double* xc = Wl + (int64_t)nb * nloc;  // [nloc]
-  double* vf = xc + nloc;               // [2][n]
-  double* rs1 = vf + 2 * n;             // [2][CL_MAX][2]
-  double* rs2 = rs1 + 2 * CL_MAX * 2;   // [2][CL_MAX][2nb]
-  double* rs3 = rs2 + 2 * CL_MAX * 2 * nb;  // [2][CL_MAX]
-  double* Vp = rs3 + 2 * CL_MAX;        // [nb][nb]: Vp[t nb + s] = v_t[k0 + s]
-  double* Wq = Vp + nb * nb;            // [nb][nb]: Wq[t nb + s] = w_t[k0 + s]
-  double* wpend = Wq + nb * nb;         // [2][nb]: pushed w' on the panel's rows
-  double* cvt = wpend + 2 * nb;         // [nb]: V^T v
-  double* cwt = cvt + nb;               // [nb]: W^T v
+  double* Vl = sm;                            // [nb][nloc]
+  double* Wl = Vl + (int64_t)nb * nloc;       // [nb][nloc]
+  double* xc = Wl + (int64_t)nb * nloc;       // [2][nloc]: own rows of a column, by parity of jj
+  // Vectors over all rows are kept owner-major: row i = r + CL l at [r nloc + l],
+  // so what one CTA pushes to another is contiguous on both sides
+  const int lg = __ffs(CL) - 1;  // CL is a power of two
+  auto om = [&](int i) { return ((i & (CL - 1)) * nloc) + (i >> lg); };
+  double* xo = xc + 2 * nloc;                 // [CL][nloc]: column j as pushed, then v
+  double* yl = xo + (int64_t)CL * nloc;       // [CL][nloc]: this CTA's row sums of A22 v
+  double* yb = yl + (int64_t)CL * nloc;       // [CL][nloc]: row sums of A22 v on the own rows, by sender
+  double* dw = yb + (int64_t)CL * nloc;       // [NWARP][nloc]: column dots by warp
+  double* r2 = dw + (int64_t)NWARP * nloc;    // [CL_MAX][2nb]: V^T v, W^T v partials by sender
+  double* r3 = r2 + CL_MAX * 2 * nb;          // [CL_MAX]: v^T A22 v partials by sender
+  double* yp = r3 + CL_MAX;                   // [CL_MAX][nb]: row sums on the panel's rows by sender
+  double* dp = yp + CL_MAX * nb;              // [nb]: column dots of the panel's rows
+  double* Vp = dp + nb;                       // [nb][nb]: Vp[t nb + s] = v_t[k0 + s]
+  double* Wq = Vp + nb * nb;                  // [nb][nb]: Wq[t nb + s] = w_t[k0 + s]
+  double* cvt = Wq + nb * nb;                 // [nb]: V^T v
+  double* cwt = cvt + nb;                     // [nb]: W^T v
   for (int k0 = 0; k0 + 2 < n; k0 += nb) {
     const int nbe = min(nb, n - 2 - k0);  // reflector columns k0 .. k0 + nbe - 1
     for (int jj = 0; jj < nbe; ++jj) {
-      const int j = k0 + jj, par = j & 1;
-      // ---- 1: column j on the own rows >= j, |x|^2 over rows >= j + 2 ----
-      if (tid == 0) s_alpha = 0.0;
-      __syncthreads();
-      double part = 0.0;
-      for (int l = tid; l < lown; l += blockDim.x) {
-        const int i = rank + CL * l;
-        if (i < j) continue;
-        double a = Gp[i + (int64_t)n * j];
+      const int j = k0 + jj;
+      double* xcur = xc + (jj & 1) * nloc;
+      // ---- 1: column j on the own rows >= j, pushed to every CTA ----
+      const int l1 = first_owned(j, rank, CL);
+      for (int l = l1 + tid; l < lown; l += blockDim.x) {
+        double a = jj == 0 ? Gp[(rank + CL * l) + (int64_t)n * j] : xcur[l];
         for (int t = 0; t < jj; ++t) a -= Vl[t * nloc + l] * Wq[t * nb + jj] + Wl[t * nloc + l] * Vp[t * nb + jj];
-        Gp[i + (int64_t)n * j] = a;
-        xc[l] = a;
-        if (i == j) dg[j] = a;
-        if (i == j + 1) s_alpha = a;
-        if (i >= j + 2) part += a * a;
+        xcur[l] = a;
       }
-      part = block_reduce(part, red, false);
-      if (tid < CL) {
-        double* dst = cluster.map_shared_rank(rs1 + (par * CL_MAX + rank) * 2, tid);
-        dst[0] = part;
-        dst[1] = s_alpha;
+      __syncthreads();
+      for (int e = tid; e < (lown - l1) * CL; e += blockDim.x) {
+        const int q = e / (lown - l1), l = l1 + e % (lown - l1);
+        *cluster.map_shared_rank(xo + rank * nloc + l, q) = xcur[l];
       }
-      cluster.sync();
-      // ---- 2: the reflector (same in every CTA), v pushed, V^T v and W^T v partials ----
-      double sigma = 0.0, alpha = 0.0;
-      for (int q = 0; q < CL; ++q) {
-        sigma += rs1[(par * CL_MAX + q) * 2];
-        alpha += rs1[(par * CL_MAX + q) * 2 + 1];
-      }
+      cluster.sync();  // A
+      // ---- 2: the reflector (same in every CTA), v kept, V^T v and W^T v partials ----
+      const double alpha = xo[om(j + 1)];  // read before the reduction's barriers, overwritten below
+      double part = 0.0;
+      for (int i = j + 2 + tid; i < n; i += blockDim.x) part += xo[om(i)] * xo[om(i)];
+      const double sigma = block_reduce(part, red, false);
       double tau = 0.0, beta = alpha, scale = 0.0;
       if (sigma != 0.0) {
         const double mu = sqrt(alpha * alpha + sigma);
@@ -606,93 +772,203 @@ tridiag_eigvals_cluster(const EigDev* __restrict__ probs, double* G, double* Tg,
         scale = 1.0 / (alpha - beta);
       }
       if (rank == j % CL && tid == 0) {
+        dg[j] = xo[om(j)];
         tg[j] = tau;
         eg[j] = beta;
       }
+      for (int i = j + 1 + tid; i < n; i += blockDim.x) xo[om(i)] = i == j + 1 ? 1.0 : xo[om(i)] * scale;
+      __syncthreads();
       for (int l = tid; l < lown; l += blockDim.x) {
         const int i = rank + CL * l;
-        const double vi = i == j + 1 ? 1.0 : (i >= j + 2 ? xc[l] * scale : 0.0);
+        const double vi = i >= j + 1 ? xo[rank * nloc + l] : 0.0;
         Vl[jj * nloc + l] = vi;
         Wl[jj * nloc + l] = 0.0;
         if (i >= j + 2) Gp[i + (int64_t)n * j] = vi;  // reflector kept below the subdiagonal for phase 2
       }
-      __syncthreads();
-      for (int e = tid; e < lown * CL; e += blockDim.x) {
-        const int l = e / CL, q = e - l * CL;
-        const int i = rank + CL * l;
-        if (i >= j + 1) *cluster.map_shared_rank(vf + par * n + i, q) = Vl[jj * nloc + l];
+      for (int s = tid; s < nb; s += blockDim.x) {
+        const int row = k0 + s;
+        Vp[jj * nb + s] = row >= j + 1 && row < n ? xo[om(row)] : 0.0;
       }
-      for (int idx = warp; idx < 2 * jj; idx += nw) {
+      __syncthreads();
+      const int lf = first_owned(j + 1, rank, CL);
+      for (int idx = warp; idx < 2 * jj; idx += NWARP) {
         const int t = idx < jj ? idx : idx - jj;
         const double* M = idx < jj ? Vl : Wl;
         double sacc = 0.0;
-        for (int l = first_owned(j + 1, rank, CL) + lane; l < lown; l += 32)
-          sacc += M[t * nloc + l] * Vl[jj * nloc + l];
+        for (int l = lf + lane; l < lown; l += 32) sacc += M[t * nloc + l] * Vl[jj * nloc + l];
         sacc = warp_sum(sacc);
-        if (lane < CL)
-          *cluster.map_shared_rank(rs2 + (par * CL_MAX + rank) * 2 * nb + (idx < jj ? t : nb + t), lane) = sacc;
+        if (lane < CL) *cluster.map_shared_rank(r2 + rank * 2 * nb + (idx < jj ? t : nb + t), lane) = sacc;
       }
-      cluster.sync();
-      // ---- 3: p = A22 v on the own columns, w' and its part of w'.v ----
-      for (int t = tid; t < jj; t += blockDim.x) {
-        double a = 0.0, b = 0.0;
-        for (int q = 0; q < CL; ++q) {
-          a += rs2[(par * CL_MAX + q) * 2 * nb + t];
-          b += rs2[(par * CL_MAX + q) * 2 * nb + nb + t];
+      // ---- 3: p = A22 v from the lower triangle of the own columns ----
+      if (jj + 1 < nbe)  // the next column's own rows: unchanged until its step 1
+        for (int l = lf + tid; l < lown; l += blockDim.x)
+          xc[((jj + 1) & 1) * nloc + l] = Gp[(rank + CL * l) + (int64_t)n * (j + 1)];
+      double kp = 0.0;  // this thread's share of v^T A22 v
+      if (tau != 0.0) {
+        for (int l = lf + lane; l < lown; l += 32) dw[warp * nloc + l] = 0.0;
+        __syncwarp();
+        // blocks of 64 rows from row j + 1, two rows per lane (i0 = rb + lane,
+        // i1 = i0 + 32); the longest (last) blocks are dealt first and back and
+        // forth, so the warps' shares come out even
+        const int nrb = (n - j - 1 + 63) / 64;
+        const int64_t cstep = (int64_t)n * CL;  // from one own column to the next
+        for (int round = 0; round * NWARP < nrb; ++round) {
+          const int o = round * NWARP + ((round & 1) ? NWARP - 1 - warp : warp);
+          if (o >= nrb) continue;
+          const int rb = j + 1 + 64 * (nrb - 1 - o);
+          const int i0 = rb + lane, i1 = i0 + 32;
+          const double v0 = i0 < n ? xo[om(i0)] : 0.0, v1 = i1 < n ? xo[om(i1)] : 0.0;
+          // rows past the end read row n - 1 (weighted by v = 0, sums discarded)
+          const double* g0 = Gp + min(i0, n - 1) + (int64_t)n * rank;
+          const double* g1 = Gp + min(i1, n - 1) + (int64_t)n * rank;
+          const int le = first_owned(min(n, rb + 64), rank, CL);  // own columns c < the block's end
+          const int lfull = min(le, first_owned(rb, rank, CL));   // own columns c < rb: no masking
+          double y0 = 0.0, y1 = 0.0;
+          int lt = lf;
+          for (; lt + 16 <= lfull; lt += 16) {
+            double acc[16];
+#pragma unroll
+            for (int h = 0; h < 16; h += 8) {  // eight columns' loads in flight at a time
+              double a0[8], a1[8];
+#pragma unroll
+              for (int k = 0; k < 8; ++k) {
+                a0[k] = g0[(lt + h + k) * cstep];
+                a1[k] = g1[(lt + h + k) * cstep];
+              }
+#pragma unroll
+              for (int k = 0; k < 8; ++k) {
+                const double vc = xo[rank * nloc + lt + h + k];
+                y0 = fma(a0[k], vc, y0);
+                y1 = fma(a1[k], vc, y1);
+                acc[h + k] = fma(a1[k], v1, a0[k] * v0);
+              }
+            }
+            const double d = warp_reduce_scatter16(acc, lane);
+            if (lane < 16) dw[warp * nloc + lt + lane] += d;
+          }
+          for (; lt < le; lt += 16) {  // the rest, masked: the block's diagonal part and a short tail
+            double acc[16];
+#pragma unroll
+            for (int h = 0; h < 16; h += 8) {
+              double a0[8], a1[8];
+#pragma unroll
+              for (int k = 0; k < 8; ++k) {
+                const int c = rank + CL * (lt + h + k);
+                const bool cv = lt + h + k < le;
+                a0[k] = cv && i0 >= c ? g0[(lt + h + k) * cstep] : 0.0;
+                a1[k] = cv && i1 >= c ? g1[(lt + h + k) * cstep] : 0.0;
+              }
+#pragma unroll
+              for (int k = 0; k < 8; ++k) {
+                const int c = rank + CL * (lt + h + k);
+                const double vc = lt + h + k < le ? xo[rank * nloc + lt + h + k] : 0.0;
+                y0 = fma(i0 > c ? a0[k] : 0.0, vc, y0);
+                y1 = fma(i1 > c ? a1[k] : 0.0, vc, y1);
+                acc[h + k] = fma(a1[k], v1, a0[k] * v0);
+              }
+            }
+            const double d = warp_reduce_scatter16(acc, lane);
+            if (lane < 16 && lt + lane < le) dw[warp * nloc + lt + lane] += d;
+          }
+          if (i0 < n) {
+            yl[om(i0)] = y0;
+            kp += v0 * y0;
+          }
+          if (i1 < n) {
+            yl[om(i1)] = y1;
+            kp += v1 * y1;
+          }
         }
-        cvt[t] = a;
-        cwt[t] = b;
       }
       __syncthreads();
-      const double* v = vf + par * n;
-      double kp = 0.0;
+      if (tau != 0.0) {
+        // the row sums to their owners (rows below j + 1 and beyond n ride
+        // along unread), those of the panel's rows to every CTA
+        const int lmin = (j + 1) >> lg, cnt = nloc - lmin;
+        for (int e = tid; e < CL * cnt; e += blockDim.x) {
+          const int d = e / cnt, l = lmin + e % cnt;
+          *cluster.map_shared_rank(yb + rank * nloc + l, d) = yl[d * nloc + l];
+        }
+        for (int e = tid; e < CL * nb; e += blockDim.x) {
+          const int q = e / nb, s = e % nb, row = k0 + s;
+          if (row >= j + 1 && row < n) *cluster.map_shared_rank(yp + rank * nb + s, q) = yl[om(row)];
+        }
+      }
       if (tau != 0.0)
-        for (int l = first_owned(j + 1, rank, CL) + warp; l < lown; l += nw) {
+        for (int l = lf + tid; l < lown; l += blockDim.x) {
+          double d = 0.0;
+          for (int w = 0; w < NWARP; ++w) d += dw[w * nloc + l];
+          dw[l] = d;  // the column's dot, kept in warp 0's row
           const int c = rank + CL * l;
-          const double* __restrict__ col = Gp + (int64_t)n * c;
-          double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
-          int i = j + 1 + lane;
-          for (; i + 96 < n; i += 128) {
-            s0 += col[i] * v[i];
-            s1 += col[i + 32] * v[i + 32];
-            s2 += col[i + 64] * v[i + 64];
-            s3 += col[i + 96] * v[i + 96];
-          }
-          for (; i < n; i += 32) s0 += col[i] * v[i];
-          double corr = 0.0;
-          for (int t = lane; t < jj; t += 32) corr += Vl[t * nloc + l] * cwt[t] + Wl[t * nloc + l] * cvt[t];
-          const double pc = warp_sum((s0 + s1) + (s2 + s3));
-          corr = warp_sum(corr);
-          const double wprime = tau * (pc - corr);
-          if (lane == 0) {
-            Wl[jj * nloc + l] = wprime;
-            kp += wprime * Vl[jj * nloc + l];
-          }
-          if (c < k0 + nb && lane < CL) *cluster.map_shared_rank(wpend + par * nb + (c - k0), lane) = wprime;
+          kp += xo[rank * nloc + l] * d;
+          if (c < k0 + nb)
+            for (int q = 0; q < CL; ++q) *cluster.map_shared_rank(dp + (c - k0), q) = d;
         }
-      if (lane == 0) s_kpart[warp] = kp;
-      __syncthreads();
-      if (tid < CL) {
-        double ksum = 0.0;
-        for (int w = 0; w < nw; ++w) ksum += s_kpart[w];
-        *cluster.map_shared_rank(rs3 + par * CL_MAX + rank, tid) = ksum;
+      const double vav_part = block_reduce(kp, red, false);
+      if (tid < CL) *cluster.map_shared_rank(r3 + rank, tid) = vav_part;
+      cluster.sync();  // B
+      // ---- 4: w on the own rows and on the panel's rows ----
+      if (warp == 0) {  // V^T v, W^T v and the scalar K = (tau/2) w'.v, one lane per panel column
+        double a = 0.0, b = 0.0;
+        if (lane < jj)
+          for (int q = 0; q < CL; ++q) {
+            a += r2[q * 2 * nb + lane];
+            b += r2[q * 2 * nb + nb + lane];
+          }
+        if (lane < jj) {
+          cvt[lane] = a;
+          cwt[lane] = b;
+        }
+        const double cc = warp_sum(a * b);
+        if (lane == 0) {
+          double vav = 0.0;
+          for (int q = 0; q < CL; ++q) vav += r3[q];
+          s_K = 0.5 * tau * tau * (vav - 2.0 * cc);
+        }
       }
-      cluster.sync();
-      // ---- 4: w = w' - (tau/2)(w'.v) v on the own rows and on the panel's rows ----
-      double K = 0.0;
-      for (int q = 0; q < CL; ++q) K += rs3[par * CL_MAX + q];
-      K *= 0.5 * tau;
-      for (int l = tid; l < lown; l += blockDim.x)
-        if (rank + CL * l >= j + 1) Wl[jj * nloc + l] -= K * Vl[jj * nloc + l];
-      for (int s2 = tid; s2 < nb; s2 += blockDim.x) {
-        const int row = k0 + s2;
-        const bool live = row >= j + 1 && row < n;
-        Vp[jj * nb + s2] = live ? v[row] : 0.0;
-        Wq[jj * nb + s2] = live && tau != 0.0 ? wpend[par * nb + s2] - K * v[row] : 0.0;
+      __syncthreads();
+      if (tau != 0.0) {
+        const double K = s_K;
+        // own rows: four threads per row, each summing a quarter of the terms
+        // (the loop bound is the same for the whole warp: the shuffles need it)
+        const int sub = tid & 3;
+        for (int base = lf + (warp << 3); base < lown; base += blockDim.x >> 2) {
+          const int l = base + (lane >> 2);
+          const bool act = l < lown;
+          double p = 0.0, corr = 0.0;
+          if (act) {
+            for (int q = sub; q < CL; q += 4) p += yb[q * nloc + l];
+            for (int t = sub; t < jj; t += 4) corr += Vl[t * nloc + l] * cwt[t] + Wl[t * nloc + l] * cvt[t];
+          }
+          p += __shfl_xor_sync(0xffffffffu, p, 1);
+          p += __shfl_xor_sync(0xffffffffu, p, 2);
+          corr += __shfl_xor_sync(0xffffffffu, corr, 1);
+          corr += __shfl_xor_sync(0xffffffffu, corr, 2);
+          if (act && sub == 0) Wl[jj * nloc + l] = tau * (dw[l] + p - corr) - K * Vl[jj * nloc + l];
+        }
+        // the panel's rows: sixteen threads per row
+        const int s = tid >> 4, sub16 = tid & 15;
+        if (s < nb) {
+          const int row = k0 + s;
+          const bool live = row >= j + 1 && row < n;
+          double p = 0.0, corr = 0.0;
+          if (live) {
+            for (int q = sub16; q < CL; q += 16) p += yp[q * nb + s];
+            for (int t = sub16; t < jj; t += 16) corr += Vp[t * nb + s] * cwt[t] + Wq[t * nb + s] * cvt[t];
+          }
+#pragma unroll
+          for (int o = 1; o < 16; o <<= 1) {
+            p += __shfl_xor_sync(0xffffffffu, p, o);
+            corr += __shfl_xor_sync(0xffffffffu, corr, o);
+          }
+          if (sub16 == 0) Wq[jj * nb + s] = live ? tau * (dp[s] + p - corr) - K * Vp[jj * nb + s] : 0.0;
+        }
+      } else {
+        for (int s = tid; s < nb; s += blockDim.x) Wq[jj * nb + s] = 0.0;
       }
       __syncthreads();
     }
-    // ---- trailing update A[k1:, k1:] -= V W^T + W V^T through the global scratch ----
+    // ---- trailing update A[k1:, k1:] -= V W^T + W V^T (lower triangle) through the global scratch ----
     const int k1 = k0 + nbe;
     for (int e = tid; e < lown * 2 * nbe; e += blockDim.x) {
       const int l = e / (2 * nbe), t2 = e - l * 2 * nbe;
@@ -703,32 +979,62 @@ tridiag_eigvals_cluster(const EigDev* __restrict__ probs, double* G, double* Tg,
     }
     __threadfence();
     cluster.sync();
+    // DMMA (m8n8k4 f64) tiles: a warp takes 32 rows x 16 own columns and runs
+    // P = V W^T + W V^T over the panel's k, the rows' [V W] fragments read
+    // straight from the scratch (no shared staging, no barrier per tile); the
+    // lower triangle of its block then receives A -= P
     const int lf = first_owned(k1, rank, CL);
-    const int r = tid % TROWS, g = tid / TROWS, ng = blockDim.x / TROWS;
-    for (int i0 = k1; i0 < n; i0 += TROWS) {
-      const int rows = min(TROWS, n - i0);
-      __syncthreads();
-      for (int e = tid; e < rows * 2 * nbe; e += blockDim.x) {
-        const int rr = e / (2 * nbe), t2 = e - rr * 2 * nbe;
-        const int col = t2 < nbe ? t2 : nb + (t2 - nbe);
-        tile[col * TROWS + rr] = VW[(int64_t)(i0 + rr) * 2 * nb + col];
-      }
-      __syncthreads();
-      if (r < rows)  // four own columns per thread: the row's [V W] values are read once for all four
-        for (int lb = lf + g; lb < lown; lb += 4 * ng) {
-          double acc[4] = {0.0, 0.0, 0.0, 0.0};
-          int lc[4];
+    const int nbe4 = (nbe + 3) & ~3;
+    const int gr = lane >> 2, gk = lane & 3;
+    const int nrt = (n - k1 + 31) >> 5;                 // 32-row tiles
+    const int ncb = (first_owned(n, rank, CL) - lf + 15) >> 4;  // 16-column blocks
+    for (int task = warp; task < nrt * ncb; task += NWARP) {
+      const int i0 = k1 + 32 * (task / ncb), lb = lf + 16 * (task % ncb);
+      if (rank + CL * lb > i0 + 31) continue;  // the block lies above the diagonal
+      const int le = min(first_owned(min(n, i0 + 32), rank, CL), lb + 16);
+      double acc[4][2][2];
 #pragma unroll
-          for (int u = 0; u < 4; ++u) lc[u] = min(lb + ng * u, lown - 1);
-          for (int t = 0; t < nbe; ++t) {
-            const double vi = tile[t * TROWS + r], wi = tile[(nb + t) * TROWS + r];
+      for (int a = 0; a < 4; ++a)
 #pragma unroll
-            for (int u = 0; u < 4; ++u) acc[u] += vi * Wl[t * nloc + lc[u]] + wi * Vl[t * nloc + lc[u]];
+        for (int b = 0; b < 2; ++b) acc[a][b][0] = acc[a][b][1] = 0.0;
+#pragma unroll
+      for (int part = 0; part < 2; ++part) {
+        // part 0: V (rows) x W (columns); part 1: W x V
+        const int xo0 = part ? nb : 0;
+        const double* Y = part ? Vl : Wl;
+#pragma unroll 2
+        for (int t = 0; t < nbe4; t += 4) {
+          const int k = t + gk;
+          const bool kv = k < nbe;
+          double af[4], bf[2];
+#pragma unroll
+          for (int a = 0; a < 4; ++a) {
+            const int i = i0 + 8 * a + gr;
+            af[a] = kv && i < n ? VW[(int64_t)i * 2 * nb + xo0 + k] : 0.0;
           }
 #pragma unroll
-          for (int u = 0; u < 4; ++u)
-            if (lb + ng * u < lown) Gp[(int64_t)n * (rank + CL * lc[u]) + i0 + r] -= acc[u];
+          for (int b = 0; b < 2; ++b) {
+            const int l = lb + 8 * b + gr;
+            bf[b] = kv && l < le ? Y[k * nloc + l] : 0.0;
+          }
+#pragma unroll
+          for (int a = 0; a < 4; ++a)
+#pragma unroll
+            for (int b = 0; b < 2; ++b) dmma_tr(acc[a][b], af[a], bf[b]);
         }
+      }
+#pragma unroll
+      for (int a = 0; a < 4; ++a) {
+        const int i = i0 + 8 * a + gr;
+#pragma unroll
+        for (int b = 0; b < 2; ++b)
+#pragma unroll
+          for (int e = 0; e < 2; ++e) {
+            const int l = lb + 8 * b + 2 * gk + e;
+            const int c = rank + CL * l;
+            if (i < n && l < le && i >= c) Gp[(int64_t)n * c + i] -= acc[a][b][e];
+          }
+      }
     }
     __threadfence();
     cluster.sync();
@@ -748,8 +1054,8 @@ tridiag_eigvals_cluster(const EigDev* __restrict__ probs, double* G, double* Tg,
   }
   __threadfence();
   cluster.sync();  // also the last access of another CTA's shared memory
-  double* d = vf;
-  double* e2 = vf + n;
+  double* d = xo;  // CL * nloc >= n doubles
+  double* e2 = yb;  // CL * nloc >= n doubles
   for (int i = tid; i < n; i += blockDim.x) {
     d[i] = dg[i];
     e2[i] = i < n - 1 ? eg[i] * eg[i] : 0.0;
@@ -777,7 +1083,7 @@ tridiag_eigvals_cluster(const EigDev* __restrict__ probs, double* G, double* Tg,
     return hi - lo > fmax(atol, 2.0 * DBL_EPSILON * fmax(fabs(lo), fabs(hi)));
   };
   const int grp = lane < 30 ? lane / 3 : 0, sub = lane % 3;
-  for (int base = (rank * nw + warp) * 10; base < n; base += CL * nw * 10) {
+  for (int base = (rank * NWARP + warp) * 10; base < n; base += CL * NWARP * 10) {
     const int j = base + grp;
     const bool active = lane < 30 && j < n;
     double lo = gl - atol, hi = gu + atol;
@@ -1057,6 +1363,7 @@ constexpr int BT_NB = 32;         // reflectors per compact-WY panel
 constexpr int BT_VB = 16;         // vectors per CTA of the back-transformation
 constexpr int BT_ROWS = 64;       // row chunk of the back-transformation
 constexpr double COLLAPSE_PIVOT2 = 1e-8;  // L_jj^2 below this: collapsed vector
+__device__ unsigned long long g_eig_redo;  // problems whose vectors the cluster kernel redid (device-wide)
 
 struct VecTask {
   int32_t prob, j0;  // problem (index into the problem array) and first item
@@ -1085,16 +1392,33 @@ inv_iter_batched(const EigDev* __restrict__ probs, const VecTask* __restrict__ t
   const double* lam = W + P.w_off;
   const double tnorm = tnorm1(d, e, n, red);
   const double tiny = tnorm > 1e-250 ? fmax(DBL_EPSILON * tnorm, DBL_MIN) : 1.0;
-  const int j = tk.j0 + threadIdx.x;
-  if (j >= P.nvec) return;
-  double* y = Zg + P.g_off + (int64_t)n * j;
-  for (int i = 0; i < n; ++i) y[i] = hash_unit(((uint64_t)P.g_off << 20) ^ ((uint64_t)j << 32) ^ (uint64_t)i);
-  for (int it = 0; it < INV_ITERS; ++it) {
-    tri_solve(d, e, n, lam[j], tiny, y, work + 3 * P.g_off + (int64_t)3 * n * j, 1);
-    double s = 0.0;
-    for (int i = 0; i < n; ++i) s += y[i] * y[i];
-    const double inv = 1.0 / sqrt(s);
-    for (int i = 0; i < n; ++i) y[i] *= inv;
+  const int t = threadIdx.x, j = tk.j0 + t;
+  const int cnt = min(IV_THREADS, P.nvec - tk.j0);  // vectors of this CTA
+  const bool active = t < cnt;  // no early return: the barrier below needs every thread
+  // the CTA's iterates and LU factors interleaved (element i of its vector t
+  // at [i cnt + t]), so that the threads' accesses coalesce: the iterates and
+  // two factor rows in the problem's work area (3 n cnt doubles from
+  // work + 3 g_off + 3 n j0), the third factor row in the CTA's own columns
+  // of Z (n cnt doubles), which receive the vectors at the end
+  double* wb = work + 3 * P.g_off + (int64_t)3 * n * tk.j0;
+  double* zb = Zg + P.g_off + (int64_t)n * tk.j0;
+  double* y = wb + t;
+  const int64_t nc = (int64_t)n * cnt;
+  if (active) {
+    for (int i = 0; i < n; ++i)
+      y[(int64_t)i * cnt] = hash_unit(((uint64_t)P.g_off << 20) ^ ((uint64_t)j << 32) ^ (uint64_t)i);
+    for (int it = 0; it < INV_ITERS; ++it) {
+      tri_solve_il(d, e, n, lam[j], tiny, y, wb + nc + t, wb + 2 * nc + t, zb + t, cnt);
+      double s = 0.0;
+      for (int i = 0; i < n; ++i) s += y[(int64_t)i * cnt] * y[(int64_t)i * cnt];
+      const double inv = 1.0 / sqrt(s);
+      for (int i = 0; i < n; ++i) y[(int64_t)i * cnt] *= inv;
+    }
+  }
+  __syncthreads();  // every thread's third factor row in Z is dead
+  if (active) {
+    double* z = zb + (int64_t)n * t;
+    for (int i = 0; i < n; ++i) z[i] = y[(int64_t)i * cnt];
   }
 }
 
@@ -1198,7 +1522,7 @@ chol_cluster(const EigDev* __restrict__ probs, double* work, int* flags, int che
         const int r = e2 % pb, c = e2 / pb;
         if (r >= c) A[(p0 + r) + (int64_t)m * (p0 + c)] = Ld[r][c];
       }
-      if (tid == 0 && s_flag) atomicExch(&flags[pi], 1);
+      if (tid == 0 && s_flag && atomicExch(&flags[pi], 1) == 0) atomicAdd(&g_eig_redo, 1ull);
     }
     // (ii) rows below the block: L[i, p0:p0+pb] = A[i, p0:p0+pb] L_pp^-T
     const int rbeg = p0 + pb;
@@ -1264,17 +1588,32 @@ trsm_rows(const EigDev* __restrict__ probs, const VecTask* __restrict__ tasks, d
   const int i0 = tk.j0;
   const int tid = threadIdx.x;
   const int r = tid & 31, cg = tid >> 5;  // row in the block, column group of 4
+  // the chunks of Z (TS_ROWS x CH_PB) and L (CH_PB x CH_PB) are staged
+  // through registers one chunk ahead of the one in shared memory
+  constexpr int PER = TS_ROWS * CH_PB / 256;
+  static_assert(PER * 256 == TS_ROWS * CH_PB && TS_ROWS == CH_PB, "chunk split");
+  auto load = [&](int p0, int pb, int k0, double (&rx)[PER], double (&rl)[PER]) {
+#pragma unroll
+    for (int q = 0; q < PER; ++q) {
+      const int e2 = tid + 256 * q, rr = e2 % TS_ROWS, kk = e2 / TS_ROWS;
+      rx[q] = i0 + rr < n ? Z[(i0 + rr) + (int64_t)n * (k0 + kk)] : 0.0;
+      rl[q] = rr < pb ? L[(p0 + rr) + (int64_t)m * (k0 + kk)] : 0.0;
+    }
+  };
   for (int p0 = 0; p0 < m; p0 += CH_PB) {
     const int pb = min(CH_PB, m - p0);
     double acc[4] = {0.0, 0.0, 0.0, 0.0};
+    double rx[PER], rl[PER];
+    if (p0 > 0) load(p0, pb, 0, rx, rl);
     for (int k0 = 0; k0 < p0; k0 += CH_PB) {
       __syncthreads();
-      for (int e2 = tid; e2 < TS_ROWS * CH_PB; e2 += blockDim.x) {
-        const int rr = e2 % TS_ROWS, kk = e2 / TS_ROWS;
-        sx[rr][kk] = i0 + rr < n ? Z[(i0 + rr) + (int64_t)n * (k0 + kk)] : 0.0;
-        const int lr = e2 % CH_PB, lk = e2 / CH_PB;
-        sl[lr][lk] = lr < pb ? L[(p0 + lr) + (int64_t)m * (k0 + lk)] : 0.0;
+#pragma unroll
+      for (int q = 0; q < PER; ++q) {
+        const int e2 = tid + 256 * q, rr = e2 % TS_ROWS, kk = e2 / TS_ROWS;
+        sx[rr][kk] = rx[q];
+        sl[rr][kk] = rl[q];
       }
+      if (k0 + CH_PB < p0) load(p0, pb, k0 + CH_PB, rx, rl);
       __syncthreads();
 #pragma unroll 8
       for (int kk = 0; kk < CH_PB; ++kk) {
@@ -1380,24 +1719,44 @@ wy_apply(const EigDev* __restrict__ probs, const VecTask* __restrict__ tasks, co
   const int tid = threadIdx.x;
   const int npan = (n - 2 + BT_NB - 1) / BT_NB;
   const int xa = tid / BT_VB, xc = tid % BT_VB;  // the (reflector, vector) entry of X this thread sums
+  // Row chunks of V (BT_ROWS x BT_NB) and Y (BT_ROWS x BT_VB) are staged through
+  // registers one chunk ahead of the one in shared memory, so the global loads
+  // of chunk c + 1 are in flight while chunk c is being used.
+  constexpr int NV_PER = BT_ROWS * BT_NB / 512, NY_PER = BT_ROWS * BT_VB / 512;
+  static_assert(NV_PER * 512 == BT_ROWS * BT_NB && NY_PER * 512 == BT_ROWS * BT_VB, "chunk split");
+  auto load_v = [&](int k0, int mm, int i0, double (&rv)[NV_PER]) {
+#pragma unroll
+    for (int q = 0; q < NV_PER; ++q) {
+      const int e2 = tid + 512 * q, rr = e2 % BT_ROWS, a = e2 / BT_ROWS;
+      const int i = i0 + rr, ka = k0 + a;
+      rv[q] = (a < mm && i < n && i >= ka + 1) ? ((i == ka + 1) ? 1.0 : Gp[i + (int64_t)n * ka]) : 0.0;
+    }
+  };
+  auto load_y = [&](int i0, double (&ry)[NY_PER]) {
+#pragma unroll
+    for (int q = 0; q < NY_PER; ++q) {
+      const int e2 = tid + 512 * q, rr = e2 % BT_ROWS, c = e2 / BT_ROWS;
+      ry[q] = (i0 + rr < n && c < nv) ? Y[(i0 + rr) + (int64_t)n * c] : 0.0;
+    }
+  };
   for (int pnl = npan - 1; pnl >= 0; --pnl) {
     const int k0 = pnl * BT_NB, mm = min(BT_NB, n - 2 - k0);
     __syncthreads();
     for (int e2 = tid; e2 < BT_NB * BT_NB; e2 += blockDim.x) Tm[e2 % BT_NB][e2 / BT_NB] = Tst[(int64_t)pnl * BT_NB * BT_NB + e2];
     double xs = 0.0;
-    // X = V^T Y over rows >= k0 + 1, 64 rows at a time
+    double rv[NV_PER], ry[NY_PER];
+    // X = V^T Y over rows >= k0 + 1
+    load_v(k0, mm, k0 + 1, rv);
+    load_y(k0 + 1, ry);
     for (int i0 = k0 + 1; i0 < n; i0 += BT_ROWS) {
       __syncthreads();
-      for (int e2 = tid; e2 < BT_ROWS * BT_NB; e2 += blockDim.x) {
-        const int rr = e2 % BT_ROWS, a = e2 / BT_ROWS;
-        const int i = i0 + rr, ka = k0 + a;
-        double v = 0.0;
-        if (a < mm && i < n && i >= ka + 1) v = (i == ka + 1) ? 1.0 : Gp[i + (int64_t)n * ka];
-        sv[rr][a] = v;
-      }
-      for (int e2 = tid; e2 < BT_ROWS * BT_VB; e2 += blockDim.x) {
-        const int rr = e2 % BT_ROWS, c = e2 / BT_ROWS;
-        sy[rr][c] = (i0 + rr < n && c < nv) ? Y[(i0 + rr) + (int64_t)n * c] : 0.0;
+#pragma unroll
+      for (int q = 0; q < NV_PER; ++q) sv[(tid + 512 * q) % BT_ROWS][(tid + 512 * q) / BT_ROWS] = rv[q];
+#pragma unroll
+      for (int q = 0; q < NY_PER; ++q) sy[(tid + 512 * q) % BT_ROWS][(tid + 512 * q) / BT_ROWS] = ry[q];
+      if (i0 + BT_ROWS < n) {
+        load_v(k0, mm, i0 + BT_ROWS, rv);
+        load_y(i0 + BT_ROWS, ry);
       }
       __syncthreads();
 #pragma unroll 8
@@ -1411,26 +1770,30 @@ wy_apply(const EigDev* __restrict__ probs, const VecTask* __restrict__ tasks, co
       for (int b = xa; b < BT_NB; ++b) t2 += Tm[xa][b] * X[b][xc];
       X2[xa][xc] = t2;
     }
-    __syncthreads();
-    // Y -= V X2
+    // Y -= V X2, each thread NY_PER entries of the chunk
+    load_v(k0, mm, k0 + 1, rv);
+    load_y(k0 + 1, ry);
     for (int i0 = k0 + 1; i0 < n; i0 += BT_ROWS) {
       __syncthreads();
-      for (int e2 = tid; e2 < BT_ROWS * BT_NB; e2 += blockDim.x) {
-        const int rr = e2 % BT_ROWS, a = e2 / BT_ROWS;
-        const int i = i0 + rr, ka = k0 + a;
-        double v = 0.0;
-        if (a < mm && i < n && i >= ka + 1) v = (i == ka + 1) ? 1.0 : Gp[i + (int64_t)n * ka];
-        sv[rr][a] = v;
+#pragma unroll
+      for (int q = 0; q < NV_PER; ++q) sv[(tid + 512 * q) % BT_ROWS][(tid + 512 * q) / BT_ROWS] = rv[q];
+      double yc[NY_PER];
+#pragma unroll
+      for (int q = 0; q < NY_PER; ++q) yc[q] = ry[q];
+      if (i0 + BT_ROWS < n) {
+        load_v(k0, mm, i0 + BT_ROWS, rv);
+        load_y(i0 + BT_ROWS, ry);
       }
       __syncthreads();
-      for (int e2 = tid; e2 < BT_ROWS * BT_VB; e2 += blockDim.x) {
-        const int rr = e2 % BT_ROWS, c = e2 / BT_ROWS;
+#pragma unroll
+      for (int q = 0; q < NY_PER; ++q) {
+        const int e2 = tid + 512 * q, rr = e2 % BT_ROWS, c = e2 / BT_ROWS;
         const int i = i0 + rr;
         if (i < n && c < nv) {
           double u = 0.0;
 #pragma unroll 8
           for (int a = 0; a < BT_NB; ++a) u += sv[rr][a] * X2[a][c];
-          Y[i + (int64_t)n * c] -= u;
+          Y[i + (int64_t)n * c] = yc[q] - u;
         }
       }
     }
@@ -1501,7 +1864,7 @@ const ClusterPlan& cluster_plan(tt_ctx* ctx) {
   }
   const int64_t va = ((int64_t)optin - (int64_t)fa.sharedSizeBytes - 1024) / 8;
   const int64_t vb = ((int64_t)optin - (int64_t)fb.sharedSizeBytes - 1024) / 8;
-  if (va < blocked_smem(MAX_N, 8, 8) || vb < 6 * MAX_N) return cp;
+  if (vb < 6 * MAX_N) return cp;
   const void* kernels[2] = {(const void*)tridiag_eigvals_cluster, (const void*)tridiag_eigvecs_cluster};
   const int64_t caps[2] = {va, vb};
   for (int k = 0; k < 2; ++k) {
@@ -1517,7 +1880,7 @@ const ClusterPlan& cluster_plan(tt_ctx* ctx) {
     return cp;
   }
   for (int cl : {CL_MAX, 8}) {
-    bool ok = true;
+    bool ok = blocked_smem(MAX_N, 8, cl) <= va;  // the largest sector fits at the narrowest panel
     for (int k = 0; k < 2 && ok; ++k) {
       cudaLaunchConfig_t cfg = {};
       cudaLaunchAttribute at[1];
@@ -1618,6 +1981,16 @@ int tt_sym_eigvals_batched(tt_ctx* ctx, const tt_eig_problem* probs, int n_probs
   }
   tt::pool_free(ctx, vw);
   tt::pool_free(ctx, dp);
+  return TT_OK;
+}
+
+int tt_eig_redo_count(tt_ctx* ctx, int64_t* count) {
+  TT_REQUIRE(ctx && count, "tt_eig_redo_count: null argument");
+  unsigned long long* h = reinterpret_cast<unsigned long long*>(ctx->h_scalars);
+  TT_CUDA(cudaMemcpyFromSymbolAsync(h, g_eig_redo, sizeof(unsigned long long), 0, cudaMemcpyDeviceToHost,
+                                    ctx->stream));
+  TT_CUDA(cudaStreamSynchronize(ctx->stream));
+  *count = (int64_t)*h;
   return TT_OK;
 }
 

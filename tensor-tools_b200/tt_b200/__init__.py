@@ -190,6 +190,7 @@ _proto("tt_qdmrg_stats", P, PD, PD, PD)
 _proto("tt_qdmrg_step_profile", P, C.c_int, C.POINTER(C.c_int), PD, PD, PD, PD)
 _proto("tt_dmrg_set_profiling", C.c_int)
 _proto("tt_dmrg_planning_counters", PD, PI64, PD, PI64)
+_proto("tt_eig_redo_count", P, PI64)
 _proto("tt_sym_eig_batched", P, C.c_void_p, C.c_int, P, P, P, P)
 _proto("tt_qdmrg_num_sweeps", P, C.POINTER(C.c_int))
 _proto("tt_qdmrg_sweep_info", P, C.c_int, PD, PD)
@@ -889,6 +890,23 @@ def set_davidson_control(device: bool = True):
     """tensor_davidsonIT control on the device (one synchronisation per call,
     host loop on Gram-Schmidt failure) or on the host (reads back every iteration)."""
     _chk(lib.tt_dmrg_set_davidson(int(device)), "set_davidson")
+
+
+def eig_redo_count(ctx) -> int:
+    """Eigenproblems whose vectors were recomputed by the cluster kernel after
+    CholeskyQR2 found a collapsed inverse-iteration vector (device-wide)."""
+    n = I64()
+    _chk(lib.tt_eig_redo_count(ctx.h, C.byref(n)), "eig_redo_count")
+    return n.value
+
+
+def planning_counters() -> dict:
+    """Host time spent on contraction structures and plans (this thread):
+    seconds and counts since the thread started."""
+    ts, tp = D(), D()
+    ns, np_ = I64(), I64()
+    _chk(lib.tt_dmrg_planning_counters(C.byref(ts), C.byref(ns), C.byref(tp), C.byref(np_)), "planning_counters")
+    return {"structure_s": ts.value, "structures": ns.value, "plan_s": tp.value, "plans": np_.value}
 
 
 def davidson_refills() -> int:

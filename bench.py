@@ -468,15 +468,28 @@ def c5_arm(prec, ck, H, args, ctx, stream, flush, torch, tt_b200, sampler=None, 
         times = []
         # NVTX range "c5_timed_<precision>": lets a profiler's launch list cover the timed steps only
         torch.cuda.nvtx.range_push("c5_timed_" + prec)
+        step_pool, step_plans, step_host = [], [], []  # per step: pool GB reserved, plans built, host s
+        try:
+            import psutil
+            proc = psutil.Process()
+            psutil.cpu_percent(None)
+            cpu0 = proc.cpu_times()
+        except Exception:  # load sampling is diagnostic only
+            psutil = None
         for _ in range(args.steps):
             flush.zero_()
             torch.cuda.synchronize()
+            pa = tt_b200.planning_counters()["plans"]
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            h0 = time.perf_counter()
             e0.record(stream)
             step()
             e1.record(stream)
+            step_host.append(time.perf_counter() - h0)
             e1.synchronize()
             times.append(e0.elapsed_time(e1) * 1e-3)
+            step_plans.append(tt_b200.planning_counters()["plans"] - pa)
+            step_pool.append(ctx.memory()[2] / 2 ** 30)
         torch.cuda.nvtx.range_pop()
         ctx.sync()
         clocks = sampler.stop() if sampler else None
@@ -500,12 +513,19 @@ def c5_arm(prec, ck, H, args, ctx, stream, flush, torch, tt_b200, sampler=None, 
             / max(1, args.steps * 2 * B),
             "plans_per_update": (pc1["plans"] - pc0["plans"]) / max(1, args.steps * 2 * B),
             "eig_redos": er1 - er0,
+            "step_plans_built": step_plans, "step_pool_reserved_gb": step_pool,
+            "step_host_seconds": step_host,
             "matvecs_per_update": statistics.mean(s["matvecs"] for s in steps) if steps else None,
             "trunc_err_mean": statistics.mean(s["trunc_err"] for s in steps) if steps else None,
             "kept": [s["kept"] for s in steps[-upd:]],
             "bond_dims_block": psi.bond_dims()[mid:mid + B + 2],
             "clocks": clocks,
         })
+        if psutil is not None:
+            cpu1 = proc.cpu_times()
+            res["host_load"] = {"system_cpu_percent": psutil.cpu_percent(None), "cores": psutil.cpu_count(),
+                                "this_process_cpu_s": (cpu1.user + cpu1.system) - (cpu0.user + cpu0.system),
+                                "timed_s": sum(times)}
         pool = ctx.memory()
         res["device_memory_gb"] = {"in_use": pool[0] / 2 ** 30, "high_water": pool[1] / 2 ** 30,
                                    "reserved": pool[2] / 2 ** 30}

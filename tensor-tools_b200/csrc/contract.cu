@@ -9,8 +9,10 @@
 // descriptors when the plan is built.
 #include <algorithm>
 #include <cstring>
+#include <functional>
 #include <map>
 #include <numeric>
+#include <unordered_map>
 #include <vector>
 
 #include "tt_internal.h"
@@ -224,30 +226,34 @@ grouped_dgemm(const TaskDev* __restrict__ tasks, const OutDev* __restrict__ outs
 // thread keeps its row's n outputs in registers across all pairs of the
 // block, with the pair's B (k x n, tiny) staged in shared memory, and reads
 // its A row through the offset tables (coalesced along a unit-stride row
-// mode).  Pairs are summed in the plan's order, as in grouped_dgemm.
+// mode).  Pairs are summed in the plan's order, as in grouped_dgemm.  The
+// kernel is instantiated for NC = 4, 8, 16, 32 output columns (the plan's
+// widest block rounded up), so a narrow contraction issues no work for
+// columns it does not have and keeps few registers (more CTAs per SM).
 constexpr int SK_N = 32;
 constexpr int SK_K = 64;
 constexpr int SK_ROWS = 256;
 
+template <int NC>
 __global__ void __launch_bounds__(SK_ROWS)
 skinny_dgemm(const TaskDev* __restrict__ tasks, const OutDev* __restrict__ outs,
              const PairDev* __restrict__ pairs, const int32_t* __restrict__ tab,
              const double* __restrict__ A, const double* __restrict__ B, double* __restrict__ C,
              double alpha) {
-  __shared__ double sB[SK_K][SK_N + 1];
+  __shared__ double sB[SK_K][NC];
   __shared__ int32_t sColA[SK_K];
   const TaskDev task = tasks[blockIdx.x];
   const OutDev out = outs[task.out];
   const int r = task.m0 + threadIdx.x;
-  double acc[SK_N];
+  double acc[NC];
 #pragma unroll
-  for (int c = 0; c < SK_N; ++c) acc[c] = 0.0;
+  for (int c = 0; c < NC; ++c) acc[c] = 0.0;
   for (int p = task.p_begin; p < task.p_end; ++p) {
     const PairDev P = pairs[p];
     __syncthreads();  // the previous pair's B is no longer read
-    for (int e = threadIdx.x; e < P.k * P.n; e += blockDim.x) {
-      const int kk = e % P.k, c = e / P.k;
-      sB[kk][c] = B[P.b_off + tab[P.rowB + kk] + tab[P.colB + c]];
+    for (int e = threadIdx.x; e < P.k * NC; e += blockDim.x) {
+      const int kk = e / NC, c = e % NC;
+      sB[kk][c] = c < P.n ? B[P.b_off + tab[P.rowB + kk] + tab[P.colB + c]] : 0.0;  // zero past n
     }
     for (int kk = threadIdx.x; kk < P.k; kk += blockDim.x) sColA[kk] = tab[P.colA + kk];
     __syncthreads();
@@ -256,15 +262,14 @@ skinny_dgemm(const TaskDev* __restrict__ tasks, const OutDev* __restrict__ outs,
       for (int kk = 0; kk < P.k; ++kk) {
         const double a = arow[sColA[kk]];
 #pragma unroll
-        for (int c = 0; c < SK_N; ++c)
-          if (c < P.n) acc[c] += a * sB[kk][c];
+        for (int c = 0; c < NC; ++c) acc[c] = fma(a, sB[kk][c], acc[c]);
       }
     }
   }
   if (r < out.m) {
     double* Cb = C + out.c_off + r;
 #pragma unroll
-    for (int c = 0; c < SK_N; ++c)
+    for (int c = 0; c < NC; ++c)
       if (c < out.n) Cb[(int64_t)out.ldc * c] = alpha * acc[c];
   }
 }
@@ -398,7 +403,6 @@ struct PairTC {
 constexpr int TC_RING = 3;
 constexpr int TC_RING_STAGE = 4 * TC_BM * TC_BK * 4;  // A hi, A lo, B hi, B lo: 64 KB
 constexpr size_t TC_BULK_SMEM = (size_t)TC_RING * TC_RING_STAGE + 1024;
-constexpr uint32_t TC_BULK_COLS = TC_BN;
 
 __device__ __forceinline__ void mbar_expect_tx(uint32_t mbar, uint32_t bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mbar), "r"(bytes) : "memory");
@@ -697,6 +701,7 @@ double predict_us(const tt_out_block* outs, int n_out, const std::vector<PairDev
 struct tt_plan {
   int precision = TT_PREC_FP64;
   bool skinny = false;      // FP64 plan run by skinny_dgemm (row tasks of SK_ROWS)
+  int skinny_nc = SK_N;     // its widest output block (the kernel instance covers it)
   int* d_status = nullptr;  // tensor-core path: TT_OK or TT_ERR_TIMEOUT
   // tensor-core path: packing jobs and tiles of the unique A / B blocks, the
   // pairs in packed form, and the packed sizes (buffers are taken from the
@@ -826,7 +831,34 @@ int tt_contract_plan(tt_ctx* ctx, const tt_out_block* outs, int n_out,
   }
   std::vector<int> torder(tasks.size());
   std::iota(torder.begin(), torder.end(), 0);
-  std::stable_sort(torder.begin(), torder.end(), [&](int a, int b) { return tcost[a] > tcost[b]; });
+  if (skinny) {
+    // The skinny kernel is bound by reading A, and every output block that
+    // shares A's blocks (the same rows, other column sectors) reads them
+    // again.  Tasks of such output blocks are interleaved by row tile, so the
+    // CTAs that run together read the same A rows and all but the first read
+    // hit L2.  Groups: output blocks linked through a shared A block
+    // (union-find on the pairs' A offsets), heaviest group first.
+    std::vector<int> parent(n_out);
+    std::iota(parent.begin(), parent.end(), 0);
+    std::function<int(int)> root = [&](int o) { return parent[o] == o ? o : parent[o] = root(parent[o]); };
+    std::unordered_map<int64_t, int> owner;
+    for (int o = 0; o < n_out; ++o)
+      for (int i = first[o]; i < first[o + 1]; ++i) {
+        auto it = owner.emplace(hp[i].a_off, o).first;
+        const int ra = root(it->second), rb = root(o);
+        if (ra != rb) parent[rb] = ra;
+      }
+    std::vector<int64_t> gcost(n_out, 0);
+    for (int o = 0; o < n_out; ++o) gcost[root(o)] += work[o] + 1;
+    std::stable_sort(torder.begin(), torder.end(), [&](int a, int b) {
+      const int ga = root(tasks[a].out), gb = root(tasks[b].out);
+      if (ga != gb) return gcost[ga] != gcost[gb] ? gcost[ga] > gcost[gb] : ga < gb;
+      if (tasks[a].m0 != tasks[b].m0) return tasks[a].m0 < tasks[b].m0;
+      return tasks[a].out < tasks[b].out;
+    });
+  } else {
+    std::stable_sort(torder.begin(), torder.end(), [&](int a, int b) { return tcost[a] > tcost[b]; });
+  }
   std::vector<TaskDev> tsorted(tasks.size());
   for (size_t i = 0; i < tasks.size(); ++i) tsorted[i] = tasks[torder[i]];
   std::vector<OutDev> ho(n_out);
@@ -869,6 +901,11 @@ int tt_contract_plan(tt_ctx* ctx, const tt_out_block* outs, int n_out,
   tt_plan* plan = new tt_plan();
   plan->precision = precision;
   plan->skinny = skinny;
+  if (skinny) {
+    int wmax = 1;
+    for (int o = 0; o < n_out; ++o) wmax = std::max(wmax, outs[o].n);
+    plan->skinny_nc = wmax;
+  }
   plan->n_tilesA = (int)ta.size();
   plan->n_tilesB = (int)tb.size();
   plan->bytesA = bytesA;
@@ -954,10 +991,16 @@ int tt_contract_exec_keep(tt_ctx* ctx, const tt_plan* plan, const double* A, con
                                  (int)TC_BULK_SMEM));
   }
   if (plan->precision == TT_PREC_FP64) {
-    if (plan->skinny)
-      skinny_dgemm<<<plan->n_tasks, SK_ROWS, 0, ctx->stream>>>(plan->d_tasks, plan->d_outs, plan->d_pairs,
-                                                              plan->d_tab, A, B, C, alpha);
-    else
+    if (plan->skinny) {
+      auto launch = [&](auto kernel) {
+        kernel<<<plan->n_tasks, SK_ROWS, 0, ctx->stream>>>(plan->d_tasks, plan->d_outs, plan->d_pairs, plan->d_tab,
+                                                          A, B, C, alpha);
+      };
+      if (plan->skinny_nc <= 4) launch(skinny_dgemm<4>);
+      else if (plan->skinny_nc <= 8) launch(skinny_dgemm<8>);
+      else if (plan->skinny_nc <= 16) launch(skinny_dgemm<16>);
+      else launch(skinny_dgemm<32>);
+    } else
       grouped_dgemm<<<plan->n_tasks, THREADS, SMEM_BYTES, ctx->stream>>>(
           plan->d_tasks, plan->d_outs, plan->d_pairs, plan->d_tab, A, B, C, alpha);
     TT_LAUNCH_CHECK(ctx);

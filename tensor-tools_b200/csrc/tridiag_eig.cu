@@ -1529,9 +1529,11 @@ chol_cluster(const EigDev* __restrict__ probs, double* work, int* flags, int che
     for (int i = rbeg + rank * (int)blockDim.x + tid; i < m; i += CL * (int)blockDim.x) {
       double x[CH_PB];
 #pragma unroll
+      for (int k = 0; k < CH_PB; ++k) x[k] = k < pb ? A[i + (int64_t)m * (p0 + k)] : 0.0;  // all loads in flight
+#pragma unroll
       for (int k = 0; k < CH_PB; ++k) {
         if (k < pb) {
-          double v = A[i + (int64_t)m * (p0 + k)];
+          double v = x[k];
           for (int t = 0; t < k; ++t) v -= x[t] * Ld[k][t];
           x[k] = v / Ld[k][k];
           A[i + (int64_t)m * (p0 + k)] = x[k];

@@ -122,6 +122,7 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-full-sweep", action="store_true")
     p.add_argument("--breakdown", action="store_true", help="one further step per precision with phase times")
+    p.add_argument("--env-prec", default=ENV_PREC, help="environment-update precision of the chosen form")
     p.add_argument("--gemm-size", type=int, default=4096)
     p.add_argument("--precisions", default="fp64,tf32x3,tf32")
     p.add_argument("--chains", type=int, default=64)
@@ -403,7 +404,7 @@ def run_reference(args):
 def c5_setup(tt_b200, H, args, workdir):
     """Untimed ramp in the chosen form, one sweep at maxdim, checkpoint."""
     from oracle import qdmrg
-    tt_b200.set_precision(heff=CHOSEN, env=ENV_PREC)
+    tt_b200.set_precision(heff=CHOSEN, env=args.env_prec)
     t0 = time.perf_counter()
     try:
         psi = tt_b200.QMPS(C5_N, qdmrg.neel(C5_N))
@@ -443,8 +444,9 @@ def c5_arm(prec, ck, H, args, ctx, stream, flush, torch, tt_b200, sampler=None, 
     """Load, centre to the block, W warm-up and K timed block steps (CUDA
     events on the library stream, L2 flushed before each), then the FP64
     energy, optional end-to-end steps and a full sweep."""
-    tt_b200.set_precision(heff=prec, env=ENV_PREC)
-    res = {"precision": prec}
+    env_prec = args.env_prec if prec != "fp64" else "fp64"
+    tt_b200.set_precision(heff=prec, env=env_prec)
+    res = {"precision": prec, "env_precision": env_prec}
     B, mid = args.block, C5_MID
     cut, mr, md = C5["cutoff"], args.max_restart, args.maxdim
     try:
@@ -547,7 +549,7 @@ def c5_arm(prec, ck, H, args, ctx, stream, flush, torch, tt_b200, sampler=None, 
         res["energy"] = psi.expectation(H) / nrm
         if szsz:
             res["szsz"] = [psi.expectation(m) / nrm for m in szsz]
-        tt_b200.set_precision(heff=prec, env=ENV_PREC)
+        tt_b200.set_precision(heff=prec, env=env_prec)
         if e2e_steps > 0:
             # through the public C ABI: the block's site tensors from pinned host memory every step
             first, last = mid, mid + B + 2

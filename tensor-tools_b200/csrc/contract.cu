@@ -233,13 +233,18 @@ grouped_dgemm(const TaskDev* __restrict__ tasks, const OutDev* __restrict__ outs
 constexpr int SK_N = 32;
 constexpr int SK_K = 64;
 constexpr int SK_ROWS = 256;
+constexpr int64_t SK_STAGE_BYTES = 64 * 1024;  // dynamic shared memory for a task's staged pairs
 
 template <int NC>
 __global__ void __launch_bounds__(SK_ROWS)
 skinny_dgemm(const TaskDev* __restrict__ tasks, const OutDev* __restrict__ outs,
              const PairDev* __restrict__ pairs, const int32_t* __restrict__ tab,
              const double* __restrict__ A, const double* __restrict__ B, double* __restrict__ C,
-             double alpha) {
+             double alpha, int staged) {
+  // staged != 0: every pair's B (k x NC, zero past n) and A column offsets are
+  // staged once for the task (dynamic shared memory sized by the plan), so the
+  // pairs run without barriers; else one pair at a time through sB / sColA
+  extern __shared__ double sk_dyn[];
   __shared__ double sB[SK_K][NC];
   __shared__ int32_t sColA[SK_K];
   const TaskDev task = tasks[blockIdx.x];
@@ -248,21 +253,52 @@ skinny_dgemm(const TaskDev* __restrict__ tasks, const OutDev* __restrict__ outs,
   double acc[NC];
 #pragma unroll
   for (int c = 0; c < NC; ++c) acc[c] = 0.0;
-  for (int p = task.p_begin; p < task.p_end; ++p) {
-    const PairDev P = pairs[p];
-    __syncthreads();  // the previous pair's B is no longer read
-    for (int e = threadIdx.x; e < P.k * NC; e += blockDim.x) {
-      const int kk = e / NC, c = e % NC;
-      sB[kk][c] = c < P.n ? B[P.b_off + tab[P.rowB + kk] + tab[P.colB + c]] : 0.0;  // zero past n
+  if (staged) {
+    double* bst = sk_dyn;
+    int ktot = 0;
+    for (int p = task.p_begin; p < task.p_end; ++p) ktot += pairs[p].k;
+    int32_t* cst = reinterpret_cast<int32_t*>(sk_dyn + (int64_t)ktot * NC);
+    int k0 = 0;
+    for (int p = task.p_begin; p < task.p_end; ++p) {
+      const PairDev P = pairs[p];
+      for (int e = threadIdx.x; e < P.k * NC; e += blockDim.x) {
+        const int kk = e / NC, c = e % NC;
+        bst[(k0 + kk) * NC + c] = c < P.n ? B[P.b_off + tab[P.rowB + kk] + tab[P.colB + c]] : 0.0;
+      }
+      for (int kk = threadIdx.x; kk < P.k; kk += blockDim.x) cst[k0 + kk] = tab[P.colA + kk];
+      k0 += P.k;
     }
-    for (int kk = threadIdx.x; kk < P.k; kk += blockDim.x) sColA[kk] = tab[P.colA + kk];
     __syncthreads();
-    if (r < P.m) {
-      const double* __restrict__ arow = A + P.a_off + tab[P.rowA + r];
-      for (int kk = 0; kk < P.k; ++kk) {
-        const double a = arow[sColA[kk]];
+    k0 = 0;
+    for (int p = task.p_begin; p < task.p_end; ++p) {
+      const PairDev P = pairs[p];
+      if (r < P.m) {
+        const double* __restrict__ arow = A + P.a_off + tab[P.rowA + r];
+        for (int kk = 0; kk < P.k; ++kk) {
+          const double a = arow[cst[k0 + kk]];
 #pragma unroll
-        for (int c = 0; c < NC; ++c) acc[c] = fma(a, sB[kk][c], acc[c]);
+          for (int c = 0; c < NC; ++c) acc[c] = fma(a, bst[(k0 + kk) * NC + c], acc[c]);
+        }
+      }
+      k0 += P.k;
+    }
+  } else {
+    for (int p = task.p_begin; p < task.p_end; ++p) {
+      const PairDev P = pairs[p];
+      __syncthreads();  // the previous pair's B is no longer read
+      for (int e = threadIdx.x; e < P.k * NC; e += blockDim.x) {
+        const int kk = e / NC, c = e % NC;
+        sB[kk][c] = c < P.n ? B[P.b_off + tab[P.rowB + kk] + tab[P.colB + c]] : 0.0;  // zero past n
+      }
+      for (int kk = threadIdx.x; kk < P.k; kk += blockDim.x) sColA[kk] = tab[P.colA + kk];
+      __syncthreads();
+      if (r < P.m) {
+        const double* __restrict__ arow = A + P.a_off + tab[P.rowA + r];
+        for (int kk = 0; kk < P.k; ++kk) {
+          const double a = arow[sColA[kk]];
+#pragma unroll
+          for (int c = 0; c < NC; ++c) acc[c] = fma(a, sB[kk][c], acc[c]);
+        }
       }
     }
   }
@@ -702,6 +738,7 @@ struct tt_plan {
   int precision = TT_PREC_FP64;
   bool skinny = false;      // FP64 plan run by skinny_dgemm (row tasks of SK_ROWS)
   int skinny_nc = SK_N;     // its widest output block (the kernel instance covers it)
+  int64_t skinny_ktot = 0;  // the largest sum of k over one output block's pairs
   int* d_status = nullptr;  // tensor-core path: TT_OK or TT_ERR_TIMEOUT
   // tensor-core path: packing jobs and tiles of the unique A / B blocks, the
   // pairs in packed form, and the packed sizes (buffers are taken from the
@@ -905,6 +942,11 @@ int tt_contract_plan(tt_ctx* ctx, const tt_out_block* outs, int n_out,
     int wmax = 1;
     for (int o = 0; o < n_out; ++o) wmax = std::max(wmax, outs[o].n);
     plan->skinny_nc = wmax;
+    for (int o = 0; o < n_out; ++o) {
+      int64_t kt = 0;
+      for (int i = first[o]; i < first[o + 1]; ++i) kt += hp[i].k;
+      plan->skinny_ktot = std::max(plan->skinny_ktot, kt);
+    }
   }
   plan->n_tilesA = (int)ta.size();
   plan->n_tilesB = (int)tb.size();
@@ -992,13 +1034,21 @@ int tt_contract_exec_keep(tt_ctx* ctx, const tt_plan* plan, const double* A, con
   }
   if (plan->precision == TT_PREC_FP64) {
     if (plan->skinny) {
+      const int nc = plan->skinny_nc <= 4 ? 4 : plan->skinny_nc <= 8 ? 8 : plan->skinny_nc <= 16 ? 16 : 32;
+      // every pair of a task staged at once when the widest task fits
+      const int64_t need = plan->skinny_ktot * (int64_t)(nc * sizeof(double) + sizeof(int32_t));
+      const bool staged = need <= SK_STAGE_BYTES;
+      const size_t dyn = staged ? (size_t)need : 0;
       auto launch = [&](auto kernel) {
-        kernel<<<plan->n_tasks, SK_ROWS, 0, ctx->stream>>>(plan->d_tasks, plan->d_outs, plan->d_pairs, plan->d_tab,
-                                                          A, B, C, alpha);
+        static thread_local uint64_t attr = 0;
+        if (tt::first_on_device(attr, ctx->device))
+          cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SK_STAGE_BYTES);
+        kernel<<<plan->n_tasks, SK_ROWS, dyn, ctx->stream>>>(plan->d_tasks, plan->d_outs, plan->d_pairs, plan->d_tab,
+                                                            A, B, C, alpha, staged ? 1 : 0);
       };
-      if (plan->skinny_nc <= 4) launch(skinny_dgemm<4>);
-      else if (plan->skinny_nc <= 8) launch(skinny_dgemm<8>);
-      else if (plan->skinny_nc <= 16) launch(skinny_dgemm<16>);
+      if (nc == 4) launch(skinny_dgemm<4>);
+      else if (nc == 8) launch(skinny_dgemm<8>);
+      else if (nc == 16) launch(skinny_dgemm<16>);
       else launch(skinny_dgemm<32>);
     } else
       grouped_dgemm<<<plan->n_tasks, THREADS, SMEM_BYTES, ctx->stream>>>(

@@ -703,6 +703,7 @@ tridiag_eigvals_cluster(const EigDev* __restrict__ probs, double* G, double* Tg,
   extern __shared__ double sm[];
   __shared__ double red[33];
   __shared__ double s_K;
+  __shared__ double vw_part[NWARP * 2 * PNB_MAX];  // per-warp V^T v, W^T v sums
 
   cgx::cluster_group cluster = cgx::this_cluster();
   const int CL = (int)cluster.num_blocks();
@@ -748,10 +749,22 @@ tridiag_eigvals_cluster(const EigDev* __restrict__ probs, double* G, double* Tg,
       double* xcur = xc + (jj & 1) * nloc;
       // ---- 1: column j on the own rows >= j, pushed to every CTA ----
       const int l1 = first_owned(j, rank, CL);
-      for (int l = l1 + tid; l < lown; l += blockDim.x) {
-        double a = jj == 0 ? Gp[(rank + CL * l) + (int64_t)n * j] : xcur[l];
-        for (int t = 0; t < jj; ++t) a -= Vl[t * nloc + l] * Wq[t * nb + jj] + Wl[t * nloc + l] * Vp[t * nb + jj];
-        xcur[l] = a;
+      {
+        // four threads per row, each summing a quarter of the panel's terms
+        // (the loop bound is the same for the whole warp: the shuffles need it)
+        const int sub = tid & 3;
+        for (int base = l1 + (warp << 3); base < lown; base += blockDim.x >> 2) {
+          const int l = base + (lane >> 2);
+          const bool act = l < lown;
+          double corr = 0.0;
+          if (act)
+#pragma unroll 1
+            for (int t = sub; t < jj; t += 4)
+              corr += Vl[t * nloc + l] * Wq[t * nb + jj] + Wl[t * nloc + l] * Vp[t * nb + jj];
+          corr += __shfl_xor_sync(0xffffffffu, corr, 1);
+          corr += __shfl_xor_sync(0xffffffffu, corr, 2);
+          if (act && sub == 0) xcur[l] = (jj == 0 ? Gp[(rank + CL * l) + (int64_t)n * j] : xcur[l]) - corr;
+        }
       }
       __syncthreads();
       for (int e = tid; e < (lown - l1) * CL; e += blockDim.x) {
@@ -791,13 +804,29 @@ tridiag_eigvals_cluster(const EigDev* __restrict__ probs, double* G, double* Tg,
       }
       __syncthreads();
       const int lf = first_owned(j + 1, rank, CL);
-      for (int idx = warp; idx < 2 * jj; idx += NWARP) {
-        const int t = idx < jj ? idx : idx - jj;
-        const double* M = idx < jj ? Vl : Wl;
-        double sacc = 0.0;
-        for (int l = lf + lane; l < lown; l += 32) sacc += M[t * nloc + l] * Vl[jj * nloc + l];
-        sacc = warp_sum(sacc);
-        if (lane < CL) *cluster.map_shared_rank(r2 + rank * 2 * nb + (idx < jj ? t : nb + t), lane) = sacc;
+      // V^T v and W^T v partials over the own rows >= j + 1: lane t of each
+      // warp sums column t over every NWARP-th row, the warps' sums are added
+      // in warp order and pushed to every CTA
+      if (jj > 0) {
+        double sv = 0.0, sw = 0.0;
+        if (lane < jj)
+          for (int l = lf + warp; l < lown; l += NWARP) {
+            const double v = Vl[jj * nloc + l];
+            sv += Vl[lane * nloc + l] * v;
+            sw += Wl[lane * nloc + l] * v;
+          }
+        vw_part[warp * 2 * PNB_MAX + lane] = sv;
+        vw_part[warp * 2 * PNB_MAX + PNB_MAX + lane] = sw;
+        __syncthreads();
+        if (tid < 2 * PNB_MAX) {
+          const int t = tid & (PNB_MAX - 1);
+          if (t < jj) {
+            double a = 0.0;
+            for (int w = 0; w < NWARP; ++w) a += vw_part[w * 2 * PNB_MAX + tid];
+            const int slot = rank * 2 * nb + (tid < PNB_MAX ? t : nb + t);
+            for (int q = 0; q < CL; ++q) *cluster.map_shared_rank(r2 + slot, q) = a;
+          }
+        }
       }
       // ---- 3: p = A22 v from the lower triangle of the own columns ----
       if (jj + 1 < nbe)  // the next column's own rows: unchanged until its step 1
@@ -937,7 +966,9 @@ tridiag_eigvals_cluster(const EigDev* __restrict__ probs, double* G, double* Tg,
           const bool act = l < lown;
           double p = 0.0, corr = 0.0;
           if (act) {
+#pragma unroll 1
             for (int q = sub; q < CL; q += 4) p += yb[q * nloc + l];
+#pragma unroll 1
             for (int t = sub; t < jj; t += 4) corr += Vl[t * nloc + l] * cwt[t] + Wl[t * nloc + l] * cvt[t];
           }
           p += __shfl_xor_sync(0xffffffffu, p, 1);

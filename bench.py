@@ -470,7 +470,8 @@ def c5_arm(prec, ck, H, args, ctx, stream, flush, torch, tt_b200, sampler=None, 
         times = []
         # NVTX range "c5_timed_<precision>": lets a profiler's launch list cover the timed steps only
         torch.cuda.nvtx.range_push("c5_timed_" + prec)
-        step_pool, step_plans, step_host = [], [], []  # per step: pool GB reserved, plans built, host s
+        # per step: pool GB reserved, plans built, host seconds, of which waiting on the device
+        step_pool, step_plans, step_host, step_wait = [], [], [], []
         try:
             import psutil
             proc = psutil.Process()
@@ -482,12 +483,14 @@ def c5_arm(prec, ck, H, args, ctx, stream, flush, torch, tt_b200, sampler=None, 
             flush.zero_()
             torch.cuda.synchronize()
             pa = tt_b200.planning_counters()["plans"]
+            w0 = ctx.wait_stats()[0]
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             h0 = time.perf_counter()
             e0.record(stream)
             step()
             e1.record(stream)
             step_host.append(time.perf_counter() - h0)
+            step_wait.append(ctx.wait_stats()[0] - w0)
             e1.synchronize()
             times.append(e0.elapsed_time(e1) * 1e-3)
             step_plans.append(tt_b200.planning_counters()["plans"] - pa)
@@ -516,7 +519,7 @@ def c5_arm(prec, ck, H, args, ctx, stream, flush, torch, tt_b200, sampler=None, 
             "plans_per_update": (pc1["plans"] - pc0["plans"]) / max(1, args.steps * 2 * B),
             "eig_redos": er1 - er0,
             "step_plans_built": step_plans, "step_pool_reserved_gb": step_pool,
-            "step_host_seconds": step_host,
+            "step_host_seconds": step_host, "step_device_wait_seconds": step_wait,
             "matvecs_per_update": statistics.mean(s["matvecs"] for s in steps) if steps else None,
             "trunc_err_mean": statistics.mean(s["trunc_err"] for s in steps) if steps else None,
             "kept": [s["kept"] for s in steps[-upd:]],

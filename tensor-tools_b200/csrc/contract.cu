@@ -1039,17 +1039,15 @@ int tt_contract_exec_keep(tt_ctx* ctx, const tt_plan* plan, const double* A, con
       const int64_t need = plan->skinny_ktot * (int64_t)(nc * sizeof(double) + sizeof(int32_t));
       const bool staged = need <= SK_STAGE_BYTES;
       const size_t dyn = staged ? (size_t)need : 0;
-      auto launch = [&](auto kernel) {
-        static thread_local uint64_t attr = 0;
-        if (tt::first_on_device(attr, ctx->device))
-          cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SK_STAGE_BYTES);
-        kernel<<<plan->n_tasks, SK_ROWS, dyn, ctx->stream>>>(plan->d_tasks, plan->d_outs, plan->d_pairs, plan->d_tab,
-                                                            A, B, C, alpha, staged ? 1 : 0);
-      };
-      if (nc == 4) launch(skinny_dgemm<4>);
-      else if (nc == 8) launch(skinny_dgemm<8>);
-      else if (nc == 16) launch(skinny_dgemm<16>);
-      else launch(skinny_dgemm<32>);
+      using SkinnyFn = void (*)(const TaskDev*, const OutDev*, const PairDev*, const int32_t*, const double*,
+                                const double*, double*, double, int);
+      const int which = nc == 4 ? 0 : nc == 8 ? 1 : nc == 16 ? 2 : 3;
+      const SkinnyFn fns[4] = {skinny_dgemm<4>, skinny_dgemm<8>, skinny_dgemm<16>, skinny_dgemm<32>};
+      static thread_local uint64_t attr[4] = {0, 0, 0, 0};  // per instance, per host thread and device
+      if (tt::first_on_device(attr[which], ctx->device))
+        TT_CUDA(cudaFuncSetAttribute(fns[which], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SK_STAGE_BYTES));
+      fns[which]<<<plan->n_tasks, SK_ROWS, dyn, ctx->stream>>>(plan->d_tasks, plan->d_outs, plan->d_pairs,
+                                                              plan->d_tab, A, B, C, alpha, staged ? 1 : 0);
     } else
       grouped_dgemm<<<plan->n_tasks, THREADS, SMEM_BYTES, ctx->stream>>>(
           plan->d_tasks, plan->d_outs, plan->d_pairs, plan->d_tab, A, B, C, alpha);

@@ -172,6 +172,15 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(rows)}
 
 
+def load_hbm_peak():
+    """The measured HBM copy bandwidth (GB/s) of this pool's B200s, if present."""
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"])
+    except (OSError, KeyError, ValueError):
+        return None
+
+
 def measured_peaks(torch):
     """cuBLAS DGEMM (FP64 tensor path) and TF32 GEMM throughput, 8192^3, best of 3."""
     n = 8192
@@ -426,6 +435,22 @@ def c5_setup(tt_b200, H, args, workdir):
     return ck + ".ttmps", info
 
 
+def heff_parts_summary(a, b):
+    """Per-contraction figures of the products between two heff_parts()
+    readings: device ms and algorithmic TFLOP/s of L*x and *R, device ms and
+    algorithmic GB/s of the middle contraction."""
+    ms = [y - x for x, y in zip(a["ms"], b["ms"])]
+    fl = [y - x for x, y in zip(a["flops"], b["flops"])]
+    mb = b["mid_bytes"] - a["mid_bytes"]
+    out = {"ms": {"L*x": ms[0], "*mid": ms[1], "*R": ms[2]},
+           "flops": {"L*x": fl[0], "*mid": fl[1], "*R": fl[2]}, "mid_bytes": mb}
+    if ms[0] + ms[2] > 0:
+        out["L*x_and_*R_tflops"] = (fl[0] + fl[2]) / ((ms[0] + ms[2]) * 1e-3) / 1e12
+    if ms[1] > 0:
+        out["mid_gbs"] = mb / (ms[1] * 1e-3) / 1e9
+    return out
+
+
 # <Sz_i Sz_j> pairs in the middle of the cylinder (0-based sites, snake order):
 # along the snake, one column over, and two columns over
 C5_SZSZ_PAIRS = [(47, 48), (47, 47 + C5["Ny"]), (47, 47 + 2 * C5["Ny"])]
@@ -463,6 +488,7 @@ def c5_arm(prec, ck, H, args, ctx, stream, flush, torch, tt_b200, sampler=None, 
         ctx.sync()
         st0, fb0, l0 = run.stats(), tt_b200.davidson_fallbacks(), ctx.launches()
         pc0 = tt_b200.planning_counters()
+        hp0 = tt_b200.heff_parts()
         er0 = tt_b200.eig_redo_count(ctx)
         s0 = len(run.steps())
         if sampler:
@@ -500,6 +526,7 @@ def c5_arm(prec, ck, H, args, ctx, stream, flush, torch, tt_b200, sampler=None, 
         clocks = sampler.stop() if sampler else None
         st1, launches = run.stats(), ctx.launches() - l0
         pc1 = tt_b200.planning_counters()
+        hp1 = tt_b200.heff_parts()
         er1 = tt_b200.eig_redo_count(ctx)
         steps = run.steps()[s0:]
         t_step = statistics.mean(times)
@@ -518,6 +545,7 @@ def c5_arm(prec, ck, H, args, ctx, stream, flush, torch, tt_b200, sampler=None, 
             / max(1, args.steps * 2 * B),
             "plans_per_update": (pc1["plans"] - pc0["plans"]) / max(1, args.steps * 2 * B),
             "eig_redos": er1 - er0,
+            "heff_parts": heff_parts_summary(hp0, hp1),
             "step_plans_built": step_plans, "step_pool_reserved_gb": step_pool,
             "step_host_seconds": step_host, "step_device_wait_seconds": step_wait,
             "matvecs_per_update": statistics.mean(s["matvecs"] for s in steps) if steps else None,
@@ -672,6 +700,20 @@ def run_c5(args):
             "peak_source": "cuBLAS TF32 GEMM 8192^3 measured in this run (%.1f TFLOP/s) / 3: each algorithmic "
                            "3xTF32 flop is three TF32 products" % peaks["tf32"],
             "tf32_products_frac": 3.0 * chosen["heff_tflops"] / peaks["tf32"], "traffic": None}
+        hbm = load_hbm_peak()
+        for arm, peak_tc, kind in ((chosen, peaks["tf32"] / 3.0, "3xTF32 tcgen05 (grouped_tc_persist)"),
+                                   (fp64, peaks["fp64"], "FP64 DMMA (grouped_dgemm)")):
+            hpts = arm.get("heff_parts", {})
+            kr = {}
+            if "L*x_and_*R_tflops" in hpts:
+                kr["L*x and *R"] = {"bound": "tensor", "kernel": kind, "achieved": hpts["L*x_and_*R_tflops"],
+                                    "peak": peak_tc, "unit": "TFLOP/s",
+                                    "frac": hpts["L*x_and_*R_tflops"] / peak_tc}
+            if "mid_gbs" in hpts and hbm:
+                kr["*mid"] = {"bound": "hbm", "kernel": "skinny_dgemm (FP64)", "achieved": hpts["mid_gbs"],
+                              "peak": hbm, "unit": "GB/s", "frac": hpts["mid_gbs"] / hbm,
+                              "peak_source": "MEASURED_PEAKS.json hbm_gbs (copy bandwidth)"}
+            arm["kernel_rooflines"] = kr
         fp64["roofline"] = {
             "bound": "tensor", "kernel": "H_eff*x: grouped_dgemm (DMMA), 3 launches per product",
             "achieved": fp64["heff_tflops"], "peak": peaks["fp64"], "unit": "TFLOP/s",

@@ -87,6 +87,12 @@ int tt_dmrg_unbind(void);
 /* on != 0: synchronise between the phases of each two-site step so that
  * tt_qdmrg_step_profile reports per-phase times (slower; off by default) */
 int tt_dmrg_set_profiling(int on);
+/* Per-thread totals over the device-resident Davidson calls' H_eff*x
+ * products: device milliseconds and algorithmic flops of L*x, *mid and *R
+ * (ms[0..2], flops[0..2], event-timed on the library stream) and the
+ * algorithmic bytes of the *mid contractions (distinct operand blocks read
+ * once, the output written once). */
+int tt_dmrg_heff_parts(double* ms, double* flops, double* mid_bytes);
 /* host-side planning counters of this thread: seconds and calls spent in
  * block-structure computation and in contraction-plan creation */
 int tt_dmrg_planning_counters(double* t_structure, int64_t* n_structure, double* t_plan, int64_t* n_plan);

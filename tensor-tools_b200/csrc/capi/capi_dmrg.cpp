@@ -107,6 +107,17 @@ int tt_dmrg_set_precision(int op, int heff, int env) {
 
 int tt_dmrg_set_profiling(int on) { TT_GUARD(ttb::rt().profile = on != 0); }
 
+int tt_dmrg_heff_parts(double* ms, double* flops, double* mid_bytes) {
+  TT_ARG(ms && flops && mid_bytes);
+  TT_GUARD({
+    for (int k = 0; k < 3; ++k) {
+      ms[k] = ttb::rt().heff_part_ms[k];
+      flops[k] = ttb::rt().heff_part_flops[k];
+    }
+    *mid_bytes = ttb::rt().heff_mid_bytes;
+  });
+}
+
 int tt_dmrg_planning_counters(double* t_structure, int64_t* n_structure, double* t_plan, int64_t* n_plan) {
   TT_GUARD({
     if (t_structure) *t_structure = ttb::rt().t_structure;

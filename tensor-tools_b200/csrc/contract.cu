@@ -653,6 +653,10 @@ pack_tf32_ab(const PackJob* __restrict__ jobsA, const PackTile* __restrict__ til
              const PackJob* __restrict__ jobsB, const PackTile* __restrict__ tilesB, const int32_t* __restrict__ tab,
              const double* __restrict__ A, const double* __restrict__ B, uint8_t* __restrict__ pa,
              uint8_t* __restrict__ pb) {
+  // the tile is assembled in shared memory at its swizzled offsets, then
+  // written out with consecutive 16-byte stores (a thread's 16 bytes of a
+  // row would otherwise land in a different 128-byte line per lane)
+  __shared__ __align__(128) uint8_t st[TC_TILE_BYTES];
   const bool is_a = (int)blockIdx.x < n_a;
   const PackTile t = is_a ? tilesA[blockIdx.x] : tilesB[blockIdx.x - n_a];
   const PackJob J = is_a ? jobsA[t.job] : jobsB[t.job];
@@ -677,9 +681,14 @@ pack_tf32_ab(const PackJob* __restrict__ jobsA, const PackTile* __restrict__ til
       l[e] = SPLIT ? to_tf32(__double2float_rn(x[e] - (double)__uint_as_float(h[e]))) : 0u;
     }
     const uint32_t o = sw128_off(r, 4 * q);
-    *reinterpret_cast<uint4*>(dst + o) = make_uint4(h[0], h[1], h[2], h[3]);
-    if (SPLIT) *reinterpret_cast<uint4*>(dst + TC_TILE_BYTES / 2 + o) = make_uint4(l[0], l[1], l[2], l[3]);
+    *reinterpret_cast<uint4*>(st + o) = make_uint4(h[0], h[1], h[2], h[3]);
+    if (SPLIT) *reinterpret_cast<uint4*>(st + TC_TILE_BYTES / 2 + o) = make_uint4(l[0], l[1], l[2], l[3]);
   }
+  __syncthreads();
+  constexpr int NV = (SPLIT ? TC_TILE_BYTES : TC_TILE_BYTES / 2) / 16;
+#pragma unroll 4
+  for (int v = tid; v < NV; v += blockDim.x)
+    reinterpret_cast<uint4*>(dst)[v] = reinterpret_cast<const uint4*>(st)[v];
 }
 
 // Cost model of the *_AUTO precisions: predicted device time (microseconds)

@@ -6,6 +6,7 @@
 #include <cuda_profiler_api.h>
 
 #include <algorithm>
+#include <array>
 #include <chrono>
 #include <cmath>
 #include <cstring>
@@ -162,6 +163,8 @@ class ProductEngine {
   std::vector<BlockMeta> ublocks;
   std::unordered_map<QNKey, unsigned, QNKeyHash> uid;
   double flops = 0.0;
+  double part_flops[3] = {0.0, 0.0, 0.0};  // L*x, *mid, *R
+  double mid_bytes = 0.0;                  // algorithmic bytes of *mid
 
   Presence x_presence() const {
     Presence p(ublocks.size(), 0);
@@ -197,17 +200,22 @@ class ProductEngine {
   // R stay fixed through a Davidson call, so in the tensor-core form their
   // packed tiles are kept in the plans from the first product of the call to
   // the engine's end (~ProductEngine releases them).
-  void apply(const double* v, double* y, int precision = TT_PREC_FP64) {
+  // ev (optional): four events recorded before L*x, after it, after *mid and after *R
+  void apply(const double* v, double* y, int precision = TT_PREC_FP64, void* const* ev = nullptr) {
+    if (ev) check(tt_event_record(ctx(), ev[0]), "event");
     if (tt_plan* p = c1_->plan_for(precision)) {
       check(tt_contract_exec_keep(ctx(), p, L_data(), v, i1_->get(), 1.0, 1), "heff L*v");
       kept_.push_back(p);
     }
+    if (ev) check(tt_event_record(ctx(), ev[1]), "event");
     if (tt_plan* p = c2_->plan_for(precision))
       check(tt_contract_exec(ctx(), p, i1_->get(), A_.mid().data->get(), i2_->get(), 1.0), "heff *mid");
+    if (ev) check(tt_event_record(ctx(), ev[2]), "event");
     if (tt_plan* p = c3_->plan_for(precision)) {
       check(tt_contract_exec_keep(ctx(), p, i2_->get(), A_.right()->data->get(), y, 1.0, 2), "heff *R");
       kept_.push_back(p);
     }
+    if (ev) check(tt_event_record(ctx(), ev[3]), "event");
     for (auto& r : zero_ranges_)
       check(tt_memset_zero(ctx(), y + r.first, sizeof(double) * (size_t)r.second), "heff zero");
   }
@@ -301,6 +309,27 @@ class ProductEngine {
     for (unsigned u = (unsigned)o.blocks.size(); u < ublocks.size(); ++u)
       zero_ranges_.push_back({ublocks[u].off, ublocks[u].size});
     flops = c1_->cs.flops + c2_->cs.flops + c3_->cs.flops;
+    part_flops[0] = c1_->cs.flops;
+    part_flops[1] = c2_->cs.flops;
+    part_flops[2] = c3_->cs.flops;
+    {
+      // algorithmic bytes of the middle contraction: its distinct A and B
+      // blocks read once, its C blocks written once
+      std::unordered_map<int64_t, int64_t> ua, ub;
+      for (const tt_block_pair& q : c2_->cs.pairs) {
+        int64_t m = 1, k = 1, nn = 1;
+        for (int i = 0; i < q.n_m; ++i) m *= q.m_dims[i];
+        for (int i = 0; i < q.n_k; ++i) k *= q.k_dims[i];
+        for (int i = 0; i < q.n_n; ++i) nn *= q.n_dims[i];
+        ua[q.a_off] = m * k;
+        ub[q.b_off] = k * nn;
+      }
+      int64_t el = 0;
+      for (auto& kv : ua) el += kv.second;
+      for (auto& kv : ub) el += kv.second;
+      for (const tt_out_block& o : c2_->cs.outs) el += (int64_t)o.m * o.n;
+      mid_bytes = 8.0 * (double)el;
+    }
     i1_ = dev_alloc(std::max<int64_t>(c1_->cs.C.arena, 2));
     i2_ = dev_alloc(std::max<int64_t>(c2_->cs.C.arena, 2));
   }
@@ -380,15 +409,12 @@ static bool davidson_device(big_qtensor& A, qtensor& x, int max_restart, double 
     for (size_t i = 0; i < a.size(); ++i) a[i] |= b[i];
     return a;
   };
-  std::vector<std::pair<void*, void*>> evs;
+  std::vector<std::array<void*, 4>> evs;  // per product: before L*x, after L*x, after *mid, after *R
   auto product = [&](const KVec& in) {
     KVec out = newvec();
-    std::pair<void*, void*> e{nullptr, nullptr};
-    check(tt_event_create(ctx(), &e.first), "event");
-    check(tt_event_create(ctx(), &e.second), "event");
-    check(tt_event_record(ctx(), e.first), "event");
-    eng.apply(in.d->get(), out.d->get(), prec);
-    check(tt_event_record(ctx(), e.second), "event");
+    std::array<void*, 4> e{nullptr, nullptr, nullptr, nullptr};
+    for (auto& x : e) check(tt_event_create(ctx(), &x), "event");
+    eng.apply(in.d->get(), out.d->get(), prec, e.data());
     evs.push_back(e);
     out.p = eng.product_presence(in.p);
     return out;
@@ -472,10 +498,8 @@ static bool davidson_device(big_qtensor& A, qtensor& x, int max_restart, double 
   tt_dav_result res;
   check(tt_dav_read(ctx(), st, &res), "davidson read");  // the call's one synchronisation
   if (res.final_ii == -2 || !res.done) {
-    for (auto& e : evs) {
-      tt_event_destroy(e.first);
-      tt_event_destroy(e.second);
-    }
+    for (auto& e : evs)
+      for (void* x : e) tt_event_destroy(x);
     return false;
   }
   const int f = res.final_ii;
@@ -484,12 +508,16 @@ static bool davidson_device(big_qtensor& A, qtensor& x, int max_restart, double 
   double heff_ms = 0.0;
   for (size_t i = 0; i < evs.size(); ++i) {
     if ((int)i <= f) {  // products of the iterations that ran: the initial one and f more
-      float ms = 0.f;
-      check(tt_event_elapsed_ms(evs[i].first, evs[i].second, &ms), "event");
-      heff_ms += ms;
+      for (int k = 0; k < 3; ++k) {
+        float ms = 0.f;
+        check(tt_event_elapsed_ms(evs[i][k], evs[i][k + 1], &ms), "event");
+        heff_ms += ms;
+        rt().heff_part_ms[k] += ms;
+        rt().heff_part_flops[k] += eng.part_flops[k];
+      }
+      rt().heff_mid_bytes += eng.mid_bytes;
     }
-    tt_event_destroy(evs[i].first);
-    tt_event_destroy(evs[i].second);
+    for (void* x : evs[i]) tt_event_destroy(x);
   }
   rt().last_heff_ms = heff_ms;
   double lambda = res.lambda;

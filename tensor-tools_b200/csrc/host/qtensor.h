@@ -32,6 +32,9 @@ struct Runtime {
   uint64_t rng_counter = 0x5eed;
   std::shared_ptr<DevBuf> scalars;  // 16 device doubles for reductions
   double last_heff_ms = 0.0;        // device time of the last Davidson's H_eff*x launches
+  double heff_part_ms[3] = {0.0, 0.0, 0.0};     // device-resident Davidson: L*x, *mid, *R times
+  double heff_part_flops[3] = {0.0, 0.0, 0.0};  // and their algorithmic flops
+  double heff_mid_bytes = 0.0;                  // algorithmic bytes of the *mid contractions
   bool profile = false;             // synchronise between step phases to time them
   // host-side planning counters (always on; cheap)
   double t_structure = 0.0;         // seconds in contract_structure

@@ -191,6 +191,7 @@ _proto("tt_qdmrg_step_profile", P, C.c_int, C.POINTER(C.c_int), PD, PD, PD, PD)
 _proto("tt_dmrg_set_profiling", C.c_int)
 _proto("tt_dmrg_planning_counters", PD, PI64, PD, PI64)
 _proto("tt_eig_redo_count", P, PI64)
+_proto("tt_dmrg_heff_parts", PD, PD, PD)
 _proto("tt_sym_eig_batched", P, C.c_void_p, C.c_int, P, P, P, P)
 _proto("tt_qdmrg_num_sweeps", P, C.POINTER(C.c_int))
 _proto("tt_qdmrg_sweep_info", P, C.c_int, PD, PD)
@@ -890,6 +891,15 @@ def set_davidson_control(device: bool = True):
     """tensor_davidsonIT control on the device (one synchronisation per call,
     host loop on Gram-Schmidt failure) or on the host (reads back every iteration)."""
     _chk(lib.tt_dmrg_set_davidson(int(device)), "set_davidson")
+
+
+def heff_parts() -> dict:
+    """Totals over this thread's device-resident Davidson products: device ms
+    and algorithmic flops of L*x, *mid, *R, and the *mid contractions'
+    algorithmic bytes."""
+    ms, fl, mb = (D * 3)(), (D * 3)(), D()
+    _chk(lib.tt_dmrg_heff_parts(ms, fl, C.byref(mb)), "heff_parts")
+    return {"ms": list(ms), "flops": list(fl), "mid_bytes": mb.value}
 
 
 def eig_redo_count(ctx) -> int:

@@ -55,6 +55,7 @@ from __future__ import annotations
 import argparse
 import json
 import os
+import resource
 import shutil
 import statistics
 import subprocess
@@ -123,6 +124,7 @@ def parse():
     p.add_argument("--no-full-sweep", action="store_true")
     p.add_argument("--breakdown", action="store_true", help="one further step per precision with phase times")
     p.add_argument("--env-prec", default=ENV_PREC, help="environment-update precision of the chosen form")
+    p.add_argument("--no-clock-sampler", action="store_true", help="diagnostic: no nvidia-smi sampling")
     p.add_argument("--gemm-size", type=int, default=4096)
     p.add_argument("--precisions", default="fp64,tf32x3,tf32")
     p.add_argument("--chains", type=int, default=64)
@@ -497,7 +499,7 @@ def c5_arm(prec, ck, H, args, ctx, stream, flush, torch, tt_b200, sampler=None, 
         # NVTX range "c5_timed_<precision>": lets a profiler's launch list cover the timed steps only
         torch.cuda.nvtx.range_push("c5_timed_" + prec)
         # per step: pool GB reserved, plans built, host seconds, of which waiting on the device
-        step_pool, step_plans, step_host, step_wait = [], [], [], []
+        step_pool, step_plans, step_host, step_wait, step_os = [], [], [], [], []
         try:
             import psutil
             proc = psutil.Process()
@@ -510,6 +512,8 @@ def c5_arm(prec, ck, H, args, ctx, stream, flush, torch, tt_b200, sampler=None, 
             torch.cuda.synchronize()
             pa = tt_b200.planning_counters()["plans"]
             w0 = ctx.wait_stats()[0]
+            ru0 = resource.getrusage(resource.RUSAGE_SELF)
+            tr0 = ctx.pool_trims()
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             h0 = time.perf_counter()
             e0.record(stream)
@@ -517,6 +521,10 @@ def c5_arm(prec, ck, H, args, ctx, stream, flush, torch, tt_b200, sampler=None, 
             e1.record(stream)
             step_host.append(time.perf_counter() - h0)
             step_wait.append(ctx.wait_stats()[0] - w0)
+            ru1 = resource.getrusage(resource.RUSAGE_SELF)
+            step_os.append({"user_s": ru1.ru_utime - ru0.ru_utime, "sys_s": ru1.ru_stime - ru0.ru_stime,
+                            "minflt": ru1.ru_minflt - ru0.ru_minflt, "majflt": ru1.ru_majflt - ru0.ru_majflt,
+                            "nivcsw": ru1.ru_nivcsw - ru0.ru_nivcsw, "pool_trims": ctx.pool_trims() - tr0})
             e1.synchronize()
             times.append(e0.elapsed_time(e1) * 1e-3)
             step_plans.append(tt_b200.planning_counters()["plans"] - pa)
@@ -529,6 +537,7 @@ def c5_arm(prec, ck, H, args, ctx, stream, flush, torch, tt_b200, sampler=None, 
         hp1 = tt_b200.heff_parts()
         er1 = tt_b200.eig_redo_count(ctx)
         steps = run.steps()[s0:]
+        prof_t = run.profile()[s0:s0 + args.steps * 2 * B]  # host wall time per update, no added syncs
         t_step = statistics.mean(times)
         upd = 2 * B
         fl = st1["heff_flops"] - st0["heff_flops"]
@@ -547,7 +556,14 @@ def c5_arm(prec, ck, H, args, ctx, stream, flush, torch, tt_b200, sampler=None, 
             "eig_redos": er1 - er0,
             "heff_parts": heff_parts_summary(hp0, hp1),
             "step_plans_built": step_plans, "step_pool_reserved_gb": step_pool,
-            "step_host_seconds": step_host, "step_device_wait_seconds": step_wait,
+            "step_host_seconds": step_host, "step_device_wait_seconds": step_wait, "step_os": step_os,
+            # per timed step, host wall seconds inside Davidson (of which building the
+            # product engine), the block SVD and the environment update
+            "step_host_phases": [
+                {"davidson": sum(p[1] for p in prof_t[k * 2 * B:(k + 1) * 2 * B]),
+                 "engine": sum(p[4] for p in prof_t[k * 2 * B:(k + 1) * 2 * B]),
+                 "svd": sum(p[2] for p in prof_t[k * 2 * B:(k + 1) * 2 * B]),
+                 "env": sum(p[3] for p in prof_t[k * 2 * B:(k + 1) * 2 * B])} for k in range(args.steps)],
             "matvecs_per_update": statistics.mean(s["matvecs"] for s in steps) if steps else None,
             "trunc_err_mean": statistics.mean(s["trunc_err"] for s in steps) if steps else None,
             "kept": [s["kept"] for s in steps[-upd:]],
@@ -654,7 +670,7 @@ def run_c5(args):
     try:
         ck, setup = c5_setup(tt_b200, H, args, workdir)
         barrier()
-        sampler = ClockSampler(local)
+        sampler = None if args.no_clock_sampler else ClockSampler(local)
         sz = szsz_mpos(tt_b200)
         chosen = c5_arm(CHOSEN, ck, H, args, ctx, stream, flush, torch, tt_b200, sampler=sampler,
                         e2e_steps=args.e2e_steps, szsz=sz)

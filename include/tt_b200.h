@@ -80,6 +80,9 @@ int tt_ctx_stream(tt_ctx* ctx, void** stream);
 /* Host wall seconds spent blocked in synchronisations of this context's
  * stream (device-to-host reads, tt_ctx_synchronize) and how many there were. */
 int tt_ctx_wait_stats(tt_ctx* ctx, double* seconds, int64_t* count);
+/* Pool allocations that failed once, trimmed the pool to its use and
+ * succeeded or failed on the retry (each trim synchronises the stream). */
+int tt_ctx_pool_trims(tt_ctx* ctx, int64_t* count);
 /* Sticky device status of the context: TT_OK, or TT_ERR_TIMEOUT once a bounded
  * wait inside a tensor-core contraction has given up (that contraction's output
  * is incomplete).  Every synchronisation of the context -- tt_ctx_synchronize

@@ -50,6 +50,7 @@ cudaError_t pool_malloc(tt_ctx* ctx, void** p, size_t bytes) {
   cudaError_t e = cudaMallocAsync(p, bytes, ctx->stream);
   if (e == cudaErrorMemoryAllocation) {
     cudaGetLastError();
+    ctx->pool_trims++;
     if (cudaStreamSynchronize(ctx->stream) == cudaSuccess && cudaMemPoolTrimTo(ctx->pool, 0) == cudaSuccess)
       e = cudaMallocAsync(p, bytes, ctx->stream);
     if (e != cudaSuccess) cudaGetLastError();
@@ -190,6 +191,12 @@ int tt_ctx_wait_stats(tt_ctx* ctx, double* seconds, int64_t* count) {
   TT_REQUIRE(ctx, "null context");
   if (seconds) *seconds = ctx->wait_seconds;
   if (count) *count = ctx->waits;
+  return TT_OK;
+}
+
+int tt_ctx_pool_trims(tt_ctx* ctx, int64_t* count) {
+  TT_REQUIRE(ctx && count, "tt_ctx_pool_trims: null argument");
+  *count = ctx->pool_trims;
   return TT_OK;
 }
 

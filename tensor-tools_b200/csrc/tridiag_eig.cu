@@ -621,8 +621,8 @@ tridiag_eigvecs(const EigDev* __restrict__ probs, const double* G, const double*
 // is the same in every CTA.  The trailing update goes through a global
 // n x 2nb scratch (two barriers per panel): m8n8k4 FP64 tensor-core (DMMA)
 // products of 32 rows x 16 own columns per warp, the rows' [V W] read from
-// the scratch and the columns' from shared memory.  Bisection then runs over all
-// warps of the cluster.
+// the scratch and the columns' from shared memory.  The eigenvalues follow by
+// bisection in a separate, GPU-wide launch (bisect_sectors).
 //
 // Phase 2: CTA r owns eigenvectors [r q, r q + q), q = ceil(nvec / CL).
 // Inverse iteration runs one thread per vector.  Gram-Schmidt (twice, inside
@@ -642,6 +642,9 @@ constexpr int CL_STAGE = 4;  // reflectors staged per round of the back-transfor
 constexpr int CL_MAX = 16;   // largest cluster the kernels are launched with
 constexpr int PNB_MAX = 32;  // widest panel of the blocked reduction
 constexpr int NWARP = TT / 32;
+struct VecTaskB {
+  int32_t prob, j0;  // problem (index into the problem array) and first eigenvalue
+};
 
 // doubles of dynamic shared memory of the blocked cluster reduction
 __host__ __device__ inline int64_t blocked_smem(int n, int nb, int CL) {
@@ -1033,7 +1036,7 @@ tridiag_eigvals_cluster(const EigDev* __restrict__ probs, double* G, double* Tg,
         // part 0: V (rows) x W (columns); part 1: W x V
         const int xo0 = part ? nb : 0;
         const double* Y = part ? Vl : Wl;
-#pragma unroll 2
+#pragma unroll 1
         for (int t = 0; t < nbe4; t += 4) {
           const int k = t + gk;
           const bool kv = k < nbe;
@@ -1085,8 +1088,30 @@ tridiag_eigvals_cluster(const EigDev* __restrict__ probs, double* G, double* Tg,
   }
   __threadfence();
   cluster.sync();  // also the last access of another CTA's shared memory
-  double* d = xo;  // CL * nloc >= n doubles
-  double* e2 = yb;  // CL * nloc >= n doubles
+}
+
+// Bisection for the cluster-sized sectors after their tridiagonalisation,
+// spread over the GPU: a CTA of BS_THREADS threads takes BS_PER eigenvalues
+// of one problem (ten per warp, three lanes per eigenvalue probing the
+// midpoint and both quarter points, as in tridiag_eigvals), with the problem's
+// d and e^2 in shared memory.  Few warps per SM keep each warp's Sturm chain
+// latency-bound instead of sharing one SM's FP64 pipes with fifteen others.
+constexpr int BS_THREADS = 128;
+constexpr int BS_PER = (BS_THREADS / 32) * 10;
+
+__global__ void __launch_bounds__(BS_THREADS)
+bisect_sectors(const EigDev* __restrict__ probs, const VecTaskB* __restrict__ tasks, const double* Tg, double* W) {
+  extern __shared__ double bs_sm[];
+  __shared__ double red[33];
+  const VecTaskB tk = tasks[blockIdx.x];
+  const EigDev P = probs[tk.prob];
+  const int n = P.n;
+  const double* dg = Tg + 3 * P.w_off;
+  const double* eg = dg + n;
+  double* Wp = W + P.w_off;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  double* d = bs_sm;
+  double* e2 = bs_sm + n;
   for (int i = tid; i < n; i += blockDim.x) {
     d[i] = dg[i];
     e2[i] = i < n - 1 ? eg[i] * eg[i] : 0.0;
@@ -1106,41 +1131,38 @@ tridiag_eigvals_cluster(const EigDev* __restrict__ probs, double* G, double* Tg,
   const double pivmin = DBL_MIN * fmax(1.0, emax);
   const double atol = 4.0 * DBL_EPSILON * bnorm + 2.0 * pivmin;
   if (bnorm == 0.0) {
-    for (int j = rank * (int)blockDim.x + tid; j < n; j += CL * (int)blockDim.x) Wp[j] = 0.0;
+    for (int j = tk.j0 + tid; j < min(n, tk.j0 + BS_PER); j += blockDim.x) Wp[n - 1 - j] = 0.0;
     return;
   }
-  // bisection as in tridiag_eigvals, over every warp of the cluster
   auto open_interval = [&](double lo, double hi) {
     return hi - lo > fmax(atol, 2.0 * DBL_EPSILON * fmax(fabs(lo), fabs(hi)));
   };
   const int grp = lane < 30 ? lane / 3 : 0, sub = lane % 3;
-  for (int base = (rank * NWARP + warp) * 10; base < n; base += CL * NWARP * 10) {
-    const int j = base + grp;
-    const bool active = lane < 30 && j < n;
-    double lo = gl - atol, hi = gu + atol;
-    int it = 0;
-    bool work = active && open_interval(lo, hi);
-    while (__any_sync(0xffffffffu, work)) {
-      const double mid = 0.5 * (lo + hi), lm = 0.5 * (lo + mid), rm = 0.5 * (mid + hi);
-      const double x = sub == 0 ? mid : (sub == 1 ? lm : rm);
-      const int c = work ? sturm_count(d, e2, n, x, pivmin) : 0;
-      const int cm = __shfl_sync(0xffffffffu, c, 3 * grp);
-      const int cl = __shfl_sync(0xffffffffu, c, 3 * grp + 1);
-      const int cr = __shfl_sync(0xffffffffu, c, 3 * grp + 2);
-      if (work) {
-        const bool left = cm > j;
-        if (left) hi = mid; else lo = mid;
+  const int j = tk.j0 + warp * 10 + grp;
+  const bool active = lane < 30 && j < n;
+  double lo = gl - atol, hi = gu + atol;
+  int it = 0;
+  bool work = active && open_interval(lo, hi);
+  while (__any_sync(0xffffffffu, work)) {
+    const double mid = 0.5 * (lo + hi), lm = 0.5 * (lo + mid), rm = 0.5 * (mid + hi);
+    const double x = sub == 0 ? mid : (sub == 1 ? lm : rm);
+    const int c = work ? sturm_count(d, e2, n, x, pivmin) : 0;
+    const int cm = __shfl_sync(0xffffffffu, c, 3 * grp);
+    const int cl = __shfl_sync(0xffffffffu, c, 3 * grp + 1);
+    const int cr = __shfl_sync(0xffffffffu, c, 3 * grp + 2);
+    if (work) {
+      const bool left = cm > j;
+      if (left) hi = mid; else lo = mid;
+      ++it;
+      if (it < 128 && open_interval(lo, hi)) {
+        const double x2 = left ? lm : rm;
+        if ((left ? cl : cr) > j) hi = x2; else lo = x2;
         ++it;
-        if (it < 128 && open_interval(lo, hi)) {
-          const double x2 = left ? lm : rm;
-          if ((left ? cl : cr) > j) hi = x2; else lo = x2;
-          ++it;
-        }
-        work = it < 128 && open_interval(lo, hi);
       }
+      work = it < 128 && open_interval(lo, hi);
     }
-    if (active && sub == 0) Wp[n - 1 - j] = 0.5 * (lo + hi);
   }
+  if (active && sub == 0) Wp[n - 1 - j] = 0.5 * (lo + hi);
 }
 
 __global__ void __launch_bounds__(TT)
@@ -2011,6 +2033,24 @@ int tt_sym_eigvals_batched(tt_ctx* ctx, const tt_eig_problem* probs, int n_probs
     TT_CUDA(tt::h2d_async(ctx, dp + n_small, big.data(), sizeof(EigDev) * big.size()));
     TT_CUDA(launch_cluster(ctx, cp.cl, (int)big.size(), need, (const void*)tridiag_eigvals_cluster,
                            dp + n_small, G, T, w, vw));
+    // their eigenvalues, BS_PER per CTA over the whole GPU
+    std::vector<VecTaskB> bt;
+    int nmax = 0;
+    for (size_t b = 0; b < big.size(); ++b) {
+      nmax = std::max(nmax, big[b].n);
+      for (int j0 = 0; j0 < big[b].n; j0 += BS_PER) bt.push_back(VecTaskB{n_small + (int32_t)b, j0});
+    }
+    VecTaskB* d_bt = tt::pool_alloc<VecTaskB>(ctx, bt.size());
+    if (!d_bt) return tt::fail(TT_ERR_OOM, "tt_sym_eigvals_batched: allocation failed");
+    TT_CUDA(tt::h2d_async(ctx, d_bt, bt.data(), sizeof(VecTaskB) * bt.size()));
+    const size_t bs_smem = sizeof(double) * 2 * (size_t)nmax;
+    static thread_local uint64_t bs_attr = 0;
+    if (tt::first_on_device(bs_attr, ctx->device))
+      TT_CUDA(cudaFuncSetAttribute(bisect_sectors, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)(sizeof(double) * 2 * MAX_N)));
+    bisect_sectors<<<(unsigned)bt.size(), BS_THREADS, bs_smem, ctx->stream>>>(dp, d_bt, T, w);
+    TT_LAUNCH_CHECK(ctx);
+    tt::pool_free(ctx, d_bt);
   }
   tt::pool_free(ctx, vw);
   tt::pool_free(ctx, dp);

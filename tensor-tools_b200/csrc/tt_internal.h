@@ -30,6 +30,7 @@ struct tt_ctx {
   size_t stage_head = 0;
   // host wall time spent blocked in stream synchronisations, and their count
   double wait_seconds = 0.0;
+  int64_t pool_trims = 0;  // allocations that failed once, trimmed the pool and retried
   int64_t waits = 0;
   // sticky status of the bounded device waits (mapped pinned memory, so a
   // kernel that gives up writes TT_ERR_TIMEOUT straight into host memory);

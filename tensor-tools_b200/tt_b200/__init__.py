@@ -77,6 +77,7 @@ _proto("tt_ctx_destroy", P)
 _proto("tt_ctx_synchronize", P)
 _proto("tt_ctx_stream", P, PP)
 _proto("tt_ctx_wait_stats", P, PD, PI64)
+_proto("tt_ctx_pool_trims", P, PI64)
 _proto("tt_ctx_launch_count", P, PI64)
 lib.tt_get_last_error.restype = C.c_char_p
 lib.tt_get_last_error.argtypes = []
@@ -234,6 +235,12 @@ class Context:
         s, n = D(), I64()
         _chk(lib.tt_ctx_wait_stats(self.h, C.byref(s), C.byref(n)), "wait stats")
         return s.value, n.value
+
+    def pool_trims(self) -> int:
+        """Pool allocations that failed once and were retried after a trim."""
+        n = I64()
+        _chk(lib.tt_ctx_pool_trims(self.h, C.byref(n)), "pool trims")
+        return n.value
 
     def launches(self) -> int:
         n = I64()

@@ -152,6 +152,14 @@ typedef struct {
 int tt_contract_plan(tt_ctx* ctx, const tt_out_block* outs, int n_out,
                      const tt_block_pair* pairs, int n_pairs, int precision,
                      tt_plan** plan);
+/* As tt_contract_plan, with a hint for the *_AUTO choice: keep bit 0 (A) /
+ * bit 1 (B) marks an operand that the caller will keep packed across several
+ * execs (tt_contract_exec_keep), so its packing is charged once for several
+ * of them.  The hint changes only the precision chosen, never the results of
+ * a given precision. */
+int tt_contract_plan_keep(tt_ctx* ctx, const tt_out_block* outs, int n_out,
+                          const tt_block_pair* pairs, int n_pairs, int precision, int keep,
+                          tt_plan** plan);
 int tt_contract_exec(tt_ctx* ctx, const tt_plan* plan, const double* A,
                      const double* B, double* C, double alpha);
 /* tt_contract_exec that keeps packed operands: bit 0 of keep keeps A's

@@ -310,6 +310,90 @@ skinny_dgemm(const TaskDev* __restrict__ tasks, const OutDev* __restrict__ outs,
   }
 }
 
+// Row-stationary form of the skinny path.  Output blocks that read the same
+// A blocks (the same rows, other column sectors: for the middle contraction
+// the (s1' s2' w') sectors fed by one T1 block) are gathered into chunks of
+// at most RS_COLS columns; a task is one chunk's SK_ROWS-row tile.  Each distinct
+// A block of the chunk is read once per row and multiplied into a combined B
+// (k x NC: every pair's B block at its output's columns, zeros elsewhere), so
+// T1 crosses HBM once instead of once per output sector.
+// combined columns per chunk: 16 keeps the accumulators of a 256-row task at
+// about 70 registers a thread (three CTAs per SM); 32 halved the occupancy and
+// ran slower than reading a shared A block twice
+constexpr int RS_COLS = 16;
+struct RsChunk {
+  int32_t a_begin, a_end;  // its distinct A blocks in rs_a
+  int32_t o_begin, o_end;  // its output blocks in rs_o
+  int32_t m;               // rows (shared by the chunk's outputs)
+  int32_t ktot;            // sum of k over its A blocks
+};
+struct RsA {
+  int32_t pair;            // a pair reading this A block (its rowA / colA tables, a_off, k)
+  int32_t e_begin, e_end;  // the pairs of the chunk reading it, in rs_e
+};
+struct RsE {
+  int32_t pair, col;  // a pair and the first combined column of its output
+};
+struct RsO {
+  int32_t out, col;  // an output block and its first combined column
+};
+
+template <int NC>
+__global__ void __launch_bounds__(SK_ROWS)
+skinny_rs(const TaskDev* __restrict__ tasks, const RsChunk* __restrict__ chunks, const RsA* __restrict__ ra,
+          const RsE* __restrict__ re, const RsO* __restrict__ ro, const OutDev* __restrict__ outs,
+          const PairDev* __restrict__ pairs, const int32_t* __restrict__ tab, const double* __restrict__ A,
+          const double* __restrict__ B, double* __restrict__ C, double alpha) {
+  extern __shared__ double rs_dyn[];  // ktot x NC combined B, then ktot A column offsets
+  const TaskDev task = tasks[blockIdx.x];
+  const RsChunk ch = chunks[task.out];
+  const int r = task.m0 + threadIdx.x;
+  double* bst = rs_dyn;
+  int32_t* cst = reinterpret_cast<int32_t*>(rs_dyn + (int64_t)ch.ktot * NC);
+  for (int e = threadIdx.x; e < ch.ktot * NC; e += blockDim.x) bst[e] = 0.0;
+  __syncthreads();
+  int k0 = 0;
+  for (int a = ch.a_begin; a < ch.a_end; ++a) {
+    const RsA X = ra[a];
+    const PairDev PA = pairs[X.pair];
+    for (int kk = threadIdx.x; kk < PA.k; kk += blockDim.x) cst[k0 + kk] = tab[PA.colA + kk];
+    for (int q = X.e_begin; q < X.e_end; ++q) {
+      const RsE E = re[q];
+      const PairDev P = pairs[E.pair];
+      for (int e = threadIdx.x; e < P.k * P.n; e += blockDim.x) {
+        const int kk = e / P.n, c = e % P.n;
+        bst[(k0 + kk) * NC + E.col + c] = B[P.b_off + tab[P.rowB + kk] + tab[P.colB + c]];
+      }
+    }
+    k0 += PA.k;
+  }
+  __syncthreads();
+  double acc[NC];
+#pragma unroll
+  for (int c = 0; c < NC; ++c) acc[c] = 0.0;
+  if (r < ch.m) {
+    k0 = 0;
+    for (int a = ch.a_begin; a < ch.a_end; ++a) {
+      const PairDev PA = pairs[ra[a].pair];
+      const double* __restrict__ arow = A + PA.a_off + tab[PA.rowA + r];
+      for (int kk = 0; kk < PA.k; ++kk) {
+        const double x = arow[cst[k0 + kk]];
+#pragma unroll
+        for (int c = 0; c < NC; ++c) acc[c] = fma(x, bst[(k0 + kk) * NC + c], acc[c]);
+      }
+      k0 += PA.k;
+    }
+    for (int o = ch.o_begin; o < ch.o_end; ++o) {
+      const RsO O = ro[o];
+      const OutDev out = outs[O.out];
+      double* Cb = C + out.c_off + r;
+#pragma unroll
+      for (int c = 0; c < NC; ++c)
+        if (c >= O.col && c < O.col + out.n) Cb[(int64_t)out.ldc * (c - O.col)] = alpha * acc[c];
+    }
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Mixed-precision path: tcgen05 (5th-generation tensor cores), kind::tf32.
 //
@@ -707,7 +791,7 @@ pack_tf32_ab(const PackJob* __restrict__ jobsA, const PackTile* __restrict__ til
 // kernels on B200 (4096^3: DMMA 26 TFLOP/s, tcgen05 690 TFLOP/s of TF32
 // products).
 double predict_us(const tt_out_block* outs, int n_out, const std::vector<PairDev>& hp,
-                  const std::vector<int>& first, int prec, int num_sms) {
+                  const std::vector<int>& first, int prec, int num_sms, int keep = 0) {
   constexpr double kDmmaRate = 27e12, kTcRate = 650e12, kHbm = 6.0e12, kLaunchUs = 2.5;
   const bool tc = prec != TT_PREC_FP64;
   // the DMMA kernel stops at k rounded up to its k-step of 4; the tcgen05
@@ -735,8 +819,14 @@ double predict_us(const tt_out_block* outs, int n_out, const std::vector<PairDev
   // also writes the packed tiles (hi + lo: 8 bytes per padded element, TF32:
   // 4) and reads them back
   const double packed = prec == TT_PREC_TF32X3 ? 8.0 : 4.0;
-  for (const auto* u : {&ua, &ub})
-    for (const auto& kv : *u) bytes += 8.0 * kv.second.first + (tc ? 2.0 * packed * kv.second.second : 0.0);
+  // an operand kept packed across execs (keep bit 0: A, bit 1: B) is packed
+  // once for kKeptUses of them
+  constexpr double kKeptUses = 4.0;
+  for (int w = 0; w < 2; ++w) {
+    const double share = ((keep >> w) & 1) ? 1.0 / kKeptUses : 1.0;
+    for (const auto& kv : (w == 0 ? ua : ub))
+      bytes += 8.0 * kv.second.first + (tc ? 2.0 * packed * kv.second.second * share : 0.0);
+  }
   const double t = std::max({total / rate, longest / (rate / std::max(1, num_sms)), bytes / kHbm});
   return t * 1e6 + (tc ? 3 : 1) * kLaunchUs;
 }
@@ -748,6 +838,15 @@ struct tt_plan {
   bool skinny = false;      // FP64 plan run by skinny_dgemm (row tasks of SK_ROWS)
   int skinny_nc = SK_N;     // its widest output block (the kernel instance covers it)
   int64_t skinny_ktot = 0;  // the largest sum of k over one output block's pairs
+  // row-stationary form of a skinny plan (skinny_rs), when its chunks are valid
+  bool rs = false;
+  int rs_n_tasks = 0, rs_nc = SK_N;
+  int64_t rs_ktot = 0;
+  TaskDev* d_rs_tasks = nullptr;
+  RsChunk* d_rs_chunks = nullptr;
+  RsA* d_rs_a = nullptr;
+  RsE* d_rs_e = nullptr;
+  RsO* d_rs_o = nullptr;
   int* d_status = nullptr;  // tensor-core path: TT_OK or TT_ERR_TIMEOUT
   // tensor-core path: packing jobs and tiles of the unique A / B blocks, the
   // pairs in packed form, and the packed sizes (buffers are taken from the
@@ -779,6 +878,11 @@ extern "C" {
 int tt_contract_plan(tt_ctx* ctx, const tt_out_block* outs, int n_out,
                      const tt_block_pair* pairs, int n_pairs, int precision,
                      tt_plan** plan_out) {
+  return tt_contract_plan_keep(ctx, outs, n_out, pairs, n_pairs, precision, 0, plan_out);
+}
+
+int tt_contract_plan_keep(tt_ctx* ctx, const tt_out_block* outs, int n_out, const tt_block_pair* pairs,
+                          int n_pairs, int precision, int keep, tt_plan** plan_out) {
   TT_REQUIRE(ctx && plan_out, "tt_contract_plan: null argument");
   TT_REQUIRE(n_out >= 0 && n_pairs >= 0, "tt_contract_plan: negative count");
   TT_REQUIRE(precision >= TT_PREC_FP64 && precision <= TT_PREC_TF32X3_AUTO,
@@ -852,7 +956,7 @@ int tt_contract_plan(tt_ctx* ctx, const tt_out_block* outs, int n_out,
   for (int o = 0; o < n_out; ++o) first[o + 1] += first[o];
   // FP64 unless the tensor-core form is predicted clearly (20 %) faster: the
   // model is coarse, and FP64 is the more accurate of the two
-  if (automatic && predict_us(outs, n_out, hp, first, precision, ctx->num_sms) >
+  if (automatic && predict_us(outs, n_out, hp, first, precision, ctx->num_sms, keep) >
                        0.8 * predict_us(outs, n_out, hp, first, TT_PREC_FP64, ctx->num_sms))
     precision = TT_PREC_FP64;
   const bool tc = precision != TT_PREC_FP64;
@@ -877,6 +981,13 @@ int tt_contract_plan(tt_ctx* ctx, const tt_out_block* outs, int n_out,
   }
   std::vector<int> torder(tasks.size());
   std::iota(torder.begin(), torder.end(), 0);
+  bool rs_ok = false;
+  std::vector<RsChunk> rs_chunks;
+  std::vector<RsA> rs_a;
+  std::vector<RsE> rs_e;
+  std::vector<RsO> rs_o;
+  std::vector<TaskDev> rs_tasks;
+  int64_t rs_ktot = 0;
   if (skinny) {
     // The skinny kernel is bound by reading A, and every output block that
     // shares A's blocks (the same rows, other column sectors) reads them
@@ -902,6 +1013,81 @@ int tt_contract_plan(tt_ctx* ctx, const tt_out_block* outs, int n_out,
       if (tasks[a].m0 != tasks[b].m0) return tasks[a].m0 < tasks[b].m0;
       return tasks[a].out < tasks[b].out;
     });
+    // row-stationary chunks (skinny_rs): a group's outputs in order, at most
+    // SK_N combined columns each; valid when the group's outputs share their
+    // rows and every A block is read through the same tables by all its pairs
+    rs_ok = true;
+    std::unordered_map<int64_t, int> a_first;  // a_off -> first pair reading it
+    for (int i = 0; i < n_pairs && rs_ok; ++i) {
+      auto it = a_first.emplace(hp[i].a_off, i).first;
+      const tt_block_pair& x = pairs[order[it->second]];
+      const tt_block_pair& y = pairs[order[i]];
+      rs_ok = hp[i].m == hp[it->second].m && hp[i].k == hp[it->second].k && x.n_m == y.n_m && x.n_k == y.n_k;
+      for (int d = 0; d < x.n_m && rs_ok; ++d)
+        rs_ok = x.m_dims[d] == y.m_dims[d] && x.a_m_stride[d] == y.a_m_stride[d];
+      for (int d = 0; d < x.n_k && rs_ok; ++d)
+        rs_ok = x.k_dims[d] == y.k_dims[d] && x.a_k_stride[d] == y.a_k_stride[d];
+    }
+    std::vector<std::vector<int>> members(n_out);
+    for (int o = 0; o < n_out; ++o) members[root(o)].push_back(o);
+    for (int g = 0; g < n_out && rs_ok; ++g)
+      for (int o : members[g]) rs_ok = rs_ok && outs[o].m == outs[members[g][0]].m;
+    std::vector<int> gorder;
+    for (int g = 0; g < n_out; ++g)
+      if (!members[g].empty()) gorder.push_back(g);
+    std::stable_sort(gorder.begin(), gorder.end(), [&](int a, int b) { return gcost[a] > gcost[b]; });
+    for (int g : gorder) {
+      if (!rs_ok) break;
+      size_t c0 = rs_chunks.size();
+      auto open_chunk = [&]() {
+        RsChunk c{(int32_t)rs_a.size(), (int32_t)rs_a.size(), (int32_t)rs_o.size(), (int32_t)rs_o.size(),
+                  (int32_t)outs[members[g][0]].m, 0};
+        rs_chunks.push_back(c);
+      };
+      open_chunk();
+      int cols = 0;
+      std::unordered_map<int64_t, int> a_slot;  // a_off -> index in rs_a within the chunk
+      std::vector<std::vector<RsE>> ents;       // per rs_a entry of the chunk
+      auto close_chunk = [&]() {
+        RsChunk& c = rs_chunks.back();
+        for (size_t i = 0; i < ents.size(); ++i) {
+          rs_a[c.a_begin + i].e_begin = (int32_t)rs_e.size();
+          rs_e.insert(rs_e.end(), ents[i].begin(), ents[i].end());
+          rs_a[c.a_begin + i].e_end = (int32_t)rs_e.size();
+          c.ktot += hp[rs_a[c.a_begin + i].pair].k;
+        }
+        c.a_end = (int32_t)rs_a.size();
+        c.o_end = (int32_t)rs_o.size();
+        ents.clear();
+        a_slot.clear();
+      };
+      for (int o : members[g]) {
+        if (cols + outs[o].n > RS_COLS && cols > 0) {
+          close_chunk();
+          open_chunk();
+          cols = 0;
+        }
+        rs_o.push_back(RsO{o, cols});
+        for (int i = first[o]; i < first[o + 1]; ++i) {
+          auto it = a_slot.find(hp[i].a_off);
+          if (it == a_slot.end()) {
+            it = a_slot.emplace(hp[i].a_off, (int)ents.size()).first;
+            rs_a.push_back(RsA{i, 0, 0});
+            ents.emplace_back();
+          }
+          ents[it->second].push_back(RsE{i, cols});
+        }
+        cols += outs[o].n;
+      }
+      close_chunk();
+      // tasks: the group's row tiles, its chunks interleaved within a tile
+      const int m = outs[members[g][0]].m;
+      for (int m0 = 0; m0 < m; m0 += SK_ROWS)
+        for (size_t c = c0; c < rs_chunks.size(); ++c) rs_tasks.push_back(TaskDev{(int32_t)c, m0, 0, 0, 0});
+    }
+    for (const RsChunk& c : rs_chunks) rs_ktot = std::max<int64_t>(rs_ktot, c.ktot);
+    for (const RsO& x : rs_o) rs_ok = rs_ok && outs[x.out].n <= RS_COLS;  // every chunk fits its instance
+    if (rs_ok) rs_ok = rs_ktot * (int64_t)(RS_COLS * sizeof(double) + sizeof(int32_t)) <= SK_STAGE_BYTES;
   } else {
     std::stable_sort(torder.begin(), torder.end(), [&](int a, int b) { return tcost[a] > tcost[b]; });
   }
@@ -1009,6 +1195,32 @@ int tt_contract_plan(tt_ctx* ctx, const tt_out_block* outs, int n_out,
     TT_LAUNCH_CHECK(ctx);
   }
   tt::pool_free(ctx, d_jobs);  // stream-ordered: freed after expand_tables ran
+  if (rs_ok && !rs_tasks.empty()) {
+    plan->d_rs_tasks = tt::pool_alloc<TaskDev>(ctx, rs_tasks.size());
+    plan->d_rs_chunks = tt::pool_alloc<RsChunk>(ctx, rs_chunks.size());
+    plan->d_rs_a = tt::pool_alloc<RsA>(ctx, rs_a.size());
+    plan->d_rs_e = tt::pool_alloc<RsE>(ctx, rs_e.size());
+    plan->d_rs_o = tt::pool_alloc<RsO>(ctx, rs_o.size());
+    if (plan->d_rs_tasks && plan->d_rs_chunks && plan->d_rs_a && plan->d_rs_e && plan->d_rs_o) {
+      TT_CUDA(tt::h2d_async(ctx, plan->d_rs_tasks, rs_tasks.data(), sizeof(TaskDev) * rs_tasks.size()));
+      TT_CUDA(tt::h2d_async(ctx, plan->d_rs_chunks, rs_chunks.data(), sizeof(RsChunk) * rs_chunks.size()));
+      TT_CUDA(tt::h2d_async(ctx, plan->d_rs_a, rs_a.data(), sizeof(RsA) * rs_a.size()));
+      TT_CUDA(tt::h2d_async(ctx, plan->d_rs_e, rs_e.data(), sizeof(RsE) * rs_e.size()));
+      TT_CUDA(tt::h2d_async(ctx, plan->d_rs_o, rs_o.data(), sizeof(RsO) * rs_o.size()));
+      plan->rs = true;
+      plan->rs_n_tasks = (int)rs_tasks.size();
+      plan->rs_ktot = rs_ktot;
+      int wmax = 1;
+      for (const RsChunk& c : rs_chunks) {
+        int w = 0;
+        for (int o = c.o_begin; o < c.o_end; ++o) w += outs[rs_o[o].out].n;
+        wmax = std::max(wmax, w);
+      }
+      plan->rs_nc = wmax;
+      plan->dev_bytes += (int64_t)(sizeof(TaskDev) * rs_tasks.size() + sizeof(RsChunk) * rs_chunks.size() +
+                                   sizeof(RsA) * rs_a.size() + sizeof(RsE) * rs_e.size() + sizeof(RsO) * rs_o.size());
+    }
+  }
   *plan_out = plan;
   return TT_OK;
 }
@@ -1042,7 +1254,20 @@ int tt_contract_exec_keep(tt_ctx* ctx, const tt_plan* plan, const double* A, con
                                  (int)TC_BULK_SMEM));
   }
   if (plan->precision == TT_PREC_FP64) {
-    if (plan->skinny) {
+    if (plan->rs) {
+      const int nc = plan->rs_nc <= 4 ? 4 : plan->rs_nc <= 8 ? 8 : plan->rs_nc <= 16 ? 16 : 32;
+      const size_t dyn = (size_t)(plan->rs_ktot * (int64_t)(nc * sizeof(double) + sizeof(int32_t)));
+      using RsFn = void (*)(const TaskDev*, const RsChunk*, const RsA*, const RsE*, const RsO*, const OutDev*,
+                            const PairDev*, const int32_t*, const double*, const double*, double*, double);
+      const int which = nc == 4 ? 0 : nc == 8 ? 1 : nc == 16 ? 2 : 3;
+      const RsFn fns[4] = {skinny_rs<4>, skinny_rs<8>, skinny_rs<16>, skinny_rs<32>};
+      static thread_local uint64_t rs_attr[4] = {0, 0, 0, 0};  // per instance, per host thread and device
+      if (tt::first_on_device(rs_attr[which], ctx->device))
+        TT_CUDA(cudaFuncSetAttribute(fns[which], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SK_STAGE_BYTES));
+      fns[which]<<<plan->rs_n_tasks, SK_ROWS, dyn, ctx->stream>>>(
+          plan->d_rs_tasks, plan->d_rs_chunks, plan->d_rs_a, plan->d_rs_e, plan->d_rs_o, plan->d_outs,
+          plan->d_pairs, plan->d_tab, A, B, C, alpha);
+    } else if (plan->skinny) {
       const int nc = plan->skinny_nc <= 4 ? 4 : plan->skinny_nc <= 8 ? 8 : plan->skinny_nc <= 16 ? 16 : 32;
       // every pair of a task staged at once when the widest task fits
       const int64_t need = plan->skinny_ktot * (int64_t)(nc * sizeof(double) + sizeof(int32_t));
@@ -1144,6 +1369,11 @@ int tt_plan_destroy(tt_ctx* ctx, tt_plan* plan) {
     tt::pool_free(ctx, plan->d_tilesA);
     tt::pool_free(ctx, plan->d_tilesB);
     tt::pool_free(ctx, plan->d_pairtc);
+    tt::pool_free(ctx, plan->d_rs_tasks);
+    tt::pool_free(ctx, plan->d_rs_chunks);
+    tt::pool_free(ctx, plan->d_rs_a);
+    tt::pool_free(ctx, plan->d_rs_e);
+    tt::pool_free(ctx, plan->d_rs_o);
   }
   delete plan;
   return TT_OK;

@@ -203,7 +203,7 @@ class ProductEngine {
   // ev (optional): four events recorded before L*x, after it, after *mid and after *R
   void apply(const double* v, double* y, int precision = TT_PREC_FP64, void* const* ev = nullptr) {
     if (ev) check(tt_event_record(ctx(), ev[0]), "event");
-    if (tt_plan* p = c1_->plan_for(precision)) {
+    if (tt_plan* p = c1_->plan_for(precision, 1)) {  // L stays packed through the Davidson call
       check(tt_contract_exec_keep(ctx(), p, L_data(), v, i1_->get(), 1.0, 1), "heff L*v");
       kept_.push_back(p);
     }
@@ -211,7 +211,7 @@ class ProductEngine {
     if (tt_plan* p = c2_->plan_for(precision))
       check(tt_contract_exec(ctx(), p, i1_->get(), A_.mid().data->get(), i2_->get(), 1.0), "heff *mid");
     if (ev) check(tt_event_record(ctx(), ev[2]), "event");
-    if (tt_plan* p = c3_->plan_for(precision)) {
+    if (tt_plan* p = c3_->plan_for(precision, 2)) {  // and so does R
       check(tt_contract_exec_keep(ctx(), p, i2_->get(), A_.right()->data->get(), y, 1.0, 2), "heff *R");
       kept_.push_back(p);
     }

@@ -682,11 +682,11 @@ std::shared_ptr<const CachedContraction> contract_cached(const qtensor& A, const
   return val;
 }
 
-tt_plan* CachedContraction::plan_for(int precision) const {
+tt_plan* CachedContraction::plan_for(int precision, int keep) const {
   if (precision < TT_PREC_FP64 || precision > TT_PREC_TF32X3_AUTO) throw std::runtime_error("plan_for: bad precision");
   if (cs.outs.empty()) return nullptr;
   if (!plans[precision]) {
-    plans[precision] = make_plan(cs, precision);
+    plans[precision] = make_plan(cs, precision, keep);
     int64_t b = 0;
     if (tt_plan_device_bytes(plans[precision]->get(), &b) == TT_OK) cache().plan_bytes += b;
   }
@@ -696,7 +696,7 @@ tt_plan* CachedContraction::plan_for(int precision) const {
 PrecisionScope::PrecisionScope(int p) : saved(rt().precision) { rt().precision = p; }
 PrecisionScope::~PrecisionScope() { rt().precision = saved; }
 
-std::shared_ptr<PlanHandle> make_plan(const ContractStructure& cs, int precision) {
+std::shared_ptr<PlanHandle> make_plan(const ContractStructure& cs, int precision, int keep) {
   auto t0 = std::chrono::steady_clock::now();
   struct Acc {
     std::chrono::steady_clock::time_point t0;
@@ -707,8 +707,8 @@ std::shared_ptr<PlanHandle> make_plan(const ContractStructure& cs, int precision
   } acc{t0};
   validate_pairs(cs.outs, cs.pairs, cs.a_size, cs.b_size, cs.C.arena);
   tt_plan* p = nullptr;
-  check(tt_contract_plan(ctx(), cs.outs.data(), (int)cs.outs.size(), cs.pairs.data(), (int)cs.pairs.size(),
-                         precision, &p),
+  check(tt_contract_plan_keep(ctx(), cs.outs.data(), (int)cs.outs.size(), cs.pairs.data(), (int)cs.pairs.size(),
+                              precision, keep, &p),
         "contract plan");
   return std::make_shared<PlanHandle>(p);
 }

@@ -246,7 +246,9 @@ struct CachedContraction {
   // device plans by requested precision (TT_PREC_FP64 ... TT_PREC_TF32X3_AUTO),
   // built on first use; null when cs has no output blocks
   mutable std::shared_ptr<class PlanHandle> plans[TT_PREC_TF32X3_AUTO + 1];
-  tt_plan* plan_for(int precision) const;
+  // keep: the operands (bit 0 A, bit 1 B) the caller keeps packed across
+  // execs, a hint for the automatic precision (see tt_contract_plan_keep)
+  tt_plan* plan_for(int precision, int keep = 0) const;
 };
 // need_plan builds the plan of rt().precision right away.
 std::shared_ptr<const CachedContraction> contract_cached(const qtensor& A, const qtensor& B,
@@ -266,7 +268,7 @@ class PlanHandle {
  private:
   tt_plan* p_ = nullptr;
 };
-std::shared_ptr<PlanHandle> make_plan(const ContractStructure& cs, int precision = TT_PREC_FP64);
+std::shared_ptr<PlanHandle> make_plan(const ContractStructure& cs, int precision = TT_PREC_FP64, int keep = 0);
 
 // Scoped change of rt().precision, the precision of operator* contractions.
 struct PrecisionScope {

@@ -200,18 +200,33 @@ class ProductEngine {
   // R stay fixed through a Davidson call, so in the tensor-core form their
   // packed tiles are kept in the plans from the first product of the call to
   // the engine's end (~ProductEngine releases them).
+  // The precision each contraction of a product runs in.  Under an automatic
+  // precision the middle contraction (bandwidth-bound: T1 read, T2 written,
+  // k and n the MPO link widths) stays FP64, and L*x and *R above
+  // kTensorCoreFlops run on the tensor cores without consulting the cost
+  // model, whose choice for them flipped between updates at bond dimension
+  // 3072 although the tensor-core form was 4x faster there every time.
+  static constexpr double kTensorCoreFlops = 2e10;
+  static int part_precision(int precision, int part, double flops) {
+    const bool automatic = precision == TT_PREC_TF32_AUTO || precision == TT_PREC_TF32X3_AUTO;
+    if (!automatic) return precision;
+    if (part == 1) return TT_PREC_FP64;
+    if (flops >= kTensorCoreFlops) return precision == TT_PREC_TF32_AUTO ? TT_PREC_TF32 : TT_PREC_TF32X3;
+    return precision;
+  }
+
   // ev (optional): four events recorded before L*x, after it, after *mid and after *R
   void apply(const double* v, double* y, int precision = TT_PREC_FP64, void* const* ev = nullptr) {
     if (ev) check(tt_event_record(ctx(), ev[0]), "event");
-    if (tt_plan* p = c1_->plan_for(precision, 1)) {  // L stays packed through the Davidson call
+    if (tt_plan* p = c1_->plan_for(part_precision(precision, 0, part_flops[0]), 1)) {  // L kept through the call
       check(tt_contract_exec_keep(ctx(), p, L_data(), v, i1_->get(), 1.0, 1), "heff L*v");
       kept_.push_back(p);
     }
     if (ev) check(tt_event_record(ctx(), ev[1]), "event");
-    if (tt_plan* p = c2_->plan_for(precision))
+    if (tt_plan* p = c2_->plan_for(part_precision(precision, 1, part_flops[1])))
       check(tt_contract_exec(ctx(), p, i1_->get(), A_.mid().data->get(), i2_->get(), 1.0), "heff *mid");
     if (ev) check(tt_event_record(ctx(), ev[2]), "event");
-    if (tt_plan* p = c3_->plan_for(precision, 2)) {  // and so does R
+    if (tt_plan* p = c3_->plan_for(part_precision(precision, 2, part_flops[2]), 2)) {  // and so is R
       check(tt_contract_exec_keep(ctx(), p, i2_->get(), A_.right()->data->get(), y, 1.0, 2), "heff *R");
       kept_.push_back(p);
     }

@@ -631,6 +631,7 @@ struct ContractionCache {
   std::unordered_map<uint64_t, std::vector<CacheEntry>> map;
   size_t entries = 0;
   int64_t plan_bytes = 0;  // device bytes held by the cached plans
+  uint64_t clock = 0;      // lookups so far (least recently used entries go first)
 };
 ContractionCache& cache() {
   static thread_local ContractionCache c;
@@ -639,9 +640,38 @@ ContractionCache& cache() {
 constexpr size_t kCacheMax = 16384;
 // Plans hold device tables; at large bond dimension every step brings new
 // block structures, so the cache is also bounded by the device bytes its
-// plans hold.  Clearing it frees only plans nobody else holds (a Davidson
-// call keeps its own references).
-constexpr int64_t kCachePlanBytesMax = (int64_t)4 << 30;
+// plans hold.  Over either bound the least recently used entries are dropped
+// until both are below 3/4 of it: clearing everything made every structure
+// of the next steps a cold miss (a second of host planning per block step at
+// bond dimension 3072).  Dropping an entry frees only plans nobody else holds
+// (a Davidson call keeps its own references).
+constexpr int64_t kCachePlanBytesMax = (int64_t)8 << 30;
+
+void evict_lru() {
+  ContractionCache& c = cache();
+  std::vector<std::pair<uint64_t, std::pair<uint64_t, size_t>>> all;  // (last use, (hash, index))
+  for (auto& kv : c.map)
+    for (size_t i = 0; i < kv.second.size(); ++i) all.push_back({kv.second[i].val->last_use, {kv.first, i}});
+  std::sort(all.begin(), all.end());
+  std::unordered_map<uint64_t, std::vector<size_t>> drop;
+  size_t entries = c.entries;
+  int64_t bytes = c.plan_bytes;
+  for (auto& e : all) {
+    if (entries <= kCacheMax * 3 / 4 && bytes <= kCachePlanBytesMax * 3 / 4) break;
+    const CacheEntry& ce = c.map[e.second.first][e.second.second];
+    bytes -= ce.val->plan_bytes;
+    entries--;
+    drop[e.second.first].push_back(e.second.second);
+  }
+  for (auto& kv : drop) {
+    auto& bucket = c.map[kv.first];
+    std::sort(kv.second.rbegin(), kv.second.rend());
+    for (size_t i : kv.second) bucket.erase(bucket.begin() + (long)i);
+    if (bucket.empty()) c.map.erase(kv.first);
+  }
+  c.entries = entries;
+  c.plan_bytes = bytes;
+}
 
 }  // namespace
 
@@ -670,7 +700,7 @@ std::shared_ptr<const CachedContraction> contract_cached(const qtensor& A, const
     }
   if (!val) {
     if (cache().entries >= kCacheMax || cache().plan_bytes >= kCachePlanBytesMax) {
-      clear_contraction_cache();
+      evict_lru();
       return contract_cached(A, B, need_plan);
     }
     val = std::make_shared<CachedContraction>();
@@ -678,6 +708,7 @@ std::shared_ptr<const CachedContraction> contract_cached(const qtensor& A, const
     cache().map[h].push_back(CacheEntry{std::move(key), val});
     cache().entries++;
   }
+  val->last_use = ++cache().clock;
   if (need_plan) val->plan_for(rt().precision);
   return val;
 }
@@ -688,7 +719,10 @@ tt_plan* CachedContraction::plan_for(int precision, int keep) const {
   if (!plans[precision]) {
     plans[precision] = make_plan(cs, precision, keep);
     int64_t b = 0;
-    if (tt_plan_device_bytes(plans[precision]->get(), &b) == TT_OK) cache().plan_bytes += b;
+    if (tt_plan_device_bytes(plans[precision]->get(), &b) == TT_OK) {
+      cache().plan_bytes += b;
+      plan_bytes += b;
+    }
   }
   return plans[precision]->get();
 }

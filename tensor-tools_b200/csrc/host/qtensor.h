@@ -249,6 +249,8 @@ struct CachedContraction {
   // keep: the operands (bit 0 A, bit 1 B) the caller keeps packed across
   // execs, a hint for the automatic precision (see tt_contract_plan_keep)
   tt_plan* plan_for(int precision, int keep = 0) const;
+  mutable uint64_t last_use = 0;    // cache clock of its last lookup
+  mutable int64_t plan_bytes = 0;   // device bytes its plans hold
 };
 // need_plan builds the plan of rt().precision right away.
 std::shared_ptr<const CachedContraction> contract_cached(const qtensor& A, const qtensor& B,

@@ -168,7 +168,10 @@ int tt_contract_exec(tt_ctx* ctx, const tt_plan* plan, const double* A,
  * operand that stays fixed over many execs, such as the environments of one
  * Davidson call.  The caller vouches that the data behind a kept pointer has
  * not changed, and releases the packings (tt_plan_release_packed, or the plan's
- * destruction) before it does.  FP64 plans ignore keep. */
+ * destruction) before it does.  Bit 2 (A) / bit 3 (B) keep only the packing
+ * buffer of an operand that is packed afresh in every exec, so that a run of
+ * execs allocates it once (released with the kept packings).  FP64 plans
+ * ignore keep. */
 int tt_contract_exec_keep(tt_ctx* ctx, const tt_plan* plan, const double* A, const double* B, double* C,
                           double alpha, int keep);
 int tt_plan_release_packed(tt_ctx* ctx, const tt_plan* plan);

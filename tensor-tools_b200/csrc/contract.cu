@@ -867,6 +867,9 @@ struct tt_plan {
   // and the operand each was packed from; released by tt_plan_release_packed
   mutable uint8_t* kept[2] = {nullptr, nullptr};
   mutable const double* kept_src[2] = {nullptr, nullptr};
+  // packing buffers reused across execs for operands packed afresh each time
+  // (keep bits 2 and 3), so that a run of execs allocates them once
+  mutable uint8_t* scratch[2] = {nullptr, nullptr};
   TaskDev* d_tasks = nullptr;
   OutDev* d_outs = nullptr;
   PairDev* d_pairs = nullptr;
@@ -1236,6 +1239,8 @@ int tt_plan_release_packed(tt_ctx* ctx, const tt_plan* plan) {
     tt::pool_free(ctx, plan->kept[w]);
     plan->kept[w] = nullptr;
     plan->kept_src[w] = nullptr;
+    tt::pool_free(ctx, plan->scratch[w]);
+    plan->scratch[w] = nullptr;
   }
   return TT_OK;
 }
@@ -1296,6 +1301,7 @@ int tt_contract_exec_keep(tt_ctx* ctx, const tt_plan* plan, const double* A, con
   const int64_t bytes[2] = {plan->bytesA, plan->bytesB};
   uint8_t* pk[2] = {nullptr, nullptr};
   bool fresh[2] = {false, false};
+  bool from_scratch[2] = {false, false};
   for (int w = 0; w < 2; ++w) {
     const bool k = (keep >> w) & 1;
     if (k && plan->kept[w] && plan->kept_src[w] == src[w]) {
@@ -1307,14 +1313,20 @@ int tt_contract_exec_keep(tt_ctx* ctx, const tt_plan* plan, const double* A, con
       plan->kept[w] = nullptr;
       plan->kept_src[w] = nullptr;
     }
-    pk[w] = tt::pool_alloc<uint8_t>(ctx, (size_t)std::max<int64_t>(bytes[w], 16));
     fresh[w] = true;
+    if (!k && ((keep >> (2 + w)) & 1)) {  // repacked every exec into a buffer the plan keeps
+      if (!plan->scratch[w]) plan->scratch[w] = tt::pool_alloc<uint8_t>(ctx, (size_t)std::max<int64_t>(bytes[w], 16));
+      pk[w] = plan->scratch[w];
+      from_scratch[w] = true;
+      continue;
+    }
+    pk[w] = tt::pool_alloc<uint8_t>(ctx, (size_t)std::max<int64_t>(bytes[w], 16));
   }
   uint8_t* pa = pk[0];
   uint8_t* pb = pk[1];
   if (!pa || !pb) {
-    if (fresh[0]) tt::pool_free(ctx, pa);
-    if (fresh[1]) tt::pool_free(ctx, pb);
+    if (fresh[0] && !from_scratch[0]) tt::pool_free(ctx, pa);
+    if (fresh[1] && !from_scratch[1]) tt::pool_free(ctx, pb);
     return tt::fail(TT_ERR_OOM, "tt_contract_exec: packed operand allocation failed");
   }
   {
@@ -1342,7 +1354,7 @@ int tt_contract_exec_keep(tt_ctx* ctx, const tt_plan* plan, const double* A, con
         ctx->d_dev_status, ctx->wait_limit);
   cudaError_t le = cudaGetLastError();
   for (int w = 0; w < 2; ++w) {
-    if (!fresh[w]) continue;
+    if (!fresh[w] || from_scratch[w]) continue;
     if ((keep >> w) & 1) {
       plan->kept[w] = pk[w];
       plan->kept_src[w] = src[w];

@@ -219,7 +219,7 @@ class ProductEngine {
   void apply(const double* v, double* y, int precision = TT_PREC_FP64, void* const* ev = nullptr) {
     if (ev) check(tt_event_record(ctx(), ev[0]), "event");
     if (tt_plan* p = c1_->plan_for(part_precision(precision, 0, part_flops[0]), 1)) {  // L kept through the call
-      check(tt_contract_exec_keep(ctx(), p, L_data(), v, i1_->get(), 1.0, 1), "heff L*v");
+      check(tt_contract_exec_keep(ctx(), p, L_data(), v, i1_->get(), 1.0, 1 | 8), "heff L*v");
       kept_.push_back(p);
     }
     if (ev) check(tt_event_record(ctx(), ev[1]), "event");
@@ -227,7 +227,7 @@ class ProductEngine {
       check(tt_contract_exec(ctx(), p, i1_->get(), A_.mid().data->get(), i2_->get(), 1.0), "heff *mid");
     if (ev) check(tt_event_record(ctx(), ev[2]), "event");
     if (tt_plan* p = c3_->plan_for(part_precision(precision, 2, part_flops[2]), 2)) {  // and so is R
-      check(tt_contract_exec_keep(ctx(), p, i2_->get(), A_.right()->data->get(), y, 1.0, 2), "heff *R");
+      check(tt_contract_exec_keep(ctx(), p, i2_->get(), A_.right()->data->get(), y, 1.0, 2 | 4), "heff *R");
       kept_.push_back(p);
     }
     if (ev) check(tt_event_record(ctx(), ev[3]), "event");

@@ -119,6 +119,20 @@ namespace {
 
 using Presence = std::vector<uint8_t>;
 
+// The intermediates T1 = L x and T2 = T1 (W1 W2) of the H_eff*x products: a
+// gigabyte each at bond dimension 3072.  The bound context keeps one buffer
+// per intermediate between Davidson calls and only grows it (12.5% headroom),
+// so consecutive calls do not hand gigabytes back to the pool and map them
+// again.
+static DevPtr heff_scratch(int which, int64_t n) {
+  DevPtr& buf = rt().heff_scratch[which];
+  if (!buf || buf->size() < n) {
+    buf.reset();  // back to the pool before the larger one is taken
+    buf = dev_alloc(n + n / 8);
+  }
+  return buf;
+}
+
 class ProductEngine {
  public:
   ~ProductEngine() {
@@ -345,8 +359,8 @@ class ProductEngine {
       for (const tt_out_block& o : c2_->cs.outs) el += (int64_t)o.m * o.n;
       mid_bytes = 8.0 * (double)el;
     }
-    i1_ = dev_alloc(std::max<int64_t>(c1_->cs.C.arena, 2));
-    i2_ = dev_alloc(std::max<int64_t>(c2_->cs.C.arena, 2));
+    i1_ = heff_scratch(0, std::max<int64_t>(c1_->cs.C.arena, 2));
+    i2_ = heff_scratch(1, std::max<int64_t>(c2_->cs.C.arena, 2));
   }
 };
 

@@ -32,6 +32,8 @@ void bind_context(tt_ctx* c) {
   clear_contraction_cache();  // cached plans belong to the previous context
   rt().dense_plans.clear();
   rt().scalars.reset();
+  rt().heff_scratch[0].reset();
+  rt().heff_scratch[1].reset();
   drop_dav_state();
   rt().ctx = c;
   if (c) rt().scalars = std::make_shared<DevBuf>(kScalarSlots);
@@ -40,6 +42,8 @@ void unbind_context() {
   clear_contraction_cache();
   rt().dense_plans.clear();
   rt().scalars.reset();
+  rt().heff_scratch[0].reset();
+  rt().heff_scratch[1].reset();
   drop_dav_state();
   rt().ctx = nullptr;
 }

@@ -31,6 +31,9 @@ struct Runtime {
   tt_ctx* ctx = nullptr;
   uint64_t rng_counter = 0x5eed;
   std::shared_ptr<DevBuf> scalars;  // 16 device doubles for reductions
+  // intermediates of the H_eff*x products (L x and L x W1 W2), kept between
+  // Davidson calls and only grown
+  std::shared_ptr<DevBuf> heff_scratch[2];
   double last_heff_ms = 0.0;        // device time of the last Davidson's H_eff*x launches
   double heff_part_ms[3] = {0.0, 0.0, 0.0};     // device-resident Davidson: L*x, *mid, *R times
   double heff_part_flops[3] = {0.0, 0.0, 0.0};  // and their algorithmic flops

@@ -514,6 +514,7 @@ def c5_arm(prec, ck, H, args, ctx, stream, flush, torch, tt_b200, sampler=None, 
             w0 = ctx.wait_stats()[0]
             ru0 = resource.getrusage(resource.RUSAGE_SELF)
             tr0 = ctx.pool_trims()
+            al0 = ctx.alloc_stats(reset_max=True)
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             h0 = time.perf_counter()
             e0.record(stream)
@@ -525,6 +526,12 @@ def c5_arm(prec, ck, H, args, ctx, stream, flush, torch, tt_b200, sampler=None, 
             step_os.append({"user_s": ru1.ru_utime - ru0.ru_utime, "sys_s": ru1.ru_stime - ru0.ru_stime,
                             "minflt": ru1.ru_minflt - ru0.ru_minflt, "majflt": ru1.ru_majflt - ru0.ru_majflt,
                             "nivcsw": ru1.ru_nivcsw - ru0.ru_nivcsw, "pool_trims": ctx.pool_trims() - tr0})
+            al1 = ctx.alloc_stats()
+            step_os[-1].update({"alloc_s": al1["alloc_s"] - al0["alloc_s"], "alloc_max_s": al1["alloc_max_s"],
+                                "free_s": al1["free_s"] - al0["free_s"], "free_max_s": al1["free_max_s"],
+                                "allocs": al1["allocs"] - al0["allocs"],
+                                "cache_hits": al1["cache_hits"] - al0["cache_hits"],
+                                "cached_gb": al1["cached_bytes"] / 2 ** 30})
             e1.synchronize()
             times.append(e0.elapsed_time(e1) * 1e-3)
             step_plans.append(tt_b200.planning_counters()["plans"] - pa)
@@ -538,6 +545,7 @@ def c5_arm(prec, ck, H, args, ctx, stream, flush, torch, tt_b200, sampler=None, 
         er1 = tt_b200.eig_redo_count(ctx)
         steps = run.steps()[s0:]
         prof_t = run.profile()[s0:s0 + args.steps * 2 * B]  # host wall time per update, no added syncs
+        prof_d = run.device_profile(s0)[:args.steps * 2 * B]  # device-stream spans per update (events)
         t_step = statistics.mean(times)
         upd = 2 * B
         fl = st1["heff_flops"] - st0["heff_flops"]
@@ -564,6 +572,13 @@ def c5_arm(prec, ck, H, args, ctx, stream, flush, torch, tt_b200, sampler=None, 
                  "engine": sum(p[4] for p in prof_t[k * 2 * B:(k + 1) * 2 * B]),
                  "svd": sum(p[2] for p in prof_t[k * 2 * B:(k + 1) * 2 * B]),
                  "env": sum(p[3] for p in prof_t[k * 2 * B:(k + 1) * 2 * B])} for k in range(args.steps)],
+            # per timed step, device-stream milliseconds of the same phases, and of the
+            # gaps between consecutive updates of the step (device waiting for the host)
+            "step_device_phases_ms": [
+                {"davidson": sum(p[0] for p in prof_d[k * 2 * B:(k + 1) * 2 * B]),
+                 "svd": sum(p[1] for p in prof_d[k * 2 * B:(k + 1) * 2 * B]),
+                 "env": sum(p[2] for p in prof_d[k * 2 * B:(k + 1) * 2 * B]),
+                 "gaps": sum(p[3] for p in prof_d[k * 2 * B + 1:(k + 1) * 2 * B])} for k in range(args.steps)],
             "matvecs_per_update": statistics.mean(s["matvecs"] for s in steps) if steps else None,
             "trunc_err_mean": statistics.mean(s["trunc_err"] for s in steps) if steps else None,
             "kept": [s["kept"] for s in steps[-upd:]],

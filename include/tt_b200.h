@@ -83,6 +83,21 @@ int tt_ctx_wait_stats(tt_ctx* ctx, double* seconds, int64_t* count);
 /* Pool allocations that failed once, trimmed the pool to its use and
  * succeeded or failed on the retry (each trim synchronises the stream). */
 int tt_ctx_pool_trims(tt_ctx* ctx, int64_t* count);
+/* Host wall seconds inside the context's device allocate and free calls:
+ * totals, the largest single call since the last reset, the number of
+ * allocations, how many were served from the block cache, and the bytes the
+ * cache holds now.  reset_max != 0 zeroes the two maxima after reading. */
+int tt_ctx_alloc_stats(tt_ctx* ctx, double* alloc_s, double* alloc_max_s, double* free_s, double* free_max_s,
+                       int64_t* allocs, int64_t* cache_hits, int64_t* cached_bytes, int reset_max);
+/* Block cache: allocations of 32 MB or more are rounded up to a size class
+ * (at most 25% above the request) and, when freed, kept by the context (up
+ * to `bytes` in total, the blocks freed longest ago evicted first; default
+ * 32 GiB) for the next allocation on its stream that fits in one (a block at
+ * most 1.5x the request's class), instead of going back to the device pool,
+ * which can stall the host for seconds assembling a multi-gigabyte block.  Cached
+ * blocks count as used in tt_ctx_memory; an allocation that fails returns
+ * them to the pool and retries.  0 turns the cache off and releases it. */
+int tt_ctx_set_block_cache(tt_ctx* ctx, int64_t bytes);
 /* Sticky device status of the context: TT_OK, or TT_ERR_TIMEOUT once a bounded
  * wait inside a tensor-core contraction has given up (that contraction's output
  * is incomplete).  Every synchronisation of the context -- tt_ctx_synchronize

@@ -221,6 +221,13 @@ int tt_qdmrg_step_sectors(const tt_qdmrg* run, int i, int* n, int32_t* qn, uint3
  * seconds of the Davidson, SVD and environment-update phases */
 int tt_qdmrg_step_profile(const tt_qdmrg* run, int i, int* gram_max, double* t_davidson, double* t_svd,
                           double* t_env, double* t_engine);
+/* per-step device-stream spans in milliseconds, from events recorded on the
+ * library stream at the phase boundaries: Davidson, SVD, environment update,
+ * and the span from the previous logged step's end to this step's start
+ * (gap; negative for the first step).  A span includes any time in which the
+ * device waited for the host.  Waits for the step's last event. */
+int tt_qdmrg_step_device_ms(const tt_qdmrg* run, int i, double* davidson, double* svd, double* env,
+                            double* gap);
 int tt_qdmrg_stats(const tt_qdmrg* run, double* heff_flops, double* heff_seconds, double* initial_energy);
 /* copy of the left (which = 0, TL[i]) or right (which = 1, TR[i]) environment.
  * Only the environments on the live side of the orthogonality centre c are

@@ -620,6 +620,29 @@ int tt_qdmrg_step_profile(const tt_qdmrg* run, int i, int* gram_max, double* t_d
   });
 }
 
+int tt_qdmrg_step_device_ms(const tt_qdmrg* run, int i, double* davidson, double* svd, double* env,
+                            double* gap) {
+  TT_ARG(run && i >= 0 && i < (int)run->log.steps.size());
+  TT_GUARD({
+    auto span = [](void* a, void* b) -> double {
+      if (!a || !b) return -1.0;
+      float ms = 0.0f;
+      ttb::check(tt_event_elapsed_ms(a, b, &ms), "step event");
+      return (double)ms;
+    };
+    const auto& ev = run->log.steps[i].events;
+    void* e[4] = {nullptr, nullptr, nullptr, nullptr};
+    if (ev)
+      for (int k = 0; k < 4; ++k) e[k] = ev->ev[k];
+    void* prev_end = nullptr;
+    if (i > 0 && run->log.steps[i - 1].events) prev_end = run->log.steps[i - 1].events->ev[3];
+    if (davidson) *davidson = span(e[0], e[1]);
+    if (svd) *svd = span(e[1], e[2]);
+    if (env) *env = span(e[2], e[3]);
+    if (gap) *gap = span(prev_end, e[0]);
+  });
+}
+
 int tt_qdmrg_stats(const tt_qdmrg* run, double* heff_flops, double* heff_seconds, double* initial_energy) {
   TT_ARG(run);
   TT_GUARD({

@@ -46,16 +46,111 @@ int device_status(tt_ctx* ctx) {
   return TT_OK;
 }
 
-cudaError_t pool_malloc(tt_ctx* ctx, void** p, size_t bytes) {
+static cudaError_t pool_malloc_impl(tt_ctx* ctx, void** p, size_t bytes) {
   cudaError_t e = cudaMallocAsync(p, bytes, ctx->stream);
   if (e == cudaErrorMemoryAllocation) {
     cudaGetLastError();
     ctx->pool_trims++;
-    if (cudaStreamSynchronize(ctx->stream) == cudaSuccess && cudaMemPoolTrimTo(ctx->pool, 0) == cudaSuccess)
+    // the cached large blocks go back first, then the pool returns what it
+    // holds unused to the device
+    if (release_block_cache(ctx) == cudaSuccess && cudaStreamSynchronize(ctx->stream) == cudaSuccess &&
+        cudaMemPoolTrimTo(ctx->pool, 0) == cudaSuccess)
       e = cudaMallocAsync(p, bytes, ctx->stream);
     if (e != cudaSuccess) cudaGetLastError();
   }
   return e;
+}
+
+// Size class of a large block: 2^k + j * 2^(k-2) for the smallest such value
+// >= bytes (j = 1..4), so a class is at most 25% above the request.  With
+// bytes >= 32 MB every class is a multiple of 8 MB.
+static size_t large_class(size_t bytes) {
+  int k = 63 - __builtin_clzll((unsigned long long)bytes);
+  const size_t base = (size_t)1 << k, step = base >> 2;
+  if (bytes == base) return base;
+  return base + (bytes - base + step - 1) / step * step;
+}
+
+cudaError_t pool_malloc(tt_ctx* ctx, void** p, size_t bytes) {
+  auto t0 = std::chrono::steady_clock::now();
+  cudaError_t e = cudaSuccess;
+  if (bytes >= kLargeBlockBytes && ctx->block_cache_cap > 0) {
+    const size_t cls = large_class(bytes);
+    // the smallest cached block of this class or up to 1.5x it
+    size_t best = SIZE_MAX, at = 0;
+    for (size_t i = 0; i < ctx->large_free.size(); ++i) {
+      const size_t b = ctx->large_free[i].bytes;
+      if (b >= cls && b <= cls + cls / 2 && b < best) { best = b; at = i; }
+    }
+    if (best != SIZE_MAX) {
+      *p = ctx->large_free[at].p;  // freed earlier on this stream: stream order makes it free now
+      ctx->large_free[at] = ctx->large_free.back();
+      ctx->large_free.pop_back();
+      ctx->large_cached -= best;
+      ctx->large_hits++;
+    } else {
+      e = pool_malloc_impl(ctx, p, cls);
+      if (e == cudaSuccess) ctx->large_class_of[*p] = cls;
+    }
+  } else {
+    e = pool_malloc_impl(ctx, p, bytes);
+  }
+  const double dt = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  ctx->alloc_seconds += dt;
+  if (dt > ctx->alloc_max_seconds) ctx->alloc_max_seconds = dt;
+  ctx->allocs++;
+  return e;
+}
+
+cudaError_t pool_free(tt_ctx* ctx, void* p) {
+  if (!p) return cudaSuccess;
+  auto t0 = std::chrono::steady_clock::now();
+  cudaError_t e = cudaSuccess;
+  auto it = ctx->large_class_of.find(p);
+  bool cached = false;
+  if (it != ctx->large_class_of.end()) {
+    const size_t cls = it->second;
+    if (cls <= ctx->block_cache_cap) {
+      // room for it: the blocks freed longest ago go back to the pool
+      while (ctx->large_cached + cls > ctx->block_cache_cap && !ctx->large_free.empty()) {
+        size_t old = 0;
+        for (size_t i = 1; i < ctx->large_free.size(); ++i)
+          if (ctx->large_free[i].stamp < ctx->large_free[old].stamp) old = i;
+        const tt_ctx::CachedBlock victim = ctx->large_free[old];
+        ctx->large_free[old] = ctx->large_free.back();
+        ctx->large_free.pop_back();
+        ctx->large_cached -= victim.bytes;
+        ctx->large_class_of.erase(victim.p);
+        cudaError_t ev = cudaFreeAsync(victim.p, ctx->stream);
+        if (ev != cudaSuccess && e == cudaSuccess) e = ev;
+      }
+      ctx->large_free.push_back({p, cls, ++ctx->large_clock});
+      ctx->large_cached += cls;
+      cached = true;
+    } else {
+      ctx->large_class_of.erase(it);
+    }
+  }
+  if (!cached) {
+    cudaError_t ef = cudaFreeAsync(p, ctx->stream);
+    if (e == cudaSuccess) e = ef;
+  }
+  const double dt = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  ctx->free_seconds += dt;
+  if (dt > ctx->free_max_seconds) ctx->free_max_seconds = dt;
+  return e;
+}
+
+cudaError_t release_block_cache(tt_ctx* ctx) {
+  cudaError_t first = cudaSuccess;
+  for (const auto& b : ctx->large_free) {
+    ctx->large_class_of.erase(b.p);
+    cudaError_t e = cudaFreeAsync(b.p, ctx->stream);
+    if (e != cudaSuccess && first == cudaSuccess) first = e;
+  }
+  ctx->large_free.clear();
+  ctx->large_cached = 0;
+  return first;
 }
 
 cudaError_t h2d_async(tt_ctx* ctx, void* dst, const void* src, size_t bytes) {
@@ -64,7 +159,10 @@ cudaError_t h2d_async(tt_ctx* ctx, void* dst, const void* src, size_t bytes) {
   if (!ctx->stage || need > ctx->stage_cap)
     return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, ctx->stream);
   if (ctx->stage_head + need > ctx->stage_cap) {
+    auto t0 = std::chrono::steady_clock::now();
     cudaError_t e = cudaStreamSynchronize(ctx->stream);  // every staged copy has landed
+    ctx->wait_seconds += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    ctx->waits++;
     if (e != cudaSuccess) return e;
     ctx->stage_head = 0;
   }
@@ -132,6 +230,7 @@ int tt_ctx_create(int device, tt_ctx** out) {
 int tt_ctx_destroy(tt_ctx* ctx) {
   if (!ctx) return TT_OK;
   cudaSetDevice(ctx->device);
+  tt::release_block_cache(ctx);
   cudaStreamSynchronize(ctx->stream);
   if (ctx->d_partials) cudaFree(ctx->d_partials);
   if (ctx->d_ticket) cudaFree(ctx->d_ticket);
@@ -248,7 +347,29 @@ int tt_device_alloc(tt_ctx* ctx, size_t bytes, void** dptr) {
 
 int tt_device_free(tt_ctx* ctx, void* dptr) {
   TT_REQUIRE(ctx, "null context");
-  if (dptr) TT_CUDA(cudaFreeAsync(dptr, ctx->stream));
+  TT_CUDA(tt::pool_free(ctx, dptr));
+  return TT_OK;
+}
+
+int tt_ctx_alloc_stats(tt_ctx* ctx, double* alloc_s, double* alloc_max_s, double* free_s, double* free_max_s,
+                       int64_t* allocs, int64_t* cache_hits, int64_t* cached_bytes, int reset_max) {
+  TT_REQUIRE(ctx, "tt_ctx_alloc_stats: null context");
+  if (alloc_s) *alloc_s = ctx->alloc_seconds;
+  if (alloc_max_s) *alloc_max_s = ctx->alloc_max_seconds;
+  if (free_s) *free_s = ctx->free_seconds;
+  if (free_max_s) *free_max_s = ctx->free_max_seconds;
+  if (allocs) *allocs = ctx->allocs;
+  if (cache_hits) *cache_hits = ctx->large_hits;
+  if (cached_bytes) *cached_bytes = (int64_t)ctx->large_cached;
+  if (reset_max) ctx->alloc_max_seconds = ctx->free_max_seconds = 0.0;
+  return TT_OK;
+}
+
+int tt_ctx_set_block_cache(tt_ctx* ctx, int64_t bytes) {
+  TT_REQUIRE(ctx, "tt_ctx_set_block_cache: null context");
+  TT_REQUIRE(bytes >= 0, "tt_ctx_set_block_cache: negative size");
+  ctx->block_cache_cap = (size_t)bytes;
+  if (ctx->large_cached > ctx->block_cache_cap) TT_CUDA(tt::release_block_cache(ctx));
   return TT_OK;
 }
 

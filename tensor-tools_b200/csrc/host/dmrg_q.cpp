@@ -1043,6 +1043,15 @@ void buildEnv(qMPS& psi, qMPO& H, std::vector<qtensor>& TR, std::vector<qtensor>
   for (unsigned i = L - 1; i > 0; --i) TR[i - 1] = env_step(TR[i], psi.A[i], H.A[i]);
 }
 
+StepEvents::~StepEvents() {
+  for (void* e : ev)
+    if (e) tt_event_destroy(e);
+}
+void StepEvents::record(int i) {
+  if (!ev[i]) check(tt_event_create(ctx(), &ev[i]), "step event");
+  check(tt_event_record(ctx(), ev[i]), "step event");
+}
+
 void updateSite(qMPS& psi, qMPO& H, std::vector<qtensor>& TR, std::vector<qtensor>& TL, unsigned site,
                 double& energy, int direction, int max_bd, double cutoff, char mode, int search_space_size,
                 int max_restart, DmrgLog* log, double noise) {
@@ -1050,6 +1059,11 @@ void updateSite(qMPS& psi, qMPO& H, std::vector<qtensor>& TR, std::vector<qtenso
   unsigned l, r;
   if (direction == MoveFromLeft) { l = site; r = site + 1; } else { l = site - 1; r = site; }
   auto t0 = std::chrono::steady_clock::now();
+  std::shared_ptr<StepEvents> events;
+  if (log) {
+    events = std::make_shared<StepEvents>();
+    events->record(0);
+  }
   big_qtensor A;
   A.setLeft(&TL[l]);
   A.addMid(&H.A[l]);
@@ -1060,6 +1074,7 @@ void updateSite(qMPS& psi, qMPO& H, std::vector<qtensor>& TR, std::vector<qtenso
   energy = tensor_davidsonIT(A, x, search_space_size, max_restart, 1e-12, mode, &st);
   if (rt().profile) check(tt_ctx_synchronize(ctx()), "sync");
   auto t1 = std::chrono::steady_clock::now();
+  if (events) events->record(1);
   std::string ln = psi.link_name(r);
   qtensor_index mid;
   for (auto& ix : psi.A[l].idx_set)
@@ -1079,6 +1094,7 @@ void updateSite(qMPS& psi, qMPO& H, std::vector<qtensor>& TR, std::vector<qtenso
   }
   if (rt().profile) check(tt_ctx_synchronize(ctx()), "sync");  // the SVD's asynchronous tail counts as SVD
   auto t2 = std::chrono::steady_clock::now();
+  if (events) events->record(2);
   psi.bond_dims[r] = (unsigned)S.total_size();
   psi.center = (int)(direction == MoveFromLeft ? r : l);
   if (log) {
@@ -1097,6 +1113,7 @@ void updateSite(qMPS& psi, qMPO& H, std::vector<qtensor>& TR, std::vector<qtenso
     s.t_davidson = std::chrono::duration<double>(t1 - t0).count();
     s.t_engine = st.t_engine;
     s.t_svd = std::chrono::duration<double>(t2 - t1).count();
+    s.events = std::move(events);
     log->steps.push_back(std::move(s));
     log->heff_flops += st.heff_flops;
     log->heff_seconds += rt().last_heff_ms * 1e-3;
@@ -1157,6 +1174,7 @@ double dmrg_walk(qMPS& psi, qMPO& H, DmrgState& st, int to, int max_bd, double c
     updateEnv(psi, H, st.TR, st.TL, site, direction);
     release_stale(st, site, direction, (unsigned)L);
     if (log && !log->steps.empty()) {
+      if (log->steps.back().events) log->steps.back().events->record(3);
       if (rt().profile) check(tt_ctx_synchronize(ctx()), "sync");
       log->steps.back().t_env = std::chrono::duration<double>(std::chrono::steady_clock::now() - te0).count();
     }
@@ -1189,6 +1207,7 @@ double dmrg_sweep(qMPS& psi, qMPO& H, DmrgState& st, int max_bd, double cutoff, 
         cudaProfilerStop();
       }
       if (log && !log->steps.empty()) {
+        if (log->steps.back().events) log->steps.back().events->record(3);
         if (rt().profile) check(tt_ctx_synchronize(ctx()), "sync");
         log->steps.back().t_env =
             std::chrono::duration<double>(std::chrono::steady_clock::now() - te0).count();

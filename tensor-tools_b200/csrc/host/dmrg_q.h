@@ -85,6 +85,18 @@ qMPO make_heisenberg_qmpo(unsigned L, const double* dh = nullptr, double tE = 0.
 double spin_half_op(unsigned bra, const std::string& op, unsigned ket);
 
 // ---- DMRG ---------------------------------------------------------------
+// Stream events at the phase boundaries of a logged two-site step: Davidson
+// start, SVD start, environment start, environment end.  Their differences
+// are the device-stream spans of the phases (gaps in which the device waited
+// for the host included).
+struct StepEvents {
+  void* ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  StepEvents() = default;
+  StepEvents(const StepEvents&) = delete;
+  StepEvents& operator=(const StepEvents&) = delete;
+  ~StepEvents();
+  void record(int i);  // creates the event on first use
+};
 struct StepLog {
   int site = 0;
   int direction = 0;
@@ -101,6 +113,7 @@ struct StepLog {
   double t_svd = 0.0;
   double t_env = 0.0;
   double t_engine = 0.0;     // part of t_davidson: Krylov layout and product plans
+  std::shared_ptr<StepEvents> events;
 };
 struct DmrgLog {
   std::vector<StepLog> steps;

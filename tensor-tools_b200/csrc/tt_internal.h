@@ -1,9 +1,11 @@
 // Internal runtime shared by the sm_100a kernels and the C ABI entry points.
 #pragma once
 
+#include <chrono>
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <unordered_map>
 #include <cstdio>
 #include <string>
 #include <vector>
@@ -32,6 +34,28 @@ struct tt_ctx {
   double wait_seconds = 0.0;
   int64_t pool_trims = 0;  // allocations that failed once, trimmed the pool and retried
   int64_t waits = 0;
+  // host wall time inside the pool's allocate and free calls (total, largest
+  // single call since the last tt_ctx_alloc_stats reset) and their counts
+  double alloc_seconds = 0.0, alloc_max_seconds = 0.0;
+  double free_seconds = 0.0, free_max_seconds = 0.0;
+  int64_t allocs = 0;
+  // Blocks of at least kLargeBlockBytes are allocated in size classes (a
+  // quarter of a power of two apart) and kept by the context when freed, up
+  // to block_cache_cap bytes (the oldest evicted first), for the next
+  // allocation on this stream that fits in one (at most 1.5x its class).  The device pool can stall the host for seconds when a
+  // multi-gigabyte request has to be assembled from freed memory; a steady
+  // sweep asks for the same classes step after step and is served from here.
+  struct CachedBlock {
+    void* p;
+    size_t bytes;    // its class
+    uint64_t stamp;  // when it was freed (the oldest is evicted first)
+  };
+  std::unordered_map<void*, size_t> large_class_of;   // every live or cached large block
+  std::vector<CachedBlock> large_free;                // cached blocks (tens at most)
+  uint64_t large_clock = 0;
+  size_t large_cached = 0;
+  size_t block_cache_cap = (size_t)32 << 30;
+  int64_t large_hits = 0;
   // sticky status of the bounded device waits (mapped pinned memory, so a
   // kernel that gives up writes TT_ERR_TIMEOUT straight into host memory);
   // every synchronisation of the context checks it
@@ -66,9 +90,10 @@ inline T* pool_alloc(tt_ctx* ctx, size_t n) {
   if (pool_malloc(ctx, &p, n * sizeof(T)) != cudaSuccess) return nullptr;
   return static_cast<T*>(p);
 }
-inline void pool_free(tt_ctx* ctx, void* p) {
-  if (p) cudaFreeAsync(p, ctx->stream);
-}
+cudaError_t pool_free(tt_ctx* ctx, void* p);
+// Returns every cached large block to the device pool.
+cudaError_t release_block_cache(tt_ctx* ctx);
+constexpr size_t kLargeBlockBytes = (size_t)32 << 20;
 
 // Per-thread, per-device "done once" flags for cudaFuncSetAttribute, which
 // acts on the current device only: bit d of a thread_local mask.  Returns

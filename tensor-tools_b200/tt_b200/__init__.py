@@ -78,6 +78,8 @@ _proto("tt_ctx_synchronize", P)
 _proto("tt_ctx_stream", P, PP)
 _proto("tt_ctx_wait_stats", P, PD, PI64)
 _proto("tt_ctx_pool_trims", P, PI64)
+_proto("tt_ctx_alloc_stats", P, PD, PD, PD, PD, PI64, PI64, PI64, C.c_int)
+_proto("tt_ctx_set_block_cache", P, C.c_int64)
 _proto("tt_ctx_launch_count", P, PI64)
 lib.tt_get_last_error.restype = C.c_char_p
 lib.tt_get_last_error.argtypes = []
@@ -189,6 +191,7 @@ _proto("tt_qdmrg_step", P, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), PD, 
 _proto("tt_qdmrg_step_sectors", P, C.c_int, C.POINTER(C.c_int), PI32, C.POINTER(C.c_uint32), C.c_int)
 _proto("tt_qdmrg_stats", P, PD, PD, PD)
 _proto("tt_qdmrg_step_profile", P, C.c_int, C.POINTER(C.c_int), PD, PD, PD, PD)
+_proto("tt_qdmrg_step_device_ms", P, C.c_int, PD, PD, PD, PD)
 _proto("tt_dmrg_set_profiling", C.c_int)
 _proto("tt_dmrg_planning_counters", PD, PI64, PD, PI64)
 _proto("tt_eig_redo_count", P, PI64)
@@ -241,6 +244,19 @@ class Context:
         n = I64()
         _chk(lib.tt_ctx_pool_trims(self.h, C.byref(n)), "pool trims")
         return n.value
+
+    def alloc_stats(self, reset_max: bool = False) -> dict:
+        """Host seconds inside device-pool allocate / free calls: totals, the
+        largest single call since the last reset, and the allocation count."""
+        a, am, f, fm, n, hits, cached = D(), D(), D(), D(), I64(), I64(), I64()
+        _chk(lib.tt_ctx_alloc_stats(self.h, C.byref(a), C.byref(am), C.byref(f), C.byref(fm), C.byref(n),
+                                    C.byref(hits), C.byref(cached), int(reset_max)), "alloc stats")
+        return {"alloc_s": a.value, "alloc_max_s": am.value, "free_s": f.value, "free_max_s": fm.value,
+                "allocs": n.value, "cache_hits": hits.value, "cached_bytes": cached.value}
+
+    def set_block_cache(self, nbytes: int):
+        """Bytes of freed large blocks the context keeps for reuse (0: off)."""
+        _chk(lib.tt_ctx_set_block_cache(self.h, int(nbytes)), "block cache")
 
     def launches(self) -> int:
         n = I64()
@@ -662,6 +678,19 @@ class QDMRG:
             _chk(lib.tt_qdmrg_step_profile(self.h, i, C.byref(g), C.byref(a), C.byref(b), C.byref(c), C.byref(e)),
                  "profile")
             out.append((g.value, a.value, b.value, c.value, e.value))
+        return out
+
+    def device_profile(self, first: int = 0):
+        """Per step from `first` on: device-stream milliseconds of (Davidson,
+        SVD, env update, gap since the previous step's end), event-timed."""
+        n = C.c_int()
+        _chk(lib.tt_qdmrg_num_steps(self.h, C.byref(n)), "num_steps")
+        out = []
+        for i in range(first, n.value):
+            a, b, c, g = D(), D(), D(), D()
+            _chk(lib.tt_qdmrg_step_device_ms(self.h, i, C.byref(a), C.byref(b), C.byref(c), C.byref(g)),
+                 "device profile")
+            out.append((a.value, b.value, c.value, g.value))
         return out
 
     def env(self, which: int, i: int) -> QTensor:

@@ -18,6 +18,9 @@
  *   tt_qtensor_svd           svd(A,left,right,U,V,S,dir,cutoff,K)
  *                                                            qtensor/qtensor_op.cpp:1097-1453
  *   tt_qtensor_svd_bond      svd_bond(combined,...)          qtensor/qtensor_op.cpp:1506-1544
+ *   tt_qtensor_svd_bond_sectors  the same, with the kept count of every mid-QN sector
+ *   tt_qtensor_env_update    TL[i+1] / TR[i-1] = ((A^dag' env) W) A
+ *                                                            algos/dmrg/dmrg.cpp:56-85,491-509
  *   tt_bigq_*                big_qtensor<T> setLeft/addMid/setRight/product/size
  *                                                            qtensor/big_qtensor.{h,cpp}
  *   tt_bigq_davidson         tensor_davidsonIT               linalg/tensor_davidson.cpp:193-347
@@ -152,6 +155,22 @@ int tt_qtensor_svd(const tt_qtensor* A, int nleft, const int* left_axes, int dir
 int tt_qtensor_svd_bond(const tt_qtensor* combined, tt_qtensor* A_left, tt_qtensor* A_right, int mid_axis,
                         int direction, double cutoff, unsigned long K, tt_qtensor** S, double* trunc_err,
                         unsigned* kept);
+/* svd_bond as above, also reporting the mid-QN sectors of the SVD in
+ * ascending QN order: *n_sectors of them (sectors that keep no state
+ * included), their QNs as pairs qn[2j], qn[2j+1] and their kept counts (the
+ * first `cap` are written).  The truncation log of svd
+ * (qtensor/qtensor_op.cpp:1290-1330) reports the same per-sector counts. */
+int tt_qtensor_svd_bond_sectors(const tt_qtensor* combined, tt_qtensor* A_left, tt_qtensor* A_right,
+                                int mid_axis, int direction, double cutoff, unsigned long K, tt_qtensor** S,
+                                double* trunc_err, unsigned* kept, int* n_sectors, int32_t* qn,
+                                uint32_t* kept_per_sector, int cap);
+/* One environment update, the step of buildEnv and updateEnv
+ * (algos/dmrg/dmrg.cpp:56-85 q buildEnv, :491-509 q updateEnv): out =
+ * ((A^dag' * env) * W) * A, contracted by index tags, so the same call
+ * extends a left environment TL[i] -> TL[i+1] with site i or a right one
+ * TR[i] -> TR[i-1].  Contractions run at the precision set by
+ * tt_dmrg_set_precision for environments.  *out is a new handle. */
+int tt_qtensor_env_update(const tt_qtensor* env, const tt_qtensor* A, const tt_qtensor* W, tt_qtensor** out);
 
 /* ---- big_qtensor and Davidson --------------------------------------------- */
 /* W2 may be NULL (one-site operator).  L, W1, W2, R are copied. */

@@ -320,6 +320,37 @@ int tt_qtensor_svd_bond(const tt_qtensor* combined, tt_qtensor* A_left, tt_qtens
   });
 }
 
+int tt_qtensor_svd_bond_sectors(const tt_qtensor* combined, tt_qtensor* A_left, tt_qtensor* A_right,
+                                int mid_axis, int direction, double cutoff, unsigned long K, tt_qtensor** S,
+                                double* trunc_err, unsigned* kept, int* n_sectors, int32_t* qn,
+                                uint32_t* kept_per_sector, int cap) {
+  TT_ARG(combined && A_left && A_right && mid_axis >= 0 && mid_axis < (int)A_left->t.rank && n_sectors &&
+         cap >= 0 && (cap == 0 || (qn && kept_per_sector)));
+  TT_GUARD({
+    ttb::qtensor s;
+    ttb::TruncInfo info;
+    ttb::qtensor_index mid = A_left->t.idx_set[mid_axis];
+    ttb::svd_bond(combined->t, A_left->t, A_right->t, mid, s, direction, cutoff, K, &info);
+    if (S) *S = wrap(std::move(s));
+    if (trunc_err) *trunc_err = info.trunc_err;
+    if (kept) *kept = info.kept;
+    *n_sectors = (int)info.sector_qn.size();
+    for (int j = 0; j < *n_sectors && j < cap; ++j) {
+      qn[2 * j] = info.sector_qn[j].a;
+      qn[2 * j + 1] = info.sector_qn[j].b;
+      kept_per_sector[j] = info.kept_per_sector[j];
+    }
+  });
+}
+
+int tt_qtensor_env_update(const tt_qtensor* env, const tt_qtensor* A, const tt_qtensor* W, tt_qtensor** out) {
+  TT_ARG(env && A && W && out);
+  TT_GUARD({
+    ttb::PrecisionScope prec(ttb::rt().env_precision);
+    *out = wrap(ttb::env_step(env->t, A->t, W->t));
+  });
+}
+
 // ---- big_qtensor ---------------------------------------------------------------
 int tt_bigq_create(const tt_qtensor* L, const tt_qtensor* W1, const tt_qtensor* W2, const tt_qtensor* R,
                    tt_bigq** out) {

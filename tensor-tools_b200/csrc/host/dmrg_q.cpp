@@ -1025,7 +1025,7 @@ static qtensor boundary(const qtensor_index& psi_ix, const qtensor_index& h_ix) 
   return T;
 }
 
-static qtensor env_step(const qtensor& env, const qtensor& Ai, const qtensor& W) {
+qtensor env_step(const qtensor& env, const qtensor& Ai, const qtensor& W) {
   qtensor t1 = shallow(Ai);
   t1.conj();
   t1.dag();

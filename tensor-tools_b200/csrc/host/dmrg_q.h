@@ -125,6 +125,9 @@ struct DmrgLog {
   double heff_seconds = 0.0;  // device time of the H_eff*x launches (event-timed)
 };
 
+// One environment step ((A^dag' env) W) A, for a left or a right environment
+// alike (algos/dmrg/dmrg.cpp:56-85 and :491-509 apply it site by site).
+qtensor env_step(const qtensor& env, const qtensor& Ai, const qtensor& W);
 void buildEnv(qMPS& psi, qMPO& H, std::vector<qtensor>& TR, std::vector<qtensor>& TL);
 void updateSite(qMPS& psi, qMPO& H, std::vector<qtensor>& TR, std::vector<qtensor>& TL, unsigned site,
                 double& energy, int direction, int max_bd, double cutoff, char mode,

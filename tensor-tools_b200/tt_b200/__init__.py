@@ -126,6 +126,9 @@ _proto("tt_qtensor_inner_product", P, P, PD)
 _proto("tt_qtensor_svd", P, C.c_int, C.POINTER(C.c_int), C.c_int, D, C.c_uint, PP, PP, PP, PD,
        C.POINTER(C.c_uint))
 _proto("tt_qtensor_svd_bond", P, P, P, C.c_int, C.c_int, D, C.c_ulong, PP, PD, C.POINTER(C.c_uint))
+_proto("tt_qtensor_svd_bond_sectors", P, P, P, C.c_int, C.c_int, D, C.c_ulong, PP, PD, C.POINTER(C.c_uint),
+       C.POINTER(C.c_int), PI32, C.POINTER(C.c_uint32), C.c_int)
+_proto("tt_qtensor_env_update", P, P, P, PP)
 _proto("tt_bigq_create", P, P, P, P, PP)
 _proto("tt_bigq_product", P, P, PP)
 _proto("tt_bigq_size", P, C.POINTER(C.c_uint64))
@@ -447,6 +450,31 @@ def svd_bond(combined: QTensor, A_left: QTensor, A_right: QTensor, mid_axis: int
     _chk(lib.tt_qtensor_svd_bond(combined.h, A_left.h, A_right.h, mid_axis, direction, cutoff, K, C.byref(S),
                                  C.byref(te), C.byref(kept)), "svd_bond")
     return QTensor(S), te.value, kept.value
+
+
+def svd_bond_sectors(combined: QTensor, A_left: QTensor, A_right: QTensor, mid_axis: int, direction: int,
+                     cutoff: float = 0.0, K: int = 0):
+    """svd_bond plus its mid-QN sectors: (S, trunc_err, kept, [(qn, kept_in_sector), ...])."""
+    S = P()
+    te = D()
+    kept = C.c_uint()
+    n = C.c_int()
+    cap = 256
+    qn = (C.c_int32 * (2 * cap))()
+    ks = (C.c_uint32 * cap)()
+    _chk(lib.tt_qtensor_svd_bond_sectors(combined.h, A_left.h, A_right.h, mid_axis, direction, cutoff, K,
+                                         C.byref(S), C.byref(te), C.byref(kept), C.byref(n), qn, ks, cap),
+         "svd_bond_sectors")
+    if n.value > cap:
+        raise TTError("svd_bond_sectors: more than %d sectors" % cap)
+    return QTensor(S), te.value, kept.value, [((qn[2 * j], qn[2 * j + 1]), ks[j]) for j in range(n.value)]
+
+
+def env_update(env: QTensor, A: QTensor, W: QTensor) -> QTensor:
+    """One environment step ((A^dag' env) W) A (algos/dmrg/dmrg.cpp:491-509)."""
+    h = P()
+    _chk(lib.tt_qtensor_env_update(env.h, A.h, W.h, C.byref(h)), "env_update")
+    return QTensor(h)
 
 
 class BigQTensor:

@@ -233,3 +233,47 @@ def test_davidson_matches_oracle(ctx, site):
     sgn = np.sign(got.inner_product(xo))
     for key, i in xo.bid.items():
         np.testing.assert_allclose(sgn * got.blocks[got.bid[key]], xo.blocks[i], atol=1e-9)
+
+
+@pytest.mark.parametrize("side", ["left", "right"])
+def test_env_update_matches_oracle(ctx, side):
+    """tt_qtensor_env_update against the oracle's env_step (algos/dmrg/dmrg.cpp:
+    491-509): a left environment extended over a left-orthonormal site, and a
+    right one over a right-orthonormal site, both mid-chain."""
+    import tt_b200
+    site = 4
+    psi, H, TR, TL, _ = _dmrg_state(site=site)
+    k = site - 1 if side == "left" else site + 3
+    env = TL[k] if side == "left" else TR[k]
+    assert len(env.blocks) > 4
+    want = qdmrg.env_step(env, psi.A[k], H.A[k])
+    got = tt_b200.env_update(tt_b200.QTensor.from_oracle(env), tt_b200.QTensor.from_oracle(psi.A[k]),
+                             tt_b200.QTensor.from_oracle(H.A[k]))
+    assert_same(got, want, tol=1e-12)
+    if side == "left":
+        assert_same(got, TL[k + 1], tol=1e-12)
+
+
+@pytest.mark.parametrize("direction", [qsvd.MoveFromLeft, qsvd.MoveFromRight])
+def test_svd_bond_reports_kept_states_per_sector(ctx, direction):
+    """tt_qtensor_svd_bond_sectors: the same factors as svd_bond, with the
+    kept count of every mid-QN sector equal to the oracle's truncation log."""
+    import tt_b200
+    site = 4
+    psi, H, TR, TL, _ = _dmrg_state(site=site)
+    x = contract(psi.A[site], psi.A[site + 1])
+    mid = [ix for ix in psi.A[site].idx if any(ix.tag() == jx.dagged().tag() for jx in psi.A[site + 1].idx)][0]
+    info = qsvd.TruncInfo()
+    U, V, S = qsvd.svd_bond(x, psi.A[site], psi.A[site + 1], mid, direction, 1e-8, 10, info)
+    gl, gr = tt_b200.QTensor.from_oracle(psi.A[site]), tt_b200.QTensor.from_oracle(psi.A[site + 1])
+    mid_axis = [ix.tag() for ix in psi.A[site].idx].index(mid.tag())
+    gS, te, kept, sectors = tt_b200.svd_bond_sectors(tt_b200.QTensor.from_oracle(x), gl, gr, mid_axis,
+                                                      direction, 1e-8, 10)
+    assert kept == info.kept and kept <= 10
+    assert abs(te - info.trunc_err) < 1e-12
+    assert [q for q, _ in sectors] == [tuple(q) for q in info.sector_qn]
+    assert [k for _, k in sectors] == list(info.kept_per_sector)
+    assert sum(k for _, k in sectors) == kept
+    oS = gS.to_oracle()
+    for key, i in S.bid.items():
+        np.testing.assert_allclose(oS.blocks[oS.bid[key]], S.blocks[i], rtol=1e-10, atol=1e-13)

@@ -1092,12 +1092,19 @@ tridiag_eigvals_cluster(const EigDev* __restrict__ probs, double* G, double* Tg,
 
 // Bisection for the cluster-sized sectors after their tridiagonalisation,
 // spread over the GPU: a CTA of BS_THREADS threads takes BS_PER eigenvalues
-// of one problem (ten per warp, three lanes per eigenvalue probing the
-// midpoint and both quarter points, as in tridiag_eigvals), with the problem's
-// d and e^2 in shared memory.  Few warps per SM keep each warp's Sturm chain
-// latency-bound instead of sharing one SM's FP64 pipes with fifteen others.
+// of one problem, with the problem's d and e^2 in shared memory.  Sixteen
+// lanes serve one eigenvalue: in a round they count at the 15 points that
+// four successive halvings of the current interval can probe (the nodes of a
+// four-level bisection tree, each computed by the same chain of midpoints
+// that plain bisection would compute), then every lane of the group walks
+// the tree with the shared counts.  The intervals, the stopping rule and so
+// the eigenvalues are bit for bit those of plain bisection; a round advances
+// four halvings instead of one, so an eigenvalue takes about 13 rounds of
+// Sturm chains instead of 50.
 constexpr int BS_THREADS = 128;
-constexpr int BS_PER = (BS_THREADS / 32) * 10;
+constexpr int BS_LANES = 16;  // lanes per eigenvalue: 15 probes, one idle
+constexpr int BS_LEVELS = 4;  // halvings per round
+constexpr int BS_PER = BS_THREADS / BS_LANES;
 
 __global__ void __launch_bounds__(BS_THREADS)
 bisect_sectors(const EigDev* __restrict__ probs, const VecTaskB* __restrict__ tasks, const double* Tg, double* W) {
@@ -1109,7 +1116,7 @@ bisect_sectors(const EigDev* __restrict__ probs, const VecTaskB* __restrict__ ta
   const double* dg = Tg + 3 * P.w_off;
   const double* eg = dg + n;
   double* Wp = W + P.w_off;
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int tid = threadIdx.x, lane = tid & 31;
   double* d = bs_sm;
   double* e2 = bs_sm + n;
   for (int i = tid; i < n; i += blockDim.x) {
@@ -1137,30 +1144,43 @@ bisect_sectors(const EigDev* __restrict__ probs, const VecTaskB* __restrict__ ta
   auto open_interval = [&](double lo, double hi) {
     return hi - lo > fmax(atol, 2.0 * DBL_EPSILON * fmax(fabs(lo), fabs(hi)));
   };
-  const int grp = lane < 30 ? lane / 3 : 0, sub = lane % 3;
-  const int j = tk.j0 + warp * 10 + grp;
-  const bool active = lane < 30 && j < n;
+  const int sub = lane & (BS_LANES - 1);          // this lane's tree node: in-order position sub + 1
+  const int base = lane & ~(BS_LANES - 1);        // first lane of the group
+  const int j = tk.j0 + tid / BS_LANES;
+  const bool active = j < n;
+  constexpr int ROOT = 1 << (BS_LEVELS - 1);      // in-order position of the root (8)
   double lo = gl - atol, hi = gu + atol;
   int it = 0;
   bool work = active && open_interval(lo, hi);
   while (__any_sync(0xffffffffu, work)) {
-    const double mid = 0.5 * (lo + hi), lm = 0.5 * (lo + mid), rm = 0.5 * (mid + hi);
-    const double x = sub == 0 ? mid : (sub == 1 ? lm : rm);
-    const int c = work ? sturm_count(d, e2, n, x, pivmin) : 0;
-    const int cm = __shfl_sync(0xffffffffu, c, 3 * grp);
-    const int cl = __shfl_sync(0xffffffffu, c, 3 * grp + 1);
-    const int cr = __shfl_sync(0xffffffffu, c, 3 * grp + 2);
-    if (work) {
-      const bool left = cm > j;
-      if (left) hi = mid; else lo = mid;
-      ++it;
-      if (it < 128 && open_interval(lo, hi)) {
-        const double x2 = left ? lm : rm;
-        if ((left ? cl : cr) > j) hi = x2; else lo = x2;
+    int c = 0;
+    if (work && sub < 2 * ROOT - 1) {
+      // descend from the round's interval to node sub + 1 by midpoints
+      const int p = sub + 1;
+      double a = lo, b = hi;
+      int pos = ROOT, half = ROOT >> 1;
+      while (pos != p) {
+        const double m = 0.5 * (a + b);
+        if (p < pos) { b = m; pos -= half; } else { a = m; pos += half; }
+        half >>= 1;
+      }
+      c = sturm_count(d, e2, n, 0.5 * (a + b), pivmin);
+    }
+    // every lane of the group walks the same path with the group's counts
+    int pos = ROOT, half = ROOT >> 1;
+    bool go = work;
+#pragma unroll
+    for (int lev = 0; lev < BS_LEVELS; ++lev) {
+      const int cp = __shfl_sync(0xffffffffu, c, base + pos - 1);
+      go = go && it < 128 && open_interval(lo, hi);
+      if (go) {
+        const double mid = 0.5 * (lo + hi);
+        if (cp > j) { hi = mid; pos -= half; } else { lo = mid; pos += half; }
+        half >>= 1;
         ++it;
       }
-      work = it < 128 && open_interval(lo, hi);
     }
+    if (work) work = it < 128 && open_interval(lo, hi);
   }
   if (active && sub == 0) Wp[n - 1 - j] = 0.5 * (lo + hi);
 }

@@ -89,3 +89,85 @@ def test_splits_exact_hits_and_large_norms():
         ev = np.linalg.eigvalsh(np.diag(d) + np.diag(e, 1) + np.diag(e, -1))
         xs = list(ev[:: max(1, n // 60)]) + list(0.5 * (ev[1:] + ev[:-1])[:: max(1, n // 60)]) + list(d[:20]) + [0.0]
         _check(d, e, xs, ev)
+
+
+def _bisect_plain(d, e2, j, lo, hi, open_interval, pivmin):
+    """One eigenvalue by plain bisection (the reference walk)."""
+    it = 0
+    while it < 128 and open_interval(lo, hi):
+        mid = 0.5 * (lo + hi)
+        if count_product(d, e2, mid, pivmin) > j:
+            hi = mid
+        else:
+            lo = mid
+        it += 1
+    return 0.5 * (lo + hi), it
+
+
+def _bisect_multisection(d, e2, j, lo, hi, open_interval, pivmin, levels=4):
+    """bisect_sectors: per round, counts at the 2^levels - 1 nodes of the
+    bisection tree below the current interval (each node's point computed
+    by the chain of midpoints that leads to it), then the walk down the tree
+    with those counts."""
+    root = 1 << (levels - 1)
+    it = 0
+    work = open_interval(lo, hi)
+    while work:
+        counts = {}
+        for p in range(1, 2 * root):
+            a, b, pos, half = lo, hi, root, root >> 1
+            while pos != p:
+                m = 0.5 * (a + b)
+                if p < pos:
+                    b, pos = m, pos - half
+                else:
+                    a, pos = m, pos + half
+                half >>= 1
+            counts[p] = count_product(d, e2, 0.5 * (a + b), pivmin)
+        pos, half, go = root, root >> 1, True
+        for _ in range(levels):
+            go = go and it < 128 and open_interval(lo, hi)
+            if go:
+                mid = 0.5 * (lo + hi)
+                if counts[pos] > j:
+                    hi, pos = mid, pos - half
+                else:
+                    lo, pos = mid, pos + half
+                half >>= 1
+                it += 1
+        work = it < 128 and open_interval(lo, hi)
+    return 0.5 * (lo + hi), it
+
+
+def test_multisection_walk_is_plain_bisection_bit_for_bit():
+    """The GPU-wide bisection advances four halvings per round from counts
+    at the 15 tree nodes; its intervals, and so its eigenvalues and halving
+    counts, must be exactly those of plain bisection (graded spectra as in a
+    density matrix, and a matrix with close eigenvalues)."""
+    rng = np.random.default_rng(11)
+    eps = np.finfo(float).eps
+    cases = []
+    n = 24
+    Q, _ = np.linalg.qr(rng.standard_normal((n, n)))
+    lam = np.sort(10.0 ** rng.uniform(-14, 0, n))
+    A = (Q * lam) @ Q.T
+    T = sla.hessenberg(A)  # tridiagonal: A is symmetric
+    cases.append((np.diag(T).copy(), np.diag(T, -1).copy()))
+    dd = rng.uniform(-1, 1, n)
+    ee = rng.uniform(-1e-3, 1e-3, n - 1)
+    cases.append((dd, ee))
+    for d, e in cases:
+        e2 = e * e
+        r = np.abs(np.concatenate([[0.0], e])) + np.abs(np.concatenate([e, [0.0]]))
+        gl, gu = float(np.min(d - r)), float(np.max(d + r))
+        bnorm = max(abs(gl), abs(gu))
+        pivmin = DBL_MIN * max(1.0, float(e2.max()))
+        atol = 4.0 * eps * bnorm + 2.0 * pivmin
+
+        def open_interval(lo, hi):
+            return hi - lo > max(atol, 2.0 * eps * max(abs(lo), abs(hi)))
+
+        for j in range(len(d)):
+            a = _bisect_plain(d, e2, j, gl - atol, gu + atol, open_interval, pivmin)
+            b = _bisect_multisection(d, e2, j, gl - atol, gu + atol, open_interval, pivmin)
+            assert a == b

@@ -77,9 +77,11 @@ C5_N = C5["Nx"] * C5["Ny"]
 C5_MID = C5_N // 2 - C5["block"] // 2          # 46: the block spans sites 46..50
 C5_UPDATES_PER_SWEEP = 2 * (C5_N - 1)           # 190
 CHOSEN = "tf32x3-auto"
-# the environment updates stay in FP64 in the chosen form: each of their
-# operands is used once, so the TF32 packing does not pay for itself, and
-# FP64 environments keep the Ritz values free of a first-order bias
+# the environment updates stay in FP64 in the chosen form: FP64 environments
+# keep the Ritz values free of a first-order bias.  Measured on this workload
+# with --env-prec tf32x3-auto: 6% less time per sweep, but |dE|/N = 1.1e-8
+# against FP64 after a full sweep at bond dimension 3072 (2.4e-9 with FP64
+# environments), above the 1e-8 the mixed form must hold.
 ENV_PREC = "fp64"
 
 

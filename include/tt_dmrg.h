@@ -99,6 +99,10 @@ int tt_dmrg_heff_parts(double* ms, double* flops, double* mid_bytes);
 /* host-side planning counters of this thread: seconds and calls spent in
  * block-structure computation and in contraction-plan creation */
 int tt_dmrg_planning_counters(double* t_structure, int64_t* n_structure, double* t_plan, int64_t* n_plan);
+/* this thread's contraction cache (block structures and plans keyed by the
+ * operands' structure): entries, device bytes of their plans' tables, and
+ * how often least-recently-used entries were evicted (rounds, entries) */
+int tt_dmrg_cache_stats(int64_t* entries, int64_t* plan_bytes, int64_t* evictions, int64_t* evicted);
 
 /* Precisions (TT_PREC_*) on this thread: op -- qtensor/dtensor contractions
  * (operator*); heff -- the H_eff*x products inside Davidson; env -- the

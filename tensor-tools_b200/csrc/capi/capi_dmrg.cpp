@@ -127,6 +127,10 @@ int tt_dmrg_planning_counters(double* t_structure, int64_t* n_structure, double*
   });
 }
 
+int tt_dmrg_cache_stats(int64_t* entries, int64_t* plan_bytes, int64_t* evictions, int64_t* evicted) {
+  TT_GUARD({ ttb::contraction_cache_stats(entries, plan_bytes, evictions, evicted); });
+}
+
 // ---- qtensor -------------------------------------------------------------
 int tt_qtensor_create(int rank, const tt_index_desc* idx, tt_qtensor** out) {
   TT_ARG(out && rank >= 0 && (rank == 0 || idx));

@@ -905,6 +905,8 @@ int tt_contract_plan_keep(tt_ctx* ctx, const tt_out_block* outs, int n_out, cons
   std::vector<TableJob> jobs;
   jobs.reserve(4 * (size_t)n_pairs);
   int64_t tab_len = 0;
+  std::map<std::vector<int64_t>, int32_t> tab_of;  // table contents -> its offset
+  std::vector<int64_t> tab_key;
   double flops = 0.0;
   std::vector<int> first(n_out + 1, 0);
   std::vector<int64_t> work(n_out, 0);
@@ -926,7 +928,16 @@ int tt_contract_plan_keep(tt_ctx* ctx, const tt_out_block* outs, int n_out, cons
     P.m = (int)m;
     P.n = (int)n;
     P.k = (int)k;
+    // an offset table is a function of (length, dims, strides) alone: pairs
+    // that address the same rows or columns of a block share one table
     auto add_job = [&](int len, int nmodes, const int32_t* dims, const int64_t* strides) {
+      tab_key.assign({(int64_t)len, (int64_t)nmodes});
+      for (int i = 0; i < nmodes; ++i) {
+        tab_key.push_back(dims[i]);
+        tab_key.push_back(strides[i]);
+      }
+      auto hit = tab_of.find(tab_key);
+      if (hit != tab_of.end()) return hit->second;
       TableJob J;
       memset(&J, 0, sizeof(J));
       J.dst = (int32_t)tab_len;
@@ -938,6 +949,7 @@ int tt_contract_plan_keep(tt_ctx* ctx, const tt_out_block* outs, int n_out, cons
       }
       jobs.push_back(J);
       tab_len += len;
+      tab_of.emplace(tab_key, J.dst);
       return J.dst;
     };
     P.rowA = add_job((int)m, q.n_m, q.m_dims, q.a_m_stride);

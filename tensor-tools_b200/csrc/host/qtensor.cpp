@@ -636,6 +636,7 @@ struct ContractionCache {
   size_t entries = 0;
   int64_t plan_bytes = 0;  // device bytes held by the cached plans
   uint64_t clock = 0;      // lookups so far (least recently used entries go first)
+  int64_t evictions = 0, evicted = 0;
 };
 ContractionCache& cache() {
   static thread_local ContractionCache c;
@@ -673,6 +674,8 @@ void evict_lru() {
     for (size_t i : kv.second) bucket.erase(bucket.begin() + (long)i);
     if (bucket.empty()) c.map.erase(kv.first);
   }
+  c.evictions++;
+  c.evicted += (int64_t)(c.entries - entries);
   c.entries = entries;
   c.plan_bytes = bytes;
 }
@@ -686,6 +689,12 @@ void clear_contraction_cache() {
 }
 
 size_t contraction_cache_size() { return cache().entries; }
+void contraction_cache_stats(int64_t* entries, int64_t* plan_bytes, int64_t* evictions, int64_t* evicted) {
+  if (entries) *entries = (int64_t)cache().entries;
+  if (plan_bytes) *plan_bytes = cache().plan_bytes;
+  if (evictions) *evictions = cache().evictions;
+  if (evicted) *evicted = cache().evicted;
+}
 
 std::shared_ptr<const CachedContraction> contract_cached(const qtensor& A, const qtensor& B, bool need_plan) {
   std::vector<int64_t> key;

@@ -260,6 +260,8 @@ std::shared_ptr<const CachedContraction> contract_cached(const qtensor& A, const
                                                          bool need_plan);
 void clear_contraction_cache();
 size_t contraction_cache_size();
+// entries, device bytes of their plans, eviction rounds and entries evicted
+void contraction_cache_stats(int64_t* entries, int64_t* plan_bytes, int64_t* evictions, int64_t* evicted);
 
 // A cached contraction plan on the device.
 class PlanHandle {

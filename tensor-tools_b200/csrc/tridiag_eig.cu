@@ -305,25 +305,33 @@ __device__ void tri_solve(const double* d, const double* e, int n, double lambda
 }
 
 // tri_solve for a thread's column of an interleaved batch (y, u0, u1, u2 all
-// with stride ustride), the same operations in the same order, with the
-// global loads issued PF steps ahead: the values of the next PF steps are
-// fetched while the current PF are computed (the threads of a CTA walk the
-// same rows in lockstep, so the batch's accesses coalesce and the latency of
-// one step is the arithmetic's, not memory's).
+// with stride st), with the global loads issued PF steps ahead: the values of
+// the next PF steps are fetched while the current PF are computed (the
+// threads of a CTA walk the same rows in lockstep, so the batch's accesses
+// coalesce and the latency of one step is the arithmetic's, not memory's).
+// The same elimination with partial pivoting as tri_solve, but each step
+// takes one reciprocal: u0 keeps 1 / pivot (the pivot clamped to +-tiny as
+// the back substitution of tri_solve clamps it), used for the multiplier
+// and again in the back substitution.  The right-hand side is y * scale
+// (the previous iterate's normalisation, applied as it is read), and the
+// return value is the squared norm of the solution, summed as it is solved.
 constexpr int PF = 8;
-__device__ void tri_solve_il(const double* d, const double* e, int n, double lambda, double tiny, double* y,
-                             double* u0, double* u1, double* u2, int64_t st) {
+__device__ __forceinline__ double clamped_rcp(double piv, double tiny) {
+  return 1.0 / (fabs(piv) < tiny ? (piv < 0.0 ? -tiny : tiny) : piv);
+}
+__device__ double tri_solve_il(const double* d, const double* e, int n, double lambda, double tiny, double scale,
+                               double* y, double* u0, double* u1, double* u2, int64_t st) {
   // forward elimination; step i reads y[i + 1]
   double di = d[0] - lambda, si = n > 1 ? e[0] : 0.0, ti = 0.0;
-  double bi = y[0];
+  double bi = y[0] * scale;
   double cur[PF], nxt[PF];
 #pragma unroll
-  for (int k = 0; k < PF; ++k) cur[k] = 1 + k < n ? y[(int64_t)(1 + k) * st] : 0.0;
+  for (int k = 0; k < PF; ++k) cur[k] = 1 + k < n ? y[(int64_t)(1 + k) * st] * scale : 0.0;
   for (int i0 = 0; i0 + 1 < n; i0 += PF) {
 #pragma unroll
     for (int k = 0; k < PF; ++k) {
       const int r = i0 + PF + 1 + k;
-      nxt[k] = r < n ? y[(int64_t)r * st] : 0.0;
+      nxt[k] = r < n ? y[(int64_t)r * st] * scale : 0.0;
     }
 #pragma unroll
     for (int k = 0; k < PF; ++k) {
@@ -335,8 +343,9 @@ __device__ void tri_solve_il(const double* d, const double* e, int n, double lam
         double bnext = cur[k];
         if (fabs(di) >= fabs(ci)) {
           if (di == 0.0) di = tiny;
-          double mlt = ci / di;
-          u0[(int64_t)i * st] = di;
+          const double r = 1.0 / di;
+          const double mlt = ci * r;
+          u0[(int64_t)i * st] = fabs(di) < tiny ? clamped_rcp(di, tiny) : r;
           u1[(int64_t)i * st] = si;
           u2[(int64_t)i * st] = ti;
           y[(int64_t)i * st] = bi;
@@ -346,8 +355,9 @@ __device__ void tri_solve_il(const double* d, const double* e, int n, double lam
           si = ns;
           ti = 0.0;
         } else {
-          double mlt = di / ci;
-          u0[(int64_t)i * st] = ci;
+          const double r = 1.0 / ci;
+          const double mlt = di * r;
+          u0[(int64_t)i * st] = fabs(ci) < tiny ? clamped_rcp(ci, tiny) : r;
           u1[(int64_t)i * st] = an;
           u2[(int64_t)i * st] = bn;
           y[(int64_t)i * st] = bnext;
@@ -362,11 +372,11 @@ __device__ void tri_solve_il(const double* d, const double* e, int n, double lam
 #pragma unroll
     for (int k = 0; k < PF; ++k) cur[k] = nxt[k];
   }
-  if (fabs(di) < tiny) di = di < 0.0 ? -tiny : tiny;
-  u0[(int64_t)(n - 1) * st] = di;
+  u0[(int64_t)(n - 1) * st] = clamped_rcp(di, tiny);
   y[(int64_t)(n - 1) * st] = bi;
   // back substitution, i = n - 1 down to 0; step i reads y[i], u0[i], u1[i], u2[i]
   double x1 = 0.0, x2 = 0.0;  // y[i + 1], y[i + 2] as solved
+  double ss = 0.0;
   double cy[PF], c0[PF], c1[PF], c2[PF], ny[PF], n0[PF], n1[PF], n2[PF];
 #pragma unroll
   for (int k = 0; k < PF; ++k) {
@@ -392,10 +402,9 @@ __device__ void tri_solve_il(const double* d, const double* e, int n, double lam
         double s = cy[k];
         if (i + 1 < n) s -= c1[k] * x1;
         if (i + 2 < n) s -= c2[k] * x2;
-        double piv = c0[k];
-        if (fabs(piv) < tiny) piv = piv < 0.0 ? -tiny : tiny;
-        const double xi = s / piv;
+        const double xi = s * c0[k];
         y[(int64_t)i * st] = xi;
+        ss = fma(xi, xi, ss);
         x2 = x1;
         x1 = xi;
       }
@@ -408,6 +417,7 @@ __device__ void tri_solve_il(const double* d, const double* e, int n, double lam
       c2[k] = n2[k];
     }
   }
+  return ss;
 }
 
 // U holds the three factor rows back to back (3 n doubles)
@@ -1477,21 +1487,29 @@ inv_iter_batched(const EigDev* __restrict__ probs, const VecTask* __restrict__ t
   double* zb = Zg + P.g_off + (int64_t)n * tk.j0;
   double* y = wb + t;
   const int64_t nc = (int64_t)n * cnt;
+  // each iterate's normalisation is applied as the next solve (or the final
+  // copy) reads it; its norm is summed in the solve's back substitution
+  double inv = 1.0;
   if (active) {
     for (int i = 0; i < n; ++i)
       y[(int64_t)i * cnt] = hash_unit(((uint64_t)P.g_off << 20) ^ ((uint64_t)j << 32) ^ (uint64_t)i);
     for (int it = 0; it < INV_ITERS; ++it) {
-      tri_solve_il(d, e, n, lam[j], tiny, y, wb + nc + t, wb + 2 * nc + t, zb + t, cnt);
-      double s = 0.0;
-      for (int i = 0; i < n; ++i) s += y[(int64_t)i * cnt] * y[(int64_t)i * cnt];
-      const double inv = 1.0 / sqrt(s);
-      for (int i = 0; i < n; ++i) y[(int64_t)i * cnt] *= inv;
+      const double s = tri_solve_il(d, e, n, lam[j], tiny, inv, y, wb + nc + t, wb + 2 * nc + t, zb + t, cnt);
+      inv = 1.0 / sqrt(s);
     }
   }
   __syncthreads();  // every thread's third factor row in Z is dead
   if (active) {
     double* z = zb + (int64_t)n * t;
-    for (int i = 0; i < n; ++i) z[i] = y[(int64_t)i * cnt];
+    int i = 0;
+    for (; i + PF <= n; i += PF) {
+      double v[PF];
+#pragma unroll
+      for (int k = 0; k < PF; ++k) v[k] = y[(int64_t)(i + k) * cnt];
+#pragma unroll
+      for (int k = 0; k < PF; ++k) z[i + k] = v[k] * inv;
+    }
+    for (; i < n; ++i) z[i] = y[(int64_t)i * cnt] * inv;
   }
 }
 

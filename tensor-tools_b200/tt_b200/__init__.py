@@ -197,6 +197,7 @@ _proto("tt_qdmrg_step_profile", P, C.c_int, C.POINTER(C.c_int), PD, PD, PD, PD)
 _proto("tt_qdmrg_step_device_ms", P, C.c_int, PD, PD, PD, PD)
 _proto("tt_dmrg_set_profiling", C.c_int)
 _proto("tt_dmrg_planning_counters", PD, PI64, PD, PI64)
+_proto("tt_dmrg_cache_stats", PI64, PI64, PI64, PI64)
 _proto("tt_eig_redo_count", P, PI64)
 _proto("tt_dmrg_heff_parts", PD, PD, PD)
 _proto("tt_sym_eig_batched", P, C.c_void_p, C.c_int, P, P, P, P)
@@ -981,6 +982,13 @@ def planning_counters() -> dict:
     ns, np_ = I64(), I64()
     _chk(lib.tt_dmrg_planning_counters(C.byref(ts), C.byref(ns), C.byref(tp), C.byref(np_)), "planning_counters")
     return {"structure_s": ts.value, "structures": ns.value, "plan_s": tp.value, "plans": np_.value}
+
+
+def cache_stats() -> dict:
+    """This thread's contraction cache: entries, plan device bytes, evictions."""
+    e, b, r, n = I64(), I64(), I64(), I64()
+    _chk(lib.tt_dmrg_cache_stats(C.byref(e), C.byref(b), C.byref(r), C.byref(n)), "cache_stats")
+    return {"entries": e.value, "plan_bytes": b.value, "evictions": r.value, "evicted": n.value}
 
 
 def davidson_refills() -> int:

@@ -145,6 +145,47 @@ def test_mixed_precision_dense_tfi(ctx):
     assert abs(emx - e64) / N <= 1e-8
 
 
+def test_mixed_precision_dense_tfi_cylinder_6x12(ctx):
+    """The dense transverse-field Ising configuration at its geometry: the
+    6 x 12 cylinder (periodic around the 6-site circumference, 72 sites in
+    snake order), H = -sum ZZ - 3 sum X (Z = 2 Sz, X = 2 Sx), a seeded random
+    product state, the MPO from the AutoMPO (uncompressed basis of
+    models/hams/AutoMPO.cpp: the identity states plus one string state per
+    ZZ term open across a link, at most 8 here -- the configuration quotes
+    14 for its MPO); the bond dimension is ramped to 128 instead of 1024 so
+    the test takes seconds.  The mixed
+    form (3xTF32 tensor-core H_eff*x and environment contractions, FP64 SVD)
+    must hold |dE|/N <= 1e-8 against the FP64 GPU form, with the same bond
+    dimensions."""
+    import tt_b200
+    from oracle import autompo as am
+    Nx, Ny, g = 12, 6, 3.0
+    N = Nx * Ny
+    bonds = am.snake_relabel(am.square_lattice(Nx, Ny, True), Nx, Ny)
+    a = tt_b200.AutoMPO()
+    for s1, s2, *_ in bonds:
+        a.add(-4.0, "Sz", s1 - 1, "Sz", s2 - 1)
+    for i in range(N):
+        a.add(-2.0 * g, "Sx", i)
+    assert max(a.link_dims(N, with_charges=False)) == 8
+    H = tt_b200.DMPO.from_autompo(a, N)
+    state = list(np.random.default_rng(12).integers(0, 2, N))
+    sched = ([16, 32, 64, 128, 128, 128], [1e-10], [4])
+    p64 = tt_b200.DMPS(N, state)
+    e64, s64, _ = tt_b200.ddmrg_run(p64, H, 6, *sched)
+    tt_b200.set_precision(heff="tf32x3", env="tf32x3")
+    try:
+        pmx = tt_b200.DMPS(N, state)
+        emx, smx, _ = tt_b200.ddmrg_run(pmx, H, 6, *sched)
+    finally:
+        tt_b200.set_precision()
+    assert max(p64.bond_dims()) == 128
+    assert pmx.bond_dims() == p64.bond_dims()
+    assert abs(emx - e64) / N <= 1e-8
+    # variational and converging: the last sweeps agree to well below the gap
+    assert abs(s64[-1] - s64[-2]) / N <= 1e-6
+
+
 def test_auto_precision_picks_per_contraction(ctx):
     """'tf32x3-auto' resolves per contraction: a contraction over a small MPO
     link (k = 5, bandwidth-bound) stays FP64 and is bit-identical to the FP64

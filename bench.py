@@ -492,6 +492,7 @@ def c5_arm(prec, ck, H, args, ctx, stream, flush, torch, tt_b200, sampler=None, 
         ctx.sync()
         st0, fb0, l0 = run.stats(), tt_b200.davidson_fallbacks(), ctx.launches()
         pc0 = tt_b200.planning_counters()
+        pt0 = tt_b200.plan_timers()
         hp0 = tt_b200.heff_parts()
         er0 = tt_b200.eig_redo_count(ctx)
         s0 = len(run.steps())
@@ -567,6 +568,8 @@ def c5_arm(prec, ck, H, args, ctx, stream, flush, torch, tt_b200, sampler=None, 
             "host_planning_s_per_update": ((pc1["structure_s"] - pc0["structure_s"]) + (pc1["plan_s"] - pc0["plan_s"]))
             / max(1, args.steps * 2 * B),
             "plans_per_update": (pc1["plans"] - pc0["plans"]) / max(1, args.steps * 2 * B),
+            "host_structure_s_per_update": (pc1["structure_s"] - pc0["structure_s"]) / max(1, args.steps * 2 * B),
+            "planner_stage_s_per_update": [(b - a) / max(1, args.steps * 2 * B) for a, b in zip(pt0, tt_b200.plan_timers())],
             "eig_redos": er1 - er0,
             "heff_parts": heff_parts_summary(hp0, hp1),
             "step_plans_built": step_plans, "step_pool_reserved_gb": step_pool,

@@ -193,6 +193,12 @@ int tt_plan_release_packed(tt_ctx* ctx, const tt_plan* plan);
 int tt_plan_destroy(tt_ctx* ctx, tt_plan* plan);
 /* Algorithmic work of one exec: sum over pairs of 2*m*n*k. */
 /* Device bytes a plan holds (offset tables, tasks, packing jobs). */
+/* Host seconds this thread's planner spent in its stages since the thread
+ * started (diagnostic): [0] pair offset tables, [1] the precision choice of
+ * the automatic modes, [2] tile tasks and row-stationary chunks, [3]
+ * tensor-core packing jobs, [4] device tables, uploads and the rest.  The
+ * first min(n, 5) are written. */
+int tt_contract_plan_timers(double* seconds, int n);
 int tt_plan_device_bytes(const tt_plan* plan, int64_t* bytes);
 int tt_plan_flops(const tt_plan* plan, double* flops);
 /* The precision the plan runs in (TT_PREC_FP64 / TF32 / TF32X3): an *_AUTO

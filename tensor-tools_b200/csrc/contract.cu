@@ -8,6 +8,7 @@
 // transpose pass; the tables are expanded on the device from the pair
 // descriptors when the plan is built.
 #include <algorithm>
+#include <chrono>
 #include <cstring>
 #include <functional>
 #include <map>
@@ -878,6 +879,24 @@ struct tt_plan {
 
 extern "C" {
 
+// Host seconds of the planner's stages on this thread (tt_contract_plan_timers):
+// pair tables, precision choice, tile tasks and the row-stationary chunks,
+// tensor-core packing jobs, device tables and uploads.
+static thread_local double g_plan_stage_s[5];
+struct PlanLap {
+  std::chrono::steady_clock::time_point t = std::chrono::steady_clock::now();
+  int stage = 0;
+  void operator()(int k) {
+    const auto now = std::chrono::steady_clock::now();
+    g_plan_stage_s[k] += std::chrono::duration<double>(now - t).count();
+    t = now;
+    stage = k + 1;
+  }
+  ~PlanLap() {
+    if (stage < 5) (*this)(4);
+  }
+};
+
 int tt_contract_plan(tt_ctx* ctx, const tt_out_block* outs, int n_out,
                      const tt_block_pair* pairs, int n_pairs, int precision,
                      tt_plan** plan_out) {
@@ -886,6 +905,7 @@ int tt_contract_plan(tt_ctx* ctx, const tt_out_block* outs, int n_out,
 
 int tt_contract_plan_keep(tt_ctx* ctx, const tt_out_block* outs, int n_out, const tt_block_pair* pairs,
                           int n_pairs, int precision, int keep, tt_plan** plan_out) {
+  PlanLap lap;
   TT_REQUIRE(ctx && plan_out, "tt_contract_plan: null argument");
   TT_REQUIRE(n_out >= 0 && n_pairs >= 0, "tt_contract_plan: negative count");
   TT_REQUIRE(precision >= TT_PREC_FP64 && precision <= TT_PREC_TF32X3_AUTO,
@@ -968,12 +988,14 @@ int tt_contract_plan_keep(tt_ctx* ctx, const tt_out_block* outs, int n_out, cons
     flops += 2.0 * (double)m * (double)n * (double)k;
   }
   TT_REQUIRE(tab_len < (1ll << 31), "tt_contract_plan: offset tables too large");
+  lap(0);
   for (int o = 0; o < n_out; ++o) first[o + 1] += first[o];
   // FP64 unless the tensor-core form is predicted clearly (20 %) faster: the
   // model is coarse, and FP64 is the more accurate of the two
   if (automatic && predict_us(outs, n_out, hp, first, precision, ctx->num_sms, keep) >
                        0.8 * predict_us(outs, n_out, hp, first, TT_PREC_FP64, ctx->num_sms))
     precision = TT_PREC_FP64;
+  lap(1);
   const bool tc = precision != TT_PREC_FP64;
   // FP64 plans whose output blocks are at most SK_N wide and whose pairs
   // contract at most SK_K elements run on the skinny kernel
@@ -1012,7 +1034,16 @@ int tt_contract_plan_keep(tt_ctx* ctx, const tt_out_block* outs, int n_out, cons
     // (union-find on the pairs' A offsets), heaviest group first.
     std::vector<int> parent(n_out);
     std::iota(parent.begin(), parent.end(), 0);
-    std::function<int(int)> root = [&](int o) { return parent[o] == o ? o : parent[o] = root(parent[o]); };
+    auto root = [&](int o) {
+      int r = o;
+      while (parent[r] != r) r = parent[r];
+      while (parent[o] != r) {  // path compression
+        const int up = parent[o];
+        parent[o] = r;
+        o = up;
+      }
+      return r;
+    };
     std::unordered_map<int64_t, int> owner;
     for (int o = 0; o < n_out; ++o)
       for (int i = first[o]; i < first[o + 1]; ++i) {
@@ -1020,14 +1051,10 @@ int tt_contract_plan_keep(tt_ctx* ctx, const tt_out_block* outs, int n_out, cons
         const int ra = root(it->second), rb = root(o);
         if (ra != rb) parent[rb] = ra;
       }
+    std::vector<int> groot(n_out);
+    for (int o = 0; o < n_out; ++o) groot[o] = root(o);
     std::vector<int64_t> gcost(n_out, 0);
-    for (int o = 0; o < n_out; ++o) gcost[root(o)] += work[o] + 1;
-    std::stable_sort(torder.begin(), torder.end(), [&](int a, int b) {
-      const int ga = root(tasks[a].out), gb = root(tasks[b].out);
-      if (ga != gb) return gcost[ga] != gcost[gb] ? gcost[ga] > gcost[gb] : ga < gb;
-      if (tasks[a].m0 != tasks[b].m0) return tasks[a].m0 < tasks[b].m0;
-      return tasks[a].out < tasks[b].out;
-    });
+    for (int o = 0; o < n_out; ++o) gcost[groot[o]] += work[o] + 1;
     // row-stationary chunks (skinny_rs): a group's outputs in order, at most
     // SK_N combined columns each; valid when the group's outputs share their
     // rows and every A block is read through the same tables by all its pairs
@@ -1044,7 +1071,7 @@ int tt_contract_plan_keep(tt_ctx* ctx, const tt_out_block* outs, int n_out, cons
         rs_ok = x.k_dims[d] == y.k_dims[d] && x.a_k_stride[d] == y.a_k_stride[d];
     }
     std::vector<std::vector<int>> members(n_out);
-    for (int o = 0; o < n_out; ++o) members[root(o)].push_back(o);
+    for (int o = 0; o < n_out; ++o) members[groot[o]].push_back(o);
     for (int g = 0; g < n_out && rs_ok; ++g)
       for (int o : members[g]) rs_ok = rs_ok && outs[o].m == outs[members[g][0]].m;
     std::vector<int> gorder;
@@ -1103,6 +1130,16 @@ int tt_contract_plan_keep(tt_ctx* ctx, const tt_out_block* outs, int n_out, cons
     for (const RsChunk& c : rs_chunks) rs_ktot = std::max<int64_t>(rs_ktot, c.ktot);
     for (const RsO& x : rs_o) rs_ok = rs_ok && outs[x.out].n <= RS_COLS;  // every chunk fits its instance
     if (rs_ok) rs_ok = rs_ktot * (int64_t)(RS_COLS * sizeof(double) + sizeof(int32_t)) <= SK_STAGE_BYTES;
+    // the per-pair skinny kernel (no row-stationary chunks): tasks of a group
+    // interleaved by row tile, heaviest group first; with the chunks, the
+    // tile tasks are not run and stay in their plain order
+    if (!rs_ok)
+      std::stable_sort(torder.begin(), torder.end(), [&](int a, int b) {
+        const int ga = groot[tasks[a].out], gb = groot[tasks[b].out];
+        if (ga != gb) return gcost[ga] != gcost[gb] ? gcost[ga] > gcost[gb] : ga < gb;
+        if (tasks[a].m0 != tasks[b].m0) return tasks[a].m0 < tasks[b].m0;
+        return tasks[a].out < tasks[b].out;
+      });
   } else {
     std::stable_sort(torder.begin(), torder.end(), [&](int a, int b) { return tcost[a] > tcost[b]; });
   }
@@ -1111,6 +1148,7 @@ int tt_contract_plan_keep(tt_ctx* ctx, const tt_out_block* outs, int n_out, cons
   std::vector<OutDev> ho(n_out);
   for (int o = 0; o < n_out; ++o) ho[o] = OutDev{outs[o].c_off, outs[o].m, outs[o].n, outs[o].ldc};
 
+  lap(2);
   // tensor-core path: one packing job per distinct operand block
   std::vector<PackJob> ja, jb;
   std::vector<PackTile> ta, tb;
@@ -1193,6 +1231,7 @@ int tt_contract_plan_keep(tt_ctx* ctx, const tt_out_block* outs, int n_out, cons
   }
   cudaStream_t s = ctx->stream;
   TT_CUDA(cudaMemsetAsync(plan->d_status, 0, sizeof(int), s));
+  lap(3);
   // staged copies: the host vectors may die at return without stalling the stream
   TT_CUDA(tt::h2d_async(ctx, plan->d_tasks, tsorted.data(), sizeof(TaskDev) * tsorted.size()));
   TT_CUDA(tt::h2d_async(ctx, plan->d_outs, ho.data(), sizeof(OutDev) * ho.size()));
@@ -1458,6 +1497,12 @@ int tt_contract_predict(const tt_out_block* outs, int n_out, const tt_block_pair
 int tt_plan_precision(const tt_plan* plan, int* precision) {
   TT_REQUIRE(plan && precision, "tt_plan_precision: null argument");
   *precision = plan->precision;
+  return TT_OK;
+}
+
+int tt_contract_plan_timers(double* seconds, int n) {
+  TT_REQUIRE(seconds && n >= 0, "tt_contract_plan_timers: null argument");
+  for (int i = 0; i < n && i < 5; ++i) seconds[i] = g_plan_stage_s[i];
   return TT_OK;
 }
 

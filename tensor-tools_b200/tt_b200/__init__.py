@@ -198,6 +198,7 @@ _proto("tt_qdmrg_step_device_ms", P, C.c_int, PD, PD, PD, PD)
 _proto("tt_dmrg_set_profiling", C.c_int)
 _proto("tt_dmrg_planning_counters", PD, PI64, PD, PI64)
 _proto("tt_dmrg_cache_stats", PI64, PI64, PI64, PI64)
+_proto("tt_contract_plan_timers", PD, C.c_int)
 _proto("tt_eig_redo_count", P, PI64)
 _proto("tt_dmrg_heff_parts", PD, PD, PD)
 _proto("tt_sym_eig_batched", P, C.c_void_p, C.c_int, P, P, P, P)
@@ -982,6 +983,14 @@ def planning_counters() -> dict:
     ns, np_ = I64(), I64()
     _chk(lib.tt_dmrg_planning_counters(C.byref(ts), C.byref(ns), C.byref(tp), C.byref(np_)), "planning_counters")
     return {"structure_s": ts.value, "structures": ns.value, "plan_s": tp.value, "plans": np_.value}
+
+
+def plan_timers() -> list:
+    """Host seconds of the contraction planner's stages on this thread: pair
+    tables, precision choice, tile tasks / chunks, packing jobs, uploads."""
+    out = (D * 5)()
+    _chk(lib.tt_contract_plan_timers(out, 5), "plan timers")
+    return list(out)
 
 
 def cache_stats() -> dict:

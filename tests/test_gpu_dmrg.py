@@ -155,3 +155,25 @@ def test_gram_schmidt_failures_are_refilled_on_the_device(ctx):
     assert tt_b200.davidson_fallbacks() == f0
     Eed = ed.terms_ground_energy(N, terms, N // 2)
     assert abs(e - Eed) <= 1e-8 * abs(Eed)
+
+
+def test_xx_chain_L100_matches_free_fermions(ctx):
+    """A known answer at the chain length of the L = 100 configuration, far
+    beyond exact diagonalisation: the open XX chain (S+S- + S-S+) / 2 is free
+    fermions with single-particle energies cos(pi k / 101), so its Sz = 0
+    ground energy is the sum of the 50 lowest.  The MPO comes from the
+    library's AutoMPO; the sweep ramps to bond dimension 128 (the CPU oracle,
+    same schedule, lands 6.6e-11 above the exact energy)."""
+    import tt_b200
+    L = 100
+    a = tt_b200.AutoMPO()
+    for i in range(L - 1):
+        a.add(0.5, "S+", i, "S-", i + 1)
+        a.add(0.5, "S-", i, "S+", i + 1)
+    H = tt_b200.QMPO.from_autompo(a, L)
+    psi = tt_b200.QMPS(L, qdmrg.neel(L))
+    E = tt_b200.QDMRG(psi, H).run(6, [16, 32, 64, 128, 128, 128], [1e-12], [6])
+    eps = np.sort(np.cos(np.pi * np.arange(1, L + 1) / (L + 1)))
+    Eex = eps[: L // 2].sum()
+    assert -1e-12 * abs(Eex) <= E - Eex <= 1e-9 * abs(Eex)
+    assert max(psi.bond_dims()) == 128

@@ -24,6 +24,26 @@ def test_qdmrg_heisenberg_matches_ed():
         assert min(lg.energies) >= Eed - 1e-10
 
 
+def test_qdmrg_xx_chain_matches_free_fermions():
+    """A known answer beyond exact diagonalisation: the open XX chain
+    H = sum_i (S+_i S-_{i+1} + S-_i S+_{i+1}) / 2 is a chain of free fermions
+    with single-particle energies cos(pi k / (L + 1)), k = 1..L (Jordan-Wigner),
+    so its ground energy at Sz = 0 is the sum of the L/2 lowest of them.  At
+    L = 40 the Sz = 0 sector has 1.4e11 states; the oracle's two-site DMRG
+    (AutoMPO MPO) must reach that energy from above."""
+    from oracle import autompo as am
+    L = 40
+    a = am.AutoMPO()
+    for i in range(L - 1):
+        a.add(0.5, "S+", i, "S-", i + 1)
+        a.add(0.5, "S-", i, "S+", i + 1)
+    psi = qdmrg.QMPS(L, qdmrg.neel(L))
+    E = qdmrg.dmrg(psi, am.build_qmpo(a, L), 6, [16, 32, 64, 64, 64, 64], [1e-12], [6])
+    eps = np.sort(np.cos(np.pi * np.arange(1, L + 1) / (L + 1)))
+    Eex = eps[: L // 2].sum()
+    assert -1e-12 * abs(Eex) <= E - Eex <= 1e-9 * abs(Eex)
+
+
 def test_qdmrg_field_matches_ed():
     L = 8
     rng = np.random.default_rng(3)

@@ -50,3 +50,25 @@ def test_dense_field_chain_matches_ed(ctx):
     e, _, _ = tt_b200.ddmrg_run(psi, H, 6, [8, 16, 32], [1e-12], [4])
     Eed = ed.ground_energy(L, ed.chain_bonds(L), h=h)
     assert abs(e - Eed) <= 1e-9 * abs(Eed)
+
+
+def test_dense_tfi_chain_L100_matches_free_fermions(ctx):
+    """The dense path at chain length 100 against an exact answer: the
+    critical transverse-field Ising chain H = -sum Z Z - sum X (free Majorana
+    fermions, E0 = -sum of the singular values of the bidiagonal matrix with
+    1 on and above the diagonal), AutoMPO MPO, seeded random product start,
+    bond dimension ramped to 64 (the CPU oracle, same schedule, lands within
+    1e-15)."""
+    import tt_b200
+    L = 100
+    a = tt_b200.AutoMPO()
+    for i in range(L - 1):
+        a.add(-4.0, "Sz", i, "Sz", i + 1)
+    for i in range(L):
+        a.add(-2.0, "Sx", i)
+    H = tt_b200.DMPO.from_autompo(a, L)
+    psi = tt_b200.DMPS(L, list(np.random.default_rng(5).integers(0, 2, L)))
+    E, _, _ = tt_b200.ddmrg_run(psi, H, 6, [8, 16, 32, 64, 64, 64], [1e-12], [4])
+    B = np.diag(np.ones(L)) + np.diag(np.ones(L - 1), 1)
+    Eex = -np.linalg.svd(B, compute_uv=False).sum()
+    assert abs(E - Eex) <= 1e-11 * abs(Eex)

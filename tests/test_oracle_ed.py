@@ -44,6 +44,39 @@ def test_qdmrg_xx_chain_matches_free_fermions():
     assert -1e-12 * abs(Eex) <= E - Eex <= 1e-9 * abs(Eex)
 
 
+def _tfi_chain_exact(L, g):
+    """Ground energy of the open chain H = -sum Z_i Z_{i+1} - g sum X_i: free
+    Majorana fermions, E0 = -(sum of the singular values of the L x L
+    bidiagonal matrix with g on the diagonal and 1 above it)."""
+    B = np.diag(np.full(L, g)) + np.diag(np.ones(L - 1), 1)
+    return -np.linalg.svd(B, compute_uv=False).sum()
+
+
+def test_tfi_chain_exact_energy_matches_ed():
+    L, g = 8, 0.7
+    terms = [(-4.0, ((i, "Sz"), (i + 1, "Sz"))) for i in range(L - 1)]
+    terms += [(-2.0 * g, ((i, "Sx"),)) for i in range(L)]
+    assert abs(ed.terms_ground_energy(L, terms) - _tfi_chain_exact(L, g)) < 1e-12 * L
+
+
+def test_ddmrg_tfi_chain_matches_free_fermions():
+    """Dense-path known answer beyond exact diagonalisation: the critical
+    transverse-field Ising chain (g = 1, L = 40, Z = 2 Sz, X = 2 Sx) from a
+    seeded random product state, AutoMPO MPO; the oracle's dense two-site
+    DMRG must reach the free-fermion energy."""
+    from oracle import autompo as am
+    L, g = 40, 1.0
+    a = am.AutoMPO()
+    for i in range(L - 1):
+        a.add(-4.0, "Sz", i, "Sz", i + 1)
+    for i in range(L):
+        a.add(-2.0 * g, "Sx", i)
+    psi = ddmrg.DMPS(L, list(np.random.default_rng(5).integers(0, 2, L)))
+    E = ddmrg.ddmrg(psi, am.build_dmpo(a, L), 6, [8, 16, 32, 32, 32, 32], [1e-12], [4])
+    Eex = _tfi_chain_exact(L, g)
+    assert -1e-12 * abs(Eex) <= E - Eex <= 1e-12 * abs(Eex)
+
+
 def test_qdmrg_field_matches_ed():
     L = 8
     rng = np.random.default_rng(3)

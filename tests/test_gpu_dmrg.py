@@ -8,7 +8,7 @@ energies must agree to 1e-10 relative (FP64 path).
 import numpy as np
 import pytest
 
-from oracle import ed, qdmrg
+from oracle import ed, freefermion, qdmrg
 
 pytestmark = pytest.mark.gpu
 
@@ -163,7 +163,8 @@ def test_xx_chain_L100_matches_free_fermions(ctx):
     fermions with single-particle energies cos(pi k / 101), so its Sz = 0
     ground energy is the sum of the 50 lowest.  The MPO comes from the
     library's AutoMPO; the sweep ramps to bond dimension 128 (the CPU oracle,
-    same schedule, lands 6.6e-11 above the exact energy)."""
+    same schedule, lands 6.6e-11 above the exact energy); the correlators
+    of the state follow from Wick's theorem."""
     import tt_b200
     L = 100
     a = tt_b200.AutoMPO()
@@ -173,7 +174,11 @@ def test_xx_chain_L100_matches_free_fermions(ctx):
     H = tt_b200.QMPO.from_autompo(a, L)
     psi = tt_b200.QMPS(L, qdmrg.neel(L))
     E = tt_b200.QDMRG(psi, H).run(6, [16, 32, 64, 128, 128, 128], [1e-12], [6])
-    eps = np.sort(np.cos(np.pi * np.arange(1, L + 1) / (L + 1)))
-    Eex = eps[: L // 2].sum()
+    Eex = freefermion.xx_chain_energy(L)
     assert -1e-12 * abs(Eex) <= E - Eex <= 1e-9 * abs(Eex)
     assert max(psi.bond_dims()) == 128
+    # <Sz_i> and <Sz_i Sz_j> of the DMRG state against Wick's theorem
+    sz, szsz = psi.measure_sz()
+    err = np.abs(szsz - freefermion.xx_chain_szsz(L)).max()
+    assert np.abs(sz).max() < 1e-6, np.abs(sz).max()
+    assert err < 1e-6, err

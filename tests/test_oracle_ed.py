@@ -8,7 +8,7 @@ total-Sz sector, and intermediate energies must respect the variational bound.
 import numpy as np
 import pytest
 
-from oracle import ddmrg, ed, qdmrg
+from oracle import ddmrg, ed, freefermion, qdmrg
 from oracle.qtensor import QIndex, QTensor, Inward, Outward, contract, qn, to_dense
 
 
@@ -39,24 +39,21 @@ def test_qdmrg_xx_chain_matches_free_fermions():
         a.add(0.5, "S-", i, "S+", i + 1)
     psi = qdmrg.QMPS(L, qdmrg.neel(L))
     E = qdmrg.dmrg(psi, am.build_qmpo(a, L), 6, [16, 32, 64, 64, 64, 64], [1e-12], [6])
-    eps = np.sort(np.cos(np.pi * np.arange(1, L + 1) / (L + 1)))
-    Eex = eps[: L // 2].sum()
+    Eex = freefermion.xx_chain_energy(L)
     assert -1e-12 * abs(Eex) <= E - Eex <= 1e-9 * abs(Eex)
 
 
-def _tfi_chain_exact(L, g):
-    """Ground energy of the open chain H = -sum Z_i Z_{i+1} - g sum X_i: free
-    Majorana fermions, E0 = -(sum of the singular values of the L x L
-    bidiagonal matrix with g on the diagonal and 1 above it)."""
-    B = np.diag(np.full(L, g)) + np.diag(np.ones(L - 1), 1)
-    return -np.linalg.svd(B, compute_uv=False).sum()
-
-
-def test_tfi_chain_exact_energy_matches_ed():
+def test_free_fermion_energies_match_ed():
+    """The closed forms the free-fermion tests rely on, against ED."""
     L, g = 8, 0.7
     terms = [(-4.0, ((i, "Sz"), (i + 1, "Sz"))) for i in range(L - 1)]
     terms += [(-2.0 * g, ((i, "Sx"),)) for i in range(L)]
-    assert abs(ed.terms_ground_energy(L, terms) - _tfi_chain_exact(L, g)) < 1e-12 * L
+    assert abs(ed.terms_ground_energy(L, terms) - freefermion.tfi_chain_energy(L, g)) < 1e-12 * L
+    L = 10
+    terms = [(0.5, ((i, "S+"), (i + 1, "S-"))) for i in range(L - 1)]
+    terms += [(0.5, ((i, "S-"), (i + 1, "S+"))) for i in range(L - 1)]
+    Hs = ed.terms_hamiltonian(L, terms, L // 2)
+    assert abs(np.linalg.eigvalsh(Hs.toarray())[0] - freefermion.xx_chain_energy(L)) < 1e-12 * L
 
 
 def test_ddmrg_tfi_chain_matches_free_fermions():
@@ -73,7 +70,7 @@ def test_ddmrg_tfi_chain_matches_free_fermions():
         a.add(-2.0 * g, "Sx", i)
     psi = ddmrg.DMPS(L, list(np.random.default_rng(5).integers(0, 2, L)))
     E = ddmrg.ddmrg(psi, am.build_dmpo(a, L), 6, [8, 16, 32, 32, 32, 32], [1e-12], [4])
-    Eex = _tfi_chain_exact(L, g)
+    Eex = freefermion.tfi_chain_energy(L, g)
     assert -1e-12 * abs(Eex) <= E - Eex <= 1e-12 * abs(Eex)
 
 

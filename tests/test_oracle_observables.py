@@ -4,7 +4,7 @@ amplitude vector equals the DMRG energy, and <Sz_i Sz_j> agrees with the
 exact-diagonalisation ground state."""
 import numpy as np
 
-from oracle import ed, observables, qdmrg
+from oracle import ed, freefermion, observables, qdmrg
 
 
 def test_state_vector_energy_and_correlators():
@@ -28,3 +28,19 @@ def test_state_vector_energy_and_correlators():
     assert np.abs(two - two0).max() < 1e-6
     assert np.abs(one - one0).max() < 1e-6
     assert abs(one.sum()) < 1e-12
+
+
+def test_free_fermion_correlators_match_ed():
+    """<Sz_i Sz_j> of the open XX chain by Wick's theorem (oracle/freefermion.py)
+    equal the exact-diagonalisation ground state's; the GPU correlators are
+    checked against the same closed form at L = 100."""
+    L = 10
+    terms = [(0.5, ((i, "S+"), (i + 1, "S-"))) for i in range(L - 1)]
+    terms += [(0.5, ((i, "S-"), (i + 1, "S+"))) for i in range(L - 1)]
+    Hs = ed.terms_hamiltonian(L, terms, L // 2)
+    w, U = np.linalg.eigh(Hs.toarray())
+    v0 = np.zeros(2 ** L)
+    v0[ed.sector_basis(L, L // 2)] = U[:, 0]
+    one, two = observables.sz_correlators(v0, L)
+    assert np.abs(two - freefermion.xx_chain_szsz(L)).max() < 1e-12
+    assert np.abs(one).max() < 1e-12
